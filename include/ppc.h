@@ -1,0 +1,290 @@
+/*
+ * ppc.h — C ABI of the B200 mechanics timestep of paraPhysiCell.
+ *
+ * Every entry point replaces one reference solver entry point that takes
+ * `physicell::environment&` (reference: src/solver/host/position_solver.h:7-21,
+ * src/solver/host/containers_solver.h:13-27, src/solver/solver.h:9-17). The
+ * reference functions are `void` and run inside an enclosing `omp parallel`
+ * region; these return an int status (PPC_OK on success) and must be called
+ * once per simulation step from one host thread (the C++ layer in
+ * paraphysicell_b200/host wraps them in `omp single` where needed).
+ *
+ * Agent state lives in device memory (HBM) inside a `ppc_state` between calls.
+ * Host buffers enter through ppc_upload and leave through ppc_download; the
+ * struct `ppc_agents` mirrors the structure-of-arrays fields of the reference's
+ * `physicell::cell_data` that the mechanics step reads or writes
+ * (reference: src/cell_data.h:59-79,137-196). All pointers in `ppc_agents` are
+ * plain host pointers; no CUDA or torch types appear in any signature.
+ *
+ * Threading: a ppc_state is not thread safe; calls on one state must be
+ * serialised by the caller. Device work is issued on the state's stream
+ * (ppc_set_stream) and every call returns once the work is enqueued, except
+ * calls that return data or a status that depends on device results, which
+ * synchronise the stream.
+ */
+#ifndef PPC_H
+#define PPC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PPC_ABI_VERSION 1
+
+/* Status codes. The reference has no error reporting (all entry points are
+ * void); these are new. */
+enum ppc_status
+{
+	PPC_OK = 0,
+	PPC_ERR_ARG = 1,		 /* invalid argument (null handle, bad dims, ...) */
+	PPC_ERR_CUDA = 2,		 /* a CUDA runtime call failed */
+	PPC_ERR_CAPACITY = 3,	 /* agent, neighbour or spring capacity exceeded */
+	PPC_ERR_NONFINITE = 4,	 /* a position is NaN or infinite */
+	PPC_ERR_TIMEOUT = 5,	 /* a bounded device wait gave up */
+	PPC_ERR_UNSUPPORTED = 6, /* feature not implemented on the device path */
+	PPC_ERR_OUT_OF_MESH = 7, /* an agent lies outside the mechanics mesh when binned */
+	PPC_ERR_NO_DEVICE = 8	 /* no CUDA device is available */
+};
+
+/* Cell state flags (reference: src/cell_data.h:155-160, enum cell_state_flag). */
+enum ppc_flag
+{
+	PPC_FLAG_NONE = 0,
+	PPC_FLAG_TO_REMOVE = 1,
+	PPC_FLAG_TO_DIVIDE = 2
+};
+
+/* Arithmetic used for the pairwise cell-cell forces. */
+enum ppc_precision
+{
+	PPC_FP64 = 0,		/* every operation in FP64, bit-faithful to the reference */
+	PPC_FP32_FORCE = 1	/* pair force arithmetic in FP32 with compensated sums;
+						   positions, binning, neighbour sets and integration stay FP64 */
+};
+
+/*
+ * Domain and mechanics mesh. The reference's mechanics mesh shares the
+ * bounding box of the diffusion mesh and uses 30 um voxels by default
+ * (reference: src/environment.cpp:16, src/environment.h:10). The bounding box
+ * is integer, as in the reference's builder (src/builder.cpp:84-105).
+ * grid_shape[d] = ceil((max-min)/voxel_shape) for d < dims, 1 otherwise.
+ */
+typedef struct ppc_mesh
+{
+	int32_t dims; /* 1, 2 or 3 */
+	int32_t bounding_box_mins[3];
+	int32_t bounding_box_maxs[3];
+	int32_t voxel_shape[3]; /* mechanics voxel edge lengths (um) */
+} ppc_mesh;
+
+/* Per-environment switches (reference: src/environment.h:30-46). */
+typedef struct ppc_params
+{
+	double mechanics_time_step;			  /* e.mechanics_time_step (min) */
+	int32_t cell_definitions_count;		  /* e.cell_definitions_count */
+	int32_t virtual_wall_at_domain_edges; /* e.virtual_wall_at_domain_edges */
+	int32_t automated_spring_adhesion;	  /* e.automated_spring_adhesion */
+	int32_t reserved;
+} ppc_params;
+
+/*
+ * Host view of the agents of one simulation (structure of arrays, host memory).
+ * Positions, velocities, previous velocities and orientation are AoS by dims,
+ * exactly like the reference (`positions[i*dims+d]`). Any pointer may be NULL:
+ * on upload the field then takes the reference's default
+ * (src/data_storage_phenotype.cpp:120-125,194-214, src/cell.cpp:47-61);
+ * on download it is skipped.
+ * `count` is the number of agents; `capacity` is how many agents the arrays can
+ * hold (used by ppc_download; on upload it must be >= count).
+ */
+typedef struct ppc_agents
+{
+	int32_t count;
+	int32_t capacity;
+
+	double* positions;			 /* [capacity*dims] */
+	double* velocities;			 /* [capacity*dims] */
+	double* previous_velocities; /* [capacity*dims] */
+	double* simple_pressure;	 /* [capacity] */
+
+	double* radius;								/* geometries.radius */
+	double* cell_cell_repulsion_strength;		/* mechanics.* */
+	double* cell_cell_adhesion_strength;
+	double* relative_maximum_adhesion_distance;
+	double* cell_BM_repulsion_strength;
+	double* attachment_elastic_constant;
+	double* attachment_rate;
+	double* detachment_rate;
+	int32_t* maximum_number_of_attachments;
+	double* cell_adhesion_affinities; /* [capacity*cell_definitions_count], row per agent */
+
+	int32_t* cell_definition_indices;
+	uint8_t* is_movable;
+	uint8_t* flags; /* enum ppc_flag */
+	int64_t* agent_ids;
+
+	/* fields that division reads or writes (reference: src/cell.cpp:108-163) */
+	double* total_volume;	/* agent_data.volumes */
+	double* nuclear_volume; /* volumes.nuclear */
+	double* nuclear_radius;
+	double* surface_area;
+	double* polarity;
+	double* orientation; /* [capacity*dims] */
+
+	/* spring attachments, one row of `spring_capacity` slots per agent
+	   (reference: states.springs, vector<vector<index_t>>) */
+	int32_t spring_capacity;
+	int32_t* spring_counts; /* [capacity] */
+	int32_t* springs;		/* [capacity*spring_capacity] */
+} ppc_agents;
+
+typedef struct ppc_state ppc_state;
+
+/* ---- lifetime ----------------------------------------------------------- */
+
+/* Creates the device state of one simulation (counterpart of constructing the
+ * environment plus `solver::initialize`, reference src/solver/solver.cpp:5 and
+ * src/solver/host/containers_solver.cpp:10-13). `agent_capacity` bounds the
+ * agent count reachable by division. */
+int ppc_create(const ppc_mesh* mesh, const ppc_params* params, int32_t agent_capacity, ppc_state** out);
+
+/* Creates a batch of `replicates` independent simulations advanced together
+ * (ensemble form; no reference counterpart: the reference runs one
+ * environment per process). meshes[r] and capacities[r] describe replicate r;
+ * all replicates share `params`. */
+int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t replicates, const ppc_params* params,
+					 ppc_state** out);
+
+int ppc_destroy(ppc_state* s);
+
+/* Sets the CUDA stream (a cudaStream_t passed as void*) used for all device
+ * work of this state; NULL selects the state's own stream. */
+int ppc_set_stream(ppc_state* s, void* cuda_stream);
+
+int ppc_set_precision(ppc_state* s, int32_t precision);
+
+/* Seed of the counter-based random stream that replaces the reference's
+ * per-thread mt19937 (src/random.cpp:8-49) for division directions. */
+int ppc_set_random_seed(ppc_state* s, uint64_t seed);
+
+/* Neighbour-list capacity per agent for ppc_update_cell_neighbors (default 64). */
+int ppc_set_neighbor_capacity(ppc_state* s, int32_t per_agent);
+
+/* ---- host <-> device ---------------------------------------------------- */
+
+/* Replaces the agents of replicate `replicate` (0 for ppc_create states) with
+ * the host view. Synchronises the stream. */
+int ppc_upload(ppc_state* s, int32_t replicate, const ppc_agents* agents);
+
+/* Copies the agents of replicate `replicate` back to the host view. Sets
+ * agents->count; returns PPC_ERR_CAPACITY if it exceeds agents->capacity.
+ * Synchronises the stream. */
+int ppc_download(ppc_state* s, int32_t replicate, ppc_agents* agents);
+
+int ppc_get_count(ppc_state* s, int32_t replicate, int32_t* count);
+
+/* Counters kept like environment::divisions_count / deaths_count
+ * (reference: src/environment.h:34-35). */
+int ppc_get_event_counts(ppc_state* s, int32_t replicate, int64_t* divisions, int64_t* deaths);
+
+/* ---- reference entry points --------------------------------------------- */
+
+/* containers_solver::update_mechanics_mesh (reference: src/solver/host/containers_solver.cpp:15-56).
+ * Bins agents into mechanics voxels; the order inside a voxel is descending
+ * agent index, the order a serial run of the reference produces. */
+int ppc_update_mechanics_mesh(ppc_state* s);
+
+/* position_solver::update_cell_neighbors (reference: src/solver/host/position_solver.cpp:262-286).
+ * Requires a current mesh. Returns PPC_ERR_CAPACITY if a list overflows the
+ * neighbour capacity (the lists are then incomplete). */
+int ppc_update_cell_neighbors(ppc_state* s);
+
+/* position_solver::update_cell_forces (reference: src/solver/host/position_solver.cpp:233-260).
+ * Uses the neighbour lists of the last ppc_update_cell_neighbors. */
+int ppc_update_cell_forces(ppc_state* s);
+
+/* position_solver::update_motility (reference: src/solver/host/position_solver.cpp:288-314).
+ * No-op when no agent is motile; motile agents are not supported on the device
+ * (the host view carries no motility fields), so this always succeeds. */
+int ppc_update_motility(ppc_state* s);
+
+/* position_solver::update_basement_membrane_interactions (reference: src/solver/host/position_solver.cpp:316-335). */
+int ppc_update_basement_membrane_interactions(ppc_state* s);
+
+/* position_solver::update_spring_attachments (reference: src/solver/host/position_solver.cpp:451-479).
+ * Spring contraction over the stored springs. Stochastic attachment and
+ * detachment with non-zero rates is not implemented on the device and returns
+ * PPC_ERR_UNSUPPORTED; with all rates zero it leaves the springs unchanged,
+ * as the reference does. */
+int ppc_update_spring_attachments(ppc_state* s);
+
+/* position_solver::update_positions (reference: src/solver/host/position_solver.cpp:481-520). */
+int ppc_update_positions(ppc_state* s);
+
+/* containers_solver::update_cell_container_for_mechanics (reference: src/solver/host/containers_solver.cpp:140-147).
+ * Removes agents outside the domain bounding box or flagged PPC_FLAG_TO_REMOVE
+ * by swap-with-last, in the order a serial run of the reference produces. */
+int ppc_update_cell_container_for_mechanics(ppc_state* s);
+
+/* containers_solver::update_cell_container_for_phenotype (reference: src/solver/host/containers_solver.cpp:149-188)
+ * without BioFVM's release_internalized_substrates: divides agents flagged
+ * PPC_FLAG_TO_DIVIDE (src/cell.cpp:108-163), then removes as above. */
+int ppc_update_cell_container_for_phenotype(ppc_state* s);
+
+/* Sets PPC_FLAG_TO_REMOVE with probability p_death and otherwise
+ * PPC_FLAG_TO_DIVIDE with probability p_divide per agent, from the state's
+ * counter-based random stream (stand-in for the reference's phenotype models,
+ * src/original/core/standard_models.cpp:478-540). */
+int ppc_flag_by_draws(ppc_state* s, double p_divide, double p_death);
+
+/* ---- fused step ----------------------------------------------------------- */
+
+/* Advances `steps` mechanics steps in the order of simulator::simulate_mechanics
+ * (reference: src/simulator.cpp:157-196, without gradient, custom rules,
+ * interactions and motility): forces, membrane, springs, positions, container
+ * compaction, mesh rebuild. Neighbour lists are recomputed inside the force
+ * pass; call ppc_update_cell_neighbors to materialise them. Requires a current
+ * mesh (ppc_update_mechanics_mesh once after upload). With `with_phenotype`
+ * non-zero, each step is followed by ppc_flag_by_draws(p_divide, p_death) and
+ * the phenotype container update, then a mesh rebuild. */
+int ppc_step(ppc_state* s, int32_t steps);
+int ppc_step_with_phenotype(ppc_state* s, int32_t steps, double p_divide, double p_death);
+
+/* ---- readback of derived structures -------------------------------------- */
+
+/* Neighbour lists of replicate `replicate`: counts[i] and lists[i*list_capacity + k].
+ * Synchronises the stream. */
+int ppc_get_neighbors(ppc_state* s, int32_t replicate, int32_t* counts, int32_t* lists, int32_t list_capacity);
+
+/* Mechanics mesh bins of replicate `replicate` as CSR over voxels:
+ * voxel_counts[v] (size voxel_count) and agents (size count) concatenated in
+ * voxel order, each voxel's agents in bin order. Synchronises the stream. */
+int ppc_get_mesh_bins(ppc_state* s, int32_t replicate, int32_t* voxel_counts, int32_t* agents);
+
+/* Voxel count of replicate `replicate`'s mechanics mesh. */
+int ppc_get_voxel_count(ppc_state* s, int32_t replicate, int64_t* voxel_count);
+
+/* ---- helpers -------------------------------------------------------------- */
+
+/* common_solver::get_mesh_position (reference: src/solver/host/common_solver.cpp:18-38). */
+int ppc_get_mesh_position(const ppc_mesh* mesh, const double* position, int32_t* voxel_coords3);
+
+/* common_solver::get_mesh_index (reference: src/solver/host/common_solver.cpp:10-16). */
+int ppc_get_mesh_index(const ppc_mesh* mesh, const int32_t* voxel_coords3, int32_t* index);
+
+/* Number of kernel launches this state has issued (for launch accounting). */
+int ppc_get_launch_count(ppc_state* s, int64_t* launches);
+
+/* Message of the last error on the calling thread ("" if none). */
+const char* ppc_last_error(void);
+
+int ppc_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PPC_H */

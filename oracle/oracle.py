@@ -1,0 +1,133 @@
+"""Python binding of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads oracle/_build/libppc_oracle.so (building it with `make` when it is
+missing). Only tests, the smoke check and the benchmark's CPU-baseline leg
+import this module; the product path never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+from paraphysicell_b200.abi import Agents, Mesh, Params, PPCError
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libppc_oracle.so")
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.orc_create.argtypes = [C.POINTER(Mesh), C.POINTER(Params), C.POINTER(vp)]
+        L.orc_destroy.argtypes = [vp]
+        L.orc_upload.argtypes = [vp, C.POINTER(Agents)]
+        L.orc_download.argtypes = [vp, C.POINTER(Agents)]
+        L.orc_count.argtypes = [vp]
+        L.orc_count.restype = C.c_int32
+        L.orc_event_counts.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.orc_set_random_seed.argtypes = [vp, C.c_uint64]
+        L.orc_voxel_count.argtypes = [vp]
+        L.orc_voxel_count.restype = C.c_int64
+        for name in ("orc_update_mechanics_mesh", "orc_update_cell_neighbors", "orc_update_cell_forces",
+                     "orc_update_basement_membrane_interactions", "orc_update_spring_attachments",
+                     "orc_update_positions", "orc_update_cell_container_for_mechanics",
+                     "orc_update_cell_container_for_phenotype"):
+            getattr(L, name).argtypes = [vp]
+        L.orc_flag_by_draws.argtypes = [vp, C.c_double, C.c_double]
+        L.orc_step.argtypes = [vp, C.c_int32, C.c_int32, C.c_double, C.c_double]
+        L.orc_time_steps.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double]
+        L.orc_time_steps.restype = C.c_double
+        L.orc_get_neighbors.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_int32]
+        L.orc_get_mesh_bins.argtypes = [vp, C.c_void_p, C.c_void_p]
+        L.orc_get_mesh_position.argtypes = [vp, C.c_void_p, C.c_void_p]
+        _lib = L
+    return _lib
+
+
+class Oracle:
+    """One serial, deterministic restatement of the reference solver state."""
+
+    def __init__(self, mesh: Mesh, params: Params, seed: int = 0):
+        self.L = lib()
+        self.mesh = mesh
+        self.params = params
+        h = C.c_void_p()
+        rc = self.L.orc_create(C.byref(mesh), C.byref(params), C.byref(h))
+        if rc:
+            raise PPCError(rc, "orc_create")
+        self.h = h
+        self.L.orc_set_random_seed(self.h, seed)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.orc_destroy(self.h)
+            self.h = None
+
+    def upload(self, agents):
+        s = agents.struct()
+        rc = self.L.orc_upload(self.h, C.byref(s))
+        if rc:
+            raise PPCError(rc, "orc_upload")
+
+    def download(self, agents):
+        s = agents.struct()
+        rc = self.L.orc_download(self.h, C.byref(s))
+        agents.count = s.count
+        if rc:
+            raise PPCError(rc, "orc_download")
+        return agents
+
+    @property
+    def count(self):
+        return self.L.orc_count(self.h)
+
+    def event_counts(self):
+        d, k = C.c_int64(), C.c_int64()
+        self.L.orc_event_counts(self.h, C.byref(d), C.byref(k))
+        return d.value, k.value
+
+    def voxel_count(self):
+        return self.L.orc_voxel_count(self.h)
+
+    def __getattr__(self, name):
+        # reference entry points: update_mechanics_mesh(), update_cell_forces(), ...
+        fn = getattr(lib(), "orc_" + name, None)
+        if fn is None:
+            raise AttributeError(name)
+        return lambda *a: fn(self.h, *a)
+
+    def time_steps(self, steps, threads, with_phenotype=False, p_divide=0.0, p_death=0.0):
+        return self.L.orc_time_steps(self.h, steps, threads, int(with_phenotype), p_divide, p_death)
+
+    def neighbors(self, capacity=None):
+        import numpy as np
+        n = self.count
+        cap = capacity or 64
+        while True:
+            counts = np.zeros(max(n, 1), np.int32)
+            lists = np.zeros(max(n, 1) * cap, np.int32)
+            rc = self.L.orc_get_neighbors(self.h, counts.ctypes.data, lists.ctypes.data, cap)
+            if rc == 0:
+                break
+            cap = int(counts.max()) + 1
+        lists = lists.reshape(max(n, 1), cap)
+        return [list(lists[i, : counts[i]]) for i in range(n)]
+
+    def mesh_bins(self):
+        import numpy as np
+        V = self.voxel_count()
+        counts = np.zeros(V, np.int32)
+        agents = np.zeros(max(self.count, 1), np.int32)
+        self.L.orc_get_mesh_bins(self.h, counts.ctypes.data, agents.ctypes.data)
+        return counts, agents[: self.count]

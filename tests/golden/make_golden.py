@@ -1,0 +1,77 @@
+"""Extracts the reference's known-answer values into known_answers.json.
+
+The reference (asmelko/paraPhysiCell) cannot be built here: its paraBioFVM,
+pugixml and googletest submodules are absent. Its unit tests
+(test/test.cpp) still carry known answers as text. This script reads them
+from the reference source tree and writes the committed fixture, so the
+numbers in the fixture have a scripted provenance:
+
+- host_velocity_solver.simple (test/test.cpp:141-191): the x/y/z velocity
+  of cell 1 after one force pass, per dimensionality;
+- host_velocity_solver.complex (test/test.cpp:265-320): expected neighbour
+  counts;
+- host_neighbors_solver.grid (test/test.cpp:333-400): parameter grid;
+- cell_container.add_and_remove (test/test.cpp:52-115): volumes and
+  velocities after each removal.
+
+Usage: python tests/golden/make_golden.py [path/to/reference]
+"""
+import json
+import os
+import re
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def main(ref):
+    src = open(os.path.join(ref, "test", "test.cpp")).read()
+
+    # velocities: "if (dims == 3) expected = X; else if (dims == 2) expected = Y; else expected = Z;"
+    m = re.search(r"if \(dims == 3\)\s*expected = ([0-9.eE+-]+);\s*else if \(dims == 2\)\s*expected = ([0-9.eE+-]+);"
+                  r"\s*else\s*expected = ([0-9.eE+-]+);", src)
+    assert m, "known-answer block not found"
+    simple = {"3": m.group(1), "2": m.group(2), "1": m.group(3)}
+
+    counts = [int(x) for x in re.findall(r"states\.neighbors\[(?:\d)\]\.size\(\), (\d+)\)", src)]
+    assert len(counts) == 3, counts
+
+    m = re.search(r"INSTANTIATE_TEST_SUITE_P\(neis, host_neighbors_solver,\s*testing::Combine\(testing::Values\(([^)]*)\),"
+                  r" testing::Values\(([^)]*)\), testing::Values\(([^)]*)\)\)\)", src)
+    assert m, "grid parameters not found"
+    grid = {
+        "dims": [int(x) for x in m.group(1).split(",")],
+        "cells_in_one_voxel": [int(x) for x in m.group(2).split(",")],
+        "adhesion": [int(x) for x in m.group(3).split(",")],
+    }
+    m = re.search(r"TEST_P\(host_neighbors_solver, grid\).*?cartesian_mesh mesh\(dims, \{ 0, 0, 0 \}, \{ (\d+), (\d+), (\d+) \},"
+                  r" \{ (\d+), (\d+), (\d+) \}\);.*?radius\(\) = (\d+);", src, re.S)
+    assert m, "grid mesh not found"
+    grid["mesh_max"] = [int(m.group(i)) for i in (1, 2, 3)]
+    grid["diffusion_voxel"] = [int(m.group(i)) for i in (4, 5, 6)]
+    grid["radius"] = float(m.group(7))
+
+    block = src[src.index("TEST(cell_container, add_and_remove)"): src.index("void update_cell_for_velocity")]
+    removes = []
+    for part in block.split("cont.remove_agent(")[1:]:
+        seg = part.split("}")[0]
+        vols = [float(x) for x in re.findall(r"volumes\[\d\], (\d+)\)", seg)]
+        vels = [float(x) for x in re.findall(r"velocities\[\d\], (\d+)\)", seg)]
+        removes.append({"removed": part.split(")")[0], "volumes": vols, "velocities": vels})
+
+    out = {
+        "source": "reference test/test.cpp (asmelko/paraPhysiCell), read as text",
+        "host_velocity_solver_simple": {"expected_velocity_cell1": simple,
+                                        "lines": "test/test.cpp:141-191"},
+        "host_velocity_solver_complex": {"neighbor_counts": counts, "lines": "test/test.cpp:265-320"},
+        "host_neighbors_solver_grid": dict(grid, lines="test/test.cpp:333-400"),
+        "cell_container_add_and_remove": {"after_removals": removes, "lines": "test/test.cpp:52-115"},
+    }
+    with open(os.path.join(HERE, "known_answers.json"), "w") as f:
+        json.dump(out, f, indent=1)
+        f.write("\n")
+    print(json.dumps(out, indent=1))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
