@@ -1,0 +1,382 @@
+"""Benchmark of the B200 mechanics timestep (agent-steps/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload config3|config2|config5|config1]
+
+One step is one mechanics timestep of the whole simulation (forces,
+membrane, springs, Adams-Bashforth update, container compaction, mesh
+rebuild) in simulator::simulate_mechanics order. The default workload is
+the 3-D 88,700-agent case with springs (ball of radius 1300 um in a 4000 um
+cube, three cell types, 20% of agents with 1-3 springs), FP64. Inputs are
+seeded synthetic agents (the reference's sample XML setups are not used).
+
+`value`: device time of K steps with the state resident in HBM, each step
+bracketed by CUDA events on the library's stream with L2 flushed (a 256 MiB
+write) before every timed step. `e2e`: the same steps through the C ABI with
+host buffers: every step uploads positions and previous velocities from
+pinned host memory and downloads positions, velocities, previous velocities
+and pressure. `roofline`: algorithmic bytes of the fused force kernel per
+launch over its event-timed duration. `cpu_baseline`: the CPU restatement of
+the reference's OpenMP path on this host's cores, on a bounded number of
+steps of the same workload.
+
+With torchrun (N > 1) every rank advances its own replica of the workload
+(the single-simulation path does not shard; replicas only) and the max over
+ranks of the device time is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "mechanics agent-steps/s at 1 B200 (FP64 vs FP32-force vs batched) vs OpenMP host"
+UNIT = "agent-steps/s"
+
+WORKLOADS = {
+    "config3": "3-D 88,700 agents in a ball r=1300 um (4000 um cube, 134^3 mechanics voxels), "
+               "3 cell types, 20% with 1-3 springs k=0.05, dt 0.1 min, FP64",
+    "config2": "3-D 14,300 agents in a ball r=450 um (2000 um cube), 2 types, BM walls on, FP64",
+    "config5": "3-D 1,000,000 agents in a ball r=2900 um (8000 um cube), 2 types, division 1e-4 / death 5e-5 "
+               "per step, FP64",
+    "config1": "2-D 900 agents in 2000x2000 um, one type, FP64",
+}
+
+
+def make_workload(name):
+    from paraphysicell_b200 import workloads as wl
+    return {"config1": wl.config1, "config2": wl.config2, "config3": wl.config3, "config5": wl.config5}[name]()
+
+
+def phenotype_args(name):
+    from paraphysicell_b200 import workloads as wl
+    return (wl.P_DIVIDE, wl.P_DEATH) if name == "config5" else None
+
+
+def algorithmic_bytes_per_agent(dims, ndefs, walls, springs_per_agent, spring_agents_fraction):
+    """Bytes the fused force pass must move per agent: reads of position,
+    previous velocity, the four pair parameters (radius, repulsion,
+    adhesion, rmad), the BM strength when walls are on, the affinity row,
+    definition index and movable flag; writes of position, previous velocity
+    and pressure; spring rows (count, elastic constant, partner indices)."""
+    s = 8
+    reads = 8 * dims + 8 * dims + 4 * s + (s if walls else 0) + s * ndefs + 4 + 1
+    writes = 8 * dims + 8 * dims + s
+    springs = 4 + spring_agents_fraction * s + 4 * springs_per_agent
+    return reads + writes + springs
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        rows = []
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5], f[6], f[7], f[8]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[2 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(name, budget_s=8.0, max_steps=400):
+    """Times the oracle's OpenMP restatement of the reference on all host
+    threads for a bounded number of steps of the workload."""
+    from oracle.oracle import Oracle
+
+    threads = len(os.sched_getaffinity(0))
+    mesh, params, a = make_workload(name)
+    o = Oracle(mesh, params, seed=1)
+    o.upload(a)
+    o.update_mechanics_mesh()
+    o.update_cell_neighbors()
+    ph = phenotype_args(name)
+    kw = dict(with_phenotype=ph is not None, p_divide=ph[0] if ph else 0.0, p_death=ph[1] if ph else 0.0)
+    t = o.time_steps(2, threads, **kw)  # warm-up and step-time estimate
+    steps = int(max(3, min(max_steps, budget_s / max(t / 2, 1e-6))))
+    t = o.time_steps(steps, threads, **kw)
+    return {"value": a.count * steps / t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} steps of the full {a.count}-agent workload, OpenMP over {threads} threads, "
+                      f"std::chrono around the step loop ({t:.2f} s)"}
+
+
+def run_reference(args, rank, world):
+    """`--impl reference`: the reference's CPU path (its OpenMP structure as
+    restated by the oracle; the reference itself cannot be built here) on
+    all host threads, K timed steps after W warm-up steps."""
+    if rank != 0:
+        return
+    from oracle.oracle import Oracle
+
+    threads = len(os.sched_getaffinity(0))
+    mesh, params, a = make_workload(args.workload)
+    o = Oracle(mesh, params, seed=1)
+    o.upload(a)
+    o.update_mechanics_mesh()
+    o.update_cell_neighbors()
+    ph = phenotype_args(args.workload)
+    kw = dict(with_phenotype=ph is not None, p_divide=ph[0] if ph else 0.0, p_death=ph[1] if ph else 0.0)
+    o.time_steps(args.warmup, threads, **kw)
+    t = o.time_steps(args.steps, threads, **kw)
+    value = a.count * args.steps / t * world
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "description": WORKLOADS[args.workload], "agents": a.count},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} timed steps of the full workload after {args.warmup} warm-up "
+                                   f"steps, OpenMP over {threads} threads (reference not buildable here: "
+                                   f"paraBioFVM/pugixml/googletest absent)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from paraphysicell_b200 import build
+    from paraphysicell_b200.abi import AgentArrays
+    from paraphysicell_b200.device import PinnedPool, Simulation
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local_rank)
+    build.ensure_built()
+
+    mesh, params, a = make_workload(args.workload)
+    ph = phenotype_args(args.workload)
+    n0 = a.count
+    stream = torch.cuda.Stream()
+    sim = Simulation(mesh, params, a.capacity, seed=1)
+    sim.set_stream(stream.cuda_stream)
+    sim.upload(a)
+    sim.update_mechanics_mesh()
+
+    def step(k):
+        if ph:
+            sim.step_with_phenotype(k, ph[0], ph[1])
+        else:
+            sim.step(k)
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    with torch.cuda.stream(stream):
+        step(max(args.warmup, 3))
+    sim.synchronize()
+
+    # ---- value: K steps, L2 flushed before each, device-timed ----
+    K = args.steps
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    counts = []
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    sim.set_profiling(True)
+    l0 = sim.launches()
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    if sampler:
+        sampler.__enter__()
+    with torch.cuda.stream(stream):
+        for k in range(K):
+            flush.zero_()
+            starts[k].record(stream)
+            step(1)
+            ends[k].record(stream)
+            if ph:
+                counts.append(sim.count())
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.__exit__(None, None, None)
+    launches = sim.launches() - l0
+    fused_ms, fused_launches = sim.profile()
+    sim.set_profiling(False)
+    sim.synchronize()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    agent_steps = float(sum(counts)) if ph else float(n0 * K)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+        agent_steps *= world
+        torch.distributed.barrier()
+    value = agent_steps / (total_ms / 1e3)
+
+    # ---- steady state: graph-replayed back-to-back steps (L2 warm) ----
+    with torch.cuda.stream(stream):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step(max(K, 10))
+        e1.record(stream)
+    torch.cuda.synchronize()
+    steady = (n0 * max(K, 10)) / (e0.elapsed_time(e1) / 1e3)
+
+    # ---- e2e through the C ABI with pinned host buffers ----
+    pool = PinnedPool()
+    host = AgentArrays(n0, a.dims, a.ndefs, a.capacity, a.spring_capacity, pinned=pool)
+    for k_, v_ in a.arrays.items():
+        host.arrays[k_][:] = v_
+    sim.upload(host)
+    sim.update_mechanics_mesh()
+    up_fields = ("positions", "previous_velocities")
+    down_fields = ("positions", "velocities", "previous_velocities", "simple_pressure")
+    d = a.dims
+    sim.download(host, fields=down_fields)
+    torch.cuda.synchronize()
+    e2e_counts = []
+    E = max(3, min(K, 50))
+    t0 = time.perf_counter()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for k in range(E):
+        sim.upload_fields(host, up_fields)
+        step(1)
+        sim.download(host, fields=down_fields)
+        e2e_counts.append(host.count)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    e2e_ms = max(ev0.elapsed_time(ev1), wall * 1e3)
+    n_e2e = float(sum(e2e_counts))
+    e2e = {"value": n_e2e / (e2e_ms / 1e3) * world, "unit": UNIT,
+           "h2d_bytes_per_step": int(np.mean(e2e_counts) * 2 * 8 * d),
+           "d2h_bytes_per_step": int(np.mean(e2e_counts) * (3 * 8 * d + 8)),
+           "steps": E, "wall_s": wall}
+    pool_free = pool.free
+
+    if rank != 0:
+        sim.close()
+        del host
+        pool_free()
+        return
+
+    import json as _json
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak = _json.load(open(peaks_path))["hbm_gbs"]
+        peak_src = "measured"
+    else:
+        peak = 6650.0
+        peak_src = "fallback"
+    spring_counts = a.arrays["spring_counts"][:n0]
+    per_agent = algorithmic_bytes_per_agent(d, a.ndefs, bool(params.virtual_wall_at_domain_edges),
+                                            float(spring_counts.mean()), float((spring_counts > 0).mean()))
+    fused_avg_ms = fused_ms / max(fused_launches, 1)
+    achieved = (per_agent * n0) / (fused_avg_ms / 1e3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"fused_traffic_{args.workload}.json")
+    if os.path.exists(prof):
+        traffic = _json.load(open(prof)).get("dram_bytes_per_launch")
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
+        "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "description": WORKLOADS[args.workload], "agents": n0,
+                   "l2": "flushed (256 MiB write) before every timed step", "form": "FP64 drop-in",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single simulation"},
+        "steady_state": {"value": steady, "unit": UNIT, "note": "back-to-back graph-replayed steps, L2 warm"},
+        "roofline": {"bound": "hbm", "kernel": "k_fused (neighbour search + forces + membrane + springs + AB2)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_src, "traffic": traffic, "bytes_per_agent": per_agent,
+                     "avg_launch_us": fused_avg_ms * 1e3, "launches": fused_launches},
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": sampler.summary() if sampler else None,
+    }
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(args.workload)
+    print(json.dumps(line), flush=True)
+    sim.close()
+    del host
+    pool_free()
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="config3", choices=sorted(WORKLOADS))
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    args = p.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        if args.impl == "ours":
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

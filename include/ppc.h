@@ -184,7 +184,23 @@ int ppc_upload(ppc_state* s, int32_t replicate, const ppc_agents* agents);
  * Synchronises the stream. */
 int ppc_download(ppc_state* s, int32_t replicate, ppc_agents* agents);
 
+/* Overwrites only the fields whose pointers are non-NULL, keeping every other
+ * device field; agents->count must equal the device count. This is the
+ * per-step host sync of a caller that keeps cell_data authoritative on the
+ * host. Synchronises the stream. */
+int ppc_upload_fields(ppc_state* s, int32_t replicate, const ppc_agents* agents);
+
 int ppc_get_count(ppc_state* s, int32_t replicate, int32_t* count);
+
+/* Waits for the state's queued device work and returns the first error any
+ * kernel reported since the last check (e.g. PPC_ERR_NONFINITE from
+ * ppc_step, which itself returns as soon as the work is queued). */
+int ppc_synchronize(ppc_state* s);
+
+/* Page-locked host memory for fast host <-> device copies (cudaHostAlloc);
+ * NULL on failure. */
+void* ppc_host_alloc(size_t bytes);
+void ppc_host_free(void* p);
 
 /* Counters kept like environment::divisions_count / deaths_count
  * (reference: src/environment.h:34-35). */
@@ -241,6 +257,9 @@ int ppc_update_cell_container_for_phenotype(ppc_state* s);
 int ppc_flag_by_draws(ppc_state* s, double p_divide, double p_death);
 
 /* ---- fused step ----------------------------------------------------------- */
+/* ppc_step returns once the work is queued (device errors surface at the
+ * next ppc_synchronize or syncing call). Blocks of steps are captured once in
+ * a CUDA graph and replayed. */
 
 /* Advances `steps` mechanics steps in the order of simulator::simulate_mechanics
  * (reference: src/simulator.cpp:157-196, without gradient, custom rules,
@@ -277,6 +296,14 @@ int ppc_get_mesh_index(const ppc_mesh* mesh, const int32_t* voxel_coords3, int32
 
 /* Number of kernel launches this state has issued (for launch accounting). */
 int ppc_get_launch_count(ppc_state* s, int64_t* launches);
+
+/* Kernel timing: while on, every launch of the fused force kernel is
+ * bracketed by CUDA events on the state's stream (steps then run without
+ * graph capture). ppc_get_profile synchronises and returns the summed
+ * device time (ms) and the number of timed launches since profiling was
+ * switched on. */
+int ppc_set_profiling(ppc_state* s, int32_t on);
+int ppc_get_profile(ppc_state* s, double* fused_ms, int64_t* fused_launches);
 
 /* Message of the last error on the calling thread ("" if none). */
 const char* ppc_last_error(void);

@@ -1,0 +1,1047 @@
+// ppc_api.cu — the extern "C" entry points of libppc (include/ppc.h).
+//
+// Host side of the device state: allocation, host <-> device transfer in the
+// reference's cell_data layout, the reference solver entry points, and the
+// fused step with CUDA-graph replay.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ppc_internal.cuh"
+
+namespace ppc {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int cuda_fail(cudaError_t e, const char* where)
+{
+	set_error(std::string(where) + ": " + cudaGetErrorString(e));
+	return PPC_ERR_CUDA;
+}
+
+namespace {
+
+int fail(int rc, const std::string& msg)
+{
+	set_error(msg);
+	return rc;
+}
+
+template <typename T>
+int alloc(ppc_state* s, T*& p, size_t count, bool zero = true)
+{
+	size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+	void* q = nullptr;
+	PPC_CUDA(cudaMalloc(&q, bytes));
+	if (zero)
+		PPC_CUDA(cudaMemset(q, 0, bytes));
+	s->allocations.push_back({ q, bytes });
+	p = static_cast<T*>(q);
+	return PPC_OK;
+}
+
+#define PPC_TRY(x)                                                                                                     \
+	do                                                                                                                 \
+	{                                                                                                                  \
+		int rc_ = (x);                                                                                                 \
+		if (rc_ != PPC_OK)                                                                                             \
+			return rc_;                                                                                                \
+	} while (0)
+
+int ensure_stage(ppc_state* s, size_t bytes)
+{
+	if (bytes <= s->stage_bytes)
+		return PPC_OK;
+	if (s->stage)
+	{
+		PPC_CUDA(cudaStreamSynchronize(s->stream));
+		PPC_CUDA(cudaFree(s->stage));
+		s->stage = nullptr;
+	}
+	PPC_CUDA(cudaMalloc(&s->stage, bytes));
+	s->stage_bytes = bytes;
+	return PPC_OK;
+}
+
+int device_errors(ppc_state* s)
+{
+	int32_t err = 0;
+	PPC_CUDA(cudaMemcpyAsync(&err, s->v.err, sizeof err, cudaMemcpyDeviceToHost, s->stream));
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	if (err == 0)
+		return PPC_OK;
+	PPC_CUDA(cudaMemsetAsync(s->v.err, 0, sizeof(int32_t), s->stream));
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	if (err & ERR_NONFINITE)
+		return fail(PPC_ERR_NONFINITE, "an agent position is NaN or infinite");
+	if (err & ERR_OUT_OF_MESH)
+		return fail(PPC_ERR_OUT_OF_MESH, "an agent lies outside the mechanics mesh");
+	if (err & ERR_NEIGHBOR_CAPACITY)
+		return fail(PPC_ERR_CAPACITY, "a neighbour list exceeds the neighbour capacity");
+	if (err & ERR_AGENT_CAPACITY)
+		return fail(PPC_ERR_CAPACITY, "division exceeds the agent capacity of a replicate");
+	if (err & ERR_SPRING_CAPACITY)
+		return fail(PPC_ERR_ARG, "spring rows are not symmetric");
+	if (err & ERR_LIST_CAPACITY)
+		return fail(PPC_ERR_CAPACITY, "removal or division list overflow");
+	return fail(PPC_ERR_CUDA, "unknown device error");
+}
+
+int finish(ppc_state* s)
+{
+	PPC_CUDA(cudaGetLastError());
+	return device_errors(s);
+}
+
+bool valid(ppc_state* s, int32_t r) { return s && r >= 0 && r < s->nreps; }
+
+int read_counters(ppc_state* s, std::vector<rep_counters>& c)
+{
+	c.resize(s->nreps);
+	PPC_CUDA(cudaMemcpyAsync(c.data(), s->v.ctr, sizeof(rep_counters) * s->nreps, cudaMemcpyDeviceToHost, s->stream));
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	return PPC_OK;
+}
+
+int release_graph(ppc_state* s)
+{
+	if (s->graph)
+	{
+		cudaGraphExecDestroy(s->graph);
+		s->graph = nullptr;
+	}
+	return PPC_OK;
+}
+
+// ---- host <-> device transfer --------------------------------------------------
+
+template <typename T>
+int put_scalar(ppc_state* s, T* dev, const T* host, int32_t base, int32_t n, size_t width, bool defaults, T dflt)
+{
+	T* dst = dev + (size_t)base * width;
+	size_t cnt = (size_t)n * width;
+	if (host)
+	{
+		PPC_CUDA(cudaMemcpyAsync(dst, host, cnt * sizeof(T), cudaMemcpyHostToDevice, s->stream));
+	}
+	else if (defaults && cnt)
+	{
+		std::vector<T> tmp(cnt, dflt);
+		PPC_CUDA(cudaMemcpyAsync(dst, tmp.data(), cnt * sizeof(T), cudaMemcpyHostToDevice, s->stream));
+		PPC_CUDA(cudaStreamSynchronize(s->stream));
+	}
+	return PPC_OK;
+}
+
+template <typename T>
+int get_scalar(ppc_state* s, T* host, const T* dev, int32_t base, int32_t n, size_t width)
+{
+	if (host && n)
+		PPC_CUDA(cudaMemcpyAsync(host, dev + (size_t)base * width, (size_t)n * width * sizeof(T), cudaMemcpyDeviceToHost,
+								 s->stream));
+	return PPC_OK;
+}
+
+int put_vec(ppc_state* s, double4* dev, const double* host, int32_t r, int32_t n, bool defaults)
+{
+	if (!host && !defaults)
+		return PPC_OK;
+	if (n == 0)
+		return PPC_OK;
+	const size_t bytes = (size_t)n * s->dims * sizeof(double);
+	PPC_TRY(ensure_stage(s, bytes));
+	if (host)
+		PPC_CUDA(cudaMemcpyAsync(s->stage, host, bytes, cudaMemcpyHostToDevice, s->stream));
+	else
+		PPC_CUDA(cudaMemsetAsync(s->stage, 0, bytes, s->stream));
+	PPC_TRY(launch_unpack_vec(s, dev, static_cast<const double*>(s->stage), r, n));
+	// the stage is reused by the next field: keep copies ordered
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	return PPC_OK;
+}
+
+int get_vec(ppc_state* s, double* host, const double4* dev, int32_t r, int32_t n)
+{
+	if (!host || n == 0)
+		return PPC_OK;
+	const size_t bytes = (size_t)n * s->dims * sizeof(double);
+	PPC_TRY(ensure_stage(s, bytes));
+	PPC_TRY(launch_pack_vec(s, static_cast<double*>(s->stage), dev, r, n));
+	PPC_CUDA(cudaMemcpyAsync(host, s->stage, bytes, cudaMemcpyDeviceToHost, s->stream));
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	return PPC_OK;
+}
+
+int put_prm(ppc_state* s, int field, const double* host, int32_t r, int32_t n, bool defaults, double dflt)
+{
+	if ((!host && !defaults) || n == 0)
+		return PPC_OK;
+	const size_t bytes = (size_t)n * sizeof(double);
+	PPC_TRY(ensure_stage(s, bytes));
+	if (host)
+		PPC_CUDA(cudaMemcpyAsync(s->stage, host, bytes, cudaMemcpyHostToDevice, s->stream));
+	else
+	{
+		std::vector<double> tmp(n, dflt);
+		PPC_CUDA(cudaMemcpyAsync(s->stage, tmp.data(), bytes, cudaMemcpyHostToDevice, s->stream));
+	}
+	PPC_TRY(launch_unpack_prm(s, field, static_cast<const double*>(s->stage), r, n));
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	return PPC_OK;
+}
+
+int get_prm(ppc_state* s, int field, double* host, int32_t r, int32_t n)
+{
+	if (!host || n == 0)
+		return PPC_OK;
+	const size_t bytes = (size_t)n * sizeof(double);
+	PPC_TRY(ensure_stage(s, bytes));
+	PPC_TRY(launch_pack_prm(s, field, static_cast<double*>(s->stage), r, n));
+	PPC_CUDA(cudaMemcpyAsync(host, s->stage, bytes, cudaMemcpyDeviceToHost, s->stream));
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	return PPC_OK;
+}
+
+// reference defaults (src/data_storage_phenotype.cpp:62-125,194-214, src/cell.cpp:47-61)
+constexpr double kRadius = 8.412710547954228, kNuclearRadius = 5.051670902881889, kSurface = 889.3685284131693;
+
+int transfer_in(ppc_state* s, int32_t r, const ppc_agents* a, bool defaults)
+{
+	const rep_info& R = s->reps[r];
+	const int32_t n = a->count;
+	const int32_t base = R.base;
+	const int D = s->ndefs;
+	view& v = s->v;
+	PPC_TRY(release_graph(s));
+	if (a->cell_definition_indices)
+		for (int32_t i = 0; i < n; i++)
+			if (a->cell_definition_indices[i] < 0 || a->cell_definition_indices[i] >= D)
+				return fail(PPC_ERR_ARG, "cell definition index out of range");
+
+	PPC_TRY(put_vec(s, v.pos[s->cur], a->positions, r, n, defaults));
+	PPC_TRY(put_vec(s, v.vel, a->velocities, r, n, defaults));
+	PPC_TRY(put_vec(s, v.vprev, a->previous_velocities, r, n, defaults));
+	PPC_TRY(put_vec(s, v.orient, a->orientation, r, n, defaults));
+	PPC_TRY(put_prm(s, 0, a->radius, r, n, defaults, kRadius));
+	PPC_TRY(put_prm(s, 1, a->cell_cell_repulsion_strength, r, n, defaults, 10.0));
+	PPC_TRY(put_prm(s, 2, a->cell_cell_adhesion_strength, r, n, defaults, 0.4));
+	PPC_TRY(put_prm(s, 3, a->cell_BM_repulsion_strength, r, n, defaults, 100.0));
+	PPC_TRY(put_scalar(s, v.rmad, a->relative_maximum_adhesion_distance, base, n, 1, defaults, 1.25));
+	PPC_TRY(put_scalar(s, v.ec, a->attachment_elastic_constant, base, n, 1, defaults, 0.01));
+	PPC_TRY(put_scalar(s, v.arate, a->attachment_rate, base, n, 1, defaults, 0.0));
+	PPC_TRY(put_scalar(s, v.drate, a->detachment_rate, base, n, 1, defaults, 0.0));
+	PPC_TRY(put_scalar(s, v.pressure, a->simple_pressure, base, n, 1, defaults, 0.0));
+	PPC_TRY(put_scalar(s, v.vol, a->total_volume, base, n, 1, defaults, 2494.0));
+	PPC_TRY(put_scalar(s, v.nvol, a->nuclear_volume, base, n, 1, defaults, 540.0));
+	PPC_TRY(put_scalar(s, v.nrad, a->nuclear_radius, base, n, 1, defaults, kNuclearRadius));
+	PPC_TRY(put_scalar(s, v.sarea, a->surface_area, base, n, 1, defaults, kSurface));
+	PPC_TRY(put_scalar(s, v.polarity, a->polarity, base, n, 1, defaults, 0.0));
+	PPC_TRY(put_scalar(s, v.aff, a->cell_adhesion_affinities, base, n, D, defaults, 1.0));
+	PPC_TRY(put_scalar<int32_t>(s, v.def, a->cell_definition_indices, base, n, 1, defaults, 0));
+	PPC_TRY(put_scalar<int32_t>(s, v.maxatt, a->maximum_number_of_attachments, base, n, 1, defaults, 12));
+	PPC_TRY(put_scalar<uint8_t>(s, v.movable, a->is_movable, base, n, 1, defaults, 1));
+	PPC_TRY(put_scalar<uint8_t>(s, v.flags, a->flags, base, n, 1, defaults, 0));
+
+	// ids: given or 0..n-1; the next created agent continues after the largest
+	if (a->agent_ids || defaults)
+	{
+		std::vector<int64_t> ids(n);
+		int64_t next = 0;
+		for (int32_t i = 0; i < n; i++)
+		{
+			ids[i] = a->agent_ids ? a->agent_ids[i] : i;
+			next = std::max<int64_t>(next, ids[i] + 1);
+		}
+		PPC_TRY(put_scalar<int64_t>(s, v.ids, ids.data(), base, n, 1, false, 0));
+		PPC_CUDA(cudaMemcpyAsync(&v.ctr[r].next_id, &next, sizeof next, cudaMemcpyHostToDevice, s->stream));
+		PPC_CUDA(cudaStreamSynchronize(s->stream));
+	}
+
+	// springs: host rows hold local indices, device rows hold slots
+	if (a->spring_counts || defaults)
+	{
+		bool any = false;
+		if (a->spring_counts)
+		{
+			for (int32_t i = 0; i < n; i++)
+			{
+				const int32_t c = a->spring_counts[i];
+				if (c < 0 || c > s->scap || c > a->spring_capacity)
+					return fail(PPC_ERR_CAPACITY, "spring count exceeds the spring capacity");
+				for (int32_t k = 0; k < c; k++)
+				{
+					const int32_t j = a->springs ? a->springs[(size_t)i * a->spring_capacity + k] : -1;
+					if (j < 0 || j >= n)
+						return fail(PPC_ERR_ARG, "spring partner index out of range");
+				}
+				any |= c > 0;
+			}
+		}
+		PPC_TRY(put_scalar<int32_t>(s, v.scnt, a->spring_counts, base, n, 1, true, 0));
+		if (any)
+		{
+			const size_t bytes = (size_t)n * a->spring_capacity * sizeof(int32_t);
+			PPC_TRY(ensure_stage(s, bytes));
+			PPC_CUDA(cudaMemcpyAsync(s->stage, a->springs, bytes, cudaMemcpyHostToDevice, s->stream));
+			PPC_TRY(launch_springs_local(s, r, n, static_cast<int32_t*>(s->stage), a->spring_capacity, 1));
+			PPC_CUDA(cudaStreamSynchronize(s->stream));
+		}
+		s->has_springs = s->has_springs || any;
+	}
+
+	if (defaults)
+	{
+		PPC_CUDA(cudaMemsetAsync(v.ncnt + base, 0, sizeof(int32_t) * std::max(n, 1), s->stream));
+		int32_t cnt[2] = { n, n };
+		PPC_CUDA(cudaMemcpyAsync(&v.ctr[r].count, cnt, sizeof(int32_t) * 2, cudaMemcpyHostToDevice, s->stream));
+	}
+
+	// host flags that pick kernel variants
+	if (a->velocities)
+	{
+		for (int32_t i = 0; i < n * s->dims && !s->vel_dirty; i++)
+			s->vel_dirty = a->velocities[i] != 0.0;
+	}
+	for (const double* rate : { a->attachment_rate, a->detachment_rate })
+		if (rate)
+			for (int32_t i = 0; i < n && !s->rates_nonzero; i++)
+				s->rates_nonzero = rate[i] != 0.0;
+	s->bins_valid = false;
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	return PPC_OK;
+}
+
+int transfer_out(ppc_state* s, int32_t r, ppc_agents* a)
+{
+	std::vector<rep_counters> c;
+	PPC_TRY(read_counters(s, c));
+	const int32_t n = c[r].count;
+	a->count = n;
+	if (n > a->capacity)
+		return fail(PPC_ERR_CAPACITY, "host arrays are smaller than the agent count");
+	const int32_t base = s->reps[r].base;
+	const int D = s->ndefs;
+	view& v = s->v;
+	PPC_TRY(get_vec(s, a->positions, v.pos[s->cur], r, n));
+	PPC_TRY(get_vec(s, a->velocities, v.vel, r, n));
+	PPC_TRY(get_vec(s, a->previous_velocities, v.vprev, r, n));
+	PPC_TRY(get_vec(s, a->orientation, v.orient, r, n));
+	PPC_TRY(get_prm(s, 0, a->radius, r, n));
+	PPC_TRY(get_prm(s, 1, a->cell_cell_repulsion_strength, r, n));
+	PPC_TRY(get_prm(s, 2, a->cell_cell_adhesion_strength, r, n));
+	PPC_TRY(get_prm(s, 3, a->cell_BM_repulsion_strength, r, n));
+	PPC_TRY(get_scalar(s, a->relative_maximum_adhesion_distance, v.rmad, base, n, 1));
+	PPC_TRY(get_scalar(s, a->attachment_elastic_constant, v.ec, base, n, 1));
+	PPC_TRY(get_scalar(s, a->attachment_rate, v.arate, base, n, 1));
+	PPC_TRY(get_scalar(s, a->detachment_rate, v.drate, base, n, 1));
+	PPC_TRY(get_scalar(s, a->simple_pressure, v.pressure, base, n, 1));
+	PPC_TRY(get_scalar(s, a->total_volume, v.vol, base, n, 1));
+	PPC_TRY(get_scalar(s, a->nuclear_volume, v.nvol, base, n, 1));
+	PPC_TRY(get_scalar(s, a->nuclear_radius, v.nrad, base, n, 1));
+	PPC_TRY(get_scalar(s, a->surface_area, v.sarea, base, n, 1));
+	PPC_TRY(get_scalar(s, a->polarity, v.polarity, base, n, 1));
+	PPC_TRY(get_scalar(s, a->cell_adhesion_affinities, v.aff, base, n, D));
+	PPC_TRY(get_scalar(s, a->cell_definition_indices, v.def, base, n, 1));
+	PPC_TRY(get_scalar(s, a->maximum_number_of_attachments, v.maxatt, base, n, 1));
+	PPC_TRY(get_scalar(s, a->is_movable, v.movable, base, n, 1));
+	PPC_TRY(get_scalar(s, a->flags, v.flags, base, n, 1));
+	PPC_TRY(get_scalar(s, a->agent_ids, v.ids, base, n, 1));
+	if (a->spring_counts)
+	{
+		PPC_TRY(get_scalar(s, a->spring_counts, v.scnt, base, n, 1));
+		PPC_CUDA(cudaStreamSynchronize(s->stream));
+		int32_t mx = 0;
+		for (int32_t i = 0; i < n; i++)
+			mx = std::max(mx, a->spring_counts[i]);
+		if (mx > a->spring_capacity)
+			return fail(PPC_ERR_CAPACITY, "host spring rows are shorter than a spring list");
+		if (a->springs && n)
+		{
+			const size_t bytes = (size_t)n * a->spring_capacity * sizeof(int32_t);
+			PPC_TRY(ensure_stage(s, bytes));
+			PPC_TRY(launch_springs_local(s, r, n, static_cast<int32_t*>(s->stage), a->spring_capacity, 0));
+			PPC_CUDA(cudaMemcpyAsync(a->springs, s->stage, bytes, cudaMemcpyDeviceToHost, s->stream));
+		}
+	}
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	return PPC_OK;
+}
+
+int ensure_bins(ppc_state* s)
+{
+	if (!s->bins_valid)
+	{
+		PPC_TRY(launch_bin(s));
+		s->bins_valid = true;
+	}
+	return PPC_OK;
+}
+
+bool springs_unsupported(ppc_state* s) { return s->params.automated_spring_adhesion && s->rates_nonzero; }
+
+// The fused step recomputes neighbours inside its force pass and does not
+// store them; the lists the reference would hold after the step are built
+// here when a consumer needs them.
+int ensure_lists(ppc_state* s)
+{
+	if (s->lists_stale)
+	{
+		PPC_TRY(ensure_bins(s));
+		PPC_TRY(launch_neighbors(s));
+		s->lists_stale = false;
+	}
+	return PPC_OK;
+}
+
+// one fused mechanics step (+ phenotype container update)
+int enqueue_step(ppc_state* s, bool phenotype, double p_divide, double p_death)
+{
+	PPC_TRY(launch_fused(s));
+	PPC_TRY(launch_compact(s, false));
+	if (phenotype)
+	{
+		PPC_TRY(launch_flag_by_draws(s, p_divide, p_death));
+		PPC_TRY(launch_divide(s));
+		PPC_TRY(launch_mark_remove(s));
+		PPC_TRY(launch_compact(s, true));
+	}
+	PPC_TRY(launch_bin(s));
+	return PPC_OK;
+}
+
+constexpr int kGraphSteps = 10; // even, so a replay leaves the position buffer parity unchanged
+
+int run_steps(ppc_state* s, int32_t steps, bool phenotype, double p_divide, double p_death)
+{
+	if (steps < 0)
+		return fail(PPC_ERR_ARG, "negative step count");
+	if (springs_unsupported(s))
+		return fail(PPC_ERR_UNSUPPORTED, "stochastic spring attachment with non-zero rates is not on the device path");
+	PPC_TRY(ensure_bins(s));
+	int32_t done = 0;
+	// the first step after an upload may read non-zero velocities
+	while (done < steps && s->vel_dirty)
+	{
+		PPC_TRY(enqueue_step(s, phenotype, p_divide, p_death));
+		done++;
+	}
+	if (s->use_graphs && !s->profiling && steps - done >= kGraphSteps)
+	{
+		const bool reuse = s->graph && s->graph_cur == s->cur && s->graph_phenotype == phenotype
+						   && s->graph_pdiv == p_divide && s->graph_pdeath == p_death;
+		if (!reuse)
+		{
+			PPC_TRY(release_graph(s));
+			const int cur0 = s->cur;
+			const int64_t l0 = s->launches;
+			cudaGraph_t g = nullptr;
+			PPC_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+			int rc = PPC_OK;
+			for (int k = 0; k < kGraphSteps && rc == PPC_OK; k++)
+				rc = enqueue_step(s, phenotype, p_divide, p_death);
+			cudaError_t ec = cudaStreamEndCapture(s->stream, &g);
+			if (rc != PPC_OK)
+				return rc;
+			if (ec != cudaSuccess)
+				return cuda_fail(ec, "cudaStreamEndCapture");
+			ec = cudaGraphInstantiate(&s->graph, g, 0);
+			cudaGraphDestroy(g);
+			if (ec != cudaSuccess)
+				return cuda_fail(ec, "cudaGraphInstantiate");
+			s->graph_launches = s->launches - l0;
+			s->launches = l0;
+			s->cur = cur0;
+			s->graph_cur = cur0;
+			s->graph_phenotype = phenotype;
+			s->graph_pdiv = p_divide;
+			s->graph_pdeath = p_death;
+		}
+		while (steps - done >= kGraphSteps)
+		{
+			PPC_CUDA(cudaGraphLaunch(s->graph, s->stream));
+			s->launches += s->graph_launches;
+			done += kGraphSteps;
+		}
+	}
+	while (done < steps)
+	{
+		PPC_TRY(enqueue_step(s, phenotype, p_divide, p_death));
+		done++;
+	}
+	s->bins_valid = true;
+	s->lists_stale = steps > 0 || s->lists_stale;
+	return PPC_OK;
+}
+
+void mesh_info(const ppc_mesh& m, rep_info& R)
+{
+	R.voxels = 1;
+	for (int d = 0; d < 3; d++)
+	{
+		R.mins[d] = m.bounding_box_mins[d];
+		R.maxs[d] = m.bounding_box_maxs[d];
+		R.mins_int[d] = m.bounding_box_mins[d];
+		R.maxs_int[d] = m.bounding_box_maxs[d];
+		R.shape[d] = m.voxel_shape[d];
+		int g = 1;
+		if (d < m.dims)
+			g = (m.bounding_box_maxs[d] - m.bounding_box_mins[d] + m.voxel_shape[d] - 1) / m.voxel_shape[d];
+		R.grid[d] = std::max(g, 1);
+		R.voxels *= R.grid[d];
+	}
+}
+
+} // namespace
+} // namespace ppc
+
+using namespace ppc;
+
+extern "C" {
+
+const char* ppc_last_error(void) { return g_last_error.c_str(); }
+
+int ppc_abi_version(void) { return PPC_ABI_VERSION; }
+
+int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t replicates, const ppc_params* params,
+					 ppc_state** out)
+{
+	if (!meshes || !capacities || !params || !out || replicates < 1)
+		return fail(PPC_ERR_ARG, "null argument or no replicates");
+	const int dims = meshes[0].dims;
+	if (dims < 1 || dims > 3 || params->cell_definitions_count < 1 || params->mechanics_time_step <= 0)
+		return fail(PPC_ERR_ARG, "dims must be 1..3, cell definitions >= 1, time step > 0");
+	int ndev = 0;
+	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+		return fail(PPC_ERR_NO_DEVICE, "no CUDA device");
+
+	auto* s = new ppc_state;
+	s->dims = dims;
+	s->ndefs = params->cell_definitions_count;
+	s->nreps = replicates;
+	s->params = *params;
+	int64_t vox = 0;
+	int64_t cap = 0;
+	for (int32_t r = 0; r < replicates; r++)
+	{
+		if (meshes[r].dims != dims || capacities[r] < 0)
+		{
+			delete s;
+			return fail(PPC_ERR_ARG, "replicates must share dims; capacities must be >= 0");
+		}
+		for (int d = 0; d < dims; d++)
+			if (meshes[r].voxel_shape[d] <= 0 || meshes[r].bounding_box_maxs[d] < meshes[r].bounding_box_mins[d])
+			{
+				delete s;
+				return fail(PPC_ERR_ARG, "invalid mesh");
+			}
+		rep_info R {};
+		mesh_info(meshes[r], R);
+		R.base = (int32_t)cap;
+		R.cap = capacities[r];
+		R.vox_base = vox;
+		vox += R.voxels;
+		cap += capacities[r];
+		s->reps.push_back(R);
+		s->meshes.push_back(meshes[r]);
+	}
+	if (cap > INT32_MAX / 2 || vox > INT32_MAX)
+	{
+		delete s;
+		return fail(PPC_ERR_CAPACITY, "agent capacity or voxel count exceeds 32-bit indexing");
+	}
+	s->total_cap = (int32_t)std::max<int64_t>(cap, 1);
+	s->total_voxels = vox;
+
+	cudaGetDevice(&s->device);
+	cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device);
+	int rc = PPC_OK;
+	auto try_ = [&](int x) {
+		if (rc == PPC_OK)
+			rc = x;
+	};
+	if (cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+		rc = fail(PPC_ERR_CUDA, "cudaStreamCreate failed");
+	s->stream = s->own_stream;
+
+	view& v = s->v;
+	const size_t C = s->total_cap;
+	v.dims = dims;
+	v.ndefs = s->ndefs;
+	v.nreps = replicates;
+	v.total_cap = s->total_cap;
+	v.scap = s->scap;
+	v.ncap = s->ncap;
+	v.dt = params->mechanics_time_step;
+	v.walls = params->virtual_wall_at_domain_edges;
+	rep_info* reps = nullptr;
+	try_(alloc(s, reps, replicates));
+	v.reps = reps;
+	try_(alloc(s, v.ctr, replicates));
+	try_(alloc(s, v.err, 1));
+	try_(alloc(s, v.cursor, 1));
+	try_(alloc(s, v.epoch, 1));
+	try_(alloc(s, v.pos[0], C));
+	try_(alloc(s, v.pos[1], C));
+	try_(alloc(s, v.vel, C));
+	try_(alloc(s, v.vprev, C));
+	try_(alloc(s, v.prm, C));
+	try_(alloc(s, v.rmad, C));
+	try_(alloc(s, v.ec, C));
+	try_(alloc(s, v.arate, C));
+	try_(alloc(s, v.drate, C));
+	try_(alloc(s, v.pressure, C));
+	try_(alloc(s, v.vol, C));
+	try_(alloc(s, v.nvol, C));
+	try_(alloc(s, v.nrad, C));
+	try_(alloc(s, v.sarea, C));
+	try_(alloc(s, v.polarity, C));
+	try_(alloc(s, v.orient, C));
+	try_(alloc(s, v.aff, C * s->ndefs));
+	try_(alloc(s, v.def, C));
+	try_(alloc(s, v.maxatt, C));
+	try_(alloc(s, v.scnt, C));
+	try_(alloc(s, v.springs, C * s->scap));
+	try_(alloc(s, v.movable, C));
+	try_(alloc(s, v.flags, C));
+	try_(alloc(s, v.ids, C));
+	try_(alloc(s, v.rid, C));
+	try_(alloc(s, v.vox_word, (size_t)vox));
+	try_(alloc(s, v.vox_start, (size_t)vox, false));
+	try_(alloc(s, v.key, C));
+	try_(alloc(s, v.vrank, C));
+	try_(alloc(s, v.tmp, C));
+	try_(alloc(s, v.sorted, C));
+	try_(alloc(s, v.spos4, C));
+	try_(alloc(s, v.ncnt, C));
+	try_(alloc(s, v.nidx, C * s->ncap, false));
+	try_(alloc(s, v.bad, C));
+	try_(alloc(s, v.divl, C));
+	try_(alloc(s, v.moves, 2 * C));
+	try_(alloc(s, v.nmoves, replicates));
+	try_(alloc(s, v.draw_epoch, replicates));
+	if (rc == PPC_OK)
+	{
+		std::vector<int32_t> rid(C, 0);
+		for (int32_t r = 0; r < replicates; r++)
+			for (int32_t k = 0; k < s->reps[r].cap; k++)
+				rid[s->reps[r].base + k] = r;
+		if (cudaMemcpy(v.rid, rid.data(), C * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess
+			|| cudaMemcpy(reps, s->reps.data(), sizeof(rep_info) * replicates, cudaMemcpyHostToDevice) != cudaSuccess)
+			rc = fail(PPC_ERR_CUDA, "initial copy failed");
+	}
+	if (rc != PPC_OK)
+	{
+		ppc_destroy(s);
+		return rc;
+	}
+	*out = s;
+	return PPC_OK;
+}
+
+int ppc_create(const ppc_mesh* mesh, const ppc_params* params, int32_t agent_capacity, ppc_state** out)
+{
+	return ppc_create_batch(mesh, &agent_capacity, 1, params, out);
+}
+
+int ppc_destroy(ppc_state* s)
+{
+	if (!s)
+		return PPC_OK;
+	if (s->stream)
+		cudaStreamSynchronize(s->stream);
+	release_graph(s);
+	for (auto e : s->prof_events)
+		cudaEventDestroy(e);
+	for (auto& b : s->allocations)
+		cudaFree(b.p);
+	if (s->stage)
+		cudaFree(s->stage);
+	if (s->own_stream)
+		cudaStreamDestroy(s->own_stream);
+	delete s;
+	return PPC_OK;
+}
+
+int ppc_set_stream(ppc_state* s, void* stream)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	release_graph(s);
+	s->stream = stream ? static_cast<cudaStream_t>(stream) : s->own_stream;
+	return PPC_OK;
+}
+
+int ppc_set_precision(ppc_state* s, int32_t precision)
+{
+	if (!s || (precision != PPC_FP64 && precision != PPC_FP32_FORCE))
+		return fail(PPC_ERR_ARG, "precision must be PPC_FP64 or PPC_FP32_FORCE");
+	if (precision == PPC_FP32_FORCE)
+		return fail(PPC_ERR_UNSUPPORTED, "the FP32-force form is not built yet");
+	s->precision = precision;
+	release_graph(s);
+	return PPC_OK;
+}
+
+int ppc_set_random_seed(ppc_state* s, uint64_t seed)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	s->seed = seed;
+	s->v.seed = seed;
+	release_graph(s);
+	return PPC_OK;
+}
+
+int ppc_set_neighbor_capacity(ppc_state* s, int32_t per_agent)
+{
+	if (!s || per_agent < 1)
+		return fail(PPC_ERR_ARG, "neighbour capacity must be >= 1");
+	if (per_agent == s->ncap)
+		return PPC_OK;
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	int32_t* p = nullptr;
+	size_t bytes = (size_t)s->total_cap * per_agent * sizeof(int32_t);
+	PPC_CUDA(cudaMalloc(&p, bytes));
+	for (auto& b : s->allocations)
+		if (b.p == s->v.nidx)
+		{
+			cudaFree(b.p);
+			b.p = p;
+			b.bytes = bytes;
+		}
+	s->v.nidx = p;
+	s->v.ncap = s->ncap = per_agent;
+	PPC_CUDA(cudaMemset(s->v.ncnt, 0, sizeof(int32_t) * s->total_cap));
+	release_graph(s);
+	return PPC_OK;
+}
+
+int ppc_upload(ppc_state* s, int32_t r, const ppc_agents* a)
+{
+	if (!valid(s, r) || !a || a->count < 0)
+		return fail(PPC_ERR_ARG, "invalid state, replicate or agents");
+	if (a->count > s->reps[r].cap)
+		return fail(PPC_ERR_CAPACITY, "agent count exceeds the replicate's capacity");
+	// a fresh upload resets the replicate's counters except the event totals
+	std::vector<rep_counters> all;
+	PPC_TRY(read_counters(s, all));
+	rep_counters c {};
+	c.divisions = all[r].divisions;
+	c.deaths = all[r].deaths;
+	PPC_CUDA(cudaMemcpy(&s->v.ctr[r], &c, sizeof c, cudaMemcpyHostToDevice));
+	s->lists_stale = false;
+	return transfer_in(s, r, a, true);
+}
+
+int ppc_upload_fields(ppc_state* s, int32_t r, const ppc_agents* a)
+{
+	if (!valid(s, r) || !a)
+		return fail(PPC_ERR_ARG, "invalid state, replicate or agents");
+	std::vector<rep_counters> c;
+	PPC_TRY(read_counters(s, c));
+	if (a->count != c[r].count)
+		return fail(PPC_ERR_ARG, "count differs from the device count");
+	return transfer_in(s, r, a, false);
+}
+
+int ppc_download(ppc_state* s, int32_t r, ppc_agents* a)
+{
+	if (!valid(s, r) || !a)
+		return fail(PPC_ERR_ARG, "invalid state, replicate or agents");
+	PPC_TRY(finish(s));
+	return transfer_out(s, r, a);
+}
+
+int ppc_get_count(ppc_state* s, int32_t r, int32_t* count)
+{
+	if (!valid(s, r) || !count)
+		return fail(PPC_ERR_ARG, "invalid state or replicate");
+	std::vector<rep_counters> c;
+	PPC_TRY(read_counters(s, c));
+	*count = c[r].count;
+	return finish(s);
+}
+
+int ppc_get_event_counts(ppc_state* s, int32_t r, int64_t* divisions, int64_t* deaths)
+{
+	if (!valid(s, r))
+		return fail(PPC_ERR_ARG, "invalid state or replicate");
+	std::vector<rep_counters> c;
+	PPC_TRY(read_counters(s, c));
+	if (divisions)
+		*divisions = c[r].divisions;
+	if (deaths)
+		*deaths = c[r].deaths;
+	return PPC_OK;
+}
+
+int ppc_synchronize(ppc_state* s)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	return finish(s);
+}
+
+void* ppc_host_alloc(size_t bytes)
+{
+	void* p = nullptr;
+	if (cudaHostAlloc(&p, std::max<size_t>(bytes, 1), cudaHostAllocDefault) != cudaSuccess)
+		return nullptr;
+	return p;
+}
+
+void ppc_host_free(void* p)
+{
+	if (p)
+		cudaFreeHost(p);
+}
+
+int ppc_update_mechanics_mesh(ppc_state* s)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	PPC_TRY(launch_bin(s));
+	s->bins_valid = true;
+	return finish(s);
+}
+
+int ppc_update_cell_neighbors(ppc_state* s)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	PPC_TRY(ensure_bins(s));
+	PPC_TRY(launch_neighbors(s));
+	s->lists_stale = false;
+	return finish(s);
+}
+
+int ppc_update_cell_forces(ppc_state* s)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	PPC_TRY(ensure_lists(s));
+	PPC_TRY(launch_forces(s));
+	return finish(s);
+}
+
+int ppc_update_motility(ppc_state* s)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	return PPC_OK;
+}
+
+int ppc_update_basement_membrane_interactions(ppc_state* s)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	if (!s->params.virtual_wall_at_domain_edges)
+		return PPC_OK;
+	PPC_TRY(launch_membrane(s));
+	return finish(s);
+}
+
+int ppc_update_spring_attachments(ppc_state* s)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	if (!s->params.automated_spring_adhesion)
+		return PPC_OK;
+	if (springs_unsupported(s))
+		return fail(PPC_ERR_UNSUPPORTED, "stochastic spring attachment with non-zero rates is not on the device path");
+	if (!s->has_springs)
+		return PPC_OK;
+	PPC_TRY(launch_springs(s));
+	return finish(s);
+}
+
+int ppc_update_positions(ppc_state* s)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	PPC_TRY(launch_positions(s));
+	s->bins_valid = false;
+	return finish(s);
+}
+
+int ppc_update_cell_container_for_mechanics(ppc_state* s)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	PPC_TRY(ensure_lists(s));
+	PPC_TRY(launch_mark_remove(s));
+	PPC_TRY(launch_compact(s, false));
+	s->bins_valid = false;
+	return finish(s);
+}
+
+int ppc_update_cell_container_for_phenotype(ppc_state* s)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	PPC_TRY(ensure_lists(s));
+	PPC_TRY(launch_divide(s));
+	PPC_TRY(launch_mark_remove(s));
+	PPC_TRY(launch_compact(s, true));
+	s->bins_valid = false;
+	return finish(s);
+}
+
+int ppc_flag_by_draws(ppc_state* s, double p_divide, double p_death)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	PPC_TRY(launch_flag_by_draws(s, p_divide, p_death));
+	return finish(s);
+}
+
+int ppc_step(ppc_state* s, int32_t steps)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	return run_steps(s, steps, false, 0, 0);
+}
+
+int ppc_step_with_phenotype(ppc_state* s, int32_t steps, double p_divide, double p_death)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	return run_steps(s, steps, true, p_divide, p_death);
+}
+
+int ppc_get_neighbors(ppc_state* s, int32_t r, int32_t* counts, int32_t* lists, int32_t list_capacity)
+{
+	if (!valid(s, r) || !counts || !lists || list_capacity < 1)
+		return fail(PPC_ERR_ARG, "invalid arguments");
+	PPC_TRY(ensure_lists(s));
+	std::vector<rep_counters> c;
+	PPC_TRY(read_counters(s, c));
+	const int32_t n = c[r].count;
+	if (n == 0)
+		return PPC_OK;
+	int32_t* d = nullptr;
+	const size_t bytes = (size_t)n * (list_capacity + 1) * sizeof(int32_t);
+	PPC_CUDA(cudaMalloc(&d, bytes));
+	int rc = launch_neighbors_local(s, r, n, d, d + n, list_capacity);
+	if (rc == PPC_OK)
+	{
+		cudaMemcpyAsync(counts, d, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream);
+		cudaMemcpyAsync(lists, d + n, (size_t)n * list_capacity * sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream);
+		cudaStreamSynchronize(s->stream);
+	}
+	cudaFree(d);
+	PPC_TRY(rc);
+	for (int32_t i = 0; i < n; i++)
+		if (counts[i] > list_capacity || counts[i] > s->ncap)
+			return fail(PPC_ERR_CAPACITY, "a neighbour list is longer than the capacity");
+	return finish(s);
+}
+
+int ppc_get_voxel_count(ppc_state* s, int32_t r, int64_t* voxel_count)
+{
+	if (!valid(s, r) || !voxel_count)
+		return fail(PPC_ERR_ARG, "invalid arguments");
+	*voxel_count = s->reps[r].voxels;
+	return PPC_OK;
+}
+
+int ppc_get_mesh_bins(ppc_state* s, int32_t r, int32_t* voxel_counts, int32_t* agents)
+{
+	if (!valid(s, r) || !voxel_counts || !agents)
+		return fail(PPC_ERR_ARG, "invalid arguments");
+	PPC_TRY(ensure_bins(s));
+	const rep_info& R = s->reps[r];
+	std::vector<unsigned long long> words(R.voxels);
+	std::vector<int32_t> starts(R.voxels);
+	uint32_t epoch = 0;
+	int32_t ntot = 0;
+	PPC_CUDA(cudaMemcpyAsync(words.data(), s->v.vox_word + R.vox_base, R.voxels * 8, cudaMemcpyDeviceToHost, s->stream));
+	PPC_CUDA(cudaMemcpyAsync(starts.data(), s->v.vox_start + R.vox_base, R.voxels * 4, cudaMemcpyDeviceToHost,
+							 s->stream));
+	PPC_CUDA(cudaMemcpyAsync(&epoch, s->v.epoch, 4, cudaMemcpyDeviceToHost, s->stream));
+	PPC_CUDA(cudaMemcpyAsync(&ntot, s->v.cursor, 4, cudaMemcpyDeviceToHost, s->stream));
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	std::vector<int32_t> sorted(std::max(ntot, 1));
+	PPC_CUDA(cudaMemcpy(sorted.data(), s->v.sorted, (size_t)ntot * 4, cudaMemcpyDeviceToHost));
+	size_t o = 0;
+	for (int64_t k = 0; k < R.voxels; k++)
+	{
+		const bool live = (uint32_t)(words[k] >> 32) == epoch;
+		const int32_t c = live ? (int32_t)(uint32_t)words[k] : 0;
+		voxel_counts[k] = c;
+		for (int32_t u = 0; u < c; u++)
+			agents[o++] = sorted[starts[k] + u] - R.base;
+	}
+	return finish(s);
+}
+
+int ppc_get_mesh_position(const ppc_mesh* mesh, const double* position, int32_t* c)
+{
+	if (!mesh || !position || !c)
+		return fail(PPC_ERR_ARG, "null argument");
+	rep_info R {};
+	mesh_info(*mesh, R);
+	for (int d = 0; d < 3; d++)
+	{
+		c[d] = 0;
+		if (d >= mesh->dims)
+			continue;
+		const double q = (position[d] - R.mins[d]) / R.shape[d];
+		c[d] = (q == q && q > 0) ? (q >= R.grid[d] ? R.grid[d] - 1 : (int32_t)q) : 0;
+	}
+	return PPC_OK;
+}
+
+int ppc_get_mesh_index(const ppc_mesh* mesh, const int32_t* c, int32_t* index)
+{
+	if (!mesh || !c || !index)
+		return fail(PPC_ERR_ARG, "null argument");
+	rep_info R {};
+	mesh_info(*mesh, R);
+	*index = c[0] + R.grid[0] * (c[1] + R.grid[1] * c[2]);
+	return PPC_OK;
+}
+
+int ppc_set_profiling(ppc_state* s, int32_t on)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	s->profiling = on != 0;
+	s->prof_used = 0;
+	return PPC_OK;
+}
+
+int ppc_get_profile(ppc_state* s, double* fused_ms, int64_t* fused_launches)
+{
+	if (!s || !fused_ms || !fused_launches)
+		return fail(PPC_ERR_ARG, "null argument");
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	double total = 0;
+	for (size_t k = 0; k + 1 < s->prof_used; k += 2)
+	{
+		float ms = 0;
+		PPC_CUDA(cudaEventElapsedTime(&ms, s->prof_events[k], s->prof_events[k + 1]));
+		total += ms;
+	}
+	*fused_ms = total;
+	*fused_launches = (int64_t)(s->prof_used / 2);
+	return PPC_OK;
+}
+
+int ppc_get_launch_count(ppc_state* s, int64_t* launches)
+{
+	if (!s || !launches)
+		return fail(PPC_ERR_ARG, "null argument");
+	*launches = s->launches;
+	return PPC_OK;
+}
+
+} // extern "C"

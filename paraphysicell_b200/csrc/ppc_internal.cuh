@@ -1,0 +1,221 @@
+// ppc_internal.cuh — device state layout and shared helpers of libppc.
+//
+// Layout in HBM (one allocation per array, all sized to the total slot
+// capacity C = sum of replicate capacities):
+//   replicate r owns slots [base_r, base_r + cap_r); its live agents are
+//   slots base_r .. base_r + count_r - 1 in the reference's index order.
+//   pos4[2][C]   double4 {x, y, z, 0}, double-buffered across the fused step
+//   vel[C], vprev[C]  double4 {vx, vy, vz, 0}
+//   prm[C]       double4 {radius, repulsion, adhesion, BM repulsion}
+//   rmad, ec, arate, drate, pressure, vol, nvol, nrad, sarea, polarity [C] double
+//   orient[C]    double4
+//   aff[C*D], def, maxatt, scnt [C] int32, springs [C*S] int32
+//   movable, flags [C] uint8, ids [C] int64, rid [C] int32 (replicate of slot)
+// Mechanics mesh bins, rebuilt by a counting sort each step:
+//   vox_word[V] uint64 {epoch:32 | count:32}, vox_start[V] int32
+//   key[C] (global voxel index), vrank[C] (provisional rank), tmp[C]
+//   sorted[C] slots grouped by voxel (descending slot inside a voxel),
+//   spos4[C] double4 {x, y, z, rmad*radius} in sorted order.
+// A voxel's bin is valid only when its word's epoch equals the current
+// epoch, so the V-sized table is never cleared (work stays O(agents)).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/ppc.h"
+
+namespace ppc {
+
+constexpr double simple_pressure_coefficient = 36.64504274775163; // reference: position_solver.cpp:13
+
+// device error bits (folded into a status by the host)
+enum : int32_t
+{
+	ERR_NEIGHBOR_CAPACITY = 1,
+	ERR_NONFINITE = 2,
+	ERR_OUT_OF_MESH = 4,
+	ERR_AGENT_CAPACITY = 8,
+	ERR_SPRING_CAPACITY = 16,
+	ERR_LIST_CAPACITY = 32
+};
+
+struct rep_info
+{
+	double mins[3], maxs[3], shape[3];
+	int32_t grid[3];
+	int32_t base, cap;
+	int64_t vox_base;
+	int64_t voxels;
+	int32_t maxs_int[3], mins_int[3];
+};
+
+// per-replicate device counters
+struct rep_counters
+{
+	int32_t count;		 // live agents
+	int32_t nvisit;		 // agents visited by the current removal pass
+	int32_t nbad;		 // entries in the removal candidate list
+	int32_t ndiv;		 // entries in the division list
+	int64_t divisions;	 // environment::divisions_count
+	int64_t deaths;		 // environment::deaths_count
+	int64_t next_id;	 // id of the next created agent
+};
+
+// everything a kernel needs, passed by value
+struct view
+{
+	int32_t dims, ndefs, nreps, total_cap, scap, ncap;
+	double dt;
+	int32_t walls;
+	const rep_info* reps;
+	rep_counters* ctr;
+	int32_t* err;
+	int32_t* cursor;	// number of binned agents (length of `sorted`)
+	uint32_t* epoch;	// epoch of the current bins
+
+	double4* pos[2];
+	double4* vel;
+	double4* vprev;
+	double4* prm;
+	double* rmad;
+	double* ec;
+	double* arate;
+	double* drate;
+	double* pressure;
+	double* vol;
+	double* nvol;
+	double* nrad;
+	double* sarea;
+	double* polarity;
+	double4* orient;
+	double* aff;
+	int32_t* def;
+	int32_t* maxatt;
+	int32_t* scnt;
+	int32_t* springs;
+	uint8_t* movable;
+	uint8_t* flags;
+	int64_t* ids;
+	int32_t* rid;
+
+	unsigned long long* vox_word;
+	int32_t* vox_start;
+	int32_t* key;
+	int32_t* vrank;
+	int32_t* tmp;
+	int32_t* sorted;
+	double4* spos4;
+
+	int32_t* ncnt;
+	int32_t* nidx;
+
+	int32_t* bad;	  // per replicate: removal candidates (local indices), C entries total at base_r
+	int32_t* divl;	  // per replicate: division list, same layout
+	int32_t* moves;	  // per replicate: (dst, src) pairs of the compaction, 2*C at 2*base_r
+	int32_t* nmoves;  // per replicate move counts
+
+	uint64_t seed;
+	uint64_t* draw_epoch; // per replicate draw epoch
+};
+
+struct buffer
+{
+	void* p = nullptr;
+	size_t bytes = 0;
+};
+
+} // namespace ppc
+
+struct ppc_state
+{
+	int device = 0;
+	int32_t dims = 3, ndefs = 1, nreps = 1, total_cap = 0, scap = 12, ncap = 64;
+	ppc_params params {};
+	std::vector<ppc_mesh> meshes;
+	std::vector<ppc::rep_info> reps;
+	int64_t total_voxels = 0;
+	int32_t precision = PPC_FP64;
+	uint64_t seed = 0;
+
+	cudaStream_t own_stream = nullptr;
+	cudaStream_t stream = nullptr;
+
+	ppc::view v {};
+	std::vector<ppc::buffer> allocations;
+
+	int cur = 0;				  // which pos4 buffer is current
+	bool vel_dirty = false;		  // some movable agent may have a non-zero velocity
+	bool has_springs = false;	  // some agent may have springs
+	bool rates_nonzero = false;	  // some attachment/detachment rate is non-zero
+	bool bins_valid = false;	  // bins match the current positions
+	bool lists_stale = false;	  // a fused step ran since the neighbour lists were built
+	int64_t launches = 0;
+	int max_grid_blocks = 0;
+	int sm_count = 148;
+
+	// staging for host <-> device copies
+	void* stage = nullptr;
+	size_t stage_bytes = 0;
+
+	// captured CUDA graph of a block of fused steps
+	cudaGraphExec_t graph = nullptr;
+	int graph_steps = 0;
+	int graph_cur = -1;
+	bool graph_phenotype = false;
+	double graph_pdiv = 0, graph_pdeath = 0;
+	int64_t graph_launches = 0;
+	bool use_graphs = true;
+
+	// fused-kernel timing (ppc_set_profiling)
+	bool profiling = false;
+	std::vector<cudaEvent_t> prof_events; // pairs (start, end)
+	size_t prof_used = 0;
+};
+
+namespace ppc {
+
+void set_error(const std::string& msg);
+int cuda_fail(cudaError_t e, const char* where);
+
+#define PPC_CUDA(call)                                                                                                 \
+	do                                                                                                                 \
+	{                                                                                                                  \
+		cudaError_t e_ = (call);                                                                                       \
+		if (e_ != cudaSuccess)                                                                                         \
+			return ppc::cuda_fail(e_, #call);                                                                          \
+	} while (0)
+
+#define PPC_LAUNCH(s) ((s)->launches++, (s)->stream)
+
+inline int blocks_for(int64_t n, int threads)
+{
+	int64_t b = (n + threads - 1) / threads;
+	return (int)(b < 1 ? 1 : b);
+}
+
+// ---- kernel entry points (ppc_kernels.cu) ----
+int launch_bin(ppc_state* s);
+int launch_neighbors(ppc_state* s);
+int launch_forces(ppc_state* s);
+int launch_membrane(ppc_state* s);
+int launch_springs(ppc_state* s);
+int launch_positions(ppc_state* s);
+int launch_fused(ppc_state* s);
+int launch_compact(ppc_state* s, bool phenotype_pass);
+int launch_mark_remove(ppc_state* s);
+int launch_divide(ppc_state* s);
+int launch_flag_by_draws(ppc_state* s, double p_divide, double p_death);
+
+// packing between host-layout staging buffers and device arrays
+int launch_unpack_vec(ppc_state* s, double4* dst, const double* src, int32_t r, int32_t n);
+int launch_pack_vec(ppc_state* s, double* dst, const double4* src, int32_t r, int32_t n);
+int launch_unpack_prm(ppc_state* s, int field, const double* src, int32_t r, int32_t n);
+int launch_pack_prm(ppc_state* s, int field, double* dst, int32_t r, int32_t n);
+int launch_neighbors_local(ppc_state* s, int32_t r, int32_t n, int32_t* counts, int32_t* lists, int32_t cap);
+int launch_springs_local(ppc_state* s, int32_t r, int32_t n, int32_t* rows, int32_t cap, int to_device);
+
+} // namespace ppc

@@ -1,0 +1,1349 @@
+// ppc_kernels.cu — CUDA kernels of the mechanics timestep (sm_100a).
+//
+// Built with -fmad=false: every FP64 expression rounds after each operation,
+// exactly like the reference compiled for baseline x86-64 (no FMA), so the
+// FP64 path reproduces the reference's values bit for bit when operations are
+// written in the reference's order. Each kernel cites the reference lines it
+// replaces.
+#include <cuda_runtime.h>
+
+#include "../../include/ppc_draws.h"
+#include "ppc_internal.cuh"
+
+namespace ppc {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kSortCap = 4096; // list length sorted in shared memory
+
+__device__ __forceinline__ int rep_of(const view& v, int s) { return v.nreps == 1 ? 0 : v.rid[s]; }
+
+__device__ __forceinline__ double comp(const double4& p, int d) { return d == 0 ? p.x : (d == 1 ? p.y : p.z); }
+
+__device__ __forceinline__ void set_comp(double4& p, int d, double x)
+{
+	if (d == 0)
+		p.x = x;
+	else if (d == 1)
+		p.y = x;
+	else
+		p.z = x;
+}
+
+// slot s is live when its index inside its replicate is below the count
+__device__ __forceinline__ bool live(const view& v, int s, int& r, int& local)
+{
+	r = rep_of(v, s);
+	local = s - v.reps[r].base;
+	return local < v.ctr[r].count;
+}
+
+// ---------------------------------------------------------------------------
+// mesh binning: containers_solver::update_mechanics_mesh
+// (reference: src/solver/host/containers_solver.cpp:15-56,
+//  common_solver.cpp:10-38)
+// ---------------------------------------------------------------------------
+
+// voxel coordinate along one axis: truncation of (x - min) / shape, clamped
+// into [0, grid); flags positions outside the box and non-finite values
+__device__ __forceinline__ int axis_coord(double x, const rep_info& R, int d, int32_t* err)
+{
+	double q = (x - R.mins[d]) / R.shape[d];
+	if (!(q == q))
+	{
+		atomicOr(err, ERR_NONFINITE);
+		return 0;
+	}
+	int g = R.grid[d];
+	if (q <= 0.0)
+	{
+		if (q <= -1.0)
+			atomicOr(err, ERR_OUT_OF_MESH);
+		return 0;
+	}
+	if (q >= (double)g)
+	{
+		if (x != R.maxs[d])
+			atomicOr(err, ERR_OUT_OF_MESH);
+		return g - 1;
+	}
+	return (int)q;
+}
+
+__global__ void k_bin_count(view v, int cur)
+{
+	int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s == 0)
+		*v.cursor = 0;
+	if (s >= v.total_cap)
+		return;
+	int r, local;
+	if (!live(v, s, r, local))
+		return;
+	const rep_info& R = v.reps[r];
+	const uint32_t ep = *v.epoch + 1;
+	double4 p = v.pos[cur][s];
+	int c0 = axis_coord(p.x, R, 0, v.err);
+	int c1 = v.dims >= 2 ? axis_coord(p.y, R, 1, v.err) : 0;
+	int c2 = v.dims >= 3 ? axis_coord(p.z, R, 2, v.err) : 0;
+	int64_t key = R.vox_base + c0 + (int64_t)R.grid[0] * (c1 + (int64_t)R.grid[1] * c2);
+
+	// count into the epoch-tagged voxel word; a stale epoch means the voxel
+	// is empty in this rebuild
+	unsigned long long* w = v.vox_word + key;
+	unsigned long long old = *w;
+	int rank = 0;
+	for (int it = 0; it < (1 << 24); it++)
+	{
+		uint32_t hi = (uint32_t)(old >> 32);
+		unsigned long long nw = hi == ep ? old + 1ull : (((unsigned long long)ep << 32) | 1ull);
+		unsigned long long prev = atomicCAS(w, old, nw);
+		if (prev == old)
+		{
+			rank = hi == ep ? (int)(uint32_t)old : 0;
+			break;
+		}
+		old = prev;
+	}
+	v.key[s] = (int32_t)key;
+	v.vrank[s] = rank;
+}
+
+// block-wide exclusive scan of one int per thread; returns the block total
+__device__ __forceinline__ int block_exclusive_scan(int x, int& total)
+{
+	__shared__ int warp_sums[32];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	int incl = x;
+	for (int o = 1; o < 32; o <<= 1)
+	{
+		int y = __shfl_up_sync(0xffffffffu, incl, o);
+		if (lane >= o)
+			incl += y;
+	}
+	if (lane == 31)
+		warp_sums[warp] = incl;
+	__syncthreads();
+	const int nwarps = blockDim.x >> 5;
+	if (warp == 0)
+	{
+		int w = lane < nwarps ? warp_sums[lane] : 0;
+		for (int o = 1; o < 32; o <<= 1)
+		{
+			int y = __shfl_up_sync(0xffffffffu, w, o);
+			if (lane >= o)
+				w += y;
+		}
+		if (lane < nwarps)
+			warp_sums[lane] = w;
+	}
+	__syncthreads();
+	total = warp_sums[nwarps - 1];
+	int excl = incl - x + (warp > 0 ? warp_sums[warp - 1] : 0);
+	__syncthreads();
+	return excl;
+}
+
+// the first agent counted into a voxel reserves the voxel's segment of the
+// sorted array (one atomic per block)
+__global__ void k_bin_alloc(view v)
+{
+	__shared__ int block_base;
+	int s = blockIdx.x * blockDim.x + threadIdx.x;
+	int c = 0;
+	int32_t key = -1;
+	if (s < v.total_cap)
+	{
+		int r, local;
+		if (live(v, s, r, local) && v.vrank[s] == 0)
+		{
+			key = v.key[s];
+			c = (int)(uint32_t)v.vox_word[key];
+		}
+	}
+	int total;
+	int excl = block_exclusive_scan(c, total);
+	if (threadIdx.x == 0)
+		block_base = total > 0 ? atomicAdd(v.cursor, total) : 0;
+	__syncthreads();
+	if (c > 0)
+		v.vox_start[key] = block_base + excl;
+	if (s == 0)
+		*v.epoch += 1;
+}
+
+__global__ void k_bin_scatter(view v)
+{
+	int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= v.total_cap)
+		return;
+	int r, local;
+	if (!live(v, s, r, local))
+		return;
+	v.tmp[v.vox_start[v.key[s]] + v.vrank[s]] = s;
+}
+
+// final place inside the voxel: descending slot order, which is the order
+// a serial run of the reference's fetch_sub scatter produces
+__global__ void k_bin_fixup(view v, int cur)
+{
+	int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= v.total_cap)
+		return;
+	int r, local;
+	if (!live(v, s, r, local))
+		return;
+	int32_t key = v.key[s];
+	int c = (int)(uint32_t)v.vox_word[key];
+	int st = v.vox_start[key];
+	int rank = 0;
+	for (int u = 0; u < c; u++)
+		rank += v.tmp[st + u] > s;
+	v.sorted[st + rank] = s;
+	double4 p = v.pos[cur][s];
+	p.w = v.rmad[s] * v.prm[s].x; // relative_maximum_adhesion_distance * radius
+	v.spos4[st + rank] = p;
+}
+
+// ---------------------------------------------------------------------------
+// neighbour scan: common_solver::for_each_in_mech_neighborhood +
+// update_cell_neighbors_single (reference: common_solver.h:77-105,
+// position_solver.cpp:79-97). Visits voxels z, y, x from -1 to 1 and, in each,
+// agents in bin order; calls f for every agent j != i with
+// distance <= rmad_i r_i + rmad_j r_j.
+// ---------------------------------------------------------------------------
+
+template <int DIMS, typename F>
+__device__ __forceinline__ void for_each_neighbor(const view& v, const rep_info& R, uint32_t ep, int s,
+												  const double4& pi, F&& f)
+{
+	int32_t lk = (int32_t)(v.key[s] - R.vox_base);
+	const int g0 = R.grid[0], g1 = R.grid[1], g2 = R.grid[2];
+	const int cx = lk % g0;
+	const int cy = (lk / g0) % g1;
+	const int cz = lk / (g0 * g1);
+	const int zlo = DIMS >= 3 ? -1 : 0, zhi = DIMS >= 3 ? 1 : 0;
+	const int ylo = DIMS >= 2 ? -1 : 0, yhi = DIMS >= 2 ? 1 : 0;
+	for (int dz = zlo; dz <= zhi; dz++)
+	{
+		const int z = cz + dz;
+		if (z < 0 || z >= g2)
+			continue;
+		for (int dy = ylo; dy <= yhi; dy++)
+		{
+			const int y = cy + dy;
+			if (y < 0 || y >= g1)
+				continue;
+			const int64_t row = R.vox_base + (int64_t)g0 * (y + (int64_t)g1 * z);
+			for (int dx = -1; dx <= 1; dx++)
+			{
+				const int x = cx + dx;
+				if (x < 0 || x >= g0)
+					continue;
+				const unsigned long long w = v.vox_word[row + x];
+				if ((uint32_t)(w >> 32) != ep)
+					continue;
+				const int c = (int)(uint32_t)w;
+				const int st = v.vox_start[row + x];
+				for (int u = st; u < st + c; u++)
+				{
+					const int j = v.sorted[u];
+					if (j == s)
+						continue;
+					const double4 q = v.spos4[u];
+					const double ddx = pi.x - q.x;
+					const double ddy = DIMS >= 2 ? pi.y - q.y : 0.0;
+					const double ddz = DIMS >= 3 ? pi.z - q.z : 0.0;
+					double d2 = ddx * ddx;
+					if (DIMS >= 2)
+						d2 = d2 + ddy * ddy;
+					if (DIMS >= 3)
+						d2 = d2 + ddz * ddz;
+					const double ad = pi.w + q.w;
+					// exact early reject: d2 > ad^2 (1 + 1e-12) implies sqrt(d2) > ad
+					if (d2 > ad * ad * (1.0 + 1e-12))
+						continue;
+					const double dist = DIMS == 1 ? fabs(ddx) : sqrt(d2);
+					if (dist <= ad)
+						f(j, ddx, ddy, ddz, dist, ad);
+				}
+			}
+		}
+	}
+}
+
+// solve_pair for the lhs side (reference: position_solver.cpp:24-77) with the
+// pressure contributions of the pair to lhs. Adds (repulsion - adhesion) /
+// distance * difference to v when lhs is movable.
+struct pair_fp64
+{
+	double4 prm_i;
+	const double* aff_i;
+	int def_i;
+	bool mov_i;
+	double vx = 0, vy = 0, vz = 0, p = 0;
+	double last_term = 0; // pressure contribution of the last pair
+
+	__device__ __forceinline__ void add(const view& v, int j, double ddx, double ddy, double ddz, double dist,
+										double adhesion_distance)
+	{
+		const double4 prm_j = v.prm[j];
+		const bool mov_j = v.movable[j] != 0;
+		const double d = dist < 0.00001 ? 0.00001 : dist; // std::max(distance, 0.00001)
+		double rep = 1.0 - d / (prm_i.x + prm_j.x);
+		rep = rep < 0 ? 0 : rep;
+		rep = rep * rep;
+		const double term = rep * simple_pressure_coefficient;
+		last_term = term;
+		if (mov_i)
+			p = p + term;
+		if (mov_j)
+			p = p + term;
+		if (!mov_i)
+			return;
+		rep = rep * sqrt(prm_i.y * prm_j.y);
+		double adh = 1.0 - d / adhesion_distance;
+		adh = adh * adh;
+		const int def_j = v.def[j];
+		adh = adh * sqrt(prm_i.z * prm_j.z * aff_i[def_j] * v.aff[(int64_t)j * v.ndefs + def_i]);
+		const double force = (rep - adh) / d;
+		vx = vx + force * ddx;
+		vy = vy + force * ddy;
+		vz = vz + force * ddz;
+	}
+};
+
+// update_membrane_velocity (reference: solver_helper.h:14-28)
+__device__ __forceinline__ double membrane(double x, double bb, double sign, double radius, double strength, double vel)
+{
+	double dist = fabs(bb - x);
+	dist = dist < 0.00001 ? 0.00001 : dist;
+	double rep = 1.0 - dist / radius;
+	rep = rep < 0 ? 0 : rep;
+	rep = rep * (rep * strength * sign);
+	return vel + rep * dist;
+}
+
+template <int DIMS>
+__device__ __forceinline__ void walls(const view& v, const rep_info& R, const double4& p, double radius,
+									  double strength, double4& vel)
+{
+	// update_membrane_velocities (reference: solver_helper.h:103-110,184-193,288-299);
+	// the 1-D version uses the y maximum for the upper wall, kept as in the reference
+	for (int d = 0; d < DIMS; d++)
+	{
+		double x = comp(p, d), u = comp(vel, d);
+		u = membrane(x, R.mins[d], 1.0, radius, strength, u);
+		u = membrane(x, DIMS == 1 ? R.maxs[1] : R.maxs[d], -1.0, radius, strength, u);
+		set_comp(vel, d, u);
+	}
+}
+
+// spring_contract_function for one agent (reference: position_solver.cpp:337-370)
+template <int DIMS>
+__device__ __forceinline__ void spring_contract(const view& v, int cur, int s, const double4& pi, int def_i,
+												double4& vel)
+{
+	const int n = v.scnt[s];
+	const double ec_i = v.ec[s];
+	const double* aff_i = v.aff + (int64_t)s * v.ndefs;
+	for (int k = 0; k < n; k++)
+	{
+		const int j = v.springs[(int64_t)s * v.scap + k];
+		const int def_j = v.def[j];
+		const double a = sqrt(ec_i * v.ec[j] * aff_i[def_j] * v.aff[(int64_t)j * v.ndefs + def_i]);
+		const double4 pj = v.pos[cur][j];
+		for (int d = 0; d < DIMS; d++)
+			set_comp(vel, d, comp(vel, d) + a * (comp(pj, d) - comp(pi, d)));
+	}
+}
+
+// Adams-Bashforth update (reference: position_solver.cpp:481-504)
+template <int DIMS>
+__device__ __forceinline__ void ab2(double dt, double4& p, const double4& vel, double4& vprev)
+{
+	const double factor = dt * 1.5;
+	const double previous_factor = dt * -0.5;
+	for (int d = 0; d < DIMS; d++)
+	{
+		set_comp(p, d, comp(p, d) + (comp(vel, d) * factor + comp(vprev, d) * previous_factor));
+		set_comp(vprev, d, comp(vel, d));
+	}
+}
+
+// removal test of remove_single (reference: containers_solver.cpp:85-98)
+template <int DIMS>
+__device__ __forceinline__ bool to_remove(const rep_info& R, const double4& p, uint8_t flag)
+{
+	bool out = false;
+	for (int d = 0; d < DIMS; d++)
+	{
+		double x = comp(p, d);
+		if (x < R.mins[d] || x > R.maxs[d])
+			out = true;
+	}
+	return out || flag == PPC_FLAG_TO_REMOVE;
+}
+
+__device__ __forceinline__ void append_bad(const view& v, int r, int local)
+{
+	int k = atomicAdd(&v.ctr[r].nbad, 1);
+	if (k < v.reps[r].cap)
+		v.bad[v.reps[r].base + k] = local;
+	else
+		atomicOr(v.err, ERR_LIST_CAPACITY);
+}
+
+// ---------------------------------------------------------------------------
+// fused step: neighbour search + forces + membrane + springs + AB2, one
+// thread per binned agent, reading positions from pos[cur] and writing the
+// new positions to pos[nxt] (the reference finishes all force passes before
+// the position update, so every read must see the old positions). Also marks
+// agents for the container update that follows.
+// ---------------------------------------------------------------------------
+template <int DIMS, bool WALLS, bool SPRINGS, bool VEL>
+__global__ void __launch_bounds__(kThreads) k_fused(view v, int cur)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= *v.cursor)
+		return;
+	const int nxt = cur ^ 1;
+	const int s = v.sorted[t];
+	const int r = rep_of(v, s);
+	const rep_info& R = v.reps[r];
+	const uint32_t ep = *v.epoch;
+	const double4 pi = v.spos4[t];
+
+	pair_fp64 acc;
+	acc.prm_i = v.prm[s];
+	acc.def_i = v.def[s];
+	acc.mov_i = v.movable[s] != 0;
+	acc.aff_i = v.aff + (int64_t)s * v.ndefs;
+	if (VEL && acc.mov_i)
+	{
+		const double4 v0 = v.vel[s];
+		acc.vx = v0.x;
+		acc.vy = v0.y;
+		acc.vz = v0.z;
+	}
+	for_each_neighbor<DIMS>(v, R, ep, s, pi,
+							[&](int j, double ddx, double ddy, double ddz, double dist, double ad) {
+								acc.add(v, j, ddx, ddy, ddz, dist, ad);
+							});
+	v.pressure[s] = acc.p;
+
+	double4 p = v.pos[cur][s];
+	if (acc.mov_i)
+	{
+		double4 vel = make_double4(acc.vx, acc.vy, acc.vz, 0.0);
+		if (WALLS)
+			walls<DIMS>(v, R, p, acc.prm_i.x, acc.prm_i.w, vel);
+		if (SPRINGS)
+			spring_contract<DIMS>(v, cur, s, p, acc.def_i, vel);
+		double4 vp = v.vprev[s];
+		ab2<DIMS>(v.dt, p, vel, vp);
+		v.vprev[s] = vp;
+		if (VEL)
+			v.vel[s] = make_double4(0, 0, 0, 0);
+	}
+	v.pos[nxt][s] = p;
+	if (!(p.x == p.x && p.y == p.y && p.z == p.z))
+		atomicOr(v.err, ERR_NONFINITE);
+	if (to_remove<DIMS>(R, p, v.flags[s]))
+		append_bad(v, r, s - R.base);
+}
+
+// ---------------------------------------------------------------------------
+// separate reference entry points
+// ---------------------------------------------------------------------------
+
+// position_solver::update_cell_neighbors (reference: position_solver.cpp:262-286)
+template <int DIMS>
+__global__ void __launch_bounds__(kThreads) k_neighbors(view v)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= *v.cursor)
+		return;
+	const int s = v.sorted[t];
+	if (v.movable[s] == 0)
+	{
+		v.ncnt[s] = 0;
+		return;
+	}
+	const rep_info& R = v.reps[rep_of(v, s)];
+	const uint32_t ep = *v.epoch;
+	int n = 0;
+	int32_t* out = v.nidx + (int64_t)s * v.ncap;
+	const int cap = v.ncap;
+	for_each_neighbor<DIMS>(v, R, ep, s, v.spos4[t], [&](int j, double, double, double, double, double) {
+		if (n < cap)
+			out[n] = j;
+		n++;
+	});
+	if (n > cap)
+		atomicOr(v.err, ERR_NEIGHBOR_CAPACITY);
+	v.ncnt[s] = n;
+}
+
+__global__ void k_clear_pressure(view v)
+{
+	int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= v.total_cap)
+		return;
+	int r, local;
+	if (live(v, s, r, local))
+		v.pressure[s] = 0;
+}
+
+// position_solver::update_cell_forces over the stored neighbour lists
+// (reference: position_solver.cpp:15-22,99-113,158-178,233-260). Pressure
+// of a movable agent is gathered from its own list (lists are symmetric
+// between movable agents); pressure of a non-movable agent is added
+// atomically by its movable neighbours.
+template <int DIMS>
+__global__ void __launch_bounds__(kThreads) k_forces(view v, int cur)
+{
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= v.total_cap)
+		return;
+	int r, local;
+	if (!live(v, s, r, local) || v.movable[s] == 0)
+		return;
+	pair_fp64 acc;
+	acc.prm_i = v.prm[s];
+	acc.def_i = v.def[s];
+	acc.mov_i = true;
+	acc.aff_i = v.aff + (int64_t)s * v.ndefs;
+	const double4 v0 = v.vel[s];
+	acc.vx = v0.x;
+	acc.vy = v0.y;
+	acc.vz = v0.z;
+	const double4 pi = v.pos[cur][s];
+	const double ar_i = v.rmad[s] * acc.prm_i.x;
+	const int n = min(v.ncnt[s], v.ncap);
+	for (int k = 0; k < n; k++)
+	{
+		const int j = v.nidx[(int64_t)s * v.ncap + k];
+		const double4 pj = v.pos[cur][j];
+		const double ddx = pi.x - pj.x;
+		const double ddy = DIMS >= 2 ? pi.y - pj.y : 0.0;
+		const double ddz = DIMS >= 3 ? pi.z - pj.z : 0.0;
+		double d2 = ddx * ddx;
+		if (DIMS >= 2)
+			d2 = d2 + ddy * ddy;
+		if (DIMS >= 3)
+			d2 = d2 + ddz * ddz;
+		const double dist = DIMS == 1 ? fabs(ddx) : sqrt(d2);
+		const double ad = ar_i + v.rmad[j] * v.prm[j].x;
+		acc.add(v, j, ddx, ddy, ddz, dist, ad);
+		if (v.movable[j] == 0)
+			atomicAdd(&v.pressure[j], acc.last_term);
+	}
+	v.pressure[s] = acc.p;
+	v.vel[s] = make_double4(acc.vx, acc.vy, acc.vz, 0.0);
+}
+
+template <int DIMS>
+__global__ void k_membrane(view v, int cur)
+{
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= v.total_cap)
+		return;
+	int r, local;
+	if (!live(v, s, r, local) || v.movable[s] == 0)
+		return;
+	double4 vel = v.vel[s];
+	const double4 prm = v.prm[s];
+	walls<DIMS>(v, v.reps[r], v.pos[cur][s], prm.x, prm.w, vel);
+	v.vel[s] = vel;
+}
+
+template <int DIMS>
+__global__ void k_springs(view v, int cur)
+{
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= v.total_cap)
+		return;
+	int r, local;
+	if (!live(v, s, r, local) || v.movable[s] == 0 || v.scnt[s] == 0)
+		return;
+	double4 vel = v.vel[s];
+	spring_contract<DIMS>(v, cur, s, v.pos[cur][s], v.def[s], vel);
+	v.vel[s] = vel;
+}
+
+template <int DIMS>
+__global__ void k_positions(view v, int cur)
+{
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= v.total_cap)
+		return;
+	int r, local;
+	if (!live(v, s, r, local) || v.movable[s] == 0)
+		return;
+	double4 p = v.pos[cur][s];
+	double4 vel = v.vel[s];
+	double4 vp = v.vprev[s];
+	ab2<DIMS>(v.dt, p, vel, vp);
+	v.pos[cur][s] = p;
+	v.vprev[s] = vp;
+	v.vel[s] = make_double4(0, 0, 0, 0);
+}
+
+// ---------------------------------------------------------------------------
+// container update: remove_single / update_cell_container_internal
+// (reference: containers_solver.cpp:58-147) and division
+// (containers_solver.cpp:149-188, src/cell.cpp:108-163)
+// ---------------------------------------------------------------------------
+
+template <int DIMS>
+__global__ void k_mark_remove(view v, int cur)
+{
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= v.total_cap)
+		return;
+	int r, local;
+	if (!live(v, s, r, local))
+		return;
+	if (to_remove<DIMS>(v.reps[r], v.pos[cur][s], v.flags[s]))
+		append_bad(v, r, local);
+}
+
+// ascending sort of a short list by one block (bitonic network in shared
+// memory); longer lists fall back to a single-thread heap sort
+__device__ void block_sort(int32_t* a, int n, int32_t* sh)
+{
+	if (n <= 1)
+		return;
+	if (n <= kSortCap)
+	{
+		int m = 1;
+		while (m < n)
+			m <<= 1;
+		for (int i = threadIdx.x; i < m; i += blockDim.x)
+			sh[i] = i < n ? a[i] : INT32_MAX;
+		__syncthreads();
+		for (int k = 2; k <= m; k <<= 1)
+		{
+			for (int j = k >> 1; j > 0; j >>= 1)
+			{
+				for (int i = threadIdx.x; i < m; i += blockDim.x)
+				{
+					int l = i ^ j;
+					if (l > i)
+					{
+						bool up = (i & k) == 0;
+						int x = sh[i], y = sh[l];
+						if ((x > y) == up)
+						{
+							sh[i] = y;
+							sh[l] = x;
+						}
+					}
+				}
+				__syncthreads();
+			}
+		}
+		for (int i = threadIdx.x; i < n; i += blockDim.x)
+			a[i] = sh[i];
+		__syncthreads();
+		return;
+	}
+	if (threadIdx.x == 0)
+	{
+		// heap sort
+		auto sift = [&](int start, int end) {
+			int root = start;
+			while (2 * root + 1 <= end)
+			{
+				int child = 2 * root + 1, sw = root;
+				if (a[sw] < a[child])
+					sw = child;
+				if (child + 1 <= end && a[sw] < a[child + 1])
+					sw = child + 1;
+				if (sw == root)
+					return;
+				int t = a[root];
+				a[root] = a[sw];
+				a[sw] = t;
+				root = sw;
+			}
+		};
+		for (int start = (n - 2) / 2; start >= 0; start--)
+			sift(start, n - 1);
+		for (int end = n - 1; end > 0; end--)
+		{
+			int t = a[end];
+			a[end] = a[0];
+			a[0] = t;
+			sift(0, end - 1);
+		}
+	}
+	__syncthreads();
+}
+
+// position of `x` in spring row of slot s, or -1
+__device__ __forceinline__ int find_in_row(const view& v, int s, int x)
+{
+	const int n = v.scnt[s];
+	const int32_t* row = v.springs + (int64_t)s * v.scap;
+	for (int k = 0; k < n; k++)
+		if (row[k] == x)
+			return k;
+	return -1;
+}
+
+// remove_attached (reference: containers_solver.cpp:58-68): every partner of
+// `a` drops `a` by moving its last entry into the hole
+__device__ void springs_remove_attached(const view& v, int a)
+{
+	const int n = v.scnt[a];
+	for (int k = 0; k < n; k++)
+	{
+		const int s = v.springs[(int64_t)a * v.scap + k];
+		const int at = find_in_row(v, s, a);
+		if (at < 0)
+		{
+			atomicOr(v.err, ERR_SPRING_CAPACITY);
+			continue;
+		}
+		int32_t* row = v.springs + (int64_t)s * v.scap;
+		row[at] = row[v.scnt[s] - 1];
+		v.scnt[s]--;
+	}
+}
+
+// rename_attached (reference: containers_solver.cpp:70-79)
+__device__ void springs_rename_attached(const view& v, int old_slot, int new_slot)
+{
+	const int n = v.scnt[old_slot];
+	for (int k = 0; k < n; k++)
+	{
+		const int s = v.springs[(int64_t)old_slot * v.scap + k];
+		const int at = find_in_row(v, s, old_slot);
+		if (at >= 0)
+			v.springs[(int64_t)s * v.scap + at] = new_slot;
+	}
+}
+
+// Plans the removals of one replicate (one block per replicate): the serial
+// loop of update_cell_container_internal over slots 0..nvisit-1, where each
+// removal moves the current last agent into the hole and re-tests the hole.
+// Produces (hole, source) moves for the agents that end up in holes, the new
+// count and the death count; with springs it also replays every removal on
+// the spring rows in the reference's order.
+__global__ void k_compact_plan(view v, int phenotype_pass, int springs)
+{
+	__shared__ int32_t sh[kSortCap];
+	const int r = blockIdx.x;
+	rep_counters& C = v.ctr[r];
+	const int nb = min(C.nbad, v.reps[r].cap);
+	if (nb == 0)
+	{
+		if (threadIdx.x == 0)
+			v.nmoves[r] = 0;
+		return;
+	}
+	const int base = v.reps[r].base;
+	int32_t* B = v.bad + base;
+	block_sort(B, nb, sh);
+	if (threadIdx.x != 0)
+		return;
+
+	const int nvisit = phenotype_pass ? C.nvisit : C.count;
+	int cnt = C.count;
+	int ti = nb - 1, nm = 0;
+	int64_t deaths = 0;
+	int32_t* moves = v.moves + 2 * (int64_t)base;
+	for (int bi = 0; bi < nb; bi++)
+	{
+		const int h = B[bi];
+		if (h >= nvisit || h >= cnt)
+			break;
+		int occ = h; // original index of the agent now in slot h
+		while (true)
+		{
+			deaths += v.flags[base + occ] == PPC_FLAG_TO_REMOVE;
+			const int last = cnt - 1;
+			if (springs)
+			{
+				springs_remove_attached(v, base + h);
+				if (last != h)
+				{
+					springs_rename_attached(v, base + last, base + h);
+					const int n = v.scnt[base + last];
+					for (int k = 0; k < n; k++)
+						v.springs[(int64_t)(base + h) * v.scap + k] = v.springs[(int64_t)(base + last) * v.scap + k];
+					v.scnt[base + h] = n;
+					v.scnt[base + last] = 0;
+				}
+			}
+			cnt--;
+			if (h == cnt)
+			{
+				occ = -1;
+				break;
+			}
+			occ = last;
+			while (ti >= 0 && B[ti] > last)
+				ti--;
+			if (!(ti >= 0 && B[ti] == last))
+				break;
+		}
+		if (occ >= 0)
+		{
+			moves[2 * nm] = h;
+			moves[2 * nm + 1] = occ;
+			nm++;
+		}
+	}
+	C.count = cnt;
+	C.deaths += deaths;
+	C.nbad = 0;
+	v.nmoves[r] = nm;
+}
+
+// copies every per-agent field of the planned moves (cell_data::remove,
+// reference: src/cell_data.cpp:285-313); spring rows were moved by the plan
+template <int DIMS>
+__global__ void k_compact_apply(view v, int cur)
+{
+	const int r = blockIdx.y;
+	const int nm = v.nmoves[r];
+	const int base = v.reps[r].base;
+	const int32_t* moves = v.moves + 2 * (int64_t)base;
+	for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nm; k += gridDim.x * blockDim.x)
+	{
+		const int d = base + moves[2 * k], s = base + moves[2 * k + 1];
+		v.pos[cur][d] = v.pos[cur][s];
+		v.vel[d] = v.vel[s];
+		v.vprev[d] = v.vprev[s];
+		v.prm[d] = v.prm[s];
+		v.rmad[d] = v.rmad[s];
+		v.ec[d] = v.ec[s];
+		v.arate[d] = v.arate[s];
+		v.drate[d] = v.drate[s];
+		v.pressure[d] = v.pressure[s];
+		v.vol[d] = v.vol[s];
+		v.nvol[d] = v.nvol[s];
+		v.nrad[d] = v.nrad[s];
+		v.sarea[d] = v.sarea[s];
+		v.polarity[d] = v.polarity[s];
+		v.orient[d] = v.orient[s];
+		for (int q = 0; q < v.ndefs; q++)
+			v.aff[(int64_t)d * v.ndefs + q] = v.aff[(int64_t)s * v.ndefs + q];
+		v.def[d] = v.def[s];
+		v.maxatt[d] = v.maxatt[s];
+		v.movable[d] = v.movable[s];
+		v.flags[d] = v.flags[s];
+		v.ids[d] = v.ids[s];
+		const int nn = min(v.ncnt[s], v.ncap);
+		for (int q = 0; q < nn; q++)
+			v.nidx[(int64_t)d * v.ncap + q] = v.nidx[(int64_t)s * v.ncap + q];
+		v.ncnt[d] = v.ncnt[s];
+	}
+}
+
+// stand-in for the phenotype models: death with p_death, else division with
+// p_divide, from the counter-based draws of (seed, epoch, replicate, index)
+__global__ void k_flag_by_draws(view v, double p_divide, double p_death)
+{
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= v.total_cap)
+		return;
+	int r, local;
+	if (!live(v, s, r, local))
+		return;
+	const uint64_t ep = v.draw_epoch[r];
+	if (ppc_uniform(v.seed, ep, (uint64_t)r, (uint64_t)local, PPC_DRAW_DEATH) < p_death)
+		v.flags[s] = PPC_FLAG_TO_REMOVE;
+	else if (ppc_uniform(v.seed, ep, (uint64_t)r, (uint64_t)local, PPC_DRAW_DIVIDE) < p_divide)
+		v.flags[s] = PPC_FLAG_TO_DIVIDE;
+}
+
+__global__ void k_bump_draw_epoch(view v)
+{
+	const int r = blockIdx.x * blockDim.x + threadIdx.x;
+	if (r < v.nreps)
+		v.draw_epoch[r]++;
+}
+
+__global__ void k_mark_divide(view v)
+{
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= v.total_cap)
+		return;
+	int r, local;
+	if (!live(v, s, r, local))
+		return;
+	if (v.flags[s] == PPC_FLAG_TO_DIVIDE)
+	{
+		int k = atomicAdd(&v.ctr[r].ndiv, 1);
+		if (k < v.reps[r].cap)
+			v.divl[v.reps[r].base + k] = local;
+		else
+			atomicOr(v.err, ERR_LIST_CAPACITY);
+	}
+}
+
+// Orders the dividing agents (one block per replicate); daughters are
+// appended in ascending parent order like the serial reference loop. With
+// springs, thread 0 removes each parent from its partners' rows in that order
+// (cell::divide, reference: src/cell.cpp:110-114).
+__global__ void k_divide_plan(view v, int springs)
+{
+	__shared__ int32_t sh[kSortCap];
+	const int r = blockIdx.x;
+	rep_counters& C = v.ctr[r];
+	const int nd = min(C.ndiv, v.reps[r].cap);
+	const int base = v.reps[r].base;
+	if (threadIdx.x == 0)
+		C.nvisit = C.count;
+	if (nd == 0)
+		return;
+	block_sort(v.divl + base, nd, sh);
+	if (threadIdx.x != 0)
+		return;
+	if (C.count + nd > v.reps[r].cap)
+	{
+		atomicOr(v.err, ERR_AGENT_CAPACITY);
+		C.ndiv = 0;
+		return;
+	}
+	if (springs)
+		for (int k = 0; k < nd; k++)
+		{
+			const int p = base + v.divl[base + k];
+			springs_remove_attached(v, p);
+			v.scnt[p] = 0;
+		}
+}
+
+template <int DIMS>
+__global__ void k_divide_apply(view v, int cur)
+{
+	const int r = blockIdx.y;
+	rep_counters& C = v.ctr[r];
+	const int nd = C.ndiv;
+	const int base = v.reps[r].base;
+	const int n_pre = C.nvisit;
+	const uint64_t ep = v.draw_epoch[r];
+	for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nd; k += gridDim.x * blockDim.x)
+	{
+		const int lp = v.divl[base + k];
+		const int p = base + lp;
+		const int c = base + n_pre + k;
+		v.flags[p] = PPC_FLAG_NONE;
+
+		// random direction, projected against the orientation by polarity and
+		// scaled by the parent's radius (reference: src/cell.cpp:129-150)
+		double w[3] = { 0, 0, 0 };
+		ppc_unit_vector(DIMS, v.seed, ep, (uint64_t)r, (uint64_t)lp, PPC_DRAW_WALK, w);
+		double4 prm = v.prm[p];
+		const double4 o = v.orient[p];
+		const double pol = v.polarity[p];
+		double tmp = 0;
+		for (int d = 0; d < DIMS; d++)
+			tmp = tmp + w[d] * comp(o, d);
+		for (int d = 0; d < DIMS; d++)
+			w[d] = (w[d] - tmp * comp(o, d) * pol) * prm.x;
+
+		// volume.divide() and geometry.update() (reference:
+		// data_storage_phenotype.cpp:530-550, interactions_solver.cpp:89-96)
+		const double vol = v.vol[p] * 0.5;
+		const double nvol = v.nvol[p] * 0.5;
+		const double four_thirds_pi = 3.141592653589793 * 4.0 / 3.0;
+		prm.x = ppc_cbrt(vol / four_thirds_pi);
+		const double nrad = ppc_cbrt(nvol / four_thirds_pi);
+		const double sarea = 4.0 * 3.141592653589793 * prm.x * prm.x;
+		v.vol[p] = vol;
+		v.nvol[p] = nvol;
+		v.prm[p] = prm;
+		v.nrad[p] = nrad;
+		v.sarea[p] = sarea;
+
+		// new cell: defaults of a created cell, then copy_from(parent)
+		v.prm[c] = prm;
+		v.rmad[c] = v.rmad[p];
+		v.ec[c] = v.ec[p];
+		v.arate[c] = v.arate[p];
+		v.drate[c] = v.drate[p];
+		v.vol[c] = vol;
+		v.nvol[c] = nvol;
+		v.nrad[c] = nrad;
+		v.sarea[c] = sarea;
+		v.polarity[c] = pol;
+		for (int q = 0; q < v.ndefs; q++)
+			v.aff[(int64_t)c * v.ndefs + q] = v.aff[(int64_t)p * v.ndefs + q];
+		v.def[c] = v.def[p];
+		v.maxatt[c] = v.maxatt[p];
+		v.movable[c] = 1;
+		v.flags[c] = PPC_FLAG_NONE;
+		v.ids[c] = C.next_id + k;
+		v.vel[c] = make_double4(0, 0, 0, 0);
+		v.vprev[c] = make_double4(0, 0, 0, 0);
+		v.pressure[c] = 0;
+		v.scnt[c] = 0;
+		v.ncnt[c] = 0;
+		double ow[3] = { 0, 0, 0 };
+		ppc_unit_vector(DIMS, v.seed, ep, (uint64_t)r, (uint64_t)lp, PPC_DRAW_ORIENTATION, ow);
+		v.orient[c] = make_double4(ow[0], ow[1], ow[2], 0.0);
+
+		double4 pp = v.pos[cur][p];
+		double4 pc = pp;
+		for (int d = 0; d < DIMS; d++)
+		{
+			set_comp(pc, d, comp(pp, d) + w[d]);
+			set_comp(pp, d, comp(pp, d) - w[d] * 0.5);
+		}
+		v.pos[cur][p] = pp;
+		v.pos[cur][c] = pc;
+	}
+}
+
+__global__ void k_divide_finish(view v)
+{
+	const int r = blockIdx.x * blockDim.x + threadIdx.x;
+	if (r >= v.nreps)
+		return;
+	rep_counters& C = v.ctr[r];
+	C.count += C.ndiv;
+	C.divisions += C.ndiv;
+	C.next_id += C.ndiv;
+	C.ndiv = 0;
+	v.draw_epoch[r]++;
+}
+
+// ---------------------------------------------------------------------------
+// host layout <-> device layout
+// ---------------------------------------------------------------------------
+
+__global__ void k_unpack_vec(view v, double4* dst, const double* src, int base, int n)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	double4 x = make_double4(0, 0, 0, 0);
+	for (int d = 0; d < v.dims; d++)
+		set_comp(x, d, src[(int64_t)i * v.dims + d]);
+	dst[base + i] = x;
+}
+
+__global__ void k_pack_vec(view v, double* dst, const double4* src, int base, int n)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	const double4 x = src[base + i];
+	for (int d = 0; d < v.dims; d++)
+		dst[(int64_t)i * v.dims + d] = comp(x, d);
+}
+
+__global__ void k_unpack_prm(view v, int field, const double* src, int base, int n)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	double* p = reinterpret_cast<double*>(v.prm + base + i);
+	p[field] = src[i];
+}
+
+__global__ void k_pack_prm(view v, int field, double* dst, int base, int n)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	dst[i] = reinterpret_cast<const double*>(v.prm + base + i)[field];
+}
+
+__global__ void k_neighbors_local(view v, int base, int n, int32_t* counts, int32_t* lists, int cap)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	const int s = base + i;
+	const int c = v.ncnt[s];
+	counts[i] = c;
+	const int m = min(min(c, v.ncap), cap);
+	for (int k = 0; k < m; k++)
+		lists[(int64_t)i * cap + k] = v.nidx[(int64_t)s * v.ncap + k] - base;
+}
+
+// rows: [n * cap] local indices in host layout; to_device converts to slots
+__global__ void k_springs_local(view v, int base, int n, int32_t* rows, int cap, int to_device)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	const int s = base + i;
+	if (to_device)
+	{
+		const int c = v.scnt[s];
+		for (int k = 0; k < c; k++)
+			v.springs[(int64_t)s * v.scap + k] = rows[(int64_t)i * cap + k] + base;
+	}
+	else
+	{
+		const int c = min(v.scnt[s], cap);
+		for (int k = 0; k < c; k++)
+			rows[(int64_t)i * cap + k] = v.springs[(int64_t)s * v.scap + k] - base;
+	}
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+
+#define PPC_CHECK_LAUNCH()                                                                                             \
+	do                                                                                                                 \
+	{                                                                                                                  \
+		cudaError_t e_ = cudaGetLastError();                                                                           \
+		if (e_ != cudaSuccess)                                                                                         \
+			return cuda_fail(e_, __func__);                                                                            \
+	} while (0)
+
+int launch_bin(ppc_state* s)
+{
+	const int b = blocks_for(s->total_cap, kThreads);
+	k_bin_count<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	k_bin_alloc<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+	k_bin_scatter<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+	k_bin_fixup<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+int launch_neighbors(ppc_state* s)
+{
+	const int b = blocks_for(s->total_cap, kThreads);
+	if (s->dims == 1)
+		k_neighbors<1><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+	else if (s->dims == 2)
+		k_neighbors<2><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+	else
+		k_neighbors<3><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+int launch_forces(ppc_state* s)
+{
+	const int b = blocks_for(s->total_cap, kThreads);
+	k_clear_pressure<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+	if (s->dims == 1)
+		k_forces<1><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	else if (s->dims == 2)
+		k_forces<2><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	else
+		k_forces<3><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+int launch_membrane(ppc_state* s)
+{
+	const int b = blocks_for(s->total_cap, kThreads);
+	if (s->dims == 1)
+		k_membrane<1><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	else if (s->dims == 2)
+		k_membrane<2><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	else
+		k_membrane<3><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+int launch_springs(ppc_state* s)
+{
+	const int b = blocks_for(s->total_cap, kThreads);
+	if (s->dims == 1)
+		k_springs<1><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	else if (s->dims == 2)
+		k_springs<2><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	else
+		k_springs<3><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+int launch_positions(ppc_state* s)
+{
+	const int b = blocks_for(s->total_cap, kThreads);
+	if (s->dims == 1)
+		k_positions<1><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	else if (s->dims == 2)
+		k_positions<2><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	else
+		k_positions<3><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+template <int DIMS>
+static void fused_dispatch(ppc_state* s, int b)
+{
+	const bool walls = s->params.virtual_wall_at_domain_edges != 0;
+	const bool springs = s->has_springs && s->params.automated_spring_adhesion != 0;
+	const bool vel = s->vel_dirty;
+	cudaStream_t st = PPC_LAUNCH(s);
+#define PPC_FUSED(W, S, V)                                                                                             \
+	if (walls == W && springs == S && vel == V)                                                                        \
+		k_fused<DIMS, W, S, V><<<b, kThreads, 0, st>>>(s->v, s->cur);
+	PPC_FUSED(false, false, false)
+	PPC_FUSED(false, false, true)
+	PPC_FUSED(false, true, false)
+	PPC_FUSED(false, true, true)
+	PPC_FUSED(true, false, false)
+	PPC_FUSED(true, false, true)
+	PPC_FUSED(true, true, false)
+	PPC_FUSED(true, true, true)
+#undef PPC_FUSED
+}
+
+int launch_fused(ppc_state* s)
+{
+	const int b = blocks_for(s->total_cap, kThreads);
+	cudaEvent_t ev_end = nullptr;
+	if (s->profiling)
+	{
+		if (s->prof_used + 2 > s->prof_events.size())
+		{
+			for (int k = 0; k < 256; k++)
+			{
+				cudaEvent_t e;
+				PPC_CUDA(cudaEventCreate(&e));
+				s->prof_events.push_back(e);
+			}
+		}
+		PPC_CUDA(cudaEventRecord(s->prof_events[s->prof_used], s->stream));
+		ev_end = s->prof_events[s->prof_used + 1];
+		s->prof_used += 2;
+	}
+	if (s->dims == 1)
+		fused_dispatch<1>(s, b);
+	else if (s->dims == 2)
+		fused_dispatch<2>(s, b);
+	else
+		fused_dispatch<3>(s, b);
+	PPC_CHECK_LAUNCH();
+	if (ev_end)
+		PPC_CUDA(cudaEventRecord(ev_end, s->stream));
+	s->cur ^= 1;
+	s->vel_dirty = false;
+	return PPC_OK;
+}
+
+int launch_compact(ppc_state* s, bool phenotype_pass)
+{
+	const int springs = s->has_springs ? 1 : 0;
+	k_compact_plan<<<s->nreps, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, phenotype_pass ? 1 : 0, springs);
+	dim3 g(std::max(1, std::min(64, blocks_for(s->total_cap / std::max(1, s->nreps), kThreads))), s->nreps);
+	if (s->dims == 1)
+		k_compact_apply<1><<<g, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	else if (s->dims == 2)
+		k_compact_apply<2><<<g, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	else
+		k_compact_apply<3><<<g, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+int launch_mark_remove(ppc_state* s)
+{
+	const int b = blocks_for(s->total_cap, kThreads);
+	if (s->dims == 1)
+		k_mark_remove<1><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	else if (s->dims == 2)
+		k_mark_remove<2><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	else
+		k_mark_remove<3><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+int launch_divide(ppc_state* s)
+{
+	const int b = blocks_for(s->total_cap, kThreads);
+	const int springs = s->has_springs ? 1 : 0;
+	k_mark_divide<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+	k_divide_plan<<<s->nreps, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, springs);
+	dim3 g(std::max(1, std::min(64, blocks_for(s->total_cap / std::max(1, s->nreps), kThreads))), s->nreps);
+	if (s->dims == 1)
+		k_divide_apply<1><<<g, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	else if (s->dims == 2)
+		k_divide_apply<2><<<g, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	else
+		k_divide_apply<3><<<g, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	k_divide_finish<<<blocks_for(s->nreps, kThreads), kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+int launch_flag_by_draws(ppc_state* s, double p_divide, double p_death)
+{
+	const int b = blocks_for(s->total_cap, kThreads);
+	k_flag_by_draws<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, p_divide, p_death);
+	k_bump_draw_epoch<<<blocks_for(s->nreps, kThreads), kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+int launch_unpack_vec(ppc_state* s, double4* dst, const double* src, int32_t r, int32_t n)
+{
+	if (n == 0)
+		return PPC_OK;
+	k_unpack_vec<<<blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s)>>>(s->v, dst, src, s->reps[r].base, n);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+int launch_pack_vec(ppc_state* s, double* dst, const double4* src, int32_t r, int32_t n)
+{
+	if (n == 0)
+		return PPC_OK;
+	k_pack_vec<<<blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s)>>>(s->v, dst, src, s->reps[r].base, n);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+int launch_unpack_prm(ppc_state* s, int field, const double* src, int32_t r, int32_t n)
+{
+	if (n == 0)
+		return PPC_OK;
+	k_unpack_prm<<<blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s)>>>(s->v, field, src, s->reps[r].base, n);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+int launch_pack_prm(ppc_state* s, int field, double* dst, int32_t r, int32_t n)
+{
+	if (n == 0)
+		return PPC_OK;
+	k_pack_prm<<<blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s)>>>(s->v, field, dst, s->reps[r].base, n);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+int launch_neighbors_local(ppc_state* s, int32_t r, int32_t n, int32_t* counts, int32_t* lists, int32_t cap)
+{
+	if (n == 0)
+		return PPC_OK;
+	k_neighbors_local<<<blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->reps[r].base, n, counts,
+																			 lists, cap);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+int launch_springs_local(ppc_state* s, int32_t r, int32_t n, int32_t* rows, int32_t cap, int to_device)
+{
+	if (n == 0)
+		return PPC_OK;
+	k_springs_local<<<blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->reps[r].base, n, rows, cap,
+																		   to_device);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+} // namespace ppc

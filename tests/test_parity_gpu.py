@@ -1,0 +1,285 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle and with
+the reference's known answers. Needs a CUDA device."""
+import itertools
+
+import numpy as np
+import pytest
+
+from paraphysicell_b200 import workloads as wl
+from paraphysicell_b200.abi import FLAG_TO_REMOVE
+from tests import gpu_util as gu
+from tests import scenarios as sc
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("dims", [1, 2, 3])
+def test_velocity_simple_known_answer(dims):
+    """host_velocity_solver.simple on the device: bit-exact known answers
+    (reference: test/test.cpp:141-191)."""
+    mesh, params, a = sc.velocity_simple(dims)
+    o, d = gu.make_pair(mesh, params, a)
+    d.update_mechanics_mesh()
+    d.update_cell_neighbors()
+    d.update_cell_forces()
+    got = gu.fetch(d, a)
+    expected = float(sc.known_answers()["host_velocity_solver_simple"]["expected_velocity_cell1"][str(dims)])
+    v = got["velocities"]
+    for k in range(dims):
+        assert v[0, k] == expected
+        assert v[1, k] == -expected
+        assert v[2, k] == 0.0
+
+
+@pytest.mark.parametrize("dims", [1, 2, 3])
+def test_velocity_complex_matches_oracle(dims):
+    """host_velocity_solver.complex: neighbour counts {1,2,1}, velocities
+    bit-exact with the oracle (reference: test/test.cpp:265-320)."""
+    mesh, params, a = sc.velocity_complex(dims)
+    o, d = gu.make_pair(mesh, params, a)
+    for x in (o, d):
+        x.update_mechanics_mesh()
+        x.update_cell_neighbors()
+        x.update_cell_forces()
+    assert [len(n) for n in d.neighbors()] == [1, 2, 1]
+    gu.assert_same_neighbors(d, o)
+    gu.assert_same_state(gu.fetch(d, a), gu.fetch(o, a))
+
+
+GRID = sc.known_answers()["host_neighbors_solver_grid"]
+
+
+@pytest.mark.parametrize("dims,cells,adhesion",
+                         list(itertools.product(GRID["dims"], GRID["cells_in_one_voxel"], GRID["adhesion"])))
+def test_neighbors_grid(dims, cells, adhesion):
+    """host_neighbors_solver.grid: occupancy, neighbour counts and the exact
+    neighbour lists (reference: test/test.cpp:333-400)."""
+    mesh, params, a = sc.neighbors_grid(dims, cells, adhesion)
+    cap = 27 * cells + 1
+    o, d = gu.make_pair(mesh, params, a, neighbor_capacity=cap)
+    for x in (o, d):
+        x.update_mechanics_mesh()
+        x.update_cell_neighbors()
+    counts, _ = d.mesh_bins()
+    assert (counts == cells).all()
+    gu.assert_same_bins(d, o)
+    gu.assert_same_neighbors(d, o, capacity=cap)
+    nb = d.neighbors(capacity=cap)
+    pos = a["positions"]
+    for i in range(a.count):
+        c = [int(pos[i, k] // 30) if k < dims else 0 for k in range(3)]
+        assert len(nb[i]) == sc.grid_expected_neighbors(mesh, cells, adhesion, c)
+
+
+def test_container_swap_with_last_removal():
+    """cell_container.add_and_remove on the device (reference:
+    test/test.cpp:52-115)."""
+    ka = sc.known_answers()["cell_container_add_and_remove"]["after_removals"]
+    mesh, params, a = sc.container_four()
+    o, d = gu.make_pair(mesh, params, a)
+    for step, victim in zip(ka, (2, 0)):
+        cur = gu.fetch(d, a)
+        cur.arrays["flags"][: cur.count] = 0
+        cur.arrays["flags"][victim] = FLAG_TO_REMOVE
+        d.upload(cur)
+        d.update_cell_container_for_mechanics()
+        got = gu.fetch(d, a)
+        assert list(got["total_volume"]) == step["volumes"]
+        assert list(got["velocities"][:, 0]) == step["velocities"]
+
+
+def _cases():
+    return {
+        "config1_2d": lambda: wl.config1(seed=11, n=900),
+        "config2_3d_walls": lambda: wl.scaled(wl.config2, 3000, seed=12),
+        "config3_springs": lambda: wl.scaled(wl.config3, 4000, seed=13),
+        "config5_dense": lambda: wl.scaled(wl.config5, 5000, seed=14),
+    }
+
+
+@pytest.mark.parametrize("case", list(_cases()))
+def test_fused_steps_match_oracle(case):
+    """Several fused steps (forces, membrane, springs, AB2, compaction,
+    mesh) against the serial oracle: positions, velocities and previous
+    velocities bit-exact, bins and neighbour lists identical, pressure
+    within 1e-12 relative (its summation order is not the reference's)."""
+    mesh, params, a = _cases()[case]()
+    o, d = gu.make_pair(mesh, params, a)
+    o.update_mechanics_mesh()
+    o.update_cell_neighbors()
+    d.update_mechanics_mesh()
+    for _ in range(3):
+        o.step(4, 0, 0.0, 0.0)
+        d.step(4)
+        gu.assert_same_state(gu.fetch(d, a), gu.fetch(o, a))
+        gu.assert_same_bins(d, o)
+    gu.assert_same_neighbors(d, o)
+
+
+def test_graph_replay_matches_oracle():
+    """A block of steps long enough to be captured and replayed as a CUDA
+    graph gives the same state as the oracle."""
+    mesh, params, a = wl.scaled(wl.config2, 2000, seed=21)
+    o, d = gu.make_pair(mesh, params, a)
+    o.update_mechanics_mesh()
+    o.update_cell_neighbors()
+    d.update_mechanics_mesh()
+    o.step(25, 0, 0.0, 0.0)
+    d.step(25)
+    gu.assert_same_state(gu.fetch(d, a), gu.fetch(o, a))
+    o.step(20, 0, 0.0, 0.0)
+    d.step(20)
+    gu.assert_same_state(gu.fetch(d, a), gu.fetch(o, a))
+
+
+def test_unfused_entry_points_match_fused():
+    """The reference's separate entry points, called in simulator order,
+    give bit-identical results to the fused step."""
+    mesh, params, a = wl.scaled(wl.config3, 3000, seed=31)
+    params.virtual_wall_at_domain_edges = 1
+    _, d1 = gu.make_pair(mesh, params, a)
+    _, d2 = gu.make_pair(mesh, params, a)
+    d1.update_mechanics_mesh()
+    d1.update_cell_neighbors()
+    d2.update_mechanics_mesh()
+    for _ in range(3):
+        d1.update_cell_forces()
+        d1.update_motility()
+        d1.update_basement_membrane_interactions()
+        d1.update_spring_attachments()
+        d1.update_positions()
+        d1.update_cell_container_for_mechanics()
+        d1.update_mechanics_mesh()
+        d1.update_cell_neighbors()
+        d2.step(1)
+    g1, g2 = gu.fetch(d1, a), gu.fetch(d2, a)
+    gu.assert_same_state(g1, g2)
+    gu.assert_same_neighbors(d1, d2)
+
+
+def test_division_and_death_match_oracle():
+    """Phenotype container update with counter-based draws: divisions append
+    daughters in parent order, deaths swap-with-last; ids, positions and
+    radii bit-exact with the oracle."""
+    mesh, params, a = wl.scaled(wl.config5, 4000, seed=41, capacity=8000)
+    o, d = gu.make_pair(mesh, params, a, seed=7)
+    o.update_mechanics_mesh()
+    o.update_cell_neighbors()
+    d.update_mechanics_mesh()
+    for _ in range(4):
+        o.step(3, 1, 2e-3, 1e-3)
+        d.step_with_phenotype(3, 2e-3, 1e-3)
+        gu.assert_same_state(gu.fetch(d, a), gu.fetch(o, a),
+                             fields=gu.VEC[:3] + ("radius", "total_volume", "nuclear_volume", "nuclear_radius",
+                                                  "surface_area", "orientation", "flags", "is_movable"))
+        assert d.event_counts() == o.event_counts()
+    assert d.event_counts()[0] > 0 and d.event_counts()[1] > 0
+
+
+def test_springs_survive_removals_like_oracle():
+    """Removals of agents that carry springs rewrite the partners' spring
+    rows in the reference's serial order (remove_attached/rename_attached)."""
+    mesh, params, a = wl.scaled(wl.config3, 2000, seed=51)
+    rng = np.random.default_rng(5)
+    flags = a.arrays["flags"]
+    with_springs = np.nonzero(a.arrays["spring_counts"][: a.count] > 0)[0]
+    flags[rng.choice(with_springs, size=min(40, len(with_springs)), replace=False)] = FLAG_TO_REMOVE
+    o, d = gu.make_pair(mesh, params, a)
+    o.update_cell_container_for_mechanics()
+    d.update_cell_container_for_mechanics()
+    go, gd = gu.fetch(o, a), gu.fetch(d, a)
+    assert gd.count == go.count < a.count
+    assert gd.spring_lists() == go.spring_lists()
+    gu.assert_same_state(gd, go)
+
+
+def test_batch_replicates_match_independent_oracles():
+    """Ensemble form: each replicate of one batched state evolves exactly
+    like its own single simulation in the oracle."""
+    meshes, params, sets = wl.config4(seed=61, replicates=6, n_min=200, n_max=3000)
+    from oracle.oracle import Oracle
+    from paraphysicell_b200.device import Simulation
+    gu.build.ensure_built()
+    d = Simulation(meshes, params, [s.capacity for s in sets])
+    oracles = []
+    for r, (m, s) in enumerate(zip(meshes, sets)):
+        d.upload(s, replicate=r)
+        o = Oracle(m, params)
+        o.upload(s)
+        o.update_mechanics_mesh()
+        o.update_cell_neighbors()
+        oracles.append(o)
+    d.update_mechanics_mesh()
+    d.step(12)
+    for r, (o, s) in enumerate(zip(oracles, sets)):
+        o.step(12, 0, 0.0, 0.0)
+        out = gu.AgentArrays(0, s.dims, s.ndefs, s.capacity)
+        out.count = out.capacity
+        d.download(out, replicate=r)
+        gu.assert_same_state(out, gu.fetch(o, s))
+
+
+def test_errors_are_reported():
+    """Device-detected failures come back as status codes, not faults."""
+    from paraphysicell_b200.abi import PPCError, PPC_ERR_CAPACITY, PPC_ERR_NONFINITE, PPC_ERR_UNSUPPORTED
+    mesh, params, a = wl.scaled(wl.config2, 500, seed=71)
+    bad = a.copy()
+    bad.arrays["positions"][3] = np.nan
+    _, d = gu.make_pair(mesh, params, bad)
+    with pytest.raises(PPCError) as e:
+        d.update_mechanics_mesh()
+    assert e.value.rc == PPC_ERR_NONFINITE
+
+    mesh, params, g = sc.neighbors_grid(3, 5, 3)
+    _, d = gu.make_pair(mesh, params, g, neighbor_capacity=8)
+    d.update_mechanics_mesh()
+    with pytest.raises(PPCError) as e:
+        d.update_cell_neighbors()
+    assert e.value.rc == PPC_ERR_CAPACITY
+
+    mesh, params, a = wl.scaled(wl.config5, 500, seed=72, capacity=500)
+    _, d = gu.make_pair(mesh, params, a)
+    d.update_mechanics_mesh()
+    d.flag_by_draws(0.5, 0.0)
+    with pytest.raises(PPCError) as e:
+        d.update_cell_container_for_phenotype()
+    assert e.value.rc == PPC_ERR_CAPACITY
+
+    mesh, params, a = wl.scaled(wl.config2, 300, seed=73)
+    a.arrays["attachment_rate"][:] = 0.1
+    _, d = gu.make_pair(mesh, params, a)
+    with pytest.raises(PPCError) as e:
+        d.step(1)
+    assert e.value.rc == PPC_ERR_UNSUPPORTED
+
+
+def test_full_size_config3_properties_and_oracle():
+    """At the full 88,700-agent size: one step bit-exact with the oracle, and
+    size-independent properties of the bins (each agent binned once, in the
+    voxel of its position, descending inside a voxel) and the neighbour
+    lists (symmetric between movable agents)."""
+    mesh, params, a = wl.config3(seed=3)
+    o, d = gu.make_pair(mesh, params, a)
+    o.update_mechanics_mesh()
+    o.update_cell_neighbors()
+    d.update_mechanics_mesh()
+    o.step(2, 0, 0.0, 0.0)
+    d.step(2)
+    got = gu.fetch(d, a)
+    gu.assert_same_state(got, gu.fetch(o, a))
+    counts, agents = d.mesh_bins()
+    assert counts.sum() == got.count
+    assert np.array_equal(np.sort(agents), np.arange(got.count))
+    g = mesh.grid_shape()
+    pos = got["positions"]
+    c = np.floor((pos - np.array(mesh.bounding_box_mins)) / 30.0).astype(int)
+    key = c[:, 0] + g[0] * (c[:, 1] + g[1] * c[:, 2])
+    owner = np.repeat(np.arange(len(counts)), counts)
+    assert np.array_equal(key[agents], owner)
+    starts = np.concatenate([[0], np.cumsum(counts)[:-1]])
+    for s, cnt in zip(starts[counts > 1], counts[counts > 1]):
+        seg = agents[s: s + cnt]
+        assert np.all(np.diff(seg) < 0)
+    nb = d.neighbors()
+    pairs = {(i, j) for i, lst in enumerate(nb) for j in lst}
+    assert all((j, i) in pairs for (i, j) in pairs)
