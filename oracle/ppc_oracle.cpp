@@ -65,7 +65,9 @@ struct world
 	std::unique_ptr<std::atomic<index_t>[]> bin_sizes;
 
 	int64_t divisions = 0, deaths = 0, next_id = 0;
-	uint64_t seed = 0, epoch = 0;
+	// draw epochs: `epoch` for phenotype draws (flags, division), advanced
+	// once per draw-consuming call; `spring_epoch` for the attachment loop
+	uint64_t seed = 0, epoch = 0, spring_epoch = 0;
 	bool timed = false; // timed mode draws from thread_local mt19937
 
 	std::mutex removal_mtx;
@@ -486,10 +488,10 @@ void update_springs(world& w)
 {
 	if (!w.params.automated_spring_adhesion)
 		return;
-	uint64_t epoch = w.epoch;
+	uint64_t epoch = w.spring_epoch;
 	spring_attachments_internal(w, epoch);
 #pragma omp single
-	w.epoch++;
+	w.spring_epoch++;
 
 	if (w.mesh.dims == 1)
 		spring_contract<1>(w);
