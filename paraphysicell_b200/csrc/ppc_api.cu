@@ -585,7 +585,8 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.ctr, replicates));
 	try_(alloc(s, v.err, 1));
 	try_(alloc(s, v.cursor, 1));
-	try_(alloc(s, v.epoch, 1));
+	v.nvox = (int32_t)vox;
+	v.ntiles = (int32_t)((vox + 4095) / 4096);
 	try_(alloc(s, v.pos[0], C));
 	try_(alloc(s, v.pos[1], C));
 	try_(alloc(s, v.vel, C));
@@ -611,12 +612,15 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.flags, C));
 	try_(alloc(s, v.ids, C));
 	try_(alloc(s, v.rid, C));
-	try_(alloc(s, v.vox_word, (size_t)vox));
-	try_(alloc(s, v.vox_start, (size_t)vox, false));
+	// counts padded to whole tiles so the scan can use 16-byte loads
+	try_(alloc(s, v.vcnt, (size_t)v.ntiles * 4096));
+	try_(alloc(s, v.vstart, (size_t)v.ntiles * 4096 + 1));
+	try_(alloc(s, v.tile_sum, (size_t)v.ntiles));
 	try_(alloc(s, v.key, C));
 	try_(alloc(s, v.vrank, C));
 	try_(alloc(s, v.tmp, C));
 	try_(alloc(s, v.sorted, C));
+	try_(alloc(s, v.skey, C));
 	try_(alloc(s, v.spos4, C));
 	try_(alloc(s, v.ncnt, C));
 	try_(alloc(s, v.nidx, C * s->ncap, false));
@@ -958,27 +962,18 @@ int ppc_get_mesh_bins(ppc_state* s, int32_t r, int32_t* voxel_counts, int32_t* a
 		return fail(PPC_ERR_ARG, "invalid arguments");
 	PPC_TRY(ensure_bins(s));
 	const rep_info& R = s->reps[r];
-	std::vector<unsigned long long> words(R.voxels);
-	std::vector<int32_t> starts(R.voxels);
-	uint32_t epoch = 0;
-	int32_t ntot = 0;
-	PPC_CUDA(cudaMemcpyAsync(words.data(), s->v.vox_word + R.vox_base, R.voxels * 8, cudaMemcpyDeviceToHost, s->stream));
-	PPC_CUDA(cudaMemcpyAsync(starts.data(), s->v.vox_start + R.vox_base, R.voxels * 4, cudaMemcpyDeviceToHost,
+	std::vector<int32_t> starts(R.voxels + 1);
+	PPC_CUDA(cudaMemcpyAsync(starts.data(), s->v.vstart + R.vox_base, (R.voxels + 1) * 4, cudaMemcpyDeviceToHost,
 							 s->stream));
-	PPC_CUDA(cudaMemcpyAsync(&epoch, s->v.epoch, 4, cudaMemcpyDeviceToHost, s->stream));
-	PPC_CUDA(cudaMemcpyAsync(&ntot, s->v.cursor, 4, cudaMemcpyDeviceToHost, s->stream));
 	PPC_CUDA(cudaStreamSynchronize(s->stream));
-	std::vector<int32_t> sorted(std::max(ntot, 1));
-	PPC_CUDA(cudaMemcpy(sorted.data(), s->v.sorted, (size_t)ntot * 4, cudaMemcpyDeviceToHost));
-	size_t o = 0;
+	const int32_t first = starts[0], n = starts[R.voxels] - starts[0];
+	std::vector<int32_t> sorted(std::max(n, 1));
+	if (n > 0)
+		PPC_CUDA(cudaMemcpy(sorted.data(), s->v.sorted + first, (size_t)n * 4, cudaMemcpyDeviceToHost));
 	for (int64_t k = 0; k < R.voxels; k++)
-	{
-		const bool live = (uint32_t)(words[k] >> 32) == epoch;
-		const int32_t c = live ? (int32_t)(uint32_t)words[k] : 0;
-		voxel_counts[k] = c;
-		for (int32_t u = 0; u < c; u++)
-			agents[o++] = sorted[starts[k] + u] - R.base;
-	}
+		voxel_counts[k] = starts[k + 1] - starts[k];
+	for (int32_t u = 0; u < n; u++)
+		agents[u] = sorted[u] - R.base;
 	return finish(s);
 }
 

@@ -12,12 +12,13 @@
 //   aff[C*D], def, maxatt, scnt [C] int32, springs [C*S] int32
 //   movable, flags [C] uint8, ids [C] int64, rid [C] int32 (replicate of slot)
 // Mechanics mesh bins, rebuilt by a counting sort each step:
-//   vox_word[V] uint64 {epoch:32 | count:32}, vox_start[V] int32
-//   key[C] (global voxel index), vrank[C] (provisional rank), tmp[C]
-//   sorted[C] slots grouped by voxel (descending slot inside a voxel),
-//   spos4[C] double4 {x, y, z, rmad*radius} in sorted order.
-// A voxel's bin is valid only when its word's epoch equals the current
-// epoch, so the V-sized table is never cleared (work stays O(agents)).
+//   vcnt[V] per-voxel counts (zero between rebuilds), tile_sum[V/4096]
+//   vstart[V+1] exclusive prefix of the counts over the key space of all
+//   replicates; key[C] (global voxel index), vrank[C] (provisional rank), tmp[C]
+//   sorted[C] slots in voxel-key order (descending slot inside a voxel),
+//   skey[C] their keys, spos4[C] double4 {x, y, z, rmad*radius} in that order.
+// Because the sorted array follows the key order, the voxels x-1..x+1 of one
+// stencil row are one contiguous range [vstart[k-1], vstart[k+2]).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -75,7 +76,8 @@ struct view
 	rep_counters* ctr;
 	int32_t* err;
 	int32_t* cursor;	// number of binned agents (length of `sorted`)
-	uint32_t* epoch;	// epoch of the current bins
+	int32_t nvox;		// voxels of all replicates
+	int32_t ntiles;		// scan tiles of 4096 voxels
 
 	double4* pos[2];
 	double4* vel;
@@ -102,12 +104,14 @@ struct view
 	int64_t* ids;
 	int32_t* rid;
 
-	unsigned long long* vox_word;
-	int32_t* vox_start;
+	int32_t* vcnt;
+	int32_t* vstart;
+	int32_t* tile_sum;
 	int32_t* key;
 	int32_t* vrank;
 	int32_t* tmp;
 	int32_t* sorted;
+	int32_t* skey;
 	double4* spos4;
 
 	int32_t* ncnt;

@@ -15,6 +15,8 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kSortCap = 4096; // list length sorted in shared memory
+constexpr int kTileShift = 12; // voxels per scan tile = 4096 = kThreads * kTileItems
+constexpr int kTileItems = 16;
 
 __device__ __forceinline__ int rep_of(const view& v, int s) { return v.nreps == 1 ? 0 : v.rid[s]; }
 
@@ -73,40 +75,20 @@ __device__ __forceinline__ int axis_coord(double x, const rep_info& R, int d, in
 __global__ void k_bin_count(view v, int cur)
 {
 	int s = blockIdx.x * blockDim.x + threadIdx.x;
-	if (s == 0)
-		*v.cursor = 0;
 	if (s >= v.total_cap)
 		return;
 	int r, local;
 	if (!live(v, s, r, local))
 		return;
 	const rep_info& R = v.reps[r];
-	const uint32_t ep = *v.epoch + 1;
 	double4 p = v.pos[cur][s];
 	int c0 = axis_coord(p.x, R, 0, v.err);
 	int c1 = v.dims >= 2 ? axis_coord(p.y, R, 1, v.err) : 0;
 	int c2 = v.dims >= 3 ? axis_coord(p.z, R, 2, v.err) : 0;
-	int64_t key = R.vox_base + c0 + (int64_t)R.grid[0] * (c1 + (int64_t)R.grid[1] * c2);
-
-	// count into the epoch-tagged voxel word; a stale epoch means the voxel
-	// is empty in this rebuild
-	unsigned long long* w = v.vox_word + key;
-	unsigned long long old = *w;
-	int rank = 0;
-	for (int it = 0; it < (1 << 24); it++)
-	{
-		uint32_t hi = (uint32_t)(old >> 32);
-		unsigned long long nw = hi == ep ? old + 1ull : (((unsigned long long)ep << 32) | 1ull);
-		unsigned long long prev = atomicCAS(w, old, nw);
-		if (prev == old)
-		{
-			rank = hi == ep ? (int)(uint32_t)old : 0;
-			break;
-		}
-		old = prev;
-	}
-	v.key[s] = (int32_t)key;
-	v.vrank[s] = rank;
+	int32_t key = (int32_t)(R.vox_base + c0 + (int64_t)R.grid[0] * (c1 + (int64_t)R.grid[1] * c2));
+	v.key[s] = key;
+	v.vrank[s] = atomicAdd(v.vcnt + key, 1);
+	atomicAdd(v.tile_sum + (key >> kTileShift), 1);
 }
 
 // block-wide exclusive scan of one int per thread; returns the block total
@@ -144,43 +126,94 @@ __device__ __forceinline__ int block_exclusive_scan(int x, int& total)
 	return excl;
 }
 
-// the first agent counted into a voxel reserves the voxel's segment of the
-// sorted array (one atomic per block)
-__global__ void k_bin_alloc(view v)
+// Exclusive scan of the per-voxel counts into vstart (one block per tile of
+// 4096 voxels). The tile's offset is the sum of the per-tile counts that
+// k_bin_count accumulated for the tiles before it. Clears the counts for the
+// next rebuild, so the voxel-sized arrays never need a separate clear.
+__global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
 {
-	__shared__ int block_base;
-	int s = blockIdx.x * blockDim.x + threadIdx.x;
-	int c = 0;
-	int32_t key = -1;
-	if (s < v.total_cap)
+	const int b = blockIdx.x;
+	int part = 0;
+	for (int k = threadIdx.x; k < b; k += blockDim.x)
+		part += v.tile_sum[k];
+	int tile_base;
+	block_exclusive_scan(part, tile_base);
+
+	const int64_t i0 = ((int64_t)b << kTileShift) + (int64_t)threadIdx.x * kTileItems;
+	int c[kTileItems];
+	int sum = 0;
+	if (i0 + kTileItems <= v.nvox)
 	{
-		int r, local;
-		if (live(v, s, r, local) && v.vrank[s] == 0)
+		const int4* q = reinterpret_cast<const int4*>(v.vcnt + i0);
+#pragma unroll
+		for (int k = 0; k < kTileItems / 4; k++)
 		{
-			key = v.key[s];
-			c = (int)(uint32_t)v.vox_word[key];
+			int4 x = q[k];
+			c[4 * k] = x.x;
+			c[4 * k + 1] = x.y;
+			c[4 * k + 2] = x.z;
+			c[4 * k + 3] = x.w;
 		}
 	}
-	int total;
-	int excl = block_exclusive_scan(c, total);
-	if (threadIdx.x == 0)
-		block_base = total > 0 ? atomicAdd(v.cursor, total) : 0;
-	__syncthreads();
-	if (c > 0)
-		v.vox_start[key] = block_base + excl;
-	if (s == 0)
-		*v.epoch += 1;
+	else
+	{
+#pragma unroll
+		for (int k = 0; k < kTileItems; k++)
+			c[k] = i0 + k < v.nvox ? v.vcnt[i0 + k] : 0;
+	}
+#pragma unroll
+	for (int k = 0; k < kTileItems; k++)
+		sum += c[k];
+	int tile_total;
+	int run = tile_base + block_exclusive_scan(sum, tile_total);
+	if (i0 + kTileItems <= v.nvox)
+	{
+		int4* st = reinterpret_cast<int4*>(v.vstart + i0);
+		int4* cl = reinterpret_cast<int4*>(v.vcnt + i0);
+#pragma unroll
+		for (int k = 0; k < kTileItems / 4; k++)
+		{
+			int4 x;
+			x.x = run;
+			run += c[4 * k];
+			x.y = run;
+			run += c[4 * k + 1];
+			x.z = run;
+			run += c[4 * k + 2];
+			x.w = run;
+			run += c[4 * k + 3];
+			st[k] = x;
+			cl[k] = make_int4(0, 0, 0, 0);
+		}
+	}
+	else
+	{
+		for (int k = 0; k < kTileItems; k++)
+			if (i0 + k < v.nvox)
+			{
+				v.vstart[i0 + k] = run;
+				v.vcnt[i0 + k] = 0;
+				run += c[k];
+			}
+	}
+	if (b == gridDim.x - 1 && threadIdx.x == blockDim.x - 1)
+	{
+		v.vstart[v.nvox] = run;
+		*v.cursor = run;
+	}
 }
 
 __global__ void k_bin_scatter(view v)
 {
 	int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s < v.ntiles)
+		v.tile_sum[s] = 0;
 	if (s >= v.total_cap)
 		return;
 	int r, local;
 	if (!live(v, s, r, local))
 		return;
-	v.tmp[v.vox_start[v.key[s]] + v.vrank[s]] = s;
+	v.tmp[v.vstart[v.key[s]] + v.vrank[s]] = s;
 }
 
 // final place inside the voxel: descending slot order, which is the order
@@ -193,13 +226,14 @@ __global__ void k_bin_fixup(view v, int cur)
 	int r, local;
 	if (!live(v, s, r, local))
 		return;
-	int32_t key = v.key[s];
-	int c = (int)(uint32_t)v.vox_word[key];
-	int st = v.vox_start[key];
+	const int32_t key = v.key[s];
+	const int st = v.vstart[key];
+	const int c = v.vstart[key + 1] - st;
 	int rank = 0;
 	for (int u = 0; u < c; u++)
 		rank += v.tmp[st + u] > s;
 	v.sorted[st + rank] = s;
+	v.skey[st + rank] = key;
 	double4 p = v.pos[cur][s];
 	p.w = v.rmad[s] * v.prm[s].x; // relative_maximum_adhesion_distance * radius
 	v.spos4[st + rank] = p;
@@ -214,60 +248,57 @@ __global__ void k_bin_fixup(view v, int cur)
 // ---------------------------------------------------------------------------
 
 template <int DIMS, typename F>
-__device__ __forceinline__ void for_each_neighbor(const view& v, const rep_info& R, uint32_t ep, int s,
+__device__ __forceinline__ void for_each_neighbor(const view& v, const rep_info& R, int s, int32_t key,
 												  const double4& pi, F&& f)
 {
-	int32_t lk = (int32_t)(v.key[s] - R.vox_base);
+	const int32_t lk = (int32_t)(key - R.vox_base);
 	const int g0 = R.grid[0], g1 = R.grid[1], g2 = R.grid[2];
 	const int cx = lk % g0;
 	const int cy = (lk / g0) % g1;
 	const int cz = lk / (g0 * g1);
-	const int zlo = DIMS >= 3 ? -1 : 0, zhi = DIMS >= 3 ? 1 : 0;
-	const int ylo = DIMS >= 2 ? -1 : 0, yhi = DIMS >= 2 ? 1 : 0;
-	for (int dz = zlo; dz <= zhi; dz++)
+	const int xlo = cx > 0 ? cx - 1 : 0;
+	const int xhi = cx + 1 < g0 ? cx + 1 : g0 - 1;
+	// rows of the stencil in the reference's order (z outer, then y); the
+	// voxels x-1..x+1 of a row are consecutive keys, so their agents form one
+	// contiguous range of the key-ordered array. All range bounds are loaded
+	// before any agent is visited.
+	constexpr int NR = DIMS == 3 ? 9 : (DIMS == 2 ? 3 : 1);
+	int lo[NR], hi[NR];
+#pragma unroll
+	for (int k = 0; k < NR; k++)
 	{
-		const int z = cz + dz;
-		if (z < 0 || z >= g2)
-			continue;
-		for (int dy = ylo; dy <= yhi; dy++)
+		const int dz = DIMS == 3 ? k / 3 - 1 : 0;
+		const int dy = DIMS >= 2 ? k % 3 - 1 : 0;
+		const int z = cz + dz, y = cy + dy;
+		const bool ok = z >= 0 && z < g2 && y >= 0 && y < g1;
+		const int64_t row = R.vox_base + (int64_t)g0 * (y + (int64_t)g1 * z);
+		lo[k] = ok ? v.vstart[row + xlo] : 0;
+		hi[k] = ok ? v.vstart[row + xhi + 1] : 0;
+	}
+#pragma unroll
+	for (int k = 0; k < NR; k++)
+	{
+		for (int u = lo[k]; u < hi[k]; u++)
 		{
-			const int y = cy + dy;
-			if (y < 0 || y >= g1)
+			const int j = v.sorted[u];
+			if (j == s)
 				continue;
-			const int64_t row = R.vox_base + (int64_t)g0 * (y + (int64_t)g1 * z);
-			for (int dx = -1; dx <= 1; dx++)
-			{
-				const int x = cx + dx;
-				if (x < 0 || x >= g0)
-					continue;
-				const unsigned long long w = v.vox_word[row + x];
-				if ((uint32_t)(w >> 32) != ep)
-					continue;
-				const int c = (int)(uint32_t)w;
-				const int st = v.vox_start[row + x];
-				for (int u = st; u < st + c; u++)
-				{
-					const int j = v.sorted[u];
-					if (j == s)
-						continue;
-					const double4 q = v.spos4[u];
-					const double ddx = pi.x - q.x;
-					const double ddy = DIMS >= 2 ? pi.y - q.y : 0.0;
-					const double ddz = DIMS >= 3 ? pi.z - q.z : 0.0;
-					double d2 = ddx * ddx;
-					if (DIMS >= 2)
-						d2 = d2 + ddy * ddy;
-					if (DIMS >= 3)
-						d2 = d2 + ddz * ddz;
-					const double ad = pi.w + q.w;
-					// exact early reject: d2 > ad^2 (1 + 1e-12) implies sqrt(d2) > ad
-					if (d2 > ad * ad * (1.0 + 1e-12))
-						continue;
-					const double dist = DIMS == 1 ? fabs(ddx) : sqrt(d2);
-					if (dist <= ad)
-						f(j, ddx, ddy, ddz, dist, ad);
-				}
-			}
+			const double4 q = v.spos4[u];
+			const double ddx = pi.x - q.x;
+			const double ddy = DIMS >= 2 ? pi.y - q.y : 0.0;
+			const double ddz = DIMS >= 3 ? pi.z - q.z : 0.0;
+			double d2 = ddx * ddx;
+			if (DIMS >= 2)
+				d2 = d2 + ddy * ddy;
+			if (DIMS >= 3)
+				d2 = d2 + ddz * ddz;
+			const double ad = pi.w + q.w;
+			// exact early reject: d2 > ad^2 (1 + 1e-12) implies sqrt(d2) > ad
+			if (d2 > ad * ad * (1.0 + 1e-12))
+				continue;
+			const double dist = DIMS == 1 ? fabs(ddx) : sqrt(d2);
+			if (dist <= ad)
+				f(j, ddx, ddy, ddz, dist, ad);
 		}
 	}
 }
@@ -411,7 +442,6 @@ __global__ void __launch_bounds__(kThreads) k_fused(view v, int cur)
 	const int s = v.sorted[t];
 	const int r = rep_of(v, s);
 	const rep_info& R = v.reps[r];
-	const uint32_t ep = *v.epoch;
 	const double4 pi = v.spos4[t];
 
 	pair_fp64 acc;
@@ -426,13 +456,13 @@ __global__ void __launch_bounds__(kThreads) k_fused(view v, int cur)
 		acc.vy = v0.y;
 		acc.vz = v0.z;
 	}
-	for_each_neighbor<DIMS>(v, R, ep, s, pi,
+	for_each_neighbor<DIMS>(v, R, s, v.skey[t], pi,
 							[&](int j, double ddx, double ddy, double ddz, double dist, double ad) {
 								acc.add(v, j, ddx, ddy, ddz, dist, ad);
 							});
 	v.pressure[s] = acc.p;
 
-	double4 p = v.pos[cur][s];
+	double4 p = make_double4(pi.x, pi.y, pi.z, 0.0); // spos4 holds pos[cur][s]
 	if (acc.mov_i)
 	{
 		double4 vel = make_double4(acc.vx, acc.vy, acc.vz, 0.0);
@@ -471,11 +501,10 @@ __global__ void __launch_bounds__(kThreads) k_neighbors(view v)
 		return;
 	}
 	const rep_info& R = v.reps[rep_of(v, s)];
-	const uint32_t ep = *v.epoch;
 	int n = 0;
 	int32_t* out = v.nidx + (int64_t)s * v.ncap;
 	const int cap = v.ncap;
-	for_each_neighbor<DIMS>(v, R, ep, s, v.spos4[t], [&](int j, double, double, double, double, double) {
+	for_each_neighbor<DIMS>(v, R, s, v.skey[t], v.spos4[t], [&](int j, double, double, double, double, double) {
 		if (n < cap)
 			out[n] = j;
 		n++;
@@ -1108,8 +1137,8 @@ int launch_bin(ppc_state* s)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
 	k_bin_count<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
-	k_bin_alloc<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
-	k_bin_scatter<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+	k_bin_scan<<<s->v.ntiles, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+	k_bin_scatter<<<std::max(b, blocks_for(s->v.ntiles, kThreads)), kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
 	k_bin_fixup<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
