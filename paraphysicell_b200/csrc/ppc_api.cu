@@ -479,7 +479,7 @@ int run_steps(ppc_state* s, int32_t steps, bool phenotype, double p_divide, doub
 	return PPC_OK;
 }
 
-void mesh_info(const ppc_mesh& m, rep_info& R)
+void mesh_info(const ppc_mesh& m, rep_info& R, int tile_b = 0)
 {
 	R.voxels = 1;
 	for (int d = 0; d < 3; d++)
@@ -494,6 +494,7 @@ void mesh_info(const ppc_mesh& m, rep_info& R)
 			g = (m.bounding_box_maxs[d] - m.bounding_box_mins[d] + m.voxel_shape[d] - 1) / m.voxel_shape[d];
 		R.grid[d] = std::max(g, 1);
 		R.voxels *= R.grid[d];
+		R.scg[d] = tile_b > 0 ? (R.grid[d] + tile_b - 1) / tile_b : 1;
 	}
 }
 
@@ -541,7 +542,9 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 				return fail(PPC_ERR_ARG, "invalid mesh");
 			}
 		rep_info R {};
-		mesh_info(meshes[r], R);
+		mesh_info(meshes[r], R, s->tile_b);
+		R.sc_base = (int32_t)s->total_sc;
+		s->total_sc += (int64_t)R.scg[0] * R.scg[1] * R.scg[2];
 		R.base = (int32_t)cap;
 		R.cap = capacities[r];
 		R.vox_base = vox;
@@ -587,6 +590,13 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.cursor, 1));
 	v.nvox = (int32_t)vox;
 	v.ntiles = (int32_t)((vox + 4095) / 4096);
+	v.tile_b = s->tile_b;
+	v.sc_list_cap = (int32_t)std::max<int64_t>(1, std::min<int64_t>(s->total_sc, C));
+	try_(alloc(s, v.epoch, 1));
+	try_(alloc(s, v.sc_tag, (size_t)s->total_sc));
+	try_(alloc(s, v.sc_list, 2 * (size_t)v.sc_list_cap));
+	try_(alloc(s, v.nsc, 2));
+	try_(alloc(s, v.work, 2));
 	try_(alloc(s, v.pos[0], C));
 	try_(alloc(s, v.pos[1], C));
 	try_(alloc(s, v.vel, C));
@@ -622,6 +632,8 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.sorted, C));
 	try_(alloc(s, v.skey, C));
 	try_(alloc(s, v.spos4, C));
+	try_(alloc(s, v.sprm4, C));
+	try_(alloc(s, v.saff, C * s->ndefs));
 	try_(alloc(s, v.ncnt, C));
 	try_(alloc(s, v.nidx, C * s->ncap, false));
 	try_(alloc(s, v.bad, C));

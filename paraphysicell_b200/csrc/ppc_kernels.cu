@@ -75,6 +75,14 @@ __device__ __forceinline__ int axis_coord(double x, const rep_info& R, int d, in
 __global__ void k_bin_count(view v, int cur)
 {
 	int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s == 0)
+	{
+		// list counters of the other parity: last used by the fused pass that
+		// consumed the previous-but-one rebuild, needed next by the rebuild after this one
+		const uint32_t e = *v.epoch + 1;
+		v.nsc[(e + 1) & 1] = 0;
+		v.work[(e + 1) & 1] = 0;
+	}
 	if (s >= v.total_cap)
 		return;
 	int r, local;
@@ -89,7 +97,23 @@ __global__ void k_bin_count(view v, int cur)
 	v.key[s] = key;
 	v.vrank[s] = atomicAdd(v.vcnt + key, 1);
 	atomicAdd(v.tile_sum + (key >> kTileShift), 1);
+	if (v.tile_b > 0)
+	{
+		// the first agent of this rebuild in a super-cell enters it in the
+		// list of occupied super-cells (the list of the other parity is
+		// still the previous rebuild's and is reset here for the next one)
+		const uint32_t e = *v.epoch + 1;
+		const int b = v.tile_b;
+		const int sc = c0 / b + R.scg[0] * (c1 / b + R.scg[1] * (c2 / b));
+		if ((uint32_t)atomicExch(v.sc_tag + R.sc_base + sc, (int32_t)e) != e)
+		{
+			const int k = atomicAdd(v.nsc + (e & 1), 1);
+			v.sc_list[(e & 1) * v.sc_list_cap + k] = make_int2(r, sc);
+		}
+	}
 }
+
+
 
 // block-wide exclusive scan of one int per thread; returns the block total
 __device__ __forceinline__ int block_exclusive_scan(int x, int& total)
@@ -208,6 +232,8 @@ __global__ void k_bin_scatter(view v)
 	int s = blockIdx.x * blockDim.x + threadIdx.x;
 	if (s < v.ntiles)
 		v.tile_sum[s] = 0;
+	if (s == 0)
+		*v.epoch += 1;
 	if (s >= v.total_cap)
 		return;
 	int r, local;
@@ -232,11 +258,17 @@ __global__ void k_bin_fixup(view v, int cur)
 	int rank = 0;
 	for (int u = 0; u < c; u++)
 		rank += v.tmp[st + u] > s;
-	v.sorted[st + rank] = s;
-	v.skey[st + rank] = key;
+	const int t = st + rank;
+	v.sorted[t] = s;
+	v.skey[t] = key;
+	const double4 prm = v.prm[s];
 	double4 p = v.pos[cur][s];
-	p.w = v.rmad[s] * v.prm[s].x; // relative_maximum_adhesion_distance * radius
-	v.spos4[st + rank] = p;
+	p.w = v.rmad[s] * prm.x; // relative_maximum_adhesion_distance * radius
+	v.spos4[t] = p;
+	const long long bits = (long long)(uint32_t)v.def[s] | ((long long)v.movable[s] << 32);
+	v.sprm4[t] = make_double4(prm.x, prm.y, prm.z, __longlong_as_double(bits));
+	for (int q = 0; q < v.ndefs; q++)
+		v.saff[(int64_t)t * v.ndefs + q] = v.aff[(int64_t)s * v.ndefs + q];
 }
 
 // ---------------------------------------------------------------------------
@@ -247,9 +279,21 @@ __global__ void k_bin_fixup(view v, int cur)
 // distance <= rmad_i r_i + rmad_j r_j.
 // ---------------------------------------------------------------------------
 
+constexpr int kList = 8; // neighbours recorded per thread before the pair pass runs
+
+// Visits, in the reference's order, the neighbours of the agent at position t
+// of the key-ordered array: stencil rows z outer then y; in each row the
+// voxels x-1..x+1, which are consecutive keys and so one contiguous range
+// [vstart[k-1], vstart[k+2]) of the array; inside a voxel descending slot.
+// Works in two phases: a candidate scan records the array positions of
+// neighbours (distance <= rmad_i r_i + rmad_j r_j) in `list` (kList per
+// thread, strided by the block size), then f(u) runs for each recorded
+// position. The scan loop stays short, so a warp runs the costly pair code
+// max-over-lanes(neighbour count) times rather than once per candidate
+// iteration in which any lane found a neighbour.
 template <int DIMS, typename F>
-__device__ __forceinline__ void for_each_neighbor(const view& v, const rep_info& R, int s, int32_t key,
-												  const double4& pi, F&& f)
+__device__ __forceinline__ void for_each_neighbor(const view& v, const rep_info& R, int t, int32_t key,
+												  const double4& pi, int32_t* list, F&& f)
 {
 	const int32_t lk = (int32_t)(key - R.vox_base);
 	const int g0 = R.grid[0], g1 = R.grid[1], g2 = R.grid[2];
@@ -258,10 +302,6 @@ __device__ __forceinline__ void for_each_neighbor(const view& v, const rep_info&
 	const int cz = lk / (g0 * g1);
 	const int xlo = cx > 0 ? cx - 1 : 0;
 	const int xhi = cx + 1 < g0 ? cx + 1 : g0 - 1;
-	// rows of the stencil in the reference's order (z outer, then y); the
-	// voxels x-1..x+1 of a row are consecutive keys, so their agents form one
-	// contiguous range of the key-ordered array. All range bounds are loaded
-	// before any agent is visited.
 	constexpr int NR = DIMS == 3 ? 9 : (DIMS == 2 ? 3 : 1);
 	int lo[NR], hi[NR];
 #pragma unroll
@@ -275,13 +315,14 @@ __device__ __forceinline__ void for_each_neighbor(const view& v, const rep_info&
 		lo[k] = ok ? v.vstart[row + xlo] : 0;
 		hi[k] = ok ? v.vstart[row + xhi + 1] : 0;
 	}
+	const int stride = blockDim.x;
+	int n = 0;
 #pragma unroll
 	for (int k = 0; k < NR; k++)
 	{
 		for (int u = lo[k]; u < hi[k]; u++)
 		{
-			const int j = v.sorted[u];
-			if (j == s)
+			if (u == t)
 				continue;
 			const double4 q = v.spos4[u];
 			const double ddx = pi.x - q.x;
@@ -297,15 +338,49 @@ __device__ __forceinline__ void for_each_neighbor(const view& v, const rep_info&
 			if (d2 > ad * ad * (1.0 + 1e-12))
 				continue;
 			const double dist = DIMS == 1 ? fabs(ddx) : sqrt(d2);
-			if (dist <= ad)
-				f(j, ddx, ddy, ddz, dist, ad);
+			if (!(dist <= ad))
+				continue;
+			list[n * stride] = u;
+			if (++n == kList)
+			{
+				for (int m = 0; m < n; m++)
+					f(list[m * stride]);
+				n = 0;
+			}
 		}
 	}
+	for (int m = 0; m < n; m++)
+		f(list[m * stride]);
 }
+
+// geometry of the pair (i at pi, neighbour at array position u), recomputed
+// with the same operations as the scan
+template <int DIMS>
+struct pair_geometry
+{
+	double ddx, ddy, ddz, dist, ad;
+
+	__device__ __forceinline__ pair_geometry(const view& v, const double4& pi, int u)
+	{
+		const double4 q = v.spos4[u];
+		ddx = pi.x - q.x;
+		ddy = DIMS >= 2 ? pi.y - q.y : 0.0;
+		ddz = DIMS >= 3 ? pi.z - q.z : 0.0;
+		double d2 = ddx * ddx;
+		if (DIMS >= 2)
+			d2 = d2 + ddy * ddy;
+		if (DIMS >= 3)
+			d2 = d2 + ddz * ddz;
+		ad = pi.w + q.w;
+		dist = DIMS == 1 ? fabs(ddx) : sqrt(d2);
+	}
+};
 
 // solve_pair for the lhs side (reference: position_solver.cpp:24-77) with the
 // pressure contributions of the pair to lhs. Adds (repulsion - adhesion) /
-// distance * difference to v when lhs is movable.
+// distance * difference to v when lhs is movable. `add_pair` takes the
+// neighbour's data as values so callers can read it from global or shared
+// memory; the operations and their order are the reference's.
 struct pair_fp64
 {
 	double4 prm_i;
@@ -315,13 +390,12 @@ struct pair_fp64
 	double vx = 0, vy = 0, vz = 0, p = 0;
 	double last_term = 0; // pressure contribution of the last pair
 
-	__device__ __forceinline__ void add(const view& v, int j, double ddx, double ddy, double ddz, double dist,
-										double adhesion_distance)
+	__device__ __forceinline__ void add_pair(double r_j, double rep_j, double adh_j, int def_j, bool mov_j,
+											 double aff_ji, double ddx, double ddy, double ddz, double dist,
+											 double adhesion_distance)
 	{
-		const double4 prm_j = v.prm[j];
-		const bool mov_j = v.movable[j] != 0;
 		const double d = dist < 0.00001 ? 0.00001 : dist; // std::max(distance, 0.00001)
-		double rep = 1.0 - d / (prm_i.x + prm_j.x);
+		double rep = 1.0 - d / (prm_i.x + r_j);
 		rep = rep < 0 ? 0 : rep;
 		rep = rep * rep;
 		const double term = rep * simple_pressure_coefficient;
@@ -332,17 +406,31 @@ struct pair_fp64
 			p = p + term;
 		if (!mov_i)
 			return;
-		rep = rep * sqrt(prm_i.y * prm_j.y);
+		rep = rep * sqrt(prm_i.y * rep_j);
 		double adh = 1.0 - d / adhesion_distance;
 		adh = adh * adh;
-		const int def_j = v.def[j];
-		adh = adh * sqrt(prm_i.z * prm_j.z * aff_i[def_j] * v.aff[(int64_t)j * v.ndefs + def_i]);
+		adh = adh * sqrt(prm_i.z * adh_j * aff_i[def_j] * aff_ji);
 		const double force = (rep - adh) / d;
 		vx = vx + force * ddx;
 		vy = vy + force * ddy;
 		vz = vz + force * ddz;
 	}
+
+	__device__ __forceinline__ void add(const view& v, int j, double ddx, double ddy, double ddz, double dist,
+										double adhesion_distance)
+	{
+		const double4 prm_j = v.prm[j];
+		add_pair(prm_j.x, prm_j.y, prm_j.z, v.def[j], v.movable[j] != 0, v.aff[(int64_t)j * v.ndefs + def_i], ddx,
+				 ddy, ddz, dist, adhesion_distance);
+	}
 };
+
+__device__ __forceinline__ void unpack_bits(double w, int& def, bool& mov)
+{
+	const long long b = __double_as_longlong(w);
+	def = (int)(uint32_t)(b & 0xffffffffll);
+	mov = (b >> 32) != 0;
+}
 
 // update_membrane_velocity (reference: solver_helper.h:14-28)
 __device__ __forceinline__ double membrane(double x, double bb, double sign, double radius, double strength, double vel)
@@ -456,10 +544,11 @@ __global__ void __launch_bounds__(kThreads) k_fused(view v, int cur)
 		acc.vy = v0.y;
 		acc.vz = v0.z;
 	}
-	for_each_neighbor<DIMS>(v, R, s, v.skey[t], pi,
-							[&](int j, double ddx, double ddy, double ddz, double dist, double ad) {
-								acc.add(v, j, ddx, ddy, ddz, dist, ad);
-							});
+	__shared__ int32_t list[kList * kThreads];
+	for_each_neighbor<DIMS>(v, R, t, v.skey[t], pi, list + threadIdx.x, [&](int u) {
+		const pair_geometry<DIMS> g(v, pi, u);
+		acc.add(v, v.sorted[u], g.ddx, g.ddy, g.ddz, g.dist, g.ad);
+	});
 	v.pressure[s] = acc.p;
 
 	double4 p = make_double4(pi.x, pi.y, pi.z, 0.0); // spos4 holds pos[cur][s]
@@ -484,6 +573,272 @@ __global__ void __launch_bounds__(kThreads) k_fused(view v, int cur)
 }
 
 // ---------------------------------------------------------------------------
+// fused step over super-cell tiles: a block takes one occupied super-cell of
+// B^dims voxels, stages the agents of its (B+2)^dims halo voxels (positions,
+// pair parameters, affinity rows; contiguous runs of the key-ordered arrays)
+// in shared memory, and each thread then handles one home agent of the core,
+// scanning its 27-voxel stencil out of shared memory. Halos larger than the
+// shared-memory budget are read from global memory instead. Results are
+// identical to k_fused: same neighbours, same order, same operations.
+// ---------------------------------------------------------------------------
+
+constexpr int kTileThreadsMax = 256;
+
+template <int DIMS, int B>
+struct tile_geom
+{
+	static constexpr int H = B + 2;
+	static constexpr int NROW = DIMS == 3 ? H * H : (DIMS == 2 ? H : 1);
+	static constexpr int NCORE = DIMS == 3 ? B * B : (DIMS == 2 ? B : 1);
+	// halo row of core row cr, and of the stencil row (dy, dz) around it
+	__device__ static __forceinline__ int core_row(int cr)
+	{
+		if (DIMS == 3)
+			return (cr % B + 1) + H * (cr / B + 1);
+		return DIMS == 2 ? cr + 1 : 0;
+	}
+	__device__ static __forceinline__ int stencil_row(int cr, int dy, int dz)
+	{
+		if (DIMS == 3)
+			return (cr % B + 1 + dy) + H * (cr / B + 1 + dz);
+		return DIMS == 2 ? cr + 1 + dy : 0;
+	}
+};
+
+template <int DIMS, int B, bool STAGED, bool WALLS, bool SPRINGS, bool VEL>
+__device__ __forceinline__ void tile_home(const view& v, const rep_info& R, int r, int cur, int g, int cr, int xi,
+										  const int (*vs)[B + 3], const int* rowoff, const double4* hpos,
+										  const double4* hprm, const double* haff, int32_t* list)
+{
+	using G = tile_geom<DIMS, B>;
+	const int D = v.ndefs;
+	const double4* P = STAGED ? hpos : v.spos4;
+	const double4* Q = STAGED ? hprm : v.sprm4;
+	const double* A = STAGED ? haff : v.saff;
+	const int hr0 = G::core_row(cr);
+	const int self = STAGED ? rowoff[hr0] + (g - vs[hr0][0]) : g;
+	const int s = v.sorted[g];
+	const double4 pi = P[self];
+	const double4 qi = Q[self];
+
+	pair_fp64 acc;
+	acc.prm_i = qi;
+	unpack_bits(qi.w, acc.def_i, acc.mov_i);
+	acc.aff_i = A + (int64_t)self * D;
+	if (VEL && acc.mov_i)
+	{
+		const double4 v0 = v.vel[s];
+		acc.vx = v0.x;
+		acc.vy = v0.y;
+		acc.vz = v0.z;
+	}
+
+	const int stride = blockDim.x;
+	int n = 0;
+	auto flush = [&]() {
+		for (int m = 0; m < n; m++)
+		{
+			const int u = list[m * stride];
+			const double4 q = P[u];
+			const double ddx = pi.x - q.x;
+			const double ddy = DIMS >= 2 ? pi.y - q.y : 0.0;
+			const double ddz = DIMS >= 3 ? pi.z - q.z : 0.0;
+			double d2 = ddx * ddx;
+			if (DIMS >= 2)
+				d2 = d2 + ddy * ddy;
+			if (DIMS >= 3)
+				d2 = d2 + ddz * ddz;
+			const double dist = DIMS == 1 ? fabs(ddx) : sqrt(d2);
+			const double4 qj = Q[u];
+			int def_j;
+			bool mov_j;
+			unpack_bits(qj.w, def_j, mov_j);
+			acc.add_pair(qj.x, qj.y, qj.z, def_j, mov_j, A[(int64_t)u * D + acc.def_i], ddx, ddy, ddz, dist,
+						 pi.w + q.w);
+		}
+		n = 0;
+	};
+#pragma unroll
+	for (int k = 0; k < (DIMS == 3 ? 9 : (DIMS == 2 ? 3 : 1)); k++)
+	{
+		const int dz = DIMS == 3 ? k / 3 - 1 : 0;
+		const int dy = DIMS >= 2 ? k % 3 - 1 : 0;
+		const int hr = G::stencil_row(cr, dy, dz);
+		const int shift = STAGED ? rowoff[hr] - vs[hr][0] : 0;
+		const int lo = vs[hr][xi - 1] + shift, hi = vs[hr][xi + 2] + shift;
+		for (int u = lo; u < hi; u++)
+		{
+			if (u == self)
+				continue;
+			const double4 q = P[u];
+			const double ddx = pi.x - q.x;
+			const double ddy = DIMS >= 2 ? pi.y - q.y : 0.0;
+			const double ddz = DIMS >= 3 ? pi.z - q.z : 0.0;
+			double d2 = ddx * ddx;
+			if (DIMS >= 2)
+				d2 = d2 + ddy * ddy;
+			if (DIMS >= 3)
+				d2 = d2 + ddz * ddz;
+			const double ad = pi.w + q.w;
+			if (d2 > ad * ad * (1.0 + 1e-12))
+				continue;
+			const double dist = DIMS == 1 ? fabs(ddx) : sqrt(d2);
+			if (!(dist <= ad))
+				continue;
+			list[n * stride] = u;
+			if (++n == kList)
+				flush();
+		}
+	}
+	flush();
+
+	v.pressure[s] = acc.p;
+	double4 p = make_double4(pi.x, pi.y, pi.z, 0.0);
+	if (acc.mov_i)
+	{
+		double4 vel = make_double4(acc.vx, acc.vy, acc.vz, 0.0);
+		if (WALLS)
+			walls<DIMS>(v, R, p, qi.x, v.prm[s].w, vel);
+		if (SPRINGS)
+			spring_contract<DIMS>(v, cur, s, p, acc.def_i, vel);
+		double4 vp = v.vprev[s];
+		ab2<DIMS>(v.dt, p, vel, vp);
+		v.vprev[s] = vp;
+		if (VEL)
+			v.vel[s] = make_double4(0, 0, 0, 0);
+	}
+	v.pos[cur ^ 1][s] = p;
+	if (!(p.x == p.x && p.y == p.y && p.z == p.z))
+		atomicOr(v.err, ERR_NONFINITE);
+	if (to_remove<DIMS>(R, p, v.flags[s]))
+		append_bad(v, r, s - R.base);
+}
+
+template <int DIMS, int B, bool WALLS, bool SPRINGS, bool VEL>
+__global__ void __launch_bounds__(kTileThreadsMax) k_fused_tile(view v, int cur, int cap)
+{
+	using G = tile_geom<DIMS, B>;
+	constexpr int H = G::H, NROW = G::NROW, NCORE = G::NCORE;
+	extern __shared__ double4 dyn[];
+	double4* hpos = dyn;
+	double4* hprm = dyn + cap;
+	double* haff = reinterpret_cast<double*>(dyn + 2 * cap);
+	__shared__ int vs[NROW][B + 3];
+	__shared__ int rowoff[NROW + 1];
+	__shared__ int coreoff[NCORE + 1];
+	__shared__ int item;
+	__shared__ int32_t list[kList * kTileThreadsMax];
+
+	const uint32_t e = *v.epoch;
+	const int par = e & 1;
+	const int nsc = v.nsc[par];
+	const int D = v.ndefs;
+	const int tid = threadIdx.x, nt = blockDim.x;
+	for (;;)
+	{
+		if (tid == 0)
+			item = atomicAdd(v.work + par, 1);
+		__syncthreads();
+		const int w = item;
+		if (w >= nsc)
+			break;
+		const int2 it = v.sc_list[par * v.sc_list_cap + w];
+		const int r = it.x;
+		const rep_info& R = v.reps[r];
+		const int g0 = R.grid[0], g1 = R.grid[1], g2 = R.grid[2];
+		const int sx = it.y % R.scg[0];
+		const int sy = DIMS >= 2 ? (it.y / R.scg[0]) % R.scg[1] : 0;
+		const int sz = DIMS >= 3 ? it.y / (R.scg[0] * R.scg[1]) : 0;
+		const int x0 = sx * B, y0 = sy * B, z0 = sz * B;
+
+		// vstart at the voxel boundaries of every halo row, x clipped to the grid
+		for (int k = tid; k < NROW * (H + 1); k += nt)
+		{
+			const int hr = k / (H + 1), xi = k % (H + 1);
+			const int y = DIMS >= 2 ? y0 - 1 + hr % H : 0;
+			const int z = DIMS >= 3 ? z0 - 1 + hr / H : 0;
+			int val = 0;
+			if (y >= 0 && y < g1 && z >= 0 && z < g2)
+			{
+				int x = x0 - 1 + xi;
+				x = x < 0 ? 0 : (x > g0 ? g0 : x);
+				val = v.vstart[R.vox_base + (int64_t)g0 * (y + (int64_t)g1 * z) + x];
+			}
+			vs[hr][xi] = val;
+		}
+		__syncthreads();
+		if (tid == 0)
+		{
+			int o = 0;
+			for (int hr = 0; hr < NROW; hr++)
+			{
+				rowoff[hr] = o;
+				o += vs[hr][H] - vs[hr][0];
+			}
+			rowoff[NROW] = o;
+			int c = 0;
+			for (int cr = 0; cr < NCORE; cr++)
+			{
+				const int hr = G::core_row(cr);
+				coreoff[cr] = c;
+				c += vs[hr][B + 1] - vs[hr][1];
+			}
+			coreoff[NCORE] = c;
+		}
+		__syncthreads();
+		const int total = rowoff[NROW];
+		const bool staged = total <= cap;
+		if (staged)
+		{
+			for (int f = tid; f < total; f += nt)
+			{
+				int lo = 0, hi = NROW; // last row with rowoff <= f
+				while (hi - lo > 1)
+				{
+					const int mid = (lo + hi) >> 1;
+					if (rowoff[mid] <= f)
+						lo = mid;
+					else
+						hi = mid;
+				}
+				const int g = vs[lo][0] + (f - rowoff[lo]);
+				hpos[f] = v.spos4[g];
+				hprm[f] = v.sprm4[g];
+				for (int q = 0; q < D; q++)
+					haff[f * D + q] = v.saff[(int64_t)g * D + q];
+			}
+		}
+		__syncthreads();
+		const int nhome = coreoff[NCORE];
+		for (int h = tid; h < nhome; h += nt)
+		{
+			int lo = 0, hi = NCORE;
+			while (hi - lo > 1)
+			{
+				const int mid = (lo + hi) >> 1;
+				if (coreoff[mid] <= h)
+					lo = mid;
+				else
+					hi = mid;
+			}
+			const int cr = lo;
+			const int hr = G::core_row(cr);
+			const int g = vs[hr][1] + (h - coreoff[cr]);
+			int xi = 1;
+			while (xi < B && g >= vs[hr][xi + 1])
+				xi++;
+			if (staged)
+				tile_home<DIMS, B, true, WALLS, SPRINGS, VEL>(v, R, r, cur, g, cr, xi, vs, rowoff, hpos, hprm, haff,
+															  list + tid);
+			else
+				tile_home<DIMS, B, false, WALLS, SPRINGS, VEL>(v, R, r, cur, g, cr, xi, vs, rowoff, hpos, hprm, haff,
+															   list + tid);
+		}
+		__syncthreads();
+	}
+}
+
+// ---------------------------------------------------------------------------
 // separate reference entry points
 // ---------------------------------------------------------------------------
 
@@ -504,9 +859,10 @@ __global__ void __launch_bounds__(kThreads) k_neighbors(view v)
 	int n = 0;
 	int32_t* out = v.nidx + (int64_t)s * v.ncap;
 	const int cap = v.ncap;
-	for_each_neighbor<DIMS>(v, R, s, v.skey[t], v.spos4[t], [&](int j, double, double, double, double, double) {
+	__shared__ int32_t list[kList * kThreads];
+	for_each_neighbor<DIMS>(v, R, t, v.skey[t], v.spos4[t], list + threadIdx.x, [&](int u) {
 		if (n < cap)
-			out[n] = j;
+			out[n] = v.sorted[u];
 		n++;
 	});
 	if (n > cap)
@@ -1210,6 +1566,57 @@ int launch_positions(ppc_state* s)
 	return PPC_OK;
 }
 
+template <int DIMS, int B>
+static int tile_dispatch(ppc_state* s)
+{
+	const bool walls = s->params.virtual_wall_at_domain_edges != 0;
+	const bool springs = s->has_springs && s->params.automated_spring_adhesion != 0;
+	const bool vel = s->vel_dirty;
+	const int per_agent = 2 * (int)sizeof(double4) + s->ndefs * (int)sizeof(double);
+	const int cap = s->tile_smem / per_agent;
+	const size_t dyn = (size_t)cap * per_agent;
+	cudaStream_t st = PPC_LAUNCH(s);
+	void (*k)(view, int, int) = nullptr;
+#define PPC_TILE(W, S, V)                                                                                              \
+	if (walls == W && springs == S && vel == V)                                                                        \
+		k = k_fused_tile<DIMS, B, W, S, V>;
+	PPC_TILE(false, false, false)
+	PPC_TILE(false, false, true)
+	PPC_TILE(false, true, false)
+	PPC_TILE(false, true, true)
+	PPC_TILE(true, false, false)
+	PPC_TILE(true, false, true)
+	PPC_TILE(true, true, false)
+	PPC_TILE(true, true, true)
+#undef PPC_TILE
+	PPC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+	int per_sm = 0;
+	PPC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, s->tile_threads, dyn));
+	const int blocks = std::max(1, per_sm) * s->sm_count;
+	k<<<blocks, s->tile_threads, dyn, st>>>(s->v, s->cur, cap);
+	return PPC_OK;
+}
+
+template <int DIMS>
+static int tile_by_edge(ppc_state* s)
+{
+	switch (s->tile_b)
+	{
+	case 2:
+		return tile_dispatch<DIMS, 2>(s);
+	case 3:
+		return tile_dispatch<DIMS, 3>(s);
+	case 4:
+		return tile_dispatch<DIMS, 4>(s);
+	case 6:
+		return tile_dispatch<DIMS, 6>(s);
+	case 8:
+		return tile_dispatch<DIMS, 8>(s);
+	default:
+		return PPC_ERR_ARG;
+	}
+}
+
 template <int DIMS>
 static void fused_dispatch(ppc_state* s, int b)
 {
@@ -1250,7 +1657,13 @@ int launch_fused(ppc_state* s)
 		ev_end = s->prof_events[s->prof_used + 1];
 		s->prof_used += 2;
 	}
-	if (s->dims == 1)
+	if (s->tile_b > 0)
+	{
+		int rc = s->dims == 1 ? tile_by_edge<1>(s) : (s->dims == 2 ? tile_by_edge<2>(s) : tile_by_edge<3>(s));
+		if (rc != PPC_OK)
+			return rc;
+	}
+	else if (s->dims == 1)
 		fused_dispatch<1>(s, b);
 	else if (s->dims == 2)
 		fused_dispatch<2>(s, b);
