@@ -715,6 +715,60 @@ int ppc_set_random_seed(ppc_state* s, uint64_t seed)
 	return PPC_OK;
 }
 
+int ppc_set_launch_shape(ppc_state* s, int32_t tile_edge, int32_t threads, int32_t smem_bytes)
+{
+	if (!s)
+		return fail(PPC_ERR_ARG, "null state");
+	const bool edge_ok = tile_edge == 0 || tile_edge == 2 || tile_edge == 3 || tile_edge == 4 || tile_edge == 6
+						 || tile_edge == 8;
+	if (!edge_ok || threads < 32 || threads > 256 || threads % 32 != 0 || smem_bytes < 0 || smem_bytes > 160 * 1024)
+		return fail(PPC_ERR_ARG, "tile edge 0/2/3/4/6/8, threads 32..256 (multiple of 32), smem <= 160 KiB");
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	release_graph(s);
+	s->tile_threads = threads;
+	s->tile_smem = smem_bytes;
+	if (tile_edge == s->tile_b)
+		return PPC_OK;
+	// super-cell numbering depends on the edge: rebuild it and its buffers
+	int64_t total_sc = 0;
+	for (auto& R : s->reps)
+	{
+		for (int d = 0; d < 3; d++)
+			R.scg[d] = tile_edge > 0 ? (R.grid[d] + tile_edge - 1) / tile_edge : 1;
+		R.sc_base = (int32_t)total_sc;
+		total_sc += (int64_t)R.scg[0] * R.scg[1] * R.scg[2];
+	}
+	PPC_CUDA(cudaMemcpy(const_cast<rep_info*>(s->v.reps), s->reps.data(), sizeof(rep_info) * s->nreps,
+						cudaMemcpyHostToDevice));
+	const int32_t cap = (int32_t)std::max<int64_t>(1, std::min<int64_t>(total_sc, s->total_cap));
+	int32_t* tag = nullptr;
+	int2* list = nullptr;
+	PPC_CUDA(cudaMalloc(&tag, std::max<int64_t>(total_sc, 1) * sizeof(int32_t)));
+	PPC_CUDA(cudaMemset(tag, 0, std::max<int64_t>(total_sc, 1) * sizeof(int32_t)));
+	PPC_CUDA(cudaMalloc(&list, 2 * (size_t)cap * sizeof(int2)));
+	for (auto& b : s->allocations)
+	{
+		if (b.p == s->v.sc_tag)
+		{
+			cudaFree(b.p);
+			b.p = tag;
+		}
+		else if (b.p == s->v.sc_list)
+		{
+			cudaFree(b.p);
+			b.p = list;
+		}
+	}
+	s->v.sc_tag = tag;
+	s->v.sc_list = list;
+	s->v.sc_list_cap = cap;
+	s->total_sc = total_sc;
+	s->tile_b = tile_edge;
+	s->v.tile_b = tile_edge;
+	s->bins_valid = false;
+	return PPC_OK;
+}
+
 int ppc_set_neighbor_capacity(ppc_state* s, int32_t per_agent)
 {
 	if (!s || per_agent < 1)

@@ -521,7 +521,7 @@ __device__ __forceinline__ void append_bad(const view& v, int r, int local)
 // agents for the container update that follows.
 // ---------------------------------------------------------------------------
 template <int DIMS, bool WALLS, bool SPRINGS, bool VEL>
-__global__ void __launch_bounds__(kThreads) k_fused(view v, int cur)
+__global__ void __launch_bounds__(256) k_fused(view v, int cur)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= *v.cursor)
@@ -544,7 +544,7 @@ __global__ void __launch_bounds__(kThreads) k_fused(view v, int cur)
 		acc.vy = v0.y;
 		acc.vz = v0.z;
 	}
-	__shared__ int32_t list[kList * kThreads];
+	__shared__ int32_t list[kList * 256];
 	for_each_neighbor<DIMS>(v, R, t, v.skey[t], pi, list + threadIdx.x, [&](int u) {
 		const pair_geometry<DIMS> g(v, pi, u);
 		acc.add(v, v.sorted[u], g.ddx, g.ddy, g.ddz, g.dist, g.ad);
@@ -1624,9 +1624,11 @@ static void fused_dispatch(ppc_state* s, int b)
 	const bool springs = s->has_springs && s->params.automated_spring_adhesion != 0;
 	const bool vel = s->vel_dirty;
 	cudaStream_t st = PPC_LAUNCH(s);
+	const int nt = s->tile_threads;
+	b = blocks_for(s->total_cap, nt);
 #define PPC_FUSED(W, S, V)                                                                                             \
 	if (walls == W && springs == S && vel == V)                                                                        \
-		k_fused<DIMS, W, S, V><<<b, kThreads, 0, st>>>(s->v, s->cur);
+		k_fused<DIMS, W, S, V><<<b, nt, 0, st>>>(s->v, s->cur);
 	PPC_FUSED(false, false, false)
 	PPC_FUSED(false, false, true)
 	PPC_FUSED(false, true, false)

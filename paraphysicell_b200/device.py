@@ -34,7 +34,7 @@ EXPORTS = (
     "ppc_get_event_counts", "ppc_flag_by_draws", "ppc_step", "ppc_step_with_phenotype",
     "ppc_get_neighbors", "ppc_get_mesh_bins", "ppc_get_voxel_count", "ppc_get_mesh_position",
     "ppc_get_mesh_index", "ppc_get_launch_count", "ppc_last_error", "ppc_abi_version",
-    "ppc_set_profiling", "ppc_get_profile",
+    "ppc_set_profiling", "ppc_get_profile", "ppc_set_launch_shape",
 ) + tuple("ppc_" + e for e in ENTRY_POINTS)
 
 
@@ -73,6 +73,7 @@ def lib():
         L.ppc_get_mesh_index.argtypes = [C.POINTER(Mesh), vp, vp]
         L.ppc_get_launch_count.argtypes = [vp, C.POINTER(C.c_int64)]
         L.ppc_set_profiling.argtypes = [vp, C.c_int32]
+        L.ppc_set_launch_shape.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32]
         L.ppc_get_profile.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
         L.ppc_last_error.restype = C.c_char_p
         for e in ENTRY_POINTS:
@@ -181,6 +182,9 @@ class Simulation:
         n = C.c_int64()
         _check(lib().ppc_get_launch_count(self.h, C.byref(n)), "ppc_get_launch_count")
         return n.value
+
+    def set_launch_shape(self, tile_edge, threads, smem_bytes=48 * 1024):
+        _check(lib().ppc_set_launch_shape(self.h, tile_edge, threads, smem_bytes), "ppc_set_launch_shape")
 
     def set_profiling(self, on):
         _check(lib().ppc_set_profiling(self.h, int(bool(on))), "ppc_set_profiling")
