@@ -186,7 +186,7 @@ struct ppc_state
 	bool use_graphs = true;
 
 	// fused pass: super-cell tiles staged in shared memory (0 = one thread per agent)
-	int tile_b = 4;
+	int tile_b = 0;
 	int tile_threads = 128;
 	int tile_smem = 48 * 1024;
 	int64_t total_sc = 0;

@@ -72,49 +72,6 @@ __device__ __forceinline__ int axis_coord(double x, const rep_info& R, int d, in
 	return (int)q;
 }
 
-__global__ void k_bin_count(view v, int cur)
-{
-	int s = blockIdx.x * blockDim.x + threadIdx.x;
-	if (s == 0)
-	{
-		// list counters of the other parity: last used by the fused pass that
-		// consumed the previous-but-one rebuild, needed next by the rebuild after this one
-		const uint32_t e = *v.epoch + 1;
-		v.nsc[(e + 1) & 1] = 0;
-		v.work[(e + 1) & 1] = 0;
-	}
-	if (s >= v.total_cap)
-		return;
-	int r, local;
-	if (!live(v, s, r, local))
-		return;
-	const rep_info& R = v.reps[r];
-	double4 p = v.pos[cur][s];
-	int c0 = axis_coord(p.x, R, 0, v.err);
-	int c1 = v.dims >= 2 ? axis_coord(p.y, R, 1, v.err) : 0;
-	int c2 = v.dims >= 3 ? axis_coord(p.z, R, 2, v.err) : 0;
-	int32_t key = (int32_t)(R.vox_base + c0 + (int64_t)R.grid[0] * (c1 + (int64_t)R.grid[1] * c2));
-	v.key[s] = key;
-	v.vrank[s] = atomicAdd(v.vcnt + key, 1);
-	atomicAdd(v.tile_sum + (key >> kTileShift), 1);
-	if (v.tile_b > 0)
-	{
-		// the first agent of this rebuild in a super-cell enters it in the
-		// list of occupied super-cells (the list of the other parity is
-		// still the previous rebuild's and is reset here for the next one)
-		const uint32_t e = *v.epoch + 1;
-		const int b = v.tile_b;
-		const int sc = c0 / b + R.scg[0] * (c1 / b + R.scg[1] * (c2 / b));
-		if ((uint32_t)atomicExch(v.sc_tag + R.sc_base + sc, (int32_t)e) != e)
-		{
-			const int k = atomicAdd(v.nsc + (e & 1), 1);
-			v.sc_list[(e & 1) * v.sc_list_cap + k] = make_int2(r, sc);
-		}
-	}
-}
-
-
-
 // block-wide exclusive scan of one int per thread; returns the block total
 __device__ __forceinline__ int block_exclusive_scan(int x, int& total)
 {
@@ -150,10 +107,80 @@ __device__ __forceinline__ int block_exclusive_scan(int x, int& total)
 	return excl;
 }
 
+__global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur)
+{
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	const uint32_t e = *v.epoch + 1;
+	if (s == 0)
+	{
+		// list counters of the other parity: last used by the fused pass that
+		// consumed the previous-but-one rebuild, needed next by the rebuild after this one
+		v.nsc[(e + 1) & 1] = 0;
+		v.work[(e + 1) & 1] = 0;
+	}
+	int r = 0, local = 0;
+	const bool is_live = s < v.total_cap && live(v, s, r, local);
+	int32_t key = 0, rank = 0;
+	int first = 0, sc = 0;
+	if (is_live)
+	{
+		const rep_info& R = v.reps[r];
+		const double4 p = v.pos[cur][s];
+		const int c0 = axis_coord(p.x, R, 0, v.err);
+		const int c1 = v.dims >= 2 ? axis_coord(p.y, R, 1, v.err) : 0;
+		const int c2 = v.dims >= 3 ? axis_coord(p.z, R, 2, v.err) : 0;
+		key = (int32_t)(R.vox_base + c0 + (int64_t)R.grid[0] * (c1 + (int64_t)R.grid[1] * c2));
+		rank = atomicAdd(v.vcnt + key, 1);
+		if (v.tile_b > 0)
+		{
+			// the first agent of this rebuild in a super-cell enters it in the
+			// list of occupied super-cells
+			const int b = v.tile_b;
+			sc = c0 / b + R.scg[0] * (c1 / b + R.scg[1] * (c2 / b));
+			first = (uint32_t)atomicExch(v.sc_tag + R.sc_base + sc, (int32_t)e) != e;
+		}
+	}
+	if (v.tile_b > 0)
+	{
+		// one list reservation per block
+		__shared__ int base;
+		int total;
+		const int off = block_exclusive_scan(first, total);
+		if (threadIdx.x == 0 && total > 0)
+			base = atomicAdd(v.nsc + (e & 1), total);
+		__syncthreads();
+		if (first)
+			v.sc_list[(e & 1) * v.sc_list_cap + base + off] = make_int2(r, sc);
+	}
+	if (is_live)
+	{
+		v.key[s] = key;
+		v.vrank[s] = rank;
+	}
+}
+
+// per-tile totals of the voxel counts (one block per tile of 4096 voxels)
+__global__ void __launch_bounds__(kThreads) k_bin_reduce(view v)
+{
+	const int b = blockIdx.x;
+	const int64_t i0 = ((int64_t)b << kTileShift) + (int64_t)threadIdx.x * kTileItems;
+	int sum = 0;
+	const int4* q = reinterpret_cast<const int4*>(v.vcnt + i0); // counts are padded to whole tiles
+#pragma unroll
+	for (int k = 0; k < kTileItems / 4; k++)
+	{
+		const int4 x = q[k];
+		sum += x.x + x.y + x.z + x.w;
+	}
+	int total;
+	block_exclusive_scan(sum, total);
+	if (threadIdx.x == 0)
+		v.tile_sum[b] = total;
+}
+
 // Exclusive scan of the per-voxel counts into vstart (one block per tile of
-// 4096 voxels). The tile's offset is the sum of the per-tile counts that
-// k_bin_count accumulated for the tiles before it. Clears the counts for the
-// next rebuild, so the voxel-sized arrays never need a separate clear.
+// 4096 voxels); a tile's offset is the sum of the totals of the tiles before
+// it. The counts are cleared at occupied voxels by k_bin_fixup.
 __global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
 {
 	const int b = blockIdx.x;
@@ -193,7 +220,6 @@ __global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
 	if (i0 + kTileItems <= v.nvox)
 	{
 		int4* st = reinterpret_cast<int4*>(v.vstart + i0);
-		int4* cl = reinterpret_cast<int4*>(v.vcnt + i0);
 #pragma unroll
 		for (int k = 0; k < kTileItems / 4; k++)
 		{
@@ -207,7 +233,6 @@ __global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
 			x.w = run;
 			run += c[4 * k + 3];
 			st[k] = x;
-			cl[k] = make_int4(0, 0, 0, 0);
 		}
 	}
 	else
@@ -216,7 +241,6 @@ __global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
 			if (i0 + k < v.nvox)
 			{
 				v.vstart[i0 + k] = run;
-				v.vcnt[i0 + k] = 0;
 				run += c[k];
 			}
 	}
@@ -230,8 +254,6 @@ __global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
 __global__ void k_bin_scatter(view v)
 {
 	int s = blockIdx.x * blockDim.x + threadIdx.x;
-	if (s < v.ntiles)
-		v.tile_sum[s] = 0;
 	if (s == 0)
 		*v.epoch += 1;
 	if (s >= v.total_cap)
@@ -253,22 +275,29 @@ __global__ void k_bin_fixup(view v, int cur)
 	if (!live(v, s, r, local))
 		return;
 	const int32_t key = v.key[s];
+	const double4 prm = v.prm[s];
+	double4 p = v.pos[cur][s];
+	const double rmad = v.rmad[s];
+	const long long bits = (long long)(uint32_t)v.def[s] | ((long long)v.movable[s] << 32);
+	double aff[8];
+	const int D = v.ndefs;
+	for (int q = 0; q < D && q < 8; q++)
+		aff[q] = v.aff[(int64_t)s * D + q];
 	const int st = v.vstart[key];
 	const int c = v.vstart[key + 1] - st;
 	int rank = 0;
 	for (int u = 0; u < c; u++)
 		rank += v.tmp[st + u] > s;
 	const int t = st + rank;
+	p.w = rmad * prm.x; // relative_maximum_adhesion_distance * radius
+	if (rank == 0)
+		v.vcnt[key] = 0; // ready for the next rebuild
 	v.sorted[t] = s;
 	v.skey[t] = key;
-	const double4 prm = v.prm[s];
-	double4 p = v.pos[cur][s];
-	p.w = v.rmad[s] * prm.x; // relative_maximum_adhesion_distance * radius
 	v.spos4[t] = p;
-	const long long bits = (long long)(uint32_t)v.def[s] | ((long long)v.movable[s] << 32);
 	v.sprm4[t] = make_double4(prm.x, prm.y, prm.z, __longlong_as_double(bits));
-	for (int q = 0; q < v.ndefs; q++)
-		v.saff[(int64_t)t * v.ndefs + q] = v.aff[(int64_t)s * v.ndefs + q];
+	for (int q = 0; q < D; q++)
+		v.saff[(int64_t)t * D + q] = q < 8 ? aff[q] : v.aff[(int64_t)s * D + q];
 }
 
 // ---------------------------------------------------------------------------
@@ -513,6 +542,61 @@ __device__ __forceinline__ void append_bad(const view& v, int r, int local)
 		atomicOr(v.err, ERR_LIST_CAPACITY);
 }
 
+// Per-agent data the epilogue needs, gathered before the agent's first
+// global store: on this GPU a gather that follows scattered stores of the
+// same thread stalls far longer than the same gather issued first.
+struct agent_tail
+{
+	double4 vprev;
+	double4 vel0;
+	double bm;
+	uint8_t flag;
+};
+
+template <bool WALLS, bool VEL>
+__device__ __forceinline__ agent_tail load_tail(const view& v, int s, bool mov)
+{
+	agent_tail a;
+	a.vprev = mov ? v.vprev[s] : make_double4(0, 0, 0, 0);
+	a.vel0 = (VEL && mov) ? v.vel[s] : make_double4(0, 0, 0, 0);
+	a.bm = (WALLS && mov) ? v.prm[s].w : 0.0;
+	a.flag = v.flags[s];
+	return a;
+}
+
+// membrane + springs + Adams-Bashforth for one agent, then every store of the
+// fused pass for it (pressure, previous velocity, velocity, new position) and
+// the container-update marking
+template <int DIMS, bool WALLS, bool SPRINGS, bool VEL>
+__device__ __forceinline__ void finish_agent(const view& v, const rep_info& R, int r, int cur, int s, const double4& pi,
+											 double radius, int def_i, bool mov_i, const agent_tail& tail, double vx,
+											 double vy, double vz, double pressure)
+{
+	double4 p = make_double4(pi.x, pi.y, pi.z, 0.0);
+	double4 vp = tail.vprev;
+	if (mov_i)
+	{
+		double4 vel = make_double4(vx, vy, vz, 0.0);
+		if (WALLS)
+			walls<DIMS>(v, R, p, radius, tail.bm, vel);
+		if (SPRINGS)
+			spring_contract<DIMS>(v, cur, s, p, def_i, vel);
+		ab2<DIMS>(v.dt, p, vel, vp);
+	}
+	v.pressure[s] = pressure;
+	if (mov_i)
+	{
+		v.vprev[s] = vp;
+		if (VEL)
+			v.vel[s] = make_double4(0, 0, 0, 0);
+	}
+	v.pos[cur ^ 1][s] = p;
+	if (!(p.x == p.x && p.y == p.y && p.z == p.z))
+		atomicOr(v.err, ERR_NONFINITE);
+	if (to_remove<DIMS>(R, p, tail.flag))
+		append_bad(v, r, s - R.base);
+}
+
 // ---------------------------------------------------------------------------
 // fused step: neighbour search + forces + membrane + springs + AB2, one
 // thread per binned agent, reading positions from pos[cur] and writing the
@@ -526,50 +610,33 @@ __global__ void __launch_bounds__(256) k_fused(view v, int cur)
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= *v.cursor)
 		return;
-	const int nxt = cur ^ 1;
 	const int s = v.sorted[t];
 	const int r = rep_of(v, s);
 	const rep_info& R = v.reps[r];
 	const double4 pi = v.spos4[t];
 
 	pair_fp64 acc;
-	acc.prm_i = v.prm[s];
-	acc.def_i = v.def[s];
-	acc.mov_i = v.movable[s] != 0;
-	acc.aff_i = v.aff + (int64_t)s * v.ndefs;
-	if (VEL && acc.mov_i)
-	{
-		const double4 v0 = v.vel[s];
-		acc.vx = v0.x;
-		acc.vy = v0.y;
-		acc.vz = v0.z;
-	}
+	acc.prm_i = v.sprm4[t];
+	unpack_bits(acc.prm_i.w, acc.def_i, acc.mov_i);
+	acc.aff_i = v.saff + (int64_t)t * v.ndefs;
+	const agent_tail tail = load_tail<WALLS, VEL>(v, s, acc.mov_i);
+	acc.vx = tail.vel0.x;
+	acc.vy = tail.vel0.y;
+	acc.vz = tail.vel0.z;
 	__shared__ int32_t list[kList * 256];
+	const int D = v.ndefs;
 	for_each_neighbor<DIMS>(v, R, t, v.skey[t], pi, list + threadIdx.x, [&](int u) {
+		// neighbour data from the key-ordered copies (index u, no indirection)
 		const pair_geometry<DIMS> g(v, pi, u);
-		acc.add(v, v.sorted[u], g.ddx, g.ddy, g.ddz, g.dist, g.ad);
+		const double4 qj = v.sprm4[u];
+		int def_j;
+		bool mov_j;
+		unpack_bits(qj.w, def_j, mov_j);
+		acc.add_pair(qj.x, qj.y, qj.z, def_j, mov_j, v.saff[(int64_t)u * D + acc.def_i], g.ddx, g.ddy, g.ddz, g.dist,
+					 g.ad);
 	});
-	v.pressure[s] = acc.p;
-
-	double4 p = make_double4(pi.x, pi.y, pi.z, 0.0); // spos4 holds pos[cur][s]
-	if (acc.mov_i)
-	{
-		double4 vel = make_double4(acc.vx, acc.vy, acc.vz, 0.0);
-		if (WALLS)
-			walls<DIMS>(v, R, p, acc.prm_i.x, acc.prm_i.w, vel);
-		if (SPRINGS)
-			spring_contract<DIMS>(v, cur, s, p, acc.def_i, vel);
-		double4 vp = v.vprev[s];
-		ab2<DIMS>(v.dt, p, vel, vp);
-		v.vprev[s] = vp;
-		if (VEL)
-			v.vel[s] = make_double4(0, 0, 0, 0);
-	}
-	v.pos[nxt][s] = p;
-	if (!(p.x == p.x && p.y == p.y && p.z == p.z))
-		atomicOr(v.err, ERR_NONFINITE);
-	if (to_remove<DIMS>(R, p, v.flags[s]))
-		append_bad(v, r, s - R.base);
+	finish_agent<DIMS, WALLS, SPRINGS, VEL>(v, R, r, cur, s, pi, acc.prm_i.x, acc.def_i, acc.mov_i, tail, acc.vx, acc.vy,
+											acc.vz, acc.p);
 }
 
 // ---------------------------------------------------------------------------
@@ -625,13 +692,10 @@ __device__ __forceinline__ void tile_home(const view& v, const rep_info& R, int 
 	acc.prm_i = qi;
 	unpack_bits(qi.w, acc.def_i, acc.mov_i);
 	acc.aff_i = A + (int64_t)self * D;
-	if (VEL && acc.mov_i)
-	{
-		const double4 v0 = v.vel[s];
-		acc.vx = v0.x;
-		acc.vy = v0.y;
-		acc.vz = v0.z;
-	}
+	const agent_tail tail = load_tail<WALLS, VEL>(v, s, acc.mov_i);
+	acc.vx = tail.vel0.x;
+	acc.vy = tail.vel0.y;
+	acc.vz = tail.vel0.z;
 
 	const int stride = blockDim.x;
 	int n = 0;
@@ -691,27 +755,8 @@ __device__ __forceinline__ void tile_home(const view& v, const rep_info& R, int 
 		}
 	}
 	flush();
-
-	v.pressure[s] = acc.p;
-	double4 p = make_double4(pi.x, pi.y, pi.z, 0.0);
-	if (acc.mov_i)
-	{
-		double4 vel = make_double4(acc.vx, acc.vy, acc.vz, 0.0);
-		if (WALLS)
-			walls<DIMS>(v, R, p, qi.x, v.prm[s].w, vel);
-		if (SPRINGS)
-			spring_contract<DIMS>(v, cur, s, p, acc.def_i, vel);
-		double4 vp = v.vprev[s];
-		ab2<DIMS>(v.dt, p, vel, vp);
-		v.vprev[s] = vp;
-		if (VEL)
-			v.vel[s] = make_double4(0, 0, 0, 0);
-	}
-	v.pos[cur ^ 1][s] = p;
-	if (!(p.x == p.x && p.y == p.y && p.z == p.z))
-		atomicOr(v.err, ERR_NONFINITE);
-	if (to_remove<DIMS>(R, p, v.flags[s]))
-		append_bad(v, r, s - R.base);
+	finish_agent<DIMS, WALLS, SPRINGS, VEL>(v, R, r, cur, s, pi, qi.x, acc.def_i, acc.mov_i, tail, acc.vx, acc.vy, acc.vz,
+											acc.p);
 }
 
 template <int DIMS, int B, bool WALLS, bool SPRINGS, bool VEL>
@@ -1493,8 +1538,9 @@ int launch_bin(ppc_state* s)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
 	k_bin_count<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	k_bin_reduce<<<s->v.ntiles, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
 	k_bin_scan<<<s->v.ntiles, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
-	k_bin_scatter<<<std::max(b, blocks_for(s->v.ntiles, kThreads)), kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+	k_bin_scatter<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
 	k_bin_fixup<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
