@@ -311,6 +311,31 @@ int ppc_get_launch_count(ppc_state* s, int64_t* launches);
 int ppc_set_profiling(ppc_state* s, int32_t on);
 int ppc_get_profile(ppc_state* s, double* fused_ms, int64_t* fused_launches);
 
+/* ---- binning without allocation ------------------------------------------ */
+
+/* Limits of the fixed scratch of ppc_bin_agents_noalloc (about 5.8 MB of
+ * device memory reserved on every GPU that loads the library). */
+#define PPC_NOALLOC_MAX_AGENTS 131072
+#define PPC_NOALLOC_MAX_VOXELS 1048576
+
+/* Mechanics-mesh binning for callers that cannot allocate device memory.
+ * No counterpart in the reference: it is ppc_update_mechanics_mesh followed
+ * by ppc_get_mesh_bins without a ppc_state, for code that must not call
+ * cudaMalloc (a framework allocator that forbids hidden allocations, a
+ * real-time loop that must not block in the driver's allocator).
+ * `positions` (count*dims doubles, AoS as in the reference), `voxel_counts`
+ * (one int32 per mechanics voxel) and `agents` (count int32) are the caller's
+ * device buffers; results match ppc_get_mesh_bins: per-voxel counts and the
+ * agents grouped by voxel, descending index inside a voxel. Scratch lives in
+ * one fixed device array; sizes above PPC_NOALLOC_MAX_AGENTS or
+ * PPC_NOALLOC_MAX_VOXELS return PPC_ERR_CAPACITY. Nothing is allocated. The
+ * first call on a device looks the array's address up for that device, so
+ * make that first call before any stream capture. All calls share the array:
+ * calls whose work overlaps on the GPU race. Work is queued on `cuda_stream`
+ * (NULL: the legacy default stream) and the call returns without waiting. */
+int ppc_bin_agents_noalloc(const ppc_mesh* mesh, const double* positions, int32_t count, int32_t* voxel_counts,
+						   int32_t* agents, void* cuda_stream);
+
 /* Message of the last error on the calling thread ("" if none). */
 const char* ppc_last_error(void);
 
