@@ -313,9 +313,11 @@ def run_ours(args, rank, world, local_rank):
     fused_avg_ms = fused_ms / max(fused_launches, 1)
     achieved = (per_agent * n0) / (fused_avg_ms / 1e3) / 1e9
     traffic = None
-    prof = os.path.join(ROOT, "profiles", f"fused_traffic_{args.workload}.json")
+    prof = os.path.join(ROOT, "profiles", f"k_fused_{args.workload}.md")
     if os.path.exists(prof):
-        traffic = _json.load(open(prof)).get("dram_bytes_per_launch")
+        for line in open(prof):
+            if line.startswith("| dram_bytes_per_launch |"):
+                traffic = float(line.split("|")[2])
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
