@@ -180,6 +180,78 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def fp32_form(args, mesh, params, a, ph, flush):
+    """The FP32-force form on the same workload and timing protocol, and its
+    error against the FP64 form after one step from the same state."""
+    import torch
+
+    from paraphysicell_b200.abi import PPC_FP32_FORCE, AgentArrays
+    from paraphysicell_b200.device import Simulation
+
+    def make(precision):
+        sim = Simulation(mesh, params, a.capacity, seed=1)
+        st = torch.cuda.Stream()
+        sim.set_stream(st.cuda_stream)
+        if precision:
+            sim.set_precision(precision)
+        sim.upload(a)
+        sim.update_mechanics_mesh()
+        return sim, st
+
+    def step(sim, k):
+        if ph:
+            sim.step_with_phenotype(k, ph[0], ph[1])
+        else:
+            sim.step(k)
+
+    def fetch(sim):
+        out = AgentArrays(0, a.dims, a.ndefs, a.capacity, a.spring_capacity)
+        out.count = out.capacity
+        sim.download(out, fields=("positions", "previous_velocities", "agent_ids"))
+        return out
+
+    s64, _ = make(0)
+    s32, st = make(PPC_FP32_FORCE)
+    step(s64, 1)
+    step(s32, 1)
+    g64, g32 = fetch(s64), fetch(s32)
+    v64, v32 = g64["previous_velocities"], g32["previous_velocities"]
+    norm = np.linalg.norm(v64, axis=1)
+    err = float(np.max(np.linalg.norm(v32 - v64, axis=1)) / max(np.max(norm), 1e-300))
+    s64.close()
+    K = args.steps
+    with torch.cuda.stream(st):
+        step(s32, max(args.warmup, 3))
+    s32.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    torch.cuda.synchronize()
+    s32.set_profiling(True)
+    with torch.cuda.stream(st):
+        for k in range(K):
+            flush.zero_()
+            starts[k].record(st)
+            step(s32, 1)
+            ends[k].record(st)
+    torch.cuda.synchronize()
+    fused_ms, fused_n = s32.profile()
+    s32.set_profiling(False)
+    total_ms = sum(x.elapsed_time(y) for x, y in zip(starts, ends))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(st):
+        e0.record(st)
+        step(s32, max(K, 10))
+        e1.record(st)
+    torch.cuda.synchronize()
+    steady = a.count * max(K, 10) / (e0.elapsed_time(e1) / 1e3)
+    s32.close()
+    return {"value": a.count * K / (total_ms / 1e3), "unit": UNIT, "ms_per_step": total_ms / K,
+            "steady_state": steady, "fused_avg_us": fused_ms / max(fused_n, 1) * 1e3,
+            "velocity_rel_err_vs_fp64": err,
+            "note": "pair forces in FP32 (Neumaier-compensated sums), exact FP64 neighbour predicate, FP64 "
+                    "positions/binning/integration; same L2-flushed protocol as value"}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -335,6 +407,8 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": int(launches),
         "clocks": sampler.summary() if sampler else None,
     }
+    if not args.no_forms:
+        line["forms"] = {"fp32_force": fp32_form(args, mesh, params, a, ph, flush)}
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(args.workload)
     print(json.dumps(line), flush=True)
@@ -351,6 +425,7 @@ def main():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="config3", choices=sorted(WORKLOADS))
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-forms", action="store_true", help="skip the FP32-force form's measurement")
     args = p.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -544,6 +545,16 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 		rep_info R {};
 		mesh_info(meshes[r], R, s->tile_b);
 		R.sc_base = (int32_t)s->total_sc;
+		{
+			// positions relative to the box minimum reach about the extent; the
+			// FP32 filter tolerates 16 float ulps of it per coordinate
+			double ext = 1.0;
+			for (int d = 0; d < dims; d++)
+				ext = std::max(ext, (double)(R.maxs[d] - R.mins[d]) + 2.0 * R.shape[d]);
+			int e2 = 0;
+			std::frexp(ext, &e2);
+			R.fmargin = (float)std::ldexp(16.0, e2 - 24);
+		}
 		s->total_sc += (int64_t)R.scg[0] * R.scg[1] * R.scg[2];
 		R.base = (int32_t)cap;
 		R.cap = capacities[r];
@@ -633,6 +644,9 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.skey, C));
 	try_(alloc(s, v.spos4, C));
 	try_(alloc(s, v.sprm4, C));
+	try_(alloc(s, v.sposf, C));
+	try_(alloc(s, v.sprmf, C));
+	try_(alloc(s, v.safff, C * s->ndefs));
 	try_(alloc(s, v.saff, C * s->ndefs));
 	try_(alloc(s, v.ncnt, C));
 	try_(alloc(s, v.nidx, C * s->ncap, false));
@@ -698,9 +712,12 @@ int ppc_set_precision(ppc_state* s, int32_t precision)
 {
 	if (!s || (precision != PPC_FP64 && precision != PPC_FP32_FORCE))
 		return fail(PPC_ERR_ARG, "precision must be PPC_FP64 or PPC_FP32_FORCE");
-	if (precision == PPC_FP32_FORCE)
-		return fail(PPC_ERR_UNSUPPORTED, "the FP32-force form is not built yet");
+	if (precision == PPC_FP32_FORCE && s->ndefs > 65535)
+		return fail(PPC_ERR_UNSUPPORTED, "the FP32-force form packs definition indices in 16 bits");
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
 	s->precision = precision;
+	s->v.f32 = precision == PPC_FP32_FORCE ? 1 : 0;
+	s->bins_valid = false; // the single-precision copies are written by the binning
 	release_graph(s);
 	return PPC_OK;
 }

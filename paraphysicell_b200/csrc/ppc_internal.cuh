@@ -54,6 +54,7 @@ struct rep_info
 	int32_t maxs_int[3], mins_int[3];
 	int32_t scg[3];	  // super-cell grid: ceil(grid / tile edge)
 	int32_t sc_base;  // first super-cell of this replicate in the global numbering
+	float fmargin;	  // bound on the FP32 distance error of positions relative to mins (um)
 };
 
 // per-replicate device counters
@@ -124,6 +125,11 @@ struct view
 	double4* spos4;
 	double4* sprm4;	// {radius, repulsion, adhesion, bits: def | movable << 32} in sorted order
 	double* saff;	// affinity rows in sorted order
+	// FP32-force form: key-ordered copies in single precision
+	int32_t f32;
+	float4* sposf;	// {x - min, y - min, z - min, rmad*radius}
+	float4* sprmf;	// {radius, repulsion, adhesion, bits: def | movable << 16 | springs << 24}
+	float* safff;	// affinity rows
 
 	int32_t* ncnt;
 	int32_t* nidx;

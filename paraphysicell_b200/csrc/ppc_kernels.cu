@@ -278,7 +278,8 @@ __global__ void k_bin_fixup(view v, int cur)
 	const double4 prm = v.prm[s];
 	double4 p = v.pos[cur][s];
 	const double rmad = v.rmad[s];
-	const long long bits = (long long)(uint32_t)v.def[s] | ((long long)v.movable[s] << 32);
+	const long long bits = (long long)(uint32_t)v.def[s] | ((long long)(v.movable[s] != 0) << 32)
+						   | ((long long)min(v.scnt[s], 255) << 40);
 	double aff[8];
 	const int D = v.ndefs;
 	for (int q = 0; q < D && q < 8; q++)
@@ -298,6 +299,17 @@ __global__ void k_bin_fixup(view v, int cur)
 	v.sprm4[t] = make_double4(prm.x, prm.y, prm.z, __longlong_as_double(bits));
 	for (int q = 0; q < D; q++)
 		v.saff[(int64_t)t * D + q] = q < 8 ? aff[q] : v.aff[(int64_t)s * D + q];
+	if (v.f32)
+	{
+		const rep_info& R = v.reps[r];
+		v.sposf[t] = make_float4((float)(p.x - R.mins[0]), (float)(p.y - R.mins[1]), (float)(p.z - R.mins[2]),
+								 (float)p.w);
+		const int fbits = (int)((uint32_t)(bits & 0xffff) | (uint32_t)((bits >> 32) & 1) << 16
+								| (uint32_t)((bits >> 40) & 0xff) << 24);
+		v.sprmf[t] = make_float4((float)prm.x, (float)prm.y, (float)prm.z, __int_as_float(fbits));
+		for (int q = 0; q < D; q++)
+			v.safff[(int64_t)t * D + q] = (float)(q < 8 ? aff[q] : v.aff[(int64_t)s * D + q]);
+	}
 }
 
 // ---------------------------------------------------------------------------
@@ -454,11 +466,23 @@ struct pair_fp64
 	}
 };
 
+// bits of sprm4.w: definition index (0..31), movable (32), spring count (40..47)
 __device__ __forceinline__ void unpack_bits(double w, int& def, bool& mov)
 {
 	const long long b = __double_as_longlong(w);
 	def = (int)(uint32_t)(b & 0xffffffffll);
-	mov = (b >> 32) != 0;
+	mov = ((b >> 32) & 1) != 0;
+}
+
+__device__ __forceinline__ int unpack_springs(double w) { return (int)((__double_as_longlong(w) >> 40) & 0xff); }
+
+// bits of sprmf.w: definition index (0..15), movable (16), spring count (24..31)
+__device__ __forceinline__ void unpack_fbits(float w, int& def, bool& mov, int& springs)
+{
+	const uint32_t b = (uint32_t)__float_as_int(w);
+	def = (int)(b & 0xffffu);
+	mov = ((b >> 16) & 1u) != 0;
+	springs = (int)(b >> 24);
 }
 
 // update_membrane_velocity (reference: solver_helper.h:14-28)
@@ -489,10 +513,9 @@ __device__ __forceinline__ void walls(const view& v, const rep_info& R, const do
 
 // spring_contract_function for one agent (reference: position_solver.cpp:337-370)
 template <int DIMS>
-__device__ __forceinline__ void spring_contract(const view& v, int cur, int s, const double4& pi, int def_i,
+__device__ __forceinline__ void spring_contract(const view& v, int cur, int s, int n, const double4& pi, int def_i,
 												double4& vel)
 {
-	const int n = v.scnt[s];
 	const double ec_i = v.ec[s];
 	const double* aff_i = v.aff + (int64_t)s * v.ndefs;
 	for (int k = 0; k < n; k++)
@@ -569,8 +592,8 @@ __device__ __forceinline__ agent_tail load_tail(const view& v, int s, bool mov)
 // the container-update marking
 template <int DIMS, bool WALLS, bool SPRINGS, bool VEL>
 __device__ __forceinline__ void finish_agent(const view& v, const rep_info& R, int r, int cur, int s, const double4& pi,
-											 double radius, int def_i, bool mov_i, const agent_tail& tail, double vx,
-											 double vy, double vz, double pressure)
+											 double radius, int def_i, bool mov_i, int nspr, const agent_tail& tail,
+											 double vx, double vy, double vz, double pressure)
 {
 	double4 p = make_double4(pi.x, pi.y, pi.z, 0.0);
 	double4 vp = tail.vprev;
@@ -579,8 +602,8 @@ __device__ __forceinline__ void finish_agent(const view& v, const rep_info& R, i
 		double4 vel = make_double4(vx, vy, vz, 0.0);
 		if (WALLS)
 			walls<DIMS>(v, R, p, radius, tail.bm, vel);
-		if (SPRINGS)
-			spring_contract<DIMS>(v, cur, s, p, def_i, vel);
+		if (SPRINGS && nspr > 0)
+			spring_contract<DIMS>(v, cur, s, nspr, p, def_i, vel);
 		ab2<DIMS>(v.dt, p, vel, vp);
 	}
 	v.pressure[s] = pressure;
@@ -635,8 +658,177 @@ __global__ void __launch_bounds__(256) k_fused(view v, int cur)
 		acc.add_pair(qj.x, qj.y, qj.z, def_j, mov_j, v.saff[(int64_t)u * D + acc.def_i], g.ddx, g.ddy, g.ddz, g.dist,
 					 g.ad);
 	});
-	finish_agent<DIMS, WALLS, SPRINGS, VEL>(v, R, r, cur, s, pi, acc.prm_i.x, acc.def_i, acc.mov_i, tail, acc.vx, acc.vy,
-											acc.vz, acc.p);
+	finish_agent<DIMS, WALLS, SPRINGS, VEL>(v, R, r, cur, s, pi, acc.prm_i.x, acc.def_i, acc.mov_i,
+											unpack_springs(acc.prm_i.w), tail, acc.vx, acc.vy, acc.vz, acc.p);
+}
+
+// ---------------------------------------------------------------------------
+// FP32-force form of the fused pass. Neighbour sets stay exact: a single
+// precision filter on positions relative to the box minimum rejects far
+// candidates with a margin of 16 float ulps of the domain extent, and the
+// candidates it keeps go through the FP64 predicate. The pair arithmetic
+// (distance, sqrt, potentials, force) runs in FP32 on the FP64 difference
+// rounded to FP32, and the per-agent sums of velocity and pressure are
+// Neumaier-compensated (A. Neumaier, ZAMM 54, 1974). Membrane, springs and
+// the Adams-Bashforth update stay FP64.
+// ---------------------------------------------------------------------------
+
+struct nsum
+{
+	float s = 0.f, c = 0.f;
+	__device__ __forceinline__ void add(float x)
+	{
+		const float t = s + x;
+		if (fabsf(s) >= fabsf(x))
+			c += (s - t) + x;
+		else
+			c += (x - t) + s;
+		s = t;
+	}
+	__device__ __forceinline__ double value() const { return (double)s + (double)c; }
+};
+
+struct pair_fp32
+{
+	float r_i, rep_i, adh_i;
+	const float* aff_i;
+	int def_i;
+	bool mov_i;
+	nsum vx, vy, vz, p;
+
+	__device__ __forceinline__ void add(float r_j, float rep_j, float adh_j, int def_j, bool mov_j, float aff_ji,
+										float dx, float dy, float dz, float dist, float ad)
+	{
+		const float d = dist < 0.00001f ? 0.00001f : dist;
+		float rep = 1.f - d / (r_i + r_j);
+		rep = rep < 0.f ? 0.f : rep;
+		rep = rep * rep;
+		const float term = rep * 36.64504274775163f;
+		if (mov_i)
+			p.add(term);
+		if (mov_j)
+			p.add(term);
+		if (!mov_i)
+			return;
+		rep = rep * sqrtf(rep_i * rep_j);
+		float adh = 1.f - d / ad;
+		adh = adh * adh;
+		adh = adh * sqrtf(adh_i * adh_j * aff_i[def_j] * aff_ji);
+		const float force = (rep - adh) / d;
+		vx.add(force * dx);
+		vy.add(force * dy);
+		vz.add(force * dz);
+	}
+};
+
+template <int DIMS, bool WALLS, bool SPRINGS, bool VEL>
+__global__ void __launch_bounds__(256) k_fused_f32(view v, int cur)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= *v.cursor)
+		return;
+	const int s = v.sorted[t];
+	const int r = rep_of(v, s);
+	const rep_info& R = v.reps[r];
+	const double4 pi = v.spos4[t];
+	const float4 pf = v.sposf[t];
+	const float4 qf = v.sprmf[t];
+	const int D = v.ndefs;
+	pair_fp32 acc;
+	int nspr;
+	unpack_fbits(qf.w, acc.def_i, acc.mov_i, nspr);
+	acc.r_i = qf.x;
+	acc.rep_i = qf.y;
+	acc.adh_i = qf.z;
+	acc.aff_i = v.safff + (int64_t)t * D;
+	const agent_tail tail = load_tail<WALLS, VEL>(v, s, acc.mov_i);
+	const float m = R.fmargin;
+
+	const int32_t lk = v.skey[t] - (int32_t)R.vox_base;
+	const int g0 = R.grid[0], g1 = R.grid[1], g2 = R.grid[2];
+	const int cx = lk % g0, cy = (lk / g0) % g1, cz = lk / (g0 * g1);
+	const int xlo = cx > 0 ? cx - 1 : 0;
+	const int xhi = cx + 1 < g0 ? cx + 1 : g0 - 1;
+	constexpr int NR = DIMS == 3 ? 9 : (DIMS == 2 ? 3 : 1);
+	int lo[NR], hi[NR];
+#pragma unroll
+	for (int k = 0; k < NR; k++)
+	{
+		const int dz = DIMS == 3 ? k / 3 - 1 : 0;
+		const int dy = DIMS >= 2 ? k % 3 - 1 : 0;
+		const int z = cz + dz, y = cy + dy;
+		const bool ok = z >= 0 && z < g2 && y >= 0 && y < g1;
+		const int64_t row = R.vox_base + (int64_t)g0 * (y + (int64_t)g1 * z);
+		lo[k] = ok ? v.vstart[row + xlo] : 0;
+		hi[k] = ok ? v.vstart[row + xhi + 1] : 0;
+	}
+	__shared__ int32_t list[kList * 256];
+	int32_t* lst = list + threadIdx.x;
+	const int stride = blockDim.x;
+	int n = 0;
+	auto flush = [&]() {
+		for (int q = 0; q < n; q++)
+		{
+			const int u = lst[q * stride];
+			const pair_geometry<DIMS> g(v, pi, u);
+			const float dx = (float)g.ddx, dy = (float)g.ddy, dz = (float)g.ddz;
+			float d2 = dx * dx;
+			if (DIMS >= 2)
+				d2 = d2 + dy * dy;
+			if (DIMS >= 3)
+				d2 = d2 + dz * dz;
+			const float dist = DIMS == 1 ? fabsf(dx) : sqrtf(d2);
+			const float4 qj = v.sprmf[u];
+			const float4 pj = v.sposf[u];
+			int def_j, spr_j;
+			bool mov_j;
+			unpack_fbits(qj.w, def_j, mov_j, spr_j);
+			acc.add(qj.x, qj.y, qj.z, def_j, mov_j, v.safff[(int64_t)u * D + acc.def_i], dx, dy, dz, dist, pf.w + pj.w);
+		}
+		n = 0;
+	};
+#pragma unroll
+	for (int k = 0; k < NR; k++)
+	{
+		for (int u = lo[k]; u < hi[k]; u++)
+		{
+			if (u == t)
+				continue;
+			const float4 c = v.sposf[u];
+			const float dxf = pf.x - c.x;
+			const float dyf = DIMS >= 2 ? pf.y - c.y : 0.f;
+			const float dzf = DIMS >= 3 ? pf.z - c.z : 0.f;
+			float d2f = dxf * dxf;
+			if (DIMS >= 2)
+				d2f = d2f + dyf * dyf;
+			if (DIMS >= 3)
+				d2f = d2f + dzf * dzf;
+			const float adf = pf.w + c.w + m;
+			if (d2f > adf * adf * 1.00001f)
+				continue;
+			// exact FP64 predicate for the candidates the filter keeps
+			const double4 q = v.spos4[u];
+			const double ddx = pi.x - q.x;
+			const double ddy = DIMS >= 2 ? pi.y - q.y : 0.0;
+			const double ddz = DIMS >= 3 ? pi.z - q.z : 0.0;
+			double d2 = ddx * ddx;
+			if (DIMS >= 2)
+				d2 = d2 + ddy * ddy;
+			if (DIMS >= 3)
+				d2 = d2 + ddz * ddz;
+			const double ad = pi.w + q.w;
+			const double dist = DIMS == 1 ? fabs(ddx) : sqrt(d2);
+			if (!(dist <= ad))
+				continue;
+			lst[n * stride] = u;
+			if (++n == kList)
+				flush();
+		}
+	}
+	flush();
+	finish_agent<DIMS, WALLS, SPRINGS, VEL>(v, R, r, cur, s, pi, (double)acc.r_i, acc.def_i, acc.mov_i, nspr, tail,
+											tail.vel0.x + acc.vx.value(), tail.vel0.y + acc.vy.value(),
+											tail.vel0.z + acc.vz.value(), acc.p.value());
 }
 
 // ---------------------------------------------------------------------------
@@ -755,8 +947,8 @@ __device__ __forceinline__ void tile_home(const view& v, const rep_info& R, int 
 		}
 	}
 	flush();
-	finish_agent<DIMS, WALLS, SPRINGS, VEL>(v, R, r, cur, s, pi, qi.x, acc.def_i, acc.mov_i, tail, acc.vx, acc.vy, acc.vz,
-											acc.p);
+	finish_agent<DIMS, WALLS, SPRINGS, VEL>(v, R, r, cur, s, pi, qi.x, acc.def_i, acc.mov_i, unpack_springs(qi.w), tail,
+											acc.vx, acc.vy, acc.vz, acc.p);
 }
 
 template <int DIMS, int B, bool WALLS, bool SPRINGS, bool VEL>
@@ -998,7 +1190,7 @@ __global__ void k_springs(view v, int cur)
 	if (!live(v, s, r, local) || v.movable[s] == 0 || v.scnt[s] == 0)
 		return;
 	double4 vel = v.vel[s];
-	spring_contract<DIMS>(v, cur, s, v.pos[cur][s], v.def[s], vel);
+	spring_contract<DIMS>(v, cur, s, v.scnt[s], v.pos[cur][s], v.def[s], vel);
 	v.vel[s] = vel;
 }
 
@@ -1672,9 +1864,15 @@ static void fused_dispatch(ppc_state* s, int b)
 	cudaStream_t st = PPC_LAUNCH(s);
 	const int nt = s->tile_threads;
 	b = blocks_for(s->total_cap, nt);
+	const bool f32 = s->precision == PPC_FP32_FORCE;
 #define PPC_FUSED(W, S, V)                                                                                             \
 	if (walls == W && springs == S && vel == V)                                                                        \
-		k_fused<DIMS, W, S, V><<<b, nt, 0, st>>>(s->v, s->cur);
+	{                                                                                                                  \
+		if (f32)                                                                                                       \
+			k_fused_f32<DIMS, W, S, V><<<b, nt, 0, st>>>(s->v, s->cur);                                                \
+		else                                                                                                           \
+			k_fused<DIMS, W, S, V><<<b, nt, 0, st>>>(s->v, s->cur);                                                    \
+	}
 	PPC_FUSED(false, false, false)
 	PPC_FUSED(false, false, true)
 	PPC_FUSED(false, true, false)
@@ -1705,7 +1903,7 @@ int launch_fused(ppc_state* s)
 		ev_end = s->prof_events[s->prof_used + 1];
 		s->prof_used += 2;
 	}
-	if (s->tile_b > 0)
+	if (s->tile_b > 0 && s->precision == PPC_FP64)
 	{
 		int rc = s->dims == 1 ? tile_by_edge<1>(s) : (s->dims == 2 ? tile_by_edge<2>(s) : tile_by_edge<3>(s));
 		if (rc != PPC_OK)
