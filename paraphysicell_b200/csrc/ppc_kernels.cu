@@ -18,6 +18,13 @@ constexpr int kSortCap = 4096; // list length sorted in shared memory
 constexpr int kTileShift = 12; // voxels per scan tile = 4096 = kThreads * kTileItems
 constexpr int kTileItems = 16;
 
+// Programmatic dependent launch: every kernel of the library is launched
+// with programmatic stream serialisation, so its launch and block
+// scheduling overlap the tail of the kernel before it, and waits here, before
+// its first memory access, until that kernel has finished and its writes are
+// visible. Launched without the attribute, the wait returns at once.
+__device__ __forceinline__ void grid_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ int rep_of(const view& v, int s) { return v.nreps == 1 ? 0 : v.rid[s]; }
 
 __device__ __forceinline__ double comp(const double4& p, int d) { return d == 0 ? p.x : (d == 1 ? p.y : p.z); }
@@ -109,6 +116,7 @@ __device__ __forceinline__ int block_exclusive_scan(int x, int& total)
 
 __global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur)
 {
+	grid_wait();
 	const int s = blockIdx.x * blockDim.x + threadIdx.x;
 	const uint32_t e = *v.epoch + 1;
 	if (s == 0)
@@ -162,6 +170,7 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur)
 // per-tile totals of the voxel counts (one block per tile of 4096 voxels)
 __global__ void __launch_bounds__(kThreads) k_bin_reduce(view v)
 {
+	grid_wait();
 	const int b = blockIdx.x;
 	const int64_t i0 = ((int64_t)b << kTileShift) + (int64_t)threadIdx.x * kTileItems;
 	int sum = 0;
@@ -183,6 +192,7 @@ __global__ void __launch_bounds__(kThreads) k_bin_reduce(view v)
 // it. The counts are cleared at occupied voxels by k_bin_fixup.
 __global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
 {
+	grid_wait();
 	const int b = blockIdx.x;
 	int part = 0;
 	for (int k = threadIdx.x; k < b; k += blockDim.x)
@@ -253,6 +263,7 @@ __global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
 
 __global__ void k_bin_scatter(view v)
 {
+	grid_wait();
 	int s = blockIdx.x * blockDim.x + threadIdx.x;
 	if (s == 0)
 		*v.epoch += 1;
@@ -268,6 +279,7 @@ __global__ void k_bin_scatter(view v)
 // a serial run of the reference's fetch_sub scatter produces
 __global__ void k_bin_fixup(view v, int cur)
 {
+	grid_wait();
 	int s = blockIdx.x * blockDim.x + threadIdx.x;
 	if (s >= v.total_cap)
 		return;
@@ -630,6 +642,7 @@ __device__ __forceinline__ void finish_agent(const view& v, const rep_info& R, i
 template <int DIMS, bool WALLS, bool SPRINGS, bool VEL>
 __global__ void __launch_bounds__(256) k_fused(view v, int cur)
 {
+	grid_wait();
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= *v.cursor)
 		return;
@@ -724,6 +737,7 @@ struct pair_fp32
 template <int DIMS, bool WALLS, bool SPRINGS, bool VEL>
 __global__ void __launch_bounds__(256) k_fused_f32(view v, int cur)
 {
+	grid_wait();
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= *v.cursor)
 		return;
@@ -954,6 +968,7 @@ __device__ __forceinline__ void tile_home(const view& v, const rep_info& R, int 
 template <int DIMS, int B, bool WALLS, bool SPRINGS, bool VEL>
 __global__ void __launch_bounds__(kTileThreadsMax) k_fused_tile(view v, int cur, int cap)
 {
+	grid_wait();
 	using G = tile_geom<DIMS, B>;
 	constexpr int H = G::H, NROW = G::NROW, NCORE = G::NCORE;
 	extern __shared__ double4 dyn[];
@@ -1083,6 +1098,7 @@ __global__ void __launch_bounds__(kTileThreadsMax) k_fused_tile(view v, int cur,
 template <int DIMS>
 __global__ void __launch_bounds__(kThreads) k_neighbors(view v)
 {
+	grid_wait();
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= *v.cursor)
 		return;
@@ -1109,6 +1125,7 @@ __global__ void __launch_bounds__(kThreads) k_neighbors(view v)
 
 __global__ void k_clear_pressure(view v)
 {
+	grid_wait();
 	int s = blockIdx.x * blockDim.x + threadIdx.x;
 	if (s >= v.total_cap)
 		return;
@@ -1125,6 +1142,7 @@ __global__ void k_clear_pressure(view v)
 template <int DIMS>
 __global__ void __launch_bounds__(kThreads) k_forces(view v, int cur)
 {
+	grid_wait();
 	const int s = blockIdx.x * blockDim.x + threadIdx.x;
 	if (s >= v.total_cap)
 		return;
@@ -1168,6 +1186,7 @@ __global__ void __launch_bounds__(kThreads) k_forces(view v, int cur)
 template <int DIMS>
 __global__ void k_membrane(view v, int cur)
 {
+	grid_wait();
 	const int s = blockIdx.x * blockDim.x + threadIdx.x;
 	if (s >= v.total_cap)
 		return;
@@ -1183,6 +1202,7 @@ __global__ void k_membrane(view v, int cur)
 template <int DIMS>
 __global__ void k_springs(view v, int cur)
 {
+	grid_wait();
 	const int s = blockIdx.x * blockDim.x + threadIdx.x;
 	if (s >= v.total_cap)
 		return;
@@ -1197,6 +1217,7 @@ __global__ void k_springs(view v, int cur)
 template <int DIMS>
 __global__ void k_positions(view v, int cur)
 {
+	grid_wait();
 	const int s = blockIdx.x * blockDim.x + threadIdx.x;
 	if (s >= v.total_cap)
 		return;
@@ -1221,6 +1242,7 @@ __global__ void k_positions(view v, int cur)
 template <int DIMS>
 __global__ void k_mark_remove(view v, int cur)
 {
+	grid_wait();
 	const int s = blockIdx.x * blockDim.x + threadIdx.x;
 	if (s >= v.total_cap)
 		return;
@@ -1356,6 +1378,7 @@ __device__ void springs_rename_attached(const view& v, int old_slot, int new_slo
 // the spring rows in the reference's order.
 __global__ void k_compact_plan(view v, int phenotype_pass, int springs)
 {
+	grid_wait();
 	__shared__ int32_t sh[kSortCap];
 	const int r = blockIdx.x;
 	rep_counters& C = v.ctr[r];
@@ -1430,6 +1453,7 @@ __global__ void k_compact_plan(view v, int phenotype_pass, int springs)
 template <int DIMS>
 __global__ void k_compact_apply(view v, int cur)
 {
+	grid_wait();
 	const int r = blockIdx.y;
 	const int nm = v.nmoves[r];
 	const int base = v.reps[r].base;
@@ -1470,6 +1494,7 @@ __global__ void k_compact_apply(view v, int cur)
 // p_divide, from the counter-based draws of (seed, epoch, replicate, index)
 __global__ void k_flag_by_draws(view v, double p_divide, double p_death)
 {
+	grid_wait();
 	const int s = blockIdx.x * blockDim.x + threadIdx.x;
 	if (s >= v.total_cap)
 		return;
@@ -1485,6 +1510,7 @@ __global__ void k_flag_by_draws(view v, double p_divide, double p_death)
 
 __global__ void k_bump_draw_epoch(view v)
 {
+	grid_wait();
 	const int r = blockIdx.x * blockDim.x + threadIdx.x;
 	if (r < v.nreps)
 		v.draw_epoch[r]++;
@@ -1492,6 +1518,7 @@ __global__ void k_bump_draw_epoch(view v)
 
 __global__ void k_mark_divide(view v)
 {
+	grid_wait();
 	const int s = blockIdx.x * blockDim.x + threadIdx.x;
 	if (s >= v.total_cap)
 		return;
@@ -1514,6 +1541,7 @@ __global__ void k_mark_divide(view v)
 // (cell::divide, reference: src/cell.cpp:110-114).
 __global__ void k_divide_plan(view v, int springs)
 {
+	grid_wait();
 	__shared__ int32_t sh[kSortCap];
 	const int r = blockIdx.x;
 	rep_counters& C = v.ctr[r];
@@ -1544,6 +1572,7 @@ __global__ void k_divide_plan(view v, int springs)
 template <int DIMS>
 __global__ void k_divide_apply(view v, int cur)
 {
+	grid_wait();
 	const int r = blockIdx.y;
 	rep_counters& C = v.ctr[r];
 	const int nd = C.ndiv;
@@ -1625,6 +1654,7 @@ __global__ void k_divide_apply(view v, int cur)
 
 __global__ void k_divide_finish(view v)
 {
+	grid_wait();
 	const int r = blockIdx.x * blockDim.x + threadIdx.x;
 	if (r >= v.nreps)
 		return;
@@ -1642,6 +1672,7 @@ __global__ void k_divide_finish(view v)
 
 __global__ void k_unpack_vec(view v, double4* dst, const double* src, int base, int n)
 {
+	grid_wait();
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 		return;
@@ -1653,6 +1684,7 @@ __global__ void k_unpack_vec(view v, double4* dst, const double* src, int base, 
 
 __global__ void k_pack_vec(view v, double* dst, const double4* src, int base, int n)
 {
+	grid_wait();
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 		return;
@@ -1663,6 +1695,7 @@ __global__ void k_pack_vec(view v, double* dst, const double4* src, int base, in
 
 __global__ void k_unpack_prm(view v, int field, const double* src, int base, int n)
 {
+	grid_wait();
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 		return;
@@ -1672,6 +1705,7 @@ __global__ void k_unpack_prm(view v, int field, const double* src, int base, int
 
 __global__ void k_pack_prm(view v, int field, double* dst, int base, int n)
 {
+	grid_wait();
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 		return;
@@ -1680,6 +1714,7 @@ __global__ void k_pack_prm(view v, int field, double* dst, int base, int n)
 
 __global__ void k_neighbors_local(view v, int base, int n, int32_t* counts, int32_t* lists, int cap)
 {
+	grid_wait();
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 		return;
@@ -1694,6 +1729,7 @@ __global__ void k_neighbors_local(view v, int base, int n, int32_t* counts, int3
 // rows: [n * cap] local indices in host layout; to_device converts to slots
 __global__ void k_springs_local(view v, int base, int n, int32_t* rows, int cap, int to_device)
 {
+	grid_wait();
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 		return;
@@ -1718,6 +1754,23 @@ __global__ void k_springs_local(view v, int base, int n, int32_t* rows, int cap,
 // launchers
 // ---------------------------------------------------------------------------
 
+
+template <typename... KArgs, typename... Args>
+static void pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args)
+{
+	cudaLaunchConfig_t cfg {};
+	cfg.gridDim = grid;
+	cfg.blockDim = block;
+	cfg.dynamicSmemBytes = smem;
+	cfg.stream = st;
+	cudaLaunchAttribute at[1];
+	at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	at[0].val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = at;
+	cfg.numAttrs = 1;
+	cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 #define PPC_CHECK_LAUNCH()                                                                                             \
 	do                                                                                                                 \
 	{                                                                                                                  \
@@ -1729,11 +1782,11 @@ __global__ void k_springs_local(view v, int base, int n, int32_t* rows, int cap,
 int launch_bin(ppc_state* s)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
-	k_bin_count<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
-	k_bin_reduce<<<s->v.ntiles, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
-	k_bin_scan<<<s->v.ntiles, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
-	k_bin_scatter<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
-	k_bin_fixup<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+	pdl(k_bin_count, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
+	pdl(k_bin_reduce, s->v.ntiles, kThreads, 0, PPC_LAUNCH(s), s->v);
+	pdl(k_bin_scan, s->v.ntiles, kThreads, 0, PPC_LAUNCH(s), s->v);
+	pdl(k_bin_scatter, b, kThreads, 0, PPC_LAUNCH(s), s->v);
+	pdl(k_bin_fixup, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -1742,11 +1795,11 @@ int launch_neighbors(ppc_state* s)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
 	if (s->dims == 1)
-		k_neighbors<1><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+		pdl(k_neighbors<1>, b, kThreads, 0, PPC_LAUNCH(s), s->v);
 	else if (s->dims == 2)
-		k_neighbors<2><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+		pdl(k_neighbors<2>, b, kThreads, 0, PPC_LAUNCH(s), s->v);
 	else
-		k_neighbors<3><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+		pdl(k_neighbors<3>, b, kThreads, 0, PPC_LAUNCH(s), s->v);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -1754,13 +1807,13 @@ int launch_neighbors(ppc_state* s)
 int launch_forces(ppc_state* s)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
-	k_clear_pressure<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+	pdl(k_clear_pressure, b, kThreads, 0, PPC_LAUNCH(s), s->v);
 	if (s->dims == 1)
-		k_forces<1><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_forces<1>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	else if (s->dims == 2)
-		k_forces<2><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_forces<2>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	else
-		k_forces<3><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_forces<3>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -1769,11 +1822,11 @@ int launch_membrane(ppc_state* s)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
 	if (s->dims == 1)
-		k_membrane<1><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_membrane<1>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	else if (s->dims == 2)
-		k_membrane<2><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_membrane<2>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	else
-		k_membrane<3><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_membrane<3>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -1782,11 +1835,11 @@ int launch_springs(ppc_state* s)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
 	if (s->dims == 1)
-		k_springs<1><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_springs<1>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	else if (s->dims == 2)
-		k_springs<2><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_springs<2>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	else
-		k_springs<3><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_springs<3>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -1795,11 +1848,11 @@ int launch_positions(ppc_state* s)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
 	if (s->dims == 1)
-		k_positions<1><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_positions<1>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	else if (s->dims == 2)
-		k_positions<2><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_positions<2>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	else
-		k_positions<3><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_positions<3>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -1831,7 +1884,7 @@ static int tile_dispatch(ppc_state* s)
 	int per_sm = 0;
 	PPC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, s->tile_threads, dyn));
 	const int blocks = std::max(1, per_sm) * s->sm_count;
-	k<<<blocks, s->tile_threads, dyn, st>>>(s->v, s->cur, cap);
+	pdl(k, blocks, s->tile_threads, dyn, st, s->v, s->cur, cap);
 	return PPC_OK;
 }
 
@@ -1869,9 +1922,9 @@ static void fused_dispatch(ppc_state* s, int b)
 	if (walls == W && springs == S && vel == V)                                                                        \
 	{                                                                                                                  \
 		if (f32)                                                                                                       \
-			k_fused_f32<DIMS, W, S, V><<<b, nt, 0, st>>>(s->v, s->cur);                                                \
+			pdl(k_fused_f32<DIMS, W, S, V>, b, nt, 0, st, s->v, s->cur);                                                \
 		else                                                                                                           \
-			k_fused<DIMS, W, S, V><<<b, nt, 0, st>>>(s->v, s->cur);                                                    \
+			pdl(k_fused<DIMS, W, S, V>, b, nt, 0, st, s->v, s->cur);                                                    \
 	}
 	PPC_FUSED(false, false, false)
 	PPC_FUSED(false, false, true)
@@ -1926,14 +1979,14 @@ int launch_fused(ppc_state* s)
 int launch_compact(ppc_state* s, bool phenotype_pass)
 {
 	const int springs = s->has_springs ? 1 : 0;
-	k_compact_plan<<<s->nreps, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, phenotype_pass ? 1 : 0, springs);
+	pdl(k_compact_plan, s->nreps, kThreads, 0, PPC_LAUNCH(s), s->v, phenotype_pass ? 1 : 0, springs);
 	dim3 g(std::max(1, std::min(64, blocks_for(s->total_cap / std::max(1, s->nreps), kThreads))), s->nreps);
 	if (s->dims == 1)
-		k_compact_apply<1><<<g, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_compact_apply<1>, g, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	else if (s->dims == 2)
-		k_compact_apply<2><<<g, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_compact_apply<2>, g, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	else
-		k_compact_apply<3><<<g, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_compact_apply<3>, g, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -1942,11 +1995,11 @@ int launch_mark_remove(ppc_state* s)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
 	if (s->dims == 1)
-		k_mark_remove<1><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_mark_remove<1>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	else if (s->dims == 2)
-		k_mark_remove<2><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_mark_remove<2>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	else
-		k_mark_remove<3><<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_mark_remove<3>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -1955,16 +2008,16 @@ int launch_divide(ppc_state* s)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
 	const int springs = s->has_springs ? 1 : 0;
-	k_mark_divide<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
-	k_divide_plan<<<s->nreps, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, springs);
+	pdl(k_mark_divide, b, kThreads, 0, PPC_LAUNCH(s), s->v);
+	pdl(k_divide_plan, s->nreps, kThreads, 0, PPC_LAUNCH(s), s->v, springs);
 	dim3 g(std::max(1, std::min(64, blocks_for(s->total_cap / std::max(1, s->nreps), kThreads))), s->nreps);
 	if (s->dims == 1)
-		k_divide_apply<1><<<g, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_divide_apply<1>, g, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	else if (s->dims == 2)
-		k_divide_apply<2><<<g, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
+		pdl(k_divide_apply<2>, g, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	else
-		k_divide_apply<3><<<g, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->cur);
-	k_divide_finish<<<blocks_for(s->nreps, kThreads), kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+		pdl(k_divide_apply<3>, g, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
+	pdl(k_divide_finish, blocks_for(s->nreps, kThreads), kThreads, 0, PPC_LAUNCH(s), s->v);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -1972,8 +2025,8 @@ int launch_divide(ppc_state* s)
 int launch_flag_by_draws(ppc_state* s, double p_divide, double p_death)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
-	k_flag_by_draws<<<b, kThreads, 0, PPC_LAUNCH(s)>>>(s->v, p_divide, p_death);
-	k_bump_draw_epoch<<<blocks_for(s->nreps, kThreads), kThreads, 0, PPC_LAUNCH(s)>>>(s->v);
+	pdl(k_flag_by_draws, b, kThreads, 0, PPC_LAUNCH(s), s->v, p_divide, p_death);
+	pdl(k_bump_draw_epoch, blocks_for(s->nreps, kThreads), kThreads, 0, PPC_LAUNCH(s), s->v);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -1982,7 +2035,7 @@ int launch_unpack_vec(ppc_state* s, double4* dst, const double* src, int32_t r, 
 {
 	if (n == 0)
 		return PPC_OK;
-	k_unpack_vec<<<blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s)>>>(s->v, dst, src, s->reps[r].base, n);
+	pdl(k_unpack_vec, blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s), s->v, dst, src, s->reps[r].base, n);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -1991,7 +2044,7 @@ int launch_pack_vec(ppc_state* s, double* dst, const double4* src, int32_t r, in
 {
 	if (n == 0)
 		return PPC_OK;
-	k_pack_vec<<<blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s)>>>(s->v, dst, src, s->reps[r].base, n);
+	pdl(k_pack_vec, blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s), s->v, dst, src, s->reps[r].base, n);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -2000,7 +2053,7 @@ int launch_unpack_prm(ppc_state* s, int field, const double* src, int32_t r, int
 {
 	if (n == 0)
 		return PPC_OK;
-	k_unpack_prm<<<blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s)>>>(s->v, field, src, s->reps[r].base, n);
+	pdl(k_unpack_prm, blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s), s->v, field, src, s->reps[r].base, n);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -2009,7 +2062,7 @@ int launch_pack_prm(ppc_state* s, int field, double* dst, int32_t r, int32_t n)
 {
 	if (n == 0)
 		return PPC_OK;
-	k_pack_prm<<<blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s)>>>(s->v, field, dst, s->reps[r].base, n);
+	pdl(k_pack_prm, blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s), s->v, field, dst, s->reps[r].base, n);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -2018,7 +2071,7 @@ int launch_neighbors_local(ppc_state* s, int32_t r, int32_t n, int32_t* counts, 
 {
 	if (n == 0)
 		return PPC_OK;
-	k_neighbors_local<<<blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->reps[r].base, n, counts,
+	pdl(k_neighbors_local, blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s), s->v, s->reps[r].base, n, counts,
 																			 lists, cap);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
@@ -2028,7 +2081,7 @@ int launch_springs_local(ppc_state* s, int32_t r, int32_t n, int32_t* rows, int3
 {
 	if (n == 0)
 		return PPC_OK;
-	k_springs_local<<<blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s)>>>(s->v, s->reps[r].base, n, rows, cap,
+	pdl(k_springs_local, blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s), s->v, s->reps[r].base, n, rows, cap,
 																		   to_device);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
