@@ -170,10 +170,13 @@ int ppc_set_precision(ppc_state* s, int32_t precision);
  * per-thread mt19937 (src/random.cpp:8-49) for division directions. */
 int ppc_set_random_seed(ppc_state* s, uint64_t seed);
 
-/* Launch shape of the fused force pass: `tile_edge` > 0 stages super-cells of
- * tile_edge^dims voxels in shared memory (2, 3, 4, 6 or 8; `smem_bytes` of
- * staging per block), 0 runs one thread per agent; `threads` per block
- * (32..256). Results do not depend on the shape. Invalidates the mesh. */
+/* Launch shape of the fused force pass (one thread per agent): `tile_edge` -1
+ * (the default) reads the candidates from global memory; 0 stages each
+ * block's candidate ranges in `smem_bytes` of shared memory per block
+ * (32 KiB is a good budget; a block whose ranges do not fit reads global
+ * memory), `threads` per block capped at 128 — faster where agents are dense
+ * (about one per voxel), slower where they are sparse. `threads` 32..256, a
+ * multiple of 32. Results do not depend on the shape. */
 int ppc_set_launch_shape(ppc_state* s, int32_t tile_edge, int32_t threads, int32_t smem_bytes);
 
 /* Neighbour-list capacity per agent for ppc_update_cell_neighbors (default 64). */

@@ -19,7 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libppc.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "--expt-relaxed-constexpr",
-         "-Xcompiler", "-fPIC,-O2", "-shared"]
+         "-Xcompiler", "-fPIC,-O2"]
+OBJDIR = os.path.join(HERE, "_build")
 
 
 def nvcc():
@@ -46,10 +47,23 @@ def stale():
 
 
 def build(verbose=False, extra=()):
-    cmd = [nvcc(), *ARCH, *FLAGS, *extra, "-o", LIB, *sources(), "-lcudart"]
+    """Compiles every source to an object in parallel, then links them."""
+    os.makedirs(OBJDIR, exist_ok=True)
+    jobs, objs = [], []
+    for src in sources():
+        obj = os.path.join(OBJDIR, os.path.basename(src) + ".o")
+        cmd = [nvcc(), *ARCH, *FLAGS, *extra, "-c", "-o", obj, src]
+        if verbose:
+            print(" ".join(cmd))
+        jobs.append((cmd, subprocess.Popen(cmd)))
+        objs.append(obj)
+    failed = [cmd for cmd, p in jobs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
+    link = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        print(" ".join(link))
+    subprocess.run(link, check=True)
     return LIB
 
 

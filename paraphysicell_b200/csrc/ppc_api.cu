@@ -480,7 +480,7 @@ int run_steps(ppc_state* s, int32_t steps, bool phenotype, double p_divide, doub
 	return PPC_OK;
 }
 
-void mesh_info(const ppc_mesh& m, rep_info& R, int tile_b = 0)
+void mesh_info(const ppc_mesh& m, rep_info& R)
 {
 	R.voxels = 1;
 	for (int d = 0; d < 3; d++)
@@ -495,7 +495,6 @@ void mesh_info(const ppc_mesh& m, rep_info& R, int tile_b = 0)
 			g = (m.bounding_box_maxs[d] - m.bounding_box_mins[d] + m.voxel_shape[d] - 1) / m.voxel_shape[d];
 		R.grid[d] = std::max(g, 1);
 		R.voxels *= R.grid[d];
-		R.scg[d] = tile_b > 0 ? (R.grid[d] + tile_b - 1) / tile_b : 1;
 	}
 }
 
@@ -543,8 +542,7 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 				return fail(PPC_ERR_ARG, "invalid mesh");
 			}
 		rep_info R {};
-		mesh_info(meshes[r], R, s->tile_b);
-		R.sc_base = (int32_t)s->total_sc;
+		mesh_info(meshes[r], R);
 		{
 			// positions relative to the box minimum reach about the extent; the
 			// FP32 filter tolerates 16 float ulps of it per coordinate
@@ -555,7 +553,6 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 			std::frexp(ext, &e2);
 			R.fmargin = (float)std::ldexp(16.0, e2 - 24);
 		}
-		s->total_sc += (int64_t)R.scg[0] * R.scg[1] * R.scg[2];
 		R.base = (int32_t)cap;
 		R.cap = capacities[r];
 		R.vox_base = vox;
@@ -601,13 +598,6 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.cursor, 1));
 	v.nvox = (int32_t)vox;
 	v.ntiles = (int32_t)((vox + 4095) / 4096);
-	v.tile_b = s->tile_b;
-	v.sc_list_cap = (int32_t)std::max<int64_t>(1, std::min<int64_t>(s->total_sc, C));
-	try_(alloc(s, v.epoch, 1));
-	try_(alloc(s, v.sc_tag, (size_t)s->total_sc));
-	try_(alloc(s, v.sc_list, 2 * (size_t)v.sc_list_cap));
-	try_(alloc(s, v.nsc, 2));
-	try_(alloc(s, v.work, 2));
 	try_(alloc(s, v.pos[0], C));
 	try_(alloc(s, v.pos[1], C));
 	try_(alloc(s, v.vel, C));
@@ -736,53 +726,14 @@ int ppc_set_launch_shape(ppc_state* s, int32_t tile_edge, int32_t threads, int32
 {
 	if (!s)
 		return fail(PPC_ERR_ARG, "null state");
-	const bool edge_ok = tile_edge == 0 || tile_edge == 2 || tile_edge == 3 || tile_edge == 4 || tile_edge == 6
-						 || tile_edge == 8;
-	if (!edge_ok || threads < 32 || threads > 256 || threads % 32 != 0 || smem_bytes < 0 || smem_bytes > 160 * 1024)
-		return fail(PPC_ERR_ARG, "tile edge 0/2/3/4/6/8, threads 32..256 (multiple of 32), smem <= 160 KiB");
+	if ((tile_edge != 0 && tile_edge != -1) || threads < 32 || threads > 256 || threads % 32 != 0 || smem_bytes < 0
+		|| smem_bytes > 160 * 1024)
+		return fail(PPC_ERR_ARG, "tile edge 0 or -1, threads 32..256 (multiple of 32), smem <= 160 KiB");
 	PPC_CUDA(cudaStreamSynchronize(s->stream));
 	release_graph(s);
+	s->staged = tile_edge == 0;
 	s->tile_threads = threads;
 	s->tile_smem = smem_bytes;
-	if (tile_edge == s->tile_b)
-		return PPC_OK;
-	// super-cell numbering depends on the edge: rebuild it and its buffers
-	int64_t total_sc = 0;
-	for (auto& R : s->reps)
-	{
-		for (int d = 0; d < 3; d++)
-			R.scg[d] = tile_edge > 0 ? (R.grid[d] + tile_edge - 1) / tile_edge : 1;
-		R.sc_base = (int32_t)total_sc;
-		total_sc += (int64_t)R.scg[0] * R.scg[1] * R.scg[2];
-	}
-	PPC_CUDA(cudaMemcpy(const_cast<rep_info*>(s->v.reps), s->reps.data(), sizeof(rep_info) * s->nreps,
-						cudaMemcpyHostToDevice));
-	const int32_t cap = (int32_t)std::max<int64_t>(1, std::min<int64_t>(total_sc, s->total_cap));
-	int32_t* tag = nullptr;
-	int2* list = nullptr;
-	PPC_CUDA(cudaMalloc(&tag, std::max<int64_t>(total_sc, 1) * sizeof(int32_t)));
-	PPC_CUDA(cudaMemset(tag, 0, std::max<int64_t>(total_sc, 1) * sizeof(int32_t)));
-	PPC_CUDA(cudaMalloc(&list, 2 * (size_t)cap * sizeof(int2)));
-	for (auto& b : s->allocations)
-	{
-		if (b.p == s->v.sc_tag)
-		{
-			cudaFree(b.p);
-			b.p = tag;
-		}
-		else if (b.p == s->v.sc_list)
-		{
-			cudaFree(b.p);
-			b.p = list;
-		}
-	}
-	s->v.sc_tag = tag;
-	s->v.sc_list = list;
-	s->v.sc_list_cap = cap;
-	s->total_sc = total_sc;
-	s->tile_b = tile_edge;
-	s->v.tile_b = tile_edge;
-	s->bins_valid = false;
 	return PPC_OK;
 }
 

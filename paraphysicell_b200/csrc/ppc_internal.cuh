@@ -52,8 +52,6 @@ struct rep_info
 	int64_t vox_base;
 	int64_t voxels;
 	int32_t maxs_int[3], mins_int[3];
-	int32_t scg[3];	  // super-cell grid: ceil(grid / tile edge)
-	int32_t sc_base;  // first super-cell of this replicate in the global numbering
 	float fmargin;	  // bound on the FP32 distance error of positions relative to mins (um)
 };
 
@@ -81,13 +79,6 @@ struct view
 	int32_t* cursor;	// number of binned agents (length of `sorted`)
 	int32_t nvox;		// voxels of all replicates
 	int32_t ntiles;		// scan tiles of 4096 voxels
-	int32_t tile_b;		// edge (voxels) of the super-cells the fused pass stages in shared memory
-	int32_t sc_list_cap; // entries per parity of sc_list
-	uint32_t* epoch;	// rebuild counter; its parity selects the super-cell list
-	int32_t* sc_tag;	// per super-cell: epoch of the rebuild that last saw an agent in it
-	int2* sc_list;		// [2][sc_list_cap] occupied super-cells {replicate, local index}
-	int32_t* nsc;		// [2] list lengths
-	int32_t* work;		// [2] next list entry to hand to a block
 
 	double4* pos[2];
 	double4* vel;
@@ -191,11 +182,12 @@ struct ppc_state
 	int64_t graph_launches = 0;
 	bool use_graphs = true;
 
-	// fused pass: super-cell tiles staged in shared memory (0 = one thread per agent)
-	int tile_b = 0;
+	// fused pass launch shape: candidates read from global memory (default)
+	// or the block's candidate ranges staged in shared memory; threads per
+	// block; staging bytes per block
+	bool staged = false;
 	int tile_threads = 128;
-	int tile_smem = 48 * 1024;
-	int64_t total_sc = 0;
+	int tile_smem = 32 * 1024;
 
 	// fused-kernel timing (ppc_set_profiling)
 	bool profiling = false;

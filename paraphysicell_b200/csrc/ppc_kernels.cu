@@ -118,53 +118,17 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur)
 {
 	grid_wait();
 	const int s = blockIdx.x * blockDim.x + threadIdx.x;
-	const uint32_t e = *v.epoch + 1;
-	if (s == 0)
-	{
-		// list counters of the other parity: last used by the fused pass that
-		// consumed the previous-but-one rebuild, needed next by the rebuild after this one
-		v.nsc[(e + 1) & 1] = 0;
-		v.work[(e + 1) & 1] = 0;
-	}
 	int r = 0, local = 0;
-	const bool is_live = s < v.total_cap && live(v, s, r, local);
-	int32_t key = 0, rank = 0;
-	int first = 0, sc = 0;
-	if (is_live)
-	{
-		const rep_info& R = v.reps[r];
-		const double4 p = v.pos[cur][s];
-		const int c0 = axis_coord(p.x, R, 0, v.err);
-		const int c1 = v.dims >= 2 ? axis_coord(p.y, R, 1, v.err) : 0;
-		const int c2 = v.dims >= 3 ? axis_coord(p.z, R, 2, v.err) : 0;
-		key = (int32_t)(R.vox_base + c0 + (int64_t)R.grid[0] * (c1 + (int64_t)R.grid[1] * c2));
-		rank = atomicAdd(v.vcnt + key, 1);
-		if (v.tile_b > 0)
-		{
-			// the first agent of this rebuild in a super-cell enters it in the
-			// list of occupied super-cells
-			const int b = v.tile_b;
-			sc = c0 / b + R.scg[0] * (c1 / b + R.scg[1] * (c2 / b));
-			first = (uint32_t)atomicExch(v.sc_tag + R.sc_base + sc, (int32_t)e) != e;
-		}
-	}
-	if (v.tile_b > 0)
-	{
-		// one list reservation per block
-		__shared__ int base;
-		int total;
-		const int off = block_exclusive_scan(first, total);
-		if (threadIdx.x == 0 && total > 0)
-			base = atomicAdd(v.nsc + (e & 1), total);
-		__syncthreads();
-		if (first)
-			v.sc_list[(e & 1) * v.sc_list_cap + base + off] = make_int2(r, sc);
-	}
-	if (is_live)
-	{
-		v.key[s] = key;
-		v.vrank[s] = rank;
-	}
+	if (s >= v.total_cap || !live(v, s, r, local))
+		return;
+	const rep_info& R = v.reps[r];
+	const double4 p = v.pos[cur][s];
+	const int c0 = axis_coord(p.x, R, 0, v.err);
+	const int c1 = v.dims >= 2 ? axis_coord(p.y, R, 1, v.err) : 0;
+	const int c2 = v.dims >= 3 ? axis_coord(p.z, R, 2, v.err) : 0;
+	const int32_t key = (int32_t)(R.vox_base + c0 + (int64_t)R.grid[0] * (c1 + (int64_t)R.grid[1] * c2));
+	v.key[s] = key;
+	v.vrank[s] = atomicAdd(v.vcnt + key, 1);
 }
 
 // per-tile totals of the voxel counts (one block per tile of 4096 voxels)
@@ -265,8 +229,6 @@ __global__ void k_bin_scatter(view v)
 {
 	grid_wait();
 	int s = blockIdx.x * blockDim.x + threadIdx.x;
-	if (s == 0)
-		*v.epoch += 1;
 	if (s >= v.total_cap)
 		return;
 	int r, local;
@@ -311,11 +273,15 @@ __global__ void k_bin_fixup(view v, int cur)
 	v.sprm4[t] = make_double4(prm.x, prm.y, prm.z, __longlong_as_double(bits));
 	for (int q = 0; q < D; q++)
 		v.saff[(int64_t)t * D + q] = q < 8 ? aff[q] : v.aff[(int64_t)s * D + q];
-	if (v.f32)
 	{
+		// single-precision positions relative to the box minimum: the
+		// candidate filter of the fused pass
 		const rep_info& R = v.reps[r];
 		v.sposf[t] = make_float4((float)(p.x - R.mins[0]), (float)(p.y - R.mins[1]), (float)(p.z - R.mins[2]),
 								 (float)p.w);
+	}
+	if (v.f32)
+	{
 		const int fbits = (int)((uint32_t)(bits & 0xffff) | (uint32_t)((bits >> 32) & 1) << 16
 								| (uint32_t)((bits >> 40) & 0xff) << 24);
 		v.sprmf[t] = make_float4((float)prm.x, (float)prm.y, (float)prm.z, __int_as_float(fbits));
@@ -333,6 +299,7 @@ __global__ void k_bin_fixup(view v, int cur)
 // ---------------------------------------------------------------------------
 
 constexpr int kList = 8; // neighbours recorded per thread before the pair pass runs
+constexpr int kFusedThreads = 128; // block size limit of the fused pass (five blocks per SM resident)
 
 // Visits, in the reference's order, the neighbours of the agent at position t
 // of the key-ordered array: stencil rows z outer then y; in each row the
@@ -523,21 +490,34 @@ __device__ __forceinline__ void walls(const view& v, const rep_info& R, const do
 	}
 }
 
-// spring_contract_function for one agent (reference: position_solver.cpp:337-370)
+// spring_contract_function for one agent (reference: position_solver.cpp:337-370).
+// Springs are taken two at a time, the loads of both issued before the
+// arithmetic; the terms are added in attachment order.
 template <int DIMS>
 __device__ __forceinline__ void spring_contract(const view& v, int cur, int s, int n, const double4& pi, int def_i,
 												double4& vel)
 {
 	const double ec_i = v.ec[s];
 	const double* aff_i = v.aff + (int64_t)s * v.ndefs;
-	for (int k = 0; k < n; k++)
+	for (int k0 = 0; k0 < n; k0 += 2)
 	{
-		const int j = v.springs[(int64_t)s * v.scap + k];
-		const int def_j = v.def[j];
-		const double a = sqrt(ec_i * v.ec[j] * aff_i[def_j] * v.aff[(int64_t)j * v.ndefs + def_i]);
-		const double4 pj = v.pos[cur][j];
+		const bool two = k0 + 1 < n;
+		const int j0 = v.springs[(int64_t)s * v.scap + k0];
+		const int j1 = two ? v.springs[(int64_t)s * v.scap + k0 + 1] : j0;
+		const int d0 = v.def[j0], d1 = v.def[j1];
+		const double e0 = v.ec[j0], e1 = v.ec[j1];
+		const double f0 = v.aff[(int64_t)j0 * v.ndefs + def_i], f1 = v.aff[(int64_t)j1 * v.ndefs + def_i];
+		const double4 p0 = v.pos[cur][j0], p1 = v.pos[cur][j1];
+		const double g0 = aff_i[d0], g1 = aff_i[d1];
+		const double a0 = sqrt(ec_i * e0 * g0 * f0);
 		for (int d = 0; d < DIMS; d++)
-			set_comp(vel, d, comp(vel, d) + a * (comp(pj, d) - comp(pi, d)));
+			set_comp(vel, d, comp(vel, d) + a0 * (comp(p0, d) - comp(pi, d)));
+		if (two)
+		{
+			const double a1 = sqrt(ec_i * e1 * g1 * f1);
+			for (int d = 0; d < DIMS; d++)
+				set_comp(vel, d, comp(vel, d) + a1 * (comp(p1, d) - comp(pi, d)));
+		}
 	}
 }
 
@@ -640,7 +620,7 @@ __device__ __forceinline__ void finish_agent(const view& v, const rep_info& R, i
 // agents for the container update that follows.
 // ---------------------------------------------------------------------------
 template <int DIMS, bool WALLS, bool SPRINGS, bool VEL>
-__global__ void __launch_bounds__(256) k_fused(view v, int cur)
+__global__ void __launch_bounds__(kFusedThreads, 5) k_fused(view v, int cur)
 {
 	grid_wait();
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -659,7 +639,7 @@ __global__ void __launch_bounds__(256) k_fused(view v, int cur)
 	acc.vx = tail.vel0.x;
 	acc.vy = tail.vel0.y;
 	acc.vz = tail.vel0.z;
-	__shared__ int32_t list[kList * 256];
+	__shared__ int32_t list[kList * kFusedThreads];
 	const int D = v.ndefs;
 	for_each_neighbor<DIMS>(v, R, t, v.skey[t], pi, list + threadIdx.x, [&](int u) {
 		// neighbour data from the key-ordered copies (index u, no indirection)
@@ -735,7 +715,7 @@ struct pair_fp32
 };
 
 template <int DIMS, bool WALLS, bool SPRINGS, bool VEL>
-__global__ void __launch_bounds__(256) k_fused_f32(view v, int cur)
+__global__ void __launch_bounds__(kFusedThreads, 5) k_fused_f32(view v, int cur)
 {
 	grid_wait();
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -776,7 +756,7 @@ __global__ void __launch_bounds__(256) k_fused_f32(view v, int cur)
 		lo[k] = ok ? v.vstart[row + xlo] : 0;
 		hi[k] = ok ? v.vstart[row + xhi + 1] : 0;
 	}
-	__shared__ int32_t list[kList * 256];
+	__shared__ int32_t list[kList * kFusedThreads];
 	int32_t* lst = list + threadIdx.x;
 	const int stride = blockDim.x;
 	int n = 0;
@@ -846,248 +826,295 @@ __global__ void __launch_bounds__(256) k_fused_f32(view v, int cur)
 }
 
 // ---------------------------------------------------------------------------
-// fused step over super-cell tiles: a block takes one occupied super-cell of
-// B^dims voxels, stages the agents of its (B+2)^dims halo voxels (positions,
-// pair parameters, affinity rows; contiguous runs of the key-ordered arrays)
-// in shared memory, and each thread then handles one home agent of the core,
-// scanning its 27-voxel stencil out of shared memory. Halos larger than the
-// shared-memory budget are read from global memory instead. Results are
-// identical to k_fused: same neighbours, same order, same operations.
+// fused step with the block's candidates staged in shared memory.
+//
+// A block takes blockDim consecutive agents of the key-ordered array, keys
+// kf..kl. Every candidate of every one of them for stencil row (dy, dz) has a
+// key in [kf + off - 1, kl + off + 1], off = dy g0 + dz g0 g1, so it lies in
+// one contiguous range of the key-ordered array; the block copies the nine
+// ranges (three in 2-D, one in 1-D) of the single-precision positions
+// (sposf) into shared memory with all its threads, one memory round trip, and
+// each thread then scans its stencil out of shared memory. A block whose
+// ranges exceed the budget, or that spans two replicates, reads the same
+// arrays from global memory instead.
+//
+// The scan tests candidates in single precision with the margin of the FP32
+// form (16 float ulps of the domain extent, and a relative 1e-5 on the
+// squared distance that covers the rounding of the radii and of the float
+// arithmetic), which never rejects a pair the FP64 test accepts; each kept
+// candidate then goes through the FP64 test (distance <= rmad_i r_i +
+// rmad_j r_j) before its pair code runs, so the neighbour sets and their
+// order are the reference's. With F32 false the pair arithmetic is the FP64
+// drop-in (bit-identical to the reference); with F32 true it is the
+// FP32-force form.
 // ---------------------------------------------------------------------------
 
-constexpr int kTileThreadsMax = 256;
+constexpr int kStageThreads = 128;
+constexpr size_t kStageStatic = 10 * 1024; // bound on the staged kernel's static shared memory
+#ifndef PPC_STAGE_MINB
+#define PPC_STAGE_MINB 4
+#endif
 
-template <int DIMS, int B>
-struct tile_geom
+// array bounds [lo[k], hi[k]) of the stencil rows of the agent in voxel
+// `key`: rows z outer then y, each the voxels x-1..x+1, which are consecutive
+// keys and so one contiguous range [vstart[k-1], vstart[k+2]) of the
+// key-ordered array; rows outside the grid are empty
+template <int DIMS>
+__device__ __forceinline__ void stencil_bounds(const view& v, const rep_info& R, int32_t key, int* lo, int* hi)
 {
-	static constexpr int H = B + 2;
-	static constexpr int NROW = DIMS == 3 ? H * H : (DIMS == 2 ? H : 1);
-	static constexpr int NCORE = DIMS == 3 ? B * B : (DIMS == 2 ? B : 1);
-	// halo row of core row cr, and of the stencil row (dy, dz) around it
-	__device__ static __forceinline__ int core_row(int cr)
-	{
-		if (DIMS == 3)
-			return (cr % B + 1) + H * (cr / B + 1);
-		return DIMS == 2 ? cr + 1 : 0;
-	}
-	__device__ static __forceinline__ int stencil_row(int cr, int dy, int dz)
-	{
-		if (DIMS == 3)
-			return (cr % B + 1 + dy) + H * (cr / B + 1 + dz);
-		return DIMS == 2 ? cr + 1 + dy : 0;
-	}
-};
-
-template <int DIMS, int B, bool STAGED, bool WALLS, bool SPRINGS, bool VEL>
-__device__ __forceinline__ void tile_home(const view& v, const rep_info& R, int r, int cur, int g, int cr, int xi,
-										  const int (*vs)[B + 3], const int* rowoff, const double4* hpos,
-										  const double4* hprm, const double* haff, int32_t* list)
-{
-	using G = tile_geom<DIMS, B>;
-	const int D = v.ndefs;
-	const double4* P = STAGED ? hpos : v.spos4;
-	const double4* Q = STAGED ? hprm : v.sprm4;
-	const double* A = STAGED ? haff : v.saff;
-	const int hr0 = G::core_row(cr);
-	const int self = STAGED ? rowoff[hr0] + (g - vs[hr0][0]) : g;
-	const int s = v.sorted[g];
-	const double4 pi = P[self];
-	const double4 qi = Q[self];
-
-	pair_fp64 acc;
-	acc.prm_i = qi;
-	unpack_bits(qi.w, acc.def_i, acc.mov_i);
-	acc.aff_i = A + (int64_t)self * D;
-	const agent_tail tail = load_tail<WALLS, VEL>(v, s, acc.mov_i);
-	acc.vx = tail.vel0.x;
-	acc.vy = tail.vel0.y;
-	acc.vz = tail.vel0.z;
-
-	const int stride = blockDim.x;
-	int n = 0;
-	auto flush = [&]() {
-		for (int m = 0; m < n; m++)
-		{
-			const int u = list[m * stride];
-			const double4 q = P[u];
-			const double ddx = pi.x - q.x;
-			const double ddy = DIMS >= 2 ? pi.y - q.y : 0.0;
-			const double ddz = DIMS >= 3 ? pi.z - q.z : 0.0;
-			double d2 = ddx * ddx;
-			if (DIMS >= 2)
-				d2 = d2 + ddy * ddy;
-			if (DIMS >= 3)
-				d2 = d2 + ddz * ddz;
-			const double dist = DIMS == 1 ? fabs(ddx) : sqrt(d2);
-			const double4 qj = Q[u];
-			int def_j;
-			bool mov_j;
-			unpack_bits(qj.w, def_j, mov_j);
-			acc.add_pair(qj.x, qj.y, qj.z, def_j, mov_j, A[(int64_t)u * D + acc.def_i], ddx, ddy, ddz, dist,
-						 pi.w + q.w);
-		}
-		n = 0;
-	};
+	const int32_t lk = (int32_t)(key - R.vox_base);
+	const int g0 = R.grid[0], g1 = R.grid[1], g2 = R.grid[2];
+	const int cx = lk % g0;
+	const int cy = (lk / g0) % g1;
+	const int cz = lk / (g0 * g1);
+	const int xlo = cx > 0 ? cx - 1 : 0;
+	const int xhi = cx + 1 < g0 ? cx + 1 : g0 - 1;
+	constexpr int NR = DIMS == 3 ? 9 : (DIMS == 2 ? 3 : 1);
 #pragma unroll
-	for (int k = 0; k < (DIMS == 3 ? 9 : (DIMS == 2 ? 3 : 1)); k++)
+	for (int k = 0; k < NR; k++)
 	{
 		const int dz = DIMS == 3 ? k / 3 - 1 : 0;
 		const int dy = DIMS >= 2 ? k % 3 - 1 : 0;
-		const int hr = G::stencil_row(cr, dy, dz);
-		const int shift = STAGED ? rowoff[hr] - vs[hr][0] : 0;
-		const int lo = vs[hr][xi - 1] + shift, hi = vs[hr][xi + 2] + shift;
-		for (int u = lo; u < hi; u++)
+		const int z = cz + dz, y = cy + dy;
+		const bool ok = z >= 0 && z < g2 && y >= 0 && y < g1;
+		const int64_t row = R.vox_base + (int64_t)g0 * (y + (int64_t)g1 * z);
+		lo[k] = ok ? v.vstart[row + xlo] : 0;
+		hi[k] = ok ? v.vstart[row + xhi + 1] : 0;
+	}
+}
+
+// true when the single-precision filter keeps candidate c for the agent at pf
+template <int DIMS>
+__device__ __forceinline__ bool filter_keep(const float4& pf, const float4& c, float margin)
+{
+	const float dxf = pf.x - c.x;
+	const float dyf = DIMS >= 2 ? pf.y - c.y : 0.f;
+	const float dzf = DIMS >= 3 ? pf.z - c.z : 0.f;
+	float d2f = dxf * dxf;
+	if (DIMS >= 2)
+		d2f = d2f + dyf * dyf;
+	if (DIMS >= 3)
+		d2f = d2f + dzf * dzf;
+	const float adf = pf.w + c.w + margin;
+	return !(d2f > adf * adf * 1.00001f);
+}
+
+template <int DIMS, bool WALLS, bool SPRINGS, bool VEL, bool F32>
+__global__ void __launch_bounds__(kStageThreads, PPC_STAGE_MINB) k_fused_staged(view v, int cur, int cap)
+{
+	grid_wait();
+	constexpr int NR = DIMS == 3 ? 9 : (DIMS == 2 ? 3 : 1);
+	extern __shared__ float4 stage[]; // cap staged positions, then the neighbour lists
+	__shared__ int s_a[NR], s_o[NR + 1];
+	__shared__ int2 s_rows[NR][kStageThreads]; // each thread's stencil-row bounds
+	int32_t* list = reinterpret_cast<int32_t*>(stage + cap) + threadIdx.x;
+	const int stride = blockDim.x;
+	const int nsorted = *v.cursor;
+	const int t0 = blockIdx.x * blockDim.x;
+	if (t0 >= nsorted)
+		return;
+	const int tl = min(t0 + (int)blockDim.x, nsorted) - 1;
+	const int t = t0 + threadIdx.x;
+	const bool act = t <= tl;
+
+	// block set-up (warp 0): the row ranges and their offsets in shared memory
+	if (threadIdx.x < 32)
+	{
+		const int lane = threadIdx.x;
+		const int r0 = rep_of(v, v.sorted[t0]), r1 = rep_of(v, v.sorted[tl]);
+		const int64_t kf = v.skey[t0], kl = v.skey[tl];
+		int a = 0, n = 0;
+		if (lane < NR && r0 == r1)
 		{
-			if (u == self)
-				continue;
-			const double4 q = P[u];
-			const double ddx = pi.x - q.x;
-			const double ddy = DIMS >= 2 ? pi.y - q.y : 0.0;
-			const double ddz = DIMS >= 3 ? pi.z - q.z : 0.0;
-			double d2 = ddx * ddx;
+			const rep_info& R = v.reps[r0];
+			const int dz = DIMS == 3 ? lane / 3 - 1 : 0;
+			const int dy = DIMS >= 2 ? lane % 3 - 1 : 0;
+			const int64_t off = (int64_t)dy * R.grid[0] + (int64_t)dz * R.grid[0] * R.grid[1];
+			const int64_t lo = max(R.vox_base, kf + off - 1);
+			const int64_t hi = min(R.vox_base + R.voxels, kl + off + 2);
+			if (lo < hi)
+			{
+				a = v.vstart[lo];
+				n = v.vstart[hi] - a;
+			}
+		}
+		int incl = n;
+		for (int o = 1; o < 32; o <<= 1)
+		{
+			const int y = __shfl_up_sync(0xffffffffu, incl, o);
+			if (lane >= o)
+				incl += y;
+		}
+		const int total = __shfl_sync(0xffffffffu, incl, NR - 1);
+		if (lane < NR)
+		{
+			s_a[lane] = a;
+			s_o[lane] = incl - n;
+		}
+		if (lane == 0)
+			s_o[NR] = (r0 == r1 && total <= cap) ? total : -1;
+	}
+
+	// per-agent loads, issued before the block waits for its ranges
+	const int tt = act ? t : tl;
+	const int s = v.sorted[tt];
+	const int r = rep_of(v, s);
+	const rep_info& R = v.reps[r];
+	const double4 pi = v.spos4[tt];
+	const float4 pf = v.sposf[tt];
+	const double4 qi = v.sprm4[tt];
+	int def_i;
+	bool mov_i;
+	unpack_bits(qi.w, def_i, mov_i);
+	const int nspr = unpack_springs(qi.w);
+	// the previous velocity is read after the scan; ask L2 for it now
+	if (mov_i)
+		asm volatile("prefetch.global.L2 [%0];" ::"l"(v.vprev + s));
+	const uint8_t flag = v.flags[s];
+	const double bm = (WALLS && mov_i) ? v.prm[s].w : 0.0;
+	{
+		int lo[NR], hi[NR];
+		stencil_bounds<DIMS>(v, R, v.skey[tt], lo, hi);
+#pragma unroll
+		for (int k = 0; k < NR; k++)
+			s_rows[k][threadIdx.x] = make_int2(lo[k], hi[k]);
+	}
+
+	__syncthreads();
+	const int S = s_o[NR];
+	for (int i = threadIdx.x; i < S; i += blockDim.x)
+	{
+		int k = 0;
+#pragma unroll
+		for (int kk = 1; kk < NR; kk++)
+			k = i >= s_o[kk] ? kk : k;
+		stage[i] = v.sposf[s_a[k] + (i - s_o[k])];
+	}
+	__syncthreads();
+	if (!act)
+		return;
+
+	// candidates at array positions u of row k are read at P[u + soff(k)]:
+	// shared memory when staged, else the global sposf
+	const bool staged = S >= 0;
+	const float4* P = staged ? stage : v.sposf;
+	const int D = v.ndefs;
+	const float margin = R.fmargin;
+	pair_fp64 acc;
+	acc.prm_i = qi;
+	acc.def_i = def_i;
+	acc.mov_i = mov_i;
+	acc.aff_i = v.saff + (int64_t)t * D;
+	const double4 vel0 = (VEL && mov_i) ? v.vel[s] : make_double4(0, 0, 0, 0);
+	acc.vx = vel0.x;
+	acc.vy = vel0.y;
+	acc.vz = vel0.z;
+	pair_fp32 accf;
+	if (F32)
+	{
+		const float4 qf = v.sprmf[t];
+		accf.r_i = qf.x;
+		accf.rep_i = qf.y;
+		accf.adh_i = qf.z;
+		accf.def_i = def_i;
+		accf.mov_i = mov_i;
+		accf.aff_i = v.safff + (int64_t)t * D;
+	}
+
+	// one kept candidate at array position u: the exact FP64 predicate, then
+	// the pair code, with the operations of the unstaged kernels
+	auto pair = [&](int u) {
+		const double4 q = v.spos4[u];
+		const double ddx = pi.x - q.x;
+		const double ddy = DIMS >= 2 ? pi.y - q.y : 0.0;
+		const double ddz = DIMS >= 3 ? pi.z - q.z : 0.0;
+		double d2 = ddx * ddx;
+		if (DIMS >= 2)
+			d2 = d2 + ddy * ddy;
+		if (DIMS >= 3)
+			d2 = d2 + ddz * ddz;
+		const double ad = pi.w + q.w;
+		const double dist = DIMS == 1 ? fabs(ddx) : sqrt(d2);
+		if (!(dist <= ad))
+			return;
+		if (F32)
+		{
+			const float dx = (float)ddx, dy = (float)ddy, dz = (float)ddz;
+			float d2f = dx * dx;
 			if (DIMS >= 2)
-				d2 = d2 + ddy * ddy;
+				d2f = d2f + dy * dy;
 			if (DIMS >= 3)
-				d2 = d2 + ddz * ddz;
-			const double ad = pi.w + q.w;
-			if (d2 > ad * ad * (1.0 + 1e-12))
-				continue;
-			const double dist = DIMS == 1 ? fabs(ddx) : sqrt(d2);
-			if (!(dist <= ad))
+				d2f = d2f + dz * dz;
+			const float distf = DIMS == 1 ? fabsf(dx) : sqrtf(d2f);
+			const float4 qj = v.sprmf[u];
+			const float4 pj = v.sposf[u];
+			int def_j, spr_j;
+			bool mov_j;
+			unpack_fbits(qj.w, def_j, mov_j, spr_j);
+			accf.add(qj.x, qj.y, qj.z, def_j, mov_j, v.safff[(int64_t)u * D + def_i], dx, dy, dz, distf, pf.w + pj.w);
+		}
+		else
+		{
+			const double4 qj = v.sprm4[u];
+			int def_j;
+			bool mov_j;
+			unpack_bits(qj.w, def_j, mov_j);
+			acc.add_pair(qj.x, qj.y, qj.z, def_j, mov_j, v.saff[(int64_t)u * D + def_i], ddx, ddy, ddz, dist, ad);
+		}
+	};
+	int n = 0;
+#pragma unroll 1
+	for (int k = 0; k < NR; k++)
+	{
+		const int2 b = s_rows[k][threadIdx.x];
+		const int soff = staged ? s_o[k] - s_a[k] : 0;
+		for (int u = b.x; u < b.y; u++)
+		{
+			if (u == t || !filter_keep<DIMS>(pf, P[u + soff], margin))
 				continue;
 			list[n * stride] = u;
 			if (++n == kList)
-				flush();
+			{
+				for (int m = 0; m < n; m++)
+					pair(list[m * stride]);
+				n = 0;
+			}
 		}
 	}
-	flush();
-	finish_agent<DIMS, WALLS, SPRINGS, VEL>(v, R, r, cur, s, pi, qi.x, acc.def_i, acc.mov_i, unpack_springs(qi.w), tail,
-											acc.vx, acc.vy, acc.vz, acc.p);
-}
+	for (int m = 0; m < n; m++)
+		pair(list[m * stride]);
 
-template <int DIMS, int B, bool WALLS, bool SPRINGS, bool VEL>
-__global__ void __launch_bounds__(kTileThreadsMax) k_fused_tile(view v, int cur, int cap)
-{
-	grid_wait();
-	using G = tile_geom<DIMS, B>;
-	constexpr int H = G::H, NROW = G::NROW, NCORE = G::NCORE;
-	extern __shared__ double4 dyn[];
-	double4* hpos = dyn;
-	double4* hprm = dyn + cap;
-	double* haff = reinterpret_cast<double*>(dyn + 2 * cap);
-	__shared__ int vs[NROW][B + 3];
-	__shared__ int rowoff[NROW + 1];
-	__shared__ int coreoff[NCORE + 1];
-	__shared__ int item;
-	__shared__ int32_t list[kList * kTileThreadsMax];
-
-	const uint32_t e = *v.epoch;
-	const int par = e & 1;
-	const int nsc = v.nsc[par];
-	const int D = v.ndefs;
-	const int tid = threadIdx.x, nt = blockDim.x;
-	for (;;)
+	double4 p = make_double4(pi.x, pi.y, pi.z, 0.0);
+	double4 vp = mov_i ? v.vprev[s] : make_double4(0, 0, 0, 0);
+	double vx = acc.vx, vy = acc.vy, vz = acc.vz, pressure = acc.p;
+	if (F32)
 	{
-		if (tid == 0)
-			item = atomicAdd(v.work + par, 1);
-		__syncthreads();
-		const int w = item;
-		if (w >= nsc)
-			break;
-		const int2 it = v.sc_list[par * v.sc_list_cap + w];
-		const int r = it.x;
-		const rep_info& R = v.reps[r];
-		const int g0 = R.grid[0], g1 = R.grid[1], g2 = R.grid[2];
-		const int sx = it.y % R.scg[0];
-		const int sy = DIMS >= 2 ? (it.y / R.scg[0]) % R.scg[1] : 0;
-		const int sz = DIMS >= 3 ? it.y / (R.scg[0] * R.scg[1]) : 0;
-		const int x0 = sx * B, y0 = sy * B, z0 = sz * B;
-
-		// vstart at the voxel boundaries of every halo row, x clipped to the grid
-		for (int k = tid; k < NROW * (H + 1); k += nt)
-		{
-			const int hr = k / (H + 1), xi = k % (H + 1);
-			const int y = DIMS >= 2 ? y0 - 1 + hr % H : 0;
-			const int z = DIMS >= 3 ? z0 - 1 + hr / H : 0;
-			int val = 0;
-			if (y >= 0 && y < g1 && z >= 0 && z < g2)
-			{
-				int x = x0 - 1 + xi;
-				x = x < 0 ? 0 : (x > g0 ? g0 : x);
-				val = v.vstart[R.vox_base + (int64_t)g0 * (y + (int64_t)g1 * z) + x];
-			}
-			vs[hr][xi] = val;
-		}
-		__syncthreads();
-		if (tid == 0)
-		{
-			int o = 0;
-			for (int hr = 0; hr < NROW; hr++)
-			{
-				rowoff[hr] = o;
-				o += vs[hr][H] - vs[hr][0];
-			}
-			rowoff[NROW] = o;
-			int c = 0;
-			for (int cr = 0; cr < NCORE; cr++)
-			{
-				const int hr = G::core_row(cr);
-				coreoff[cr] = c;
-				c += vs[hr][B + 1] - vs[hr][1];
-			}
-			coreoff[NCORE] = c;
-		}
-		__syncthreads();
-		const int total = rowoff[NROW];
-		const bool staged = total <= cap;
-		if (staged)
-		{
-			for (int f = tid; f < total; f += nt)
-			{
-				int lo = 0, hi = NROW; // last row with rowoff <= f
-				while (hi - lo > 1)
-				{
-					const int mid = (lo + hi) >> 1;
-					if (rowoff[mid] <= f)
-						lo = mid;
-					else
-						hi = mid;
-				}
-				const int g = vs[lo][0] + (f - rowoff[lo]);
-				hpos[f] = v.spos4[g];
-				hprm[f] = v.sprm4[g];
-				for (int q = 0; q < D; q++)
-					haff[f * D + q] = v.saff[(int64_t)g * D + q];
-			}
-		}
-		__syncthreads();
-		const int nhome = coreoff[NCORE];
-		for (int h = tid; h < nhome; h += nt)
-		{
-			int lo = 0, hi = NCORE;
-			while (hi - lo > 1)
-			{
-				const int mid = (lo + hi) >> 1;
-				if (coreoff[mid] <= h)
-					lo = mid;
-				else
-					hi = mid;
-			}
-			const int cr = lo;
-			const int hr = G::core_row(cr);
-			const int g = vs[hr][1] + (h - coreoff[cr]);
-			int xi = 1;
-			while (xi < B && g >= vs[hr][xi + 1])
-				xi++;
-			if (staged)
-				tile_home<DIMS, B, true, WALLS, SPRINGS, VEL>(v, R, r, cur, g, cr, xi, vs, rowoff, hpos, hprm, haff,
-															  list + tid);
-			else
-				tile_home<DIMS, B, false, WALLS, SPRINGS, VEL>(v, R, r, cur, g, cr, xi, vs, rowoff, hpos, hprm, haff,
-															   list + tid);
-		}
-		__syncthreads();
+		vx = vel0.x + accf.vx.value();
+		vy = vel0.y + accf.vy.value();
+		vz = vel0.z + accf.vz.value();
+		pressure = accf.p.value();
 	}
+	if (mov_i)
+	{
+		double4 vel = make_double4(vx, vy, vz, 0.0);
+		if (WALLS)
+			walls<DIMS>(v, R, p, qi.x, bm, vel);
+		if (SPRINGS && nspr > 0)
+			spring_contract<DIMS>(v, cur, s, nspr, p, def_i, vel);
+		ab2<DIMS>(v.dt, p, vel, vp);
+	}
+	v.pressure[s] = pressure;
+	if (mov_i)
+	{
+		v.vprev[s] = vp;
+		if (VEL)
+			v.vel[s] = make_double4(0, 0, 0, 0);
+	}
+	v.pos[cur ^ 1][s] = p;
+	if (!(p.x == p.x && p.y == p.y && p.z == p.z))
+		atomicOr(v.err, ERR_NONFINITE);
+	if (to_remove<DIMS>(R, p, flag))
+		append_bad(v, r, s - R.base);
 }
 
 // ---------------------------------------------------------------------------
@@ -1857,57 +1884,6 @@ int launch_positions(ppc_state* s)
 	return PPC_OK;
 }
 
-template <int DIMS, int B>
-static int tile_dispatch(ppc_state* s)
-{
-	const bool walls = s->params.virtual_wall_at_domain_edges != 0;
-	const bool springs = s->has_springs && s->params.automated_spring_adhesion != 0;
-	const bool vel = s->vel_dirty;
-	const int per_agent = 2 * (int)sizeof(double4) + s->ndefs * (int)sizeof(double);
-	const int cap = s->tile_smem / per_agent;
-	const size_t dyn = (size_t)cap * per_agent;
-	cudaStream_t st = PPC_LAUNCH(s);
-	void (*k)(view, int, int) = nullptr;
-#define PPC_TILE(W, S, V)                                                                                              \
-	if (walls == W && springs == S && vel == V)                                                                        \
-		k = k_fused_tile<DIMS, B, W, S, V>;
-	PPC_TILE(false, false, false)
-	PPC_TILE(false, false, true)
-	PPC_TILE(false, true, false)
-	PPC_TILE(false, true, true)
-	PPC_TILE(true, false, false)
-	PPC_TILE(true, false, true)
-	PPC_TILE(true, true, false)
-	PPC_TILE(true, true, true)
-#undef PPC_TILE
-	PPC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-	int per_sm = 0;
-	PPC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, s->tile_threads, dyn));
-	const int blocks = std::max(1, per_sm) * s->sm_count;
-	pdl(k, blocks, s->tile_threads, dyn, st, s->v, s->cur, cap);
-	return PPC_OK;
-}
-
-template <int DIMS>
-static int tile_by_edge(ppc_state* s)
-{
-	switch (s->tile_b)
-	{
-	case 2:
-		return tile_dispatch<DIMS, 2>(s);
-	case 3:
-		return tile_dispatch<DIMS, 3>(s);
-	case 4:
-		return tile_dispatch<DIMS, 4>(s);
-	case 6:
-		return tile_dispatch<DIMS, 6>(s);
-	case 8:
-		return tile_dispatch<DIMS, 8>(s);
-	default:
-		return PPC_ERR_ARG;
-	}
-}
-
 template <int DIMS>
 static void fused_dispatch(ppc_state* s, int b)
 {
@@ -1915,7 +1891,7 @@ static void fused_dispatch(ppc_state* s, int b)
 	const bool springs = s->has_springs && s->params.automated_spring_adhesion != 0;
 	const bool vel = s->vel_dirty;
 	cudaStream_t st = PPC_LAUNCH(s);
-	const int nt = s->tile_threads;
+	const int nt = std::min(s->tile_threads, kFusedThreads);
 	b = blocks_for(s->total_cap, nt);
 	const bool f32 = s->precision == PPC_FP32_FORCE;
 #define PPC_FUSED(W, S, V)                                                                                             \
@@ -1937,6 +1913,43 @@ static void fused_dispatch(ppc_state* s, int b)
 #undef PPC_FUSED
 }
 
+template <int DIMS>
+static int staged_dispatch(ppc_state* s)
+{
+	const bool walls = s->params.virtual_wall_at_domain_edges != 0;
+	const bool springs = s->has_springs && s->params.automated_spring_adhesion != 0;
+	const bool vel = s->vel_dirty;
+	const bool f32 = s->precision == PPC_FP32_FORCE;
+	cudaStream_t st = PPC_LAUNCH(s);
+	const int nt = std::min(s->tile_threads, kStageThreads);
+	const int list_bytes = kList * nt * (int)sizeof(int32_t);
+	const int cap = std::max(0, (s->tile_smem - list_bytes) / (int)sizeof(float4));
+	const size_t dyn = (size_t)cap * sizeof(float4) + list_bytes;
+	const int b = blocks_for(s->total_cap, nt);
+#define PPC_STAGED(W, S, V, F)                                                                                         \
+	if (walls == W && springs == S && vel == V && f32 == F)                                                            \
+	{                                                                                                                  \
+		auto k = k_fused_staged<DIMS, W, S, V, F>;                                                                     \
+		if (dyn + kStageStatic > 48 * 1024)                                                                            \
+			PPC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));                  \
+		pdl(k, b, nt, dyn, st, s->v, s->cur, cap);                                                                     \
+	}
+#define PPC_STAGED_F(W, S, V)                                                                                          \
+	PPC_STAGED(W, S, V, false)                                                                                         \
+	PPC_STAGED(W, S, V, true)
+	PPC_STAGED_F(false, false, false)
+	PPC_STAGED_F(false, false, true)
+	PPC_STAGED_F(false, true, false)
+	PPC_STAGED_F(false, true, true)
+	PPC_STAGED_F(true, false, false)
+	PPC_STAGED_F(true, false, true)
+	PPC_STAGED_F(true, true, false)
+	PPC_STAGED_F(true, true, true)
+#undef PPC_STAGED_F
+#undef PPC_STAGED
+	return PPC_OK;
+}
+
 int launch_fused(ppc_state* s)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
@@ -1956,9 +1969,9 @@ int launch_fused(ppc_state* s)
 		ev_end = s->prof_events[s->prof_used + 1];
 		s->prof_used += 2;
 	}
-	if (s->tile_b > 0 && s->precision == PPC_FP64)
+	if (s->staged)
 	{
-		int rc = s->dims == 1 ? tile_by_edge<1>(s) : (s->dims == 2 ? tile_by_edge<2>(s) : tile_by_edge<3>(s));
+		int rc = s->dims == 1 ? staged_dispatch<1>(s) : (s->dims == 2 ? staged_dispatch<2>(s) : staged_dispatch<3>(s));
 		if (rc != PPC_OK)
 			return rc;
 	}

@@ -183,7 +183,7 @@ class Simulation:
         _check(lib().ppc_get_launch_count(self.h, C.byref(n)), "ppc_get_launch_count")
         return n.value
 
-    def set_launch_shape(self, tile_edge, threads, smem_bytes=48 * 1024):
+    def set_launch_shape(self, tile_edge, threads, smem_bytes=32 * 1024):
         _check(lib().ppc_set_launch_shape(self.h, tile_edge, threads, smem_bytes), "ppc_set_launch_shape")
 
     def set_profiling(self, on):

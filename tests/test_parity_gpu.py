@@ -116,6 +116,46 @@ def test_fused_steps_match_oracle(case):
     gu.assert_same_neighbors(d, o)
 
 
+# launch shapes of the fused pass: (tile edge, threads, shared-memory bytes).
+# Edge 0 stages each block's candidate ranges in shared memory (the
+# default); a budget of 4 KiB leaves no room for them, so blocks read the
+# global arrays instead; edge -1 reads every candidate from global memory.
+SHAPES = [(0, 128, 32 * 1024), (0, 128, 40 * 1024), (0, 64, 4 * 1024), (0, 96, 24 * 1024), (-1, 128, 0),
+          (-1, 256, 0)]
+
+
+@pytest.mark.parametrize("shape", SHAPES, ids=lambda s: "edge%d_t%d_smem%d" % s)
+@pytest.mark.parametrize("case", ["config2_3d_walls", "config3_springs", "config1_2d"])
+def test_launch_shapes_match_oracle(case, shape):
+    """Every launch shape gives the oracle's state bit for bit."""
+    mesh, params, a = _cases()[case]()
+    o, d = gu.make_pair(mesh, params, a)
+    d.set_launch_shape(*shape)
+    o.update_mechanics_mesh()
+    o.update_cell_neighbors()
+    d.update_mechanics_mesh()
+    for _ in range(2):
+        o.step(5, 0, 0.0, 0.0)
+        d.step(5)
+        gu.assert_same_state(gu.fetch(d, a), gu.fetch(o, a))
+
+
+def test_single_pass_scan_on_a_large_grid():
+    """An 8000 um cube (267^3 voxels, 4,650 scan tiles, more than the GPU
+    holds at once) binned and stepped: bins and state equal the oracle's, so
+    the look-back scan is exact when tiles run in several waves."""
+    mesh, params, a = wl.config5(seed=31, n=6000, radius=2900.0, cube=8000)
+    o, d = gu.make_pair(mesh, params, a)
+    o.update_mechanics_mesh()
+    o.update_cell_neighbors()
+    d.update_mechanics_mesh()
+    gu.assert_same_bins(d, o)
+    o.step(3, 0, 0.0, 0.0)
+    d.step(3)
+    gu.assert_same_state(gu.fetch(d, a), gu.fetch(o, a))
+    gu.assert_same_bins(d, o)
+
+
 def test_graph_replay_matches_oracle():
     """A block of steps long enough to be captured and replayed as a CUDA
     graph gives the same state as the oracle."""
