@@ -52,6 +52,10 @@ WORKLOADS = {
 }
 
 
+ENSEMBLE = ("256 independent 3-D replicates, N_r log-uniform in [500, 50000], cube side 20 ceil(N_r^(1/3)) um, "
+            "one type, FP64, one batched state")
+
+
 def make_workload(name):
     from paraphysicell_b200 import workloads as wl
     return {"config1": wl.config1, "config2": wl.config2, "config3": wl.config3, "config5": wl.config5}[name]()
@@ -252,6 +256,95 @@ def fp32_form(args, mesh, params, a, ph, flush):
                     "positions/binning/integration; same L2-flushed protocol as value"}
 
 
+def _timed_steps(sim, stream, step, count, K, warmup, flush):
+    """Device-timed K steps with L2 flushed before each, the fused pass's
+    average duration, and back-to-back (graph-replayed) steady state."""
+    import torch
+
+    with torch.cuda.stream(stream):
+        step(max(warmup, 3))
+    sim.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    agent_steps = 0.0
+    torch.cuda.synchronize()
+    sim.set_profiling(True)
+    with torch.cuda.stream(stream):
+        for k in range(K):
+            n = count()
+            flush.zero_()
+            starts[k].record(stream)
+            step(1)
+            ends[k].record(stream)
+            agent_steps += 0.5 * (n + count())
+    torch.cuda.synchronize()
+    fused_ms, fused_n = sim.profile()
+    sim.set_profiling(False)
+    total_ms = sum(x.elapsed_time(y) for x, y in zip(starts, ends))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0 = count()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        step(max(K, 10))
+        e1.record(stream)
+    torch.cuda.synchronize()
+    steady = 0.5 * (n0 + count()) * max(K, 10) / (e0.elapsed_time(e1) / 1e3)
+    return {"value": agent_steps / (total_ms / 1e3), "unit": UNIT, "ms_per_step": total_ms / K,
+            "steady_state": steady, "fused_avg_us": fused_ms / max(fused_n, 1) * 1e3}
+
+
+def ensemble_form(args, flush):
+    """Config 4: 256 independent replicates of 500..50,000 agents in one
+    batched state (one launch per kernel per step for all replicates, CUDA
+    graphs over blocks of steps)."""
+    import torch
+
+    from paraphysicell_b200 import workloads as wl
+    from paraphysicell_b200.device import Simulation
+
+    meshes, params, sets = wl.config4()
+    sim = Simulation(meshes, params, [a.capacity for a in sets], seed=1)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    for r, a in enumerate(sets):
+        sim.upload(a, replicate=r)
+    sim.update_mechanics_mesh()
+    total = sum(a.count for a in sets)
+    with torch.cuda.stream(stream):
+        shape = sim.autotune(steps=5)
+    out = _timed_steps(sim, stream, sim.step, lambda: total, args.steps, args.warmup, flush)
+    out["launch_shape"] = {"tile_edge": shape[0], "threads": shape[1], "chosen_by": "ppc_autotune"}
+    sim.close()
+    out.update({"workload": "config4", "replicates": len(sets), "agents": total,
+                "description": ENSEMBLE})
+    return out
+
+
+def config5_form(args, flush):
+    """Config 5: 1,000,000 agents with division and death every step."""
+    import torch
+
+    from paraphysicell_b200 import workloads as wl
+    from paraphysicell_b200.device import Simulation
+
+    mesh, params, a = wl.config5()
+    sim = Simulation(mesh, params, a.capacity, seed=1)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    sim.upload(a)
+    sim.update_mechanics_mesh()
+    with torch.cuda.stream(stream):
+        shape = sim.autotune(steps=5)
+    out = _timed_steps(sim, stream, lambda k: sim.step_with_phenotype(k, wl.P_DIVIDE, wl.P_DEATH), sim.count,
+                       args.steps, args.warmup, flush)
+    out["launch_shape"] = {"tile_edge": shape[0], "threads": shape[1], "chosen_by": "ppc_autotune"}
+    divisions, deaths = sim.event_counts()
+    sim.close()
+    out.update({"workload": "config5", "agents": a.count, "divisions": divisions, "deaths": deaths,
+                "description": WORKLOADS["config5"]})
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -409,6 +502,9 @@ def run_ours(args, rank, world, local_rank):
     }
     if not args.no_forms:
         line["forms"] = {"fp32_force": fp32_form(args, mesh, params, a, ph, flush)}
+        if args.workload == "config3":
+            line["forms"]["batched_ensemble"] = ensemble_form(args, flush)
+            line["forms"]["config5_division_death"] = config5_form(args, flush)
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(args.workload)
     print(json.dumps(line), flush=True)

@@ -179,6 +179,16 @@ int ppc_set_random_seed(ppc_state* s, uint64_t seed);
  * multiple of 32. Results do not depend on the shape. */
 int ppc_set_launch_shape(ppc_state* s, int32_t tile_edge, int32_t threads, int32_t smem_bytes);
 
+/* Autotuner of the launch shape (no counterpart in the reference, whose
+ * OpenMP loops have no launch shape): runs 2 x `steps` mechanics steps
+ * (ppc_step) with each candidate shape — global-memory candidates with 128
+ * and 64 threads, shared-memory staging with 128 threads / 32 KiB and 64
+ * threads / 16 KiB — times the second half of each on the state's stream,
+ * and keeps the fastest. The simulation advances by 8 x `steps` steps (the
+ * trajectory does not depend on the shape). Writes the chosen shape to
+ * `tile_edge` and `threads` when they are not NULL. */
+int ppc_autotune(ppc_state* s, int32_t steps, int32_t* tile_edge, int32_t* threads);
+
 /* Neighbour-list capacity per agent for ppc_update_cell_neighbors (default 64). */
 int ppc_set_neighbor_capacity(ppc_state* s, int32_t per_agent);
 

@@ -947,6 +947,54 @@ int ppc_step(ppc_state* s, int32_t steps)
 	return run_steps(s, steps, false, 0, 0);
 }
 
+int ppc_autotune(ppc_state* s, int32_t steps, int32_t* tile_edge, int32_t* threads)
+{
+	if (!s || steps < 1)
+		return fail(PPC_ERR_ARG, "autotune needs a state and steps >= 1");
+	struct shape
+	{
+		int edge, threads, smem;
+	};
+	const shape cand[] = { { -1, 128, 0 }, { -1, 64, 0 }, { 0, 128, 32 * 1024 }, { 0, 64, 16 * 1024 } };
+	cudaEvent_t e0 = nullptr, e1 = nullptr;
+	PPC_CUDA(cudaEventCreate(&e0));
+	PPC_CUDA(cudaEventCreate(&e1));
+	int best = -1;
+	float best_ms = 0.f;
+	int rc = PPC_OK;
+	for (int k = 0; k < 4 && rc == PPC_OK; k++)
+	{
+		rc = ppc_set_launch_shape(s, cand[k].edge, cand[k].threads, cand[k].smem);
+		if (rc == PPC_OK)
+			rc = run_steps(s, steps, false, 0, 0); // warm-up: graph capture of this shape
+		if (rc != PPC_OK)
+			break;
+		float ms = 0.f;
+		if (cudaEventRecord(e0, s->stream) != cudaSuccess)
+			rc = fail(PPC_ERR_CUDA, "cudaEventRecord failed");
+		if (rc == PPC_OK)
+			rc = run_steps(s, steps, false, 0, 0);
+		if (rc == PPC_OK
+			&& (cudaEventRecord(e1, s->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess
+				|| cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+			rc = fail(PPC_ERR_CUDA, "timing the candidate shape failed");
+		if (rc == PPC_OK && (best < 0 || ms < best_ms))
+		{
+			best = k;
+			best_ms = ms;
+		}
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	PPC_TRY(rc);
+	PPC_TRY(ppc_set_launch_shape(s, cand[best].edge, cand[best].threads, cand[best].smem));
+	if (tile_edge)
+		*tile_edge = cand[best].edge;
+	if (threads)
+		*threads = cand[best].threads;
+	return PPC_OK;
+}
+
 int ppc_step_with_phenotype(ppc_state* s, int32_t steps, double p_divide, double p_death)
 {
 	if (!s)

@@ -34,7 +34,7 @@ EXPORTS = (
     "ppc_get_event_counts", "ppc_flag_by_draws", "ppc_step", "ppc_step_with_phenotype",
     "ppc_get_neighbors", "ppc_get_mesh_bins", "ppc_get_voxel_count", "ppc_get_mesh_position",
     "ppc_get_mesh_index", "ppc_get_launch_count", "ppc_last_error", "ppc_abi_version",
-    "ppc_set_profiling", "ppc_get_profile", "ppc_set_launch_shape",
+    "ppc_set_profiling", "ppc_get_profile", "ppc_set_launch_shape", "ppc_autotune",
 ) + tuple("ppc_" + e for e in ENTRY_POINTS)
 
 
@@ -74,6 +74,7 @@ def lib():
         L.ppc_get_launch_count.argtypes = [vp, C.POINTER(C.c_int64)]
         L.ppc_set_profiling.argtypes = [vp, C.c_int32]
         L.ppc_set_launch_shape.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32]
+        L.ppc_autotune.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.ppc_get_profile.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
         L.ppc_last_error.restype = C.c_char_p
         for e in ENTRY_POINTS:
@@ -185,6 +186,14 @@ class Simulation:
 
     def set_launch_shape(self, tile_edge, threads, smem_bytes=32 * 1024):
         _check(lib().ppc_set_launch_shape(self.h, tile_edge, threads, smem_bytes), "ppc_set_launch_shape")
+
+    def autotune(self, steps=10):
+        """Times each candidate launch shape over `steps` steps (after as many
+        warm-up steps) and keeps the fastest; returns (tile_edge, threads).
+        The simulation advances by 8 x steps steps."""
+        e, t = C.c_int32(), C.c_int32()
+        _check(lib().ppc_autotune(self.h, steps, C.byref(e), C.byref(t)), "ppc_autotune")
+        return e.value, t.value
 
     def set_profiling(self, on):
         _check(lib().ppc_set_profiling(self.h, int(bool(on))), "ppc_set_profiling")

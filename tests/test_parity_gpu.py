@@ -140,10 +140,28 @@ def test_launch_shapes_match_oracle(case, shape):
         gu.assert_same_state(gu.fetch(d, a), gu.fetch(o, a))
 
 
-def test_single_pass_scan_on_a_large_grid():
+def test_autotune_keeps_the_trajectory():
+    """The autotuner runs 8 x steps real steps over its candidate shapes and
+    keeps one of them; the state then equals the oracle's after as many
+    steps, and stepping on with the chosen shape stays equal."""
+    mesh, params, a = _cases()["config3_springs"]()
+    o, d = gu.make_pair(mesh, params, a)
+    o.update_mechanics_mesh()
+    o.update_cell_neighbors()
+    d.update_mechanics_mesh()
+    edge, threads = d.autotune(steps=3)
+    assert (edge, threads) in {(-1, 128), (-1, 64), (0, 128), (0, 64)}
+    o.step(24, 0, 0.0, 0.0)
+    gu.assert_same_state(gu.fetch(d, a), gu.fetch(o, a))
+    o.step(7, 0, 0.0, 0.0)
+    d.step(7)
+    gu.assert_same_state(gu.fetch(d, a), gu.fetch(o, a))
+
+
+def test_binning_on_a_large_grid():
     """An 8000 um cube (267^3 voxels, 4,650 scan tiles, more than the GPU
     holds at once) binned and stepped: bins and state equal the oracle's, so
-    the look-back scan is exact when tiles run in several waves."""
+    the two-pass scan is exact when tiles run in several waves."""
     mesh, params, a = wl.config5(seed=31, n=6000, radius=2900.0, cube=8000)
     o, d = gu.make_pair(mesh, params, a)
     o.update_mechanics_mesh()
