@@ -977,7 +977,7 @@ __global__ void __launch_bounds__(kStageThreads, PPC_STAGE_MINB) k_fused_staged(
 		stencil_bounds<DIMS>(v, R, v.skey[tt], lo, hi);
 #pragma unroll
 		for (int k = 0; k < NR; k++)
-			s_rows[k][threadIdx.x] = make_int2(lo[k], hi[k]);
+			s_rows[k][threadIdx.x] = act ? make_int2(lo[k], hi[k]) : make_int2(0, 0);
 	}
 
 	__syncthreads();
@@ -991,8 +991,6 @@ __global__ void __launch_bounds__(kStageThreads, PPC_STAGE_MINB) k_fused_staged(
 		stage[i] = v.sposf[s_a[k] + (i - s_o[k])];
 	}
 	__syncthreads();
-	if (!act)
-		return;
 
 	// candidates at array positions u of row k are read at P[u + soff(k)]:
 	// shared memory when staged, else the global sposf
@@ -1000,99 +998,218 @@ __global__ void __launch_bounds__(kStageThreads, PPC_STAGE_MINB) k_fused_staged(
 	const float4* P = staged ? stage : v.sposf;
 	const int D = v.ndefs;
 	const float margin = R.fmargin;
-	pair_fp64 acc;
-	acc.prm_i = qi;
-	acc.def_i = def_i;
-	acc.mov_i = mov_i;
-	acc.aff_i = v.saff + (int64_t)t * D;
 	const double4 vel0 = (VEL && mov_i) ? v.vel[s] : make_double4(0, 0, 0, 0);
-	acc.vx = vel0.x;
-	acc.vy = vel0.y;
-	acc.vz = vel0.z;
-	pair_fp32 accf;
-	if (F32)
-	{
-		const float4 qf = v.sprmf[t];
-		accf.r_i = qf.x;
-		accf.rep_i = qf.y;
-		accf.adh_i = qf.z;
-		accf.def_i = def_i;
-		accf.mov_i = mov_i;
-		accf.aff_i = v.safff + (int64_t)t * D;
-	}
+	// FP64 sums (drop-in) or Neumaier-compensated FP32 sums (FP32-force form)
+	double vx = vel0.x, vy = vel0.y, vz = vel0.z, pressure = 0.0;
+	nsum fx, fy, fz, fp;
 
-	// one kept candidate at array position u: the exact FP64 predicate, then
-	// the pair code, with the operations of the unstaged kernels
-	auto pair = [&](int u) {
-		const double4 q = v.spos4[u];
-		const double ddx = pi.x - q.x;
-		const double ddy = DIMS >= 2 ? pi.y - q.y : 0.0;
-		const double ddz = DIMS >= 3 ? pi.z - q.z : 0.0;
-		double d2 = ddx * ddx;
-		if (DIMS >= 2)
-			d2 = d2 + ddy * ddy;
-		if (DIMS >= 3)
-			d2 = d2 + ddz * ddz;
-		const double ad = pi.w + q.w;
-		const double dist = DIMS == 1 ? fabs(ddx) : sqrt(d2);
-		if (!(dist <= ad))
-			return;
-		if (F32)
-		{
-			const float dx = (float)ddx, dy = (float)ddy, dz = (float)ddz;
-			float d2f = dx * dx;
-			if (DIMS >= 2)
-				d2f = d2f + dy * dy;
-			if (DIMS >= 3)
-				d2f = d2f + dz * dz;
-			const float distf = DIMS == 1 ? fabsf(dx) : sqrtf(d2f);
-			const float4 qj = v.sprmf[u];
-			const float4 pj = v.sposf[u];
-			int def_j, spr_j;
-			bool mov_j;
-			unpack_fbits(qj.w, def_j, mov_j, spr_j);
-			accf.add(qj.x, qj.y, qj.z, def_j, mov_j, v.safff[(int64_t)u * D + def_i], dx, dy, dz, distf, pf.w + pj.w);
-		}
-		else
-		{
-			const double4 qj = v.sprm4[u];
-			int def_j;
-			bool mov_j;
-			unpack_bits(qj.w, def_j, mov_j);
-			acc.add_pair(qj.x, qj.y, qj.z, def_j, mov_j, v.saff[(int64_t)u * D + def_i], ddx, ddy, ddz, dist, ad);
-		}
-	};
+	// Warp-cooperative pair phase. Each lane collects its kept candidates
+	// in `list`; when a lane's list is full, or the scan ends, the warp
+	// spreads all lanes' entries over its 32 lanes (lane q of a round takes
+	// the q-th entry in lane order), each lane runs the exact predicate and
+	// the pair arithmetic for its entry and leaves the terms in shared memory,
+	// and every owner then adds its own terms in list order, which is the
+	// reference's neighbour order. The additions, their operands and their
+	// order are those of the sequential pair code.
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	__shared__ uint8_t s_owner[kStageThreads / 32][32 * kList];
+	__shared__ double4 s_term[kStageThreads / 32][32]; // {v_x, v_y, v_z, pressure} terms of one pair
+	__shared__ int s_flag[kStageThreads / 32][32];	   // 1 accepted, 2 neighbour movable
+	const int32_t* lists = reinterpret_cast<const int32_t*>(stage + cap) + warp * 32;
 	int n = 0;
-#pragma unroll 1
-	for (int k = 0; k < NR; k++)
-	{
-		const int2 b = s_rows[k][threadIdx.x];
-		const int soff = staged ? s_o[k] - s_a[k] : 0;
-		for (int u = b.x; u < b.y; u++)
+	auto flush = [&]() {
+		int off = n;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1)
 		{
-			if (u == t || !filter_keep<DIMS>(pf, P[u + soff], margin))
-				continue;
-			list[n * stride] = u;
-			if (++n == kList)
-			{
-				for (int m = 0; m < n; m++)
-					pair(list[m * stride]);
-				n = 0;
-			}
+			const int y = __shfl_up_sync(0xffffffffu, off, o);
+			if (lane >= o)
+				off += y;
 		}
-	}
-	for (int m = 0; m < n; m++)
-		pair(list[m * stride]);
+		const int total = __shfl_sync(0xffffffffu, off, 31);
+		off -= n;
+		for (int m = 0; m < n; m++)
+			s_owner[warp][off + m] = (uint8_t)lane;
+		__syncwarp();
+		for (int base = 0; base < total; base += 32)
+		{
+			const int q = base + lane;
+			const int o = q < total ? s_owner[warp][q] : lane;
+			const int off_o = __shfl_sync(0xffffffffu, off, o);
+			const int t_o = __shfl_sync(0xffffffffu, t, o);
+			const int def_o = __shfl_sync(0xffffffffu, def_i, o);
+			const bool mov_o = __shfl_sync(0xffffffffu, (int)mov_i, o) != 0;
+			const double px = __shfl_sync(0xffffffffu, pi.x, o);
+			const double py = __shfl_sync(0xffffffffu, pi.y, o);
+			const double pz = __shfl_sync(0xffffffffu, pi.z, o);
+			const double pw = __shfl_sync(0xffffffffu, pi.w, o);
+			const double ri = __shfl_sync(0xffffffffu, qi.x, o);
+			const double repi = __shfl_sync(0xffffffffu, qi.y, o);
+			const double adhi = __shfl_sync(0xffffffffu, qi.z, o);
+			const float pfw = __shfl_sync(0xffffffffu, pf.w, o);
+			if (q < total)
+			{
+				const int u = lists[(q - off_o) * stride + o];
+				const double4 qp = v.spos4[u];
+				const double ddx = px - qp.x;
+				const double ddy = DIMS >= 2 ? py - qp.y : 0.0;
+				const double ddz = DIMS >= 3 ? pz - qp.z : 0.0;
+				double d2 = ddx * ddx;
+				if (DIMS >= 2)
+					d2 = d2 + ddy * ddy;
+				if (DIMS >= 3)
+					d2 = d2 + ddz * ddz;
+				const double ad = pw + qp.w;
+				const double dist = DIMS == 1 ? fabs(ddx) : sqrt(d2);
+				int fl = 0;
+				double4 tm = make_double4(0, 0, 0, 0);
+				if (dist <= ad)
+				{
+					fl = 1;
+					if (F32)
+					{
+						// pair_fp32::add with the owner's values
+						const float dx = (float)ddx, dy = (float)ddy, dz = (float)ddz;
+						float d2f = dx * dx;
+						if (DIMS >= 2)
+							d2f = d2f + dy * dy;
+						if (DIMS >= 3)
+							d2f = d2f + dz * dz;
+						const float distf = DIMS == 1 ? fabsf(dx) : sqrtf(d2f);
+						const float4 qj = v.sprmf[u];
+						const float4 pj = v.sposf[u];
+						int def_j, spr_j;
+						bool mov_j;
+						unpack_fbits(qj.w, def_j, mov_j, spr_j);
+						fl |= mov_j ? 2 : 0;
+						const float d = distf < 0.00001f ? 0.00001f : distf;
+						float rep = 1.f - d / ((float)ri + qj.x);
+						rep = rep < 0.f ? 0.f : rep;
+						rep = rep * rep;
+						const float term = rep * 36.64504274775163f;
+						tm.w = (double)term;
+						if (mov_o)
+						{
+							rep = rep * sqrtf((float)repi * qj.y);
+							float adh = 1.f - d / (pfw + pj.w);
+							adh = adh * adh;
+							adh = adh * sqrtf((float)adhi * qj.z * v.safff[(int64_t)t_o * D + def_j]
+											  * v.safff[(int64_t)u * D + def_o]);
+							const float force = (rep - adh) / d;
+							tm.x = (double)(force * dx);
+							tm.y = (double)(force * dy);
+							tm.z = (double)(force * dz);
+						}
+					}
+					else
+					{
+						// pair_fp64::add_pair with the owner's values
+						const double4 qj = v.sprm4[u];
+						int def_j;
+						bool mov_j;
+						unpack_bits(qj.w, def_j, mov_j);
+						fl |= mov_j ? 2 : 0;
+						const double d = dist < 0.00001 ? 0.00001 : dist;
+						double rep = 1.0 - d / (ri + qj.x);
+						rep = rep < 0 ? 0 : rep;
+						rep = rep * rep;
+						tm.w = rep * simple_pressure_coefficient;
+						if (mov_o)
+						{
+							rep = rep * sqrt(repi * qj.y);
+							double adh = 1.0 - d / ad;
+							adh = adh * adh;
+							adh = adh * sqrt(adhi * qj.z * v.saff[(int64_t)t_o * D + def_j] * v.saff[(int64_t)u * D + def_o]);
+							const double force = (rep - adh) / d;
+							tm.x = force * ddx;
+							tm.y = force * ddy;
+							tm.z = force * ddz;
+						}
+					}
+				}
+				s_term[warp][lane] = tm;
+				s_flag[warp][lane] = fl;
+			}
+			__syncwarp();
+			const int lo = max(off, base), hi = min(off + n, base + 32);
+			for (int qq = lo; qq < hi; qq++)
+			{
+				const int fl = s_flag[warp][qq - base];
+				if (!(fl & 1))
+					continue;
+				const double4 tm = s_term[warp][qq - base];
+				if (F32)
+				{
+					if (mov_i)
+						fp.add((float)tm.w);
+					if (fl & 2)
+						fp.add((float)tm.w);
+					if (mov_i)
+					{
+						fx.add((float)tm.x);
+						fy.add((float)tm.y);
+						fz.add((float)tm.z);
+					}
+				}
+				else
+				{
+					if (mov_i)
+						pressure = pressure + tm.w;
+					if (fl & 2)
+						pressure = pressure + tm.w;
+					if (mov_i)
+					{
+						vx = vx + tm.x;
+						vy = vy + tm.y;
+						vz = vz + tm.z;
+					}
+				}
+			}
+			__syncwarp();
+		}
+		n = 0;
+	};
 
+	// warp-uniform scan: one candidate per lane per iteration, rows in order
+	int k = 0;
+	int2 b = s_rows[0][threadIdx.x];
+	int soff = staged ? s_o[0] - s_a[0] : 0;
+	int u = b.x;
+	while (true)
+	{
+		while (u >= b.y && k + 1 < NR)
+		{
+			k++;
+			b = s_rows[k][threadIdx.x];
+			soff = staged ? s_o[k] - s_a[k] : 0;
+			u = b.x;
+		}
+		const bool has = u < b.y;
+		if (!__any_sync(0xffffffffu, has))
+			break;
+		if (has)
+		{
+			if (u != t && filter_keep<DIMS>(pf, P[u + soff], margin))
+			{
+				list[n * stride] = u;
+				n++;
+			}
+			u++;
+		}
+		if (__any_sync(0xffffffffu, n == kList))
+			flush();
+	}
+	flush();
+	if (!act)
+		return;
 	double4 p = make_double4(pi.x, pi.y, pi.z, 0.0);
 	double4 vp = mov_i ? v.vprev[s] : make_double4(0, 0, 0, 0);
-	double vx = acc.vx, vy = acc.vy, vz = acc.vz, pressure = acc.p;
 	if (F32)
 	{
-		vx = vel0.x + accf.vx.value();
-		vy = vel0.y + accf.vy.value();
-		vz = vel0.z + accf.vz.value();
-		pressure = accf.p.value();
+		vx = vel0.x + fx.value();
+		vy = vel0.y + fy.value();
+		vz = vel0.z + fz.value();
+		pressure = fp.value();
 	}
 	if (mov_i)
 	{
