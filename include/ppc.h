@@ -170,20 +170,24 @@ int ppc_set_precision(ppc_state* s, int32_t precision);
  * per-thread mt19937 (src/random.cpp:8-49) for division directions. */
 int ppc_set_random_seed(ppc_state* s, uint64_t seed);
 
-/* Launch shape of the fused force pass (one thread per agent): `tile_edge` -1
- * (the default) reads the candidates from global memory; 0 stages each
- * block's candidate ranges in `smem_bytes` of shared memory per block
- * (32 KiB is a good budget; a block whose ranges do not fit reads global
- * memory), `threads` per block capped at 128 — faster where agents are dense
- * (about one per voxel), slower where they are sparse. `threads` 32..256, a
- * multiple of 32. Results do not depend on the shape. */
+/* Launch shape of the fused force pass, one thread per agent in every shape:
+ *  -1 (the default): each thread reads its candidates from global memory and
+ *     runs its own pair code — best where agents are sparse (well under one
+ *     per voxel);
+ *  -2: the pair code of a warp's kept candidates is spread over the warp's
+ *     32 lanes, candidates read from global memory;
+ *   0: as -2, with each block's candidate ranges staged in `smem_bytes` of
+ *     shared memory (32 KiB is a good budget; a block whose ranges do not fit
+ *     reads global memory) — best where agents are dense.
+ * `threads` per block 32..256, a multiple of 32 (the fused pass uses at most
+ * 128). Results do not depend on the shape; ppc_autotune picks one. */
 int ppc_set_launch_shape(ppc_state* s, int32_t tile_edge, int32_t threads, int32_t smem_bytes);
 
 /* Autotuner of the launch shape (no counterpart in the reference, whose
  * OpenMP loops have no launch shape): runs 2 x `steps` mechanics steps
- * (ppc_step) with each candidate shape — global-memory candidates with 128
- * and 64 threads, shared-memory staging with 128 threads / 32 KiB and 64
- * threads / 16 KiB — times the second half of each on the state's stream,
+ * (ppc_step) with each candidate shape — -1 and -2 with 128 threads, 0 with
+ * 128 threads / 32 KiB and with 64 threads / 16 KiB — times the second half
+ * of each on the state's stream,
  * and keeps the fastest. The simulation advances by 8 x `steps` steps (the
  * trajectory does not depend on the shape). Writes the chosen shape to
  * `tile_edge` and `threads` when they are not NULL. */

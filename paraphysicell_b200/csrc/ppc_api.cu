@@ -726,12 +726,13 @@ int ppc_set_launch_shape(ppc_state* s, int32_t tile_edge, int32_t threads, int32
 {
 	if (!s)
 		return fail(PPC_ERR_ARG, "null state");
-	if ((tile_edge != 0 && tile_edge != -1) || threads < 32 || threads > 256 || threads % 32 != 0 || smem_bytes < 0
+	if ((tile_edge != 0 && tile_edge != -1 && tile_edge != -2) || threads < 32 || threads > 256 || threads % 32 != 0 || smem_bytes < 0
 		|| smem_bytes > 160 * 1024)
-		return fail(PPC_ERR_ARG, "tile edge 0 or -1, threads 32..256 (multiple of 32), smem <= 160 KiB");
+		return fail(PPC_ERR_ARG, "tile edge 0, -1 or -2, threads 32..256 (multiple of 32), smem <= 160 KiB");
 	PPC_CUDA(cudaStreamSynchronize(s->stream));
 	release_graph(s);
 	s->staged = tile_edge == 0;
+	s->coop = tile_edge != -1;
 	s->tile_threads = threads;
 	s->tile_smem = smem_bytes;
 	return PPC_OK;
@@ -955,7 +956,7 @@ int ppc_autotune(ppc_state* s, int32_t steps, int32_t* tile_edge, int32_t* threa
 	{
 		int edge, threads, smem;
 	};
-	const shape cand[] = { { -1, 128, 0 }, { -1, 64, 0 }, { 0, 128, 32 * 1024 }, { 0, 64, 16 * 1024 } };
+	const shape cand[] = { { -1, 128, 0 }, { -2, 128, 0 }, { 0, 128, 32 * 1024 }, { 0, 64, 16 * 1024 } };
 	cudaEvent_t e0 = nullptr, e1 = nullptr;
 	PPC_CUDA(cudaEventCreate(&e0));
 	PPC_CUDA(cudaEventCreate(&e1));

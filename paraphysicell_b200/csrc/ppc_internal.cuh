@@ -182,10 +182,12 @@ struct ppc_state
 	int64_t graph_launches = 0;
 	bool use_graphs = true;
 
-	// fused pass launch shape: candidates read from global memory (default)
-	// or the block's candidate ranges staged in shared memory; threads per
-	// block; staging bytes per block
+	// fused pass launch shape: one thread per agent with its own pair work
+	// (default), or warp-cooperative pair work with candidates read from
+	// global memory or from the block's ranges staged in shared memory;
+	// threads per block; staging bytes per block
 	bool staged = false;
+	bool coop = false;
 	int tile_threads = 128;
 	int tile_smem = 32 * 1024;
 

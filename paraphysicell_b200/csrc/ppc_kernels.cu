@@ -918,8 +918,14 @@ __global__ void __launch_bounds__(kStageThreads, PPC_STAGE_MINB) k_fused_staged(
 	const bool act = t <= tl;
 
 	// block set-up (warp 0): the row ranges and their offsets in shared memory
-	if (threadIdx.x < 32)
+	if (cap == 0)
 	{
+		if (threadIdx.x == 0)
+			s_o[NR] = -1; // no staging: every candidate is read from global memory
+	}
+	else if (threadIdx.x < 32)
+	{
+		// the whole of warp 0 takes this branch (cap is uniform)
 		const int lane = threadIdx.x;
 		const int r0 = rep_of(v, v.sorted[t0]), r1 = rep_of(v, v.sorted[tl]);
 		const int64_t kf = v.skey[t0], kl = v.skey[tl];
@@ -2040,7 +2046,7 @@ static int staged_dispatch(ppc_state* s)
 	cudaStream_t st = PPC_LAUNCH(s);
 	const int nt = std::min(s->tile_threads, kStageThreads);
 	const int list_bytes = kList * nt * (int)sizeof(int32_t);
-	const int cap = std::max(0, (s->tile_smem - list_bytes) / (int)sizeof(float4));
+	const int cap = s->staged ? std::max(0, (s->tile_smem - list_bytes) / (int)sizeof(float4)) : 0;
 	const size_t dyn = (size_t)cap * sizeof(float4) + list_bytes;
 	const int b = blocks_for(s->total_cap, nt);
 #define PPC_STAGED(W, S, V, F)                                                                                         \
@@ -2086,7 +2092,7 @@ int launch_fused(ppc_state* s)
 		ev_end = s->prof_events[s->prof_used + 1];
 		s->prof_used += 2;
 	}
-	if (s->staged)
+	if (s->staged || s->coop)
 	{
 		int rc = s->dims == 1 ? staged_dispatch<1>(s) : (s->dims == 2 ? staged_dispatch<2>(s) : staged_dispatch<3>(s));
 		if (rc != PPC_OK)

@@ -117,11 +117,12 @@ def test_fused_steps_match_oracle(case):
 
 
 # launch shapes of the fused pass: (tile edge, threads, shared-memory bytes).
-# Edge 0 stages each block's candidate ranges in shared memory (the
-# default); a budget of 4 KiB leaves no room for them, so blocks read the
-# global arrays instead; edge -1 reads every candidate from global memory.
-SHAPES = [(0, 128, 32 * 1024), (0, 128, 40 * 1024), (0, 64, 4 * 1024), (0, 96, 24 * 1024), (-1, 128, 0),
-          (-1, 256, 0)]
+# -1 is one thread per agent with its own pair code (the default); -2
+# spreads the pair code over the warp; 0 does that with each block's
+# candidate ranges staged in shared memory, and a budget of 4 KiB leaves no
+# room for them, so blocks read the global arrays instead.
+SHAPES = [(-1, 128, 0), (-1, 256, 0), (-2, 128, 0), (-2, 64, 0), (0, 128, 32 * 1024), (0, 128, 40 * 1024),
+          (0, 64, 4 * 1024), (0, 96, 24 * 1024)]
 
 
 @pytest.mark.parametrize("shape", SHAPES, ids=lambda s: "edge%d_t%d_smem%d" % s)
@@ -150,7 +151,7 @@ def test_autotune_keeps_the_trajectory():
     o.update_cell_neighbors()
     d.update_mechanics_mesh()
     edge, threads = d.autotune(steps=3)
-    assert (edge, threads) in {(-1, 128), (-1, 64), (0, 128), (0, 64)}
+    assert (edge, threads) in {(-1, 128), (-2, 128), (0, 128), (0, 64)}
     o.step(24, 0, 0.0, 0.0)
     gu.assert_same_state(gu.fetch(d, a), gu.fetch(o, a))
     o.step(7, 0, 0.0, 0.0)
