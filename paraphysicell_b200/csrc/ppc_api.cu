@@ -630,6 +630,7 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.key, C));
 	try_(alloc(s, v.vrank, C));
 	try_(alloc(s, v.tmp, C));
+	try_(alloc(s, v.vsc, C));
 	try_(alloc(s, v.sorted, C));
 	try_(alloc(s, v.skey, C));
 	try_(alloc(s, v.spos4, C));

@@ -111,6 +111,7 @@ struct view
 	int32_t* key;
 	int32_t* vrank;
 	int32_t* tmp;
+	int2* vsc;		// [C] voxel start and count of each slot's voxel, from the scatter to the fixup
 	int32_t* sorted;
 	int32_t* skey;
 	double4* spos4;

@@ -225,6 +225,8 @@ __global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
 	}
 }
 
+// provisional scatter; also hands the fixup its voxel's start and count so
+// the fixup need not look them up again
 __global__ void k_bin_scatter(view v)
 {
 	grid_wait();
@@ -234,11 +236,17 @@ __global__ void k_bin_scatter(view v)
 	int r, local;
 	if (!live(v, s, r, local))
 		return;
-	v.tmp[v.vstart[v.key[s]] + v.vrank[s]] = s;
+	const int32_t key = v.key[s];
+	const int rank = v.vrank[s];
+	const int st = v.vstart[key];
+	const int c = v.vcnt[key];
+	v.tmp[st + rank] = s;
+	v.vsc[s] = make_int2(st, c);
 }
 
 // final place inside the voxel: descending slot order, which is the order
-// a serial run of the reference's fetch_sub scatter produces
+// a serial run of the reference's fetch_sub scatter produces. Affinity rows
+// of up to four definitions are carried in registers.
 __global__ void k_bin_fixup(view v, int cur)
 {
 	grid_wait();
@@ -249,21 +257,23 @@ __global__ void k_bin_fixup(view v, int cur)
 	if (!live(v, s, r, local))
 		return;
 	const int32_t key = v.key[s];
+	const int2 sc = v.vsc[s];
 	const double4 prm = v.prm[s];
 	double4 p = v.pos[cur][s];
 	const double rmad = v.rmad[s];
 	const long long bits = (long long)(uint32_t)v.def[s] | ((long long)(v.movable[s] != 0) << 32)
 						   | ((long long)min(v.scnt[s], 255) << 40);
-	double aff[8];
 	const int D = v.ndefs;
-	for (int q = 0; q < D && q < 8; q++)
-		aff[q] = v.aff[(int64_t)s * D + q];
-	const int st = v.vstart[key];
-	const int c = v.vstart[key + 1] - st;
+	double aff[4];
+#pragma unroll
+	for (int q = 0; q < 4; q++)
+		aff[q] = q < D ? v.aff[(int64_t)s * D + q] : 0.0;
+	const rep_info& R = v.reps[r];
+	const double m0 = R.mins[0], m1 = R.mins[1], m2 = R.mins[2];
 	int rank = 0;
-	for (int u = 0; u < c; u++)
-		rank += v.tmp[st + u] > s;
-	const int t = st + rank;
+	for (int u = 0; u < sc.y && sc.y > 1; u++)
+		rank += v.tmp[sc.x + u] > s;
+	const int t = sc.x + rank;
 	p.w = rmad * prm.x; // relative_maximum_adhesion_distance * radius
 	if (rank == 0)
 		v.vcnt[key] = 0; // ready for the next rebuild
@@ -271,22 +281,26 @@ __global__ void k_bin_fixup(view v, int cur)
 	v.skey[t] = key;
 	v.spos4[t] = p;
 	v.sprm4[t] = make_double4(prm.x, prm.y, prm.z, __longlong_as_double(bits));
-	for (int q = 0; q < D; q++)
-		v.saff[(int64_t)t * D + q] = q < 8 ? aff[q] : v.aff[(int64_t)s * D + q];
-	{
-		// single-precision positions relative to the box minimum: the
-		// candidate filter of the fused pass
-		const rep_info& R = v.reps[r];
-		v.sposf[t] = make_float4((float)(p.x - R.mins[0]), (float)(p.y - R.mins[1]), (float)(p.z - R.mins[2]),
-								 (float)p.w);
-	}
+#pragma unroll
+	for (int q = 0; q < 4; q++)
+		if (q < D)
+			v.saff[(int64_t)t * D + q] = aff[q];
+	for (int q = 4; q < D; q++)
+		v.saff[(int64_t)t * D + q] = v.aff[(int64_t)s * D + q];
+	// single-precision positions relative to the box minimum: the candidate
+	// filter of the fused pass
+	v.sposf[t] = make_float4((float)(p.x - m0), (float)(p.y - m1), (float)(p.z - m2), (float)p.w);
 	if (v.f32)
 	{
 		const int fbits = (int)((uint32_t)(bits & 0xffff) | (uint32_t)((bits >> 32) & 1) << 16
 								| (uint32_t)((bits >> 40) & 0xff) << 24);
 		v.sprmf[t] = make_float4((float)prm.x, (float)prm.y, (float)prm.z, __int_as_float(fbits));
-		for (int q = 0; q < D; q++)
-			v.safff[(int64_t)t * D + q] = (float)(q < 8 ? aff[q] : v.aff[(int64_t)s * D + q]);
+#pragma unroll
+		for (int q = 0; q < 4; q++)
+			if (q < D)
+				v.safff[(int64_t)t * D + q] = (float)aff[q];
+		for (int q = 4; q < D; q++)
+			v.safff[(int64_t)t * D + q] = (float)v.aff[(int64_t)s * D + q];
 	}
 }
 
