@@ -151,6 +151,18 @@ def cpu_baseline(name, budget_s=8.0, max_steps=400):
                       f"std::chrono around the step loop ({t:.2f} s)"}
 
 
+def max_over_ranks(x, device):
+    """Largest value of x over all ranks of the default process group (the
+    job's time is its slowest rank's); `device` "cuda" under NCCL, "cpu"
+    under gloo."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference(args, rank, world):
     """`--impl reference`: the reference's CPU path (its OpenMP structure as
     restated by the oracle; the reference itself cannot be built here) on
@@ -169,7 +181,7 @@ def run_reference(args, rank, world):
     kw = dict(with_phenotype=ph is not None, p_divide=ph[0] if ph else 0.0, p_death=ph[1] if ph else 0.0)
     o.time_steps(args.warmup, threads, **kw)
     t = o.time_steps(args.steps, threads, **kw)
-    value = a.count * args.steps / t * world
+    value = a.count * args.steps / t  # one host runs one simulation, whatever the rank count
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3,
@@ -409,9 +421,7 @@ def run_ours(args, rank, world, local_rank):
     total_ms = float(sum(step_ms))
     agent_steps = float(sum(counts)) if ph else float(n0 * K)
     if world > 1:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = max_over_ranks(total_ms, "cuda")
         agent_steps *= world
         torch.distributed.barrier()
     value = agent_steps / (total_ms / 1e3)
