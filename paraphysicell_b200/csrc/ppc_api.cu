@@ -314,6 +314,8 @@ int transfer_in(ppc_state* s, int32_t r, const ppc_agents* a, bool defaults)
 			for (int32_t i = 0; i < n && !s->rates_nonzero; i++)
 				s->rates_nonzero = rate[i] != 0.0;
 	s->bins_valid = false;
+	// slots were rewritten: the next rebuild counts by slot
+	PPC_CUDA(cudaMemsetAsync(v.order_valid, 0, sizeof(int32_t), s->stream));
 	PPC_CUDA(cudaStreamSynchronize(s->stream));
 	return PPC_OK;
 }
@@ -631,6 +633,7 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.vrank, C));
 	try_(alloc(s, v.tmp, C));
 	try_(alloc(s, v.vsc, C));
+	try_(alloc(s, v.order_valid, 1));
 	try_(alloc(s, v.sorted, C));
 	try_(alloc(s, v.skey, C));
 	try_(alloc(s, v.spos4, C));

@@ -112,6 +112,7 @@ struct view
 	int32_t* vrank;
 	int32_t* tmp;
 	int2* vsc;		// [C] voxel start and count of each slot's voxel, from the scatter to the fixup
+	int32_t* order_valid; // 1 while `sorted` lists exactly the live slots (set by the fixup)
 	int32_t* sorted;
 	int32_t* skey;
 	double4* spos4;

@@ -114,46 +114,61 @@ __device__ __forceinline__ int block_exclusive_scan(int x, int& total)
 	return excl;
 }
 
+// Voxel key and provisional rank of every live agent, and the per-tile
+// totals the scan needs. When the previous rebuild's key-ordered array still
+// lists exactly the live slots (nothing removed, divided or uploaded since),
+// thread t takes the agent at position t of that order: agents rarely change
+// voxel between steps, so a warp's agents share voxels and tiles, and one
+// atomic per distinct voxel and per distinct tile of the warp suffices.
+// Otherwise thread t takes slot t. The provisional rank only has to be a
+// permutation of 0..count-1 inside the voxel; k_bin_fixup sets the final one.
 __global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur)
 {
 	grid_wait();
-	const int s = blockIdx.x * blockDim.x + threadIdx.x;
-	int r = 0, local = 0;
-	if (s >= v.total_cap || !live(v, s, r, local))
-		return;
-	const rep_info& R = v.reps[r];
-	const double4 p = v.pos[cur][s];
-	const int c0 = axis_coord(p.x, R, 0, v.err);
-	const int c1 = v.dims >= 2 ? axis_coord(p.y, R, 1, v.err) : 0;
-	const int c2 = v.dims >= 3 ? axis_coord(p.z, R, 2, v.err) : 0;
-	const int32_t key = (int32_t)(R.vox_base + c0 + (int64_t)R.grid[0] * (c1 + (int64_t)R.grid[1] * c2));
-	v.key[s] = key;
-	v.vrank[s] = atomicAdd(v.vcnt + key, 1);
-}
-
-// per-tile totals of the voxel counts (one block per tile of 4096 voxels)
-__global__ void __launch_bounds__(kThreads) k_bin_reduce(view v)
-{
-	grid_wait();
-	const int b = blockIdx.x;
-	const int64_t i0 = ((int64_t)b << kTileShift) + (int64_t)threadIdx.x * kTileItems;
-	int sum = 0;
-	const int4* q = reinterpret_cast<const int4*>(v.vcnt + i0); // counts are padded to whole tiles
-#pragma unroll
-	for (int k = 0; k < kTileItems / 4; k++)
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	const int lane = threadIdx.x & 31;
+	int s = -1, r = 0, local = 0;
+	if (*v.order_valid)
 	{
-		const int4 x = q[k];
-		sum += x.x + x.y + x.z + x.w;
+		if (t < *v.cursor)
+		{
+			s = v.sorted[t];
+			r = rep_of(v, s);
+		}
 	}
-	int total;
-	block_exclusive_scan(sum, total);
-	if (threadIdx.x == 0)
-		v.tile_sum[b] = total;
+	else if (t < v.total_cap && live(v, t, r, local))
+		s = t;
+	int32_t key = -1 - lane; // distinct per idle lane, so idle lanes never group
+	if (s >= 0)
+	{
+		const rep_info& R = v.reps[r];
+		const double4 p = v.pos[cur][s];
+		const int c0 = axis_coord(p.x, R, 0, v.err);
+		const int c1 = v.dims >= 2 ? axis_coord(p.y, R, 1, v.err) : 0;
+		const int c2 = v.dims >= 3 ? axis_coord(p.z, R, 2, v.err) : 0;
+		key = (int32_t)(R.vox_base + c0 + (int64_t)R.grid[0] * (c1 + (int64_t)R.grid[1] * c2));
+	}
+	const unsigned same = __match_any_sync(0xffffffffu, key);
+	const int lead = __ffs(same) - 1;
+	int base = 0;
+	if (s >= 0 && lane == lead)
+		base = atomicAdd(v.vcnt + key, __popc(same));
+	base = __shfl_sync(0xffffffffu, base, lead);
+	const int32_t tile = s >= 0 ? (key >> kTileShift) : -1 - lane;
+	const unsigned same_tile = __match_any_sync(0xffffffffu, tile);
+	if (s >= 0 && lane == __ffs(same_tile) - 1)
+		atomicAdd(v.tile_sum + tile, __popc(same_tile));
+	if (s >= 0)
+	{
+		v.key[s] = key;
+		v.vrank[s] = base + __popc(same & ((1u << lane) - 1));
+	}
 }
 
 // Exclusive scan of the per-voxel counts into vstart (one block per tile of
 // 4096 voxels); a tile's offset is the sum of the totals of the tiles before
-// it. The counts are cleared at occupied voxels by k_bin_fixup.
+// it (k_bin_count accumulates them). The counts are cleared at occupied
+// voxels by k_bin_fixup, the tile totals by k_bin_scatter.
 __global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
 {
 	grid_wait();
@@ -231,6 +246,9 @@ __global__ void k_bin_scatter(view v)
 {
 	grid_wait();
 	int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (blockIdx.x == 0)
+		for (int k = threadIdx.x; k < v.ntiles; k += blockDim.x)
+			v.tile_sum[k] = 0; // ready for the next rebuild's k_bin_count
 	if (s >= v.total_cap)
 		return;
 	int r, local;
@@ -274,6 +292,8 @@ __global__ void k_bin_fixup(view v, int cur)
 	for (int u = 0; u < sc.y && sc.y > 1; u++)
 		rank += v.tmp[sc.x + u] > s;
 	const int t = sc.x + rank;
+	if (s == 0)
+		*v.order_valid = 1; // `sorted` now lists exactly the live slots
 	p.w = rmad * prm.x; // relative_maximum_adhesion_distance * radius
 	if (rank == 0)
 		v.vcnt[key] = 0; // ready for the next rebuild
@@ -1560,7 +1580,8 @@ __global__ void k_compact_plan(view v, int phenotype_pass, int springs)
 		return;
 
 	const int nvisit = phenotype_pass ? C.nvisit : C.count;
-	int cnt = C.count;
+	const int cnt0 = C.count;
+	int cnt = cnt0;
 	int ti = nb - 1, nm = 0;
 	int64_t deaths = 0;
 	int32_t* moves = v.moves + 2 * (int64_t)base;
@@ -1610,6 +1631,8 @@ __global__ void k_compact_plan(view v, int phenotype_pass, int springs)
 	C.deaths += deaths;
 	C.nbad = 0;
 	v.nmoves[r] = nm;
+	if (cnt != cnt0 || nm > 0)
+		*v.order_valid = 0; // the live slots changed: the next count goes by slot
 }
 
 // copies every per-agent field of the planned moves (cell_data::remove,
@@ -1724,6 +1747,7 @@ __global__ void k_divide_plan(view v, int springs)
 		C.ndiv = 0;
 		return;
 	}
+	*v.order_valid = 0; // daughters are appended: the next count goes by slot
 	if (springs)
 		for (int k = 0; k < nd; k++)
 		{
@@ -1947,7 +1971,6 @@ int launch_bin(ppc_state* s)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
 	pdl(k_bin_count, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
-	pdl(k_bin_reduce, s->v.ntiles, kThreads, 0, PPC_LAUNCH(s), s->v);
 	pdl(k_bin_scan, s->v.ntiles, kThreads, 0, PPC_LAUNCH(s), s->v);
 	pdl(k_bin_scatter, b, kThreads, 0, PPC_LAUNCH(s), s->v);
 	pdl(k_bin_fixup, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
