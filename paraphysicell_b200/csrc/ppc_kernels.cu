@@ -173,16 +173,11 @@ __global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
 {
 	grid_wait();
 	const int b = blockIdx.x;
-	int part = 0;
-	for (int k = threadIdx.x; k < b; k += blockDim.x)
-		part += v.tile_sum[k];
-	int tile_base;
-	block_exclusive_scan(part, tile_base);
-
+	// the tile's counts first (counts are padded to whole tiles and zero past
+	// the last voxel), so their loads overlap the predecessor totals' loads
 	const int64_t i0 = ((int64_t)b << kTileShift) + (int64_t)threadIdx.x * kTileItems;
 	int c[kTileItems];
 	int sum = 0;
-	if (i0 + kTileItems <= v.nvox)
 	{
 		const int4* q = reinterpret_cast<const int4*>(v.vcnt + i0);
 #pragma unroll
@@ -195,12 +190,12 @@ __global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
 			c[4 * k + 3] = x.w;
 		}
 	}
-	else
-	{
-#pragma unroll
-		for (int k = 0; k < kTileItems; k++)
-			c[k] = i0 + k < v.nvox ? v.vcnt[i0 + k] : 0;
-	}
+	int part = 0;
+	for (int k = threadIdx.x; k < b; k += blockDim.x)
+		part += v.tile_sum[k];
+	int tile_base;
+	block_exclusive_scan(part, tile_base);
+
 #pragma unroll
 	for (int k = 0; k < kTileItems; k++)
 		sum += c[k];
