@@ -879,6 +879,11 @@ __global__ void __launch_bounds__(kFusedThreads, 5) k_fused_f32(view v, int cur)
 // ---------------------------------------------------------------------------
 
 constexpr int kStageThreads = 128;
+#ifndef PPC_STAGE_SCAN
+#define PPC_STAGE_SCAN 4
+#endif
+constexpr int kStageScan = PPC_STAGE_SCAN; // candidates a lane tests per scan iteration, loads issued together
+static_assert(kStageScan >= 1 && kStageScan <= kList, "a scan iteration must fit in the neighbour list");
 constexpr size_t kStageStatic = 10 * 1024; // bound on the staged kernel's static shared memory
 #ifndef PPC_STAGE_MINB
 #define PPC_STAGE_MINB 4
@@ -1224,14 +1229,23 @@ __global__ void __launch_bounds__(kStageThreads, PPC_STAGE_MINB) k_fused_staged(
 			break;
 		if (has)
 		{
-			if (u != t && filter_keep<DIMS>(pf, P[u + soff], margin))
-			{
-				list[n * stride] = u;
-				n++;
-			}
-			u++;
+			// up to kStageScan candidates of the current row, loads first
+			const int m = min(kStageScan, b.y - u);
+			float4 q[kStageScan];
+#pragma unroll
+			for (int j = 0; j < kStageScan; j++)
+				if (j < m)
+					q[j] = P[u + j + soff];
+#pragma unroll
+			for (int j = 0; j < kStageScan; j++)
+				if (j < m && u + j != t && filter_keep<DIMS>(pf, q[j], margin))
+				{
+					list[n * stride] = u + j;
+					n++;
+				}
+			u += m;
 		}
-		if (__any_sync(0xffffffffu, n == kList))
+		if (__any_sync(0xffffffffu, n > kList - kStageScan))
 			flush();
 	}
 	flush();
