@@ -405,14 +405,15 @@ int ensure_lists(ppc_state* s)
 // one fused mechanics step (+ phenotype container update)
 int enqueue_step(ppc_state* s, bool phenotype, double p_divide, double p_death)
 {
+	// the compaction right before the rebuild leaves its moves to k_bin_count
 	PPC_TRY(launch_fused(s));
-	PPC_TRY(launch_compact(s, false));
+	PPC_TRY(launch_compact(s, false, !phenotype));
 	if (phenotype)
 	{
 		PPC_TRY(launch_flag_by_draws(s, p_divide, p_death));
 		PPC_TRY(launch_divide(s));
 		PPC_TRY(launch_mark_remove(s));
-		PPC_TRY(launch_compact(s, true));
+		PPC_TRY(launch_compact(s, true, true));
 	}
 	PPC_TRY(launch_bin(s));
 	return PPC_OK;
@@ -634,6 +635,9 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.tmp, C));
 	try_(alloc(s, v.vsc, C));
 	try_(alloc(s, v.order_valid, 1));
+	try_(alloc(s, v.move_src, C)); // -1: no pending move into the slot
+	if (rc == PPC_OK && cudaMemset(v.move_src, 0xff, sizeof(int32_t) * std::max<size_t>(C, 1)) != cudaSuccess)
+		rc = fail(PPC_ERR_CUDA, "cudaMemset failed");
 	try_(alloc(s, v.sorted, C));
 	try_(alloc(s, v.skey, C));
 	try_(alloc(s, v.spos4, C));

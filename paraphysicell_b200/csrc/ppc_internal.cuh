@@ -113,6 +113,7 @@ struct view
 	int32_t* tmp;
 	int2* vsc;		// [C] voxel start and count of each slot's voxel, from the scatter to the fixup
 	int32_t* order_valid; // 1 while `sorted` lists exactly the live slots (set by the fixup)
+	int32_t* move_src;	  // [C] tail slot whose agent the next k_bin_count moves into this hole, or -1
 	int32_t* sorted;
 	int32_t* skey;
 	double4* spos4;
@@ -228,7 +229,7 @@ int launch_membrane(ppc_state* s);
 int launch_springs(ppc_state* s);
 int launch_positions(ppc_state* s);
 int launch_fused(ppc_state* s);
-int launch_compact(ppc_state* s, bool phenotype_pass);
+int launch_compact(ppc_state* s, bool phenotype_pass, bool fold = false);
 int launch_mark_remove(ppc_state* s);
 int launch_divide(ppc_state* s);
 int launch_flag_by_draws(ppc_state* s, double p_divide, double p_death);

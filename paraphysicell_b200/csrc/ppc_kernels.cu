@@ -114,6 +114,38 @@ __device__ __forceinline__ int block_exclusive_scan(int x, int& total)
 	return excl;
 }
 
+// copies every per-agent field of slot s into slot d (cell_data::remove,
+// reference: src/cell_data.cpp:285-313); spring rows were moved by the plan
+__device__ __forceinline__ void move_agent(const view& v, int cur, int d, int s)
+{
+	v.pos[cur][d] = v.pos[cur][s];
+	v.vel[d] = v.vel[s];
+	v.vprev[d] = v.vprev[s];
+	v.prm[d] = v.prm[s];
+	v.rmad[d] = v.rmad[s];
+	v.ec[d] = v.ec[s];
+	v.arate[d] = v.arate[s];
+	v.drate[d] = v.drate[s];
+	v.pressure[d] = v.pressure[s];
+	v.vol[d] = v.vol[s];
+	v.nvol[d] = v.nvol[s];
+	v.nrad[d] = v.nrad[s];
+	v.sarea[d] = v.sarea[s];
+	v.polarity[d] = v.polarity[s];
+	v.orient[d] = v.orient[s];
+	for (int q = 0; q < v.ndefs; q++)
+		v.aff[(int64_t)d * v.ndefs + q] = v.aff[(int64_t)s * v.ndefs + q];
+	v.def[d] = v.def[s];
+	v.maxatt[d] = v.maxatt[s];
+	v.movable[d] = v.movable[s];
+	v.flags[d] = v.flags[s];
+	v.ids[d] = v.ids[s];
+	const int nn = min(v.ncnt[s], v.ncap);
+	for (int q = 0; q < nn; q++)
+		v.nidx[(int64_t)d * v.ncap + q] = v.nidx[(int64_t)s * v.ncap + q];
+	v.ncnt[d] = v.ncnt[s];
+}
+
 // Voxel key and provisional rank of every live agent, and the per-tile
 // totals the scan needs. When the previous rebuild's key-ordered array still
 // lists exactly the live slots (nothing removed, divided or uploaded since),
@@ -137,7 +169,16 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur)
 		}
 	}
 	else if (t < v.total_cap && live(v, t, r, local))
+	{
 		s = t;
+		// a hole that the compaction plan filled with a tail agent
+		const int src = v.move_src[s];
+		if (src >= 0)
+		{
+			move_agent(v, cur, s, src);
+			v.move_src[s] = -1;
+		}
+	}
 	int32_t key = -1 - lane; // distinct per idle lane, so idle lanes never group
 	if (s >= 0)
 	{
@@ -1569,7 +1610,7 @@ __device__ void springs_rename_attached(const view& v, int old_slot, int new_slo
 // Produces (hole, source) moves for the agents that end up in holes, the new
 // count and the death count; with springs it also replays every removal on
 // the spring rows in the reference's order.
-__global__ void k_compact_plan(view v, int phenotype_pass, int springs)
+__global__ void k_compact_plan(view v, int phenotype_pass, int springs, int fold)
 {
 	grid_wait();
 	__shared__ int32_t sh[kSortCap];
@@ -1634,6 +1675,8 @@ __global__ void k_compact_plan(view v, int phenotype_pass, int springs)
 			moves[2 * nm] = h;
 			moves[2 * nm + 1] = occ;
 			nm++;
+			if (fold)
+				v.move_src[base + h] = base + occ; // applied by the next k_bin_count
 		}
 	}
 	C.count = cnt;
@@ -1644,9 +1687,7 @@ __global__ void k_compact_plan(view v, int phenotype_pass, int springs)
 		*v.order_valid = 0; // the live slots changed: the next count goes by slot
 }
 
-// copies every per-agent field of the planned moves (cell_data::remove,
-// reference: src/cell_data.cpp:285-313); spring rows were moved by the plan
-template <int DIMS>
+// the planned moves, one thread per move
 __global__ void k_compact_apply(view v, int cur)
 {
 	grid_wait();
@@ -1655,35 +1696,7 @@ __global__ void k_compact_apply(view v, int cur)
 	const int base = v.reps[r].base;
 	const int32_t* moves = v.moves + 2 * (int64_t)base;
 	for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nm; k += gridDim.x * blockDim.x)
-	{
-		const int d = base + moves[2 * k], s = base + moves[2 * k + 1];
-		v.pos[cur][d] = v.pos[cur][s];
-		v.vel[d] = v.vel[s];
-		v.vprev[d] = v.vprev[s];
-		v.prm[d] = v.prm[s];
-		v.rmad[d] = v.rmad[s];
-		v.ec[d] = v.ec[s];
-		v.arate[d] = v.arate[s];
-		v.drate[d] = v.drate[s];
-		v.pressure[d] = v.pressure[s];
-		v.vol[d] = v.vol[s];
-		v.nvol[d] = v.nvol[s];
-		v.nrad[d] = v.nrad[s];
-		v.sarea[d] = v.sarea[s];
-		v.polarity[d] = v.polarity[s];
-		v.orient[d] = v.orient[s];
-		for (int q = 0; q < v.ndefs; q++)
-			v.aff[(int64_t)d * v.ndefs + q] = v.aff[(int64_t)s * v.ndefs + q];
-		v.def[d] = v.def[s];
-		v.maxatt[d] = v.maxatt[s];
-		v.movable[d] = v.movable[s];
-		v.flags[d] = v.flags[s];
-		v.ids[d] = v.ids[s];
-		const int nn = min(v.ncnt[s], v.ncap);
-		for (int q = 0; q < nn; q++)
-			v.nidx[(int64_t)d * v.ncap + q] = v.nidx[(int64_t)s * v.ncap + q];
-		v.ncnt[d] = v.ncnt[s];
-	}
+		move_agent(v, cur, base + moves[2 * k], base + moves[2 * k + 1]);
 }
 
 // stand-in for the phenotype models: death with p_death, else division with
@@ -2158,17 +2171,15 @@ int launch_fused(ppc_state* s)
 	return PPC_OK;
 }
 
-int launch_compact(ppc_state* s, bool phenotype_pass)
+int launch_compact(ppc_state* s, bool phenotype_pass, bool fold)
 {
 	const int springs = s->has_springs ? 1 : 0;
-	pdl(k_compact_plan, s->nreps, kThreads, 0, PPC_LAUNCH(s), s->v, phenotype_pass ? 1 : 0, springs);
-	dim3 g(std::max(1, std::min(64, blocks_for(s->total_cap / std::max(1, s->nreps), kThreads))), s->nreps);
-	if (s->dims == 1)
-		pdl(k_compact_apply<1>, g, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
-	else if (s->dims == 2)
-		pdl(k_compact_apply<2>, g, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
-	else
-		pdl(k_compact_apply<3>, g, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
+	pdl(k_compact_plan, s->nreps, kThreads, 0, PPC_LAUNCH(s), s->v, phenotype_pass ? 1 : 0, springs, fold ? 1 : 0);
+	if (!fold)
+	{
+		dim3 g(std::max(1, std::min(64, blocks_for(s->total_cap / std::max(1, s->nreps), kThreads))), s->nreps);
+		pdl(k_compact_apply, g, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
+	}
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
