@@ -311,6 +311,17 @@ def test_errors_are_reported():
         d.step(1)
     assert e.value.rc == PPC_ERR_UNSUPPORTED
 
+    from paraphysicell_b200.abi import PPC_ERR_ARG
+    mesh, params, a = wl.scaled(wl.config2, 300, seed=74)
+    _, d = gu.make_pair(mesh, params, a)
+    for shape in ((3, 128, 0), (-3, 128, 0), (0, 100, 0), (0, 512, 0), (0, 128, 200 * 1024)):
+        with pytest.raises(PPCError) as e:
+            d.set_launch_shape(*shape)
+        assert e.value.rc == PPC_ERR_ARG
+    with pytest.raises(PPCError) as e:
+        d.autotune(steps=0)
+    assert e.value.rc == PPC_ERR_ARG
+
 
 def test_full_size_config3_properties_and_oracle():
     """At the full 88,700-agent size: one step bit-exact with the oracle, and
