@@ -446,8 +446,13 @@ def run_ours(args, rank, world, local_rank):
         host.arrays[k_][:] = v_
     sim.upload(host)
     sim.update_mechanics_mesh()
+    # inputs the step reads from the host's copy: positions and the previous
+    # velocities (Adams-Bashforth); its result: new positions, the step's
+    # velocity (which update_positions moves into previous_velocities and
+    # clears from velocities, src/solver/host/position_solver.cpp:481-504)
+    # and pressure
     up_fields = ("positions", "previous_velocities")
-    down_fields = ("positions", "velocities", "previous_velocities", "simple_pressure")
+    down_fields = ("positions", "previous_velocities", "simple_pressure")
     d = a.dims
     sim.download(host, fields=down_fields)
     torch.cuda.synchronize()
@@ -468,7 +473,7 @@ def run_ours(args, rank, world, local_rank):
     n_e2e = float(sum(e2e_counts))
     e2e = {"value": n_e2e / (e2e_ms / 1e3) * world, "unit": UNIT,
            "h2d_bytes_per_step": int(np.mean(e2e_counts) * 2 * 8 * d),
-           "d2h_bytes_per_step": int(np.mean(e2e_counts) * (3 * 8 * d + 8)),
+           "d2h_bytes_per_step": int(np.mean(e2e_counts) * (2 * 8 * d + 8)),
            "steps": E, "wall_s": wall}
     pool_free = pool.free
 

@@ -204,7 +204,10 @@ int ppc_upload(ppc_state* s, int32_t replicate, const ppc_agents* agents);
 
 /* Copies the agents of replicate `replicate` back to the host view. Sets
  * agents->count; returns PPC_ERR_CAPACITY if it exceeds agents->capacity.
- * Synchronises the stream. */
+ * Synchronises the stream, once when the count has not grown since the
+ * state last reported it (the copies are queued with that count, next to the
+ * counters); rows past the new count but within the last reported count and
+ * agents->capacity may then be overwritten. */
 int ppc_download(ppc_state* s, int32_t replicate, ppc_agents* agents);
 
 /* Overwrites only the fields whose pointers are non-NULL, keeping every other

@@ -107,6 +107,8 @@ int read_counters(ppc_state* s, std::vector<rep_counters>& c)
 	c.resize(s->nreps);
 	PPC_CUDA(cudaMemcpyAsync(c.data(), s->v.ctr, sizeof(rep_counters) * s->nreps, cudaMemcpyDeviceToHost, s->stream));
 	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	for (int32_t k = 0; k < s->nreps; k++)
+		s->host_count[k] = c[k].count;
 	return PPC_OK;
 }
 
@@ -161,9 +163,9 @@ int put_vec(ppc_state* s, double4* dev, const double* host, int32_t r, int32_t n
 		PPC_CUDA(cudaMemcpyAsync(s->stage, host, bytes, cudaMemcpyHostToDevice, s->stream));
 	else
 		PPC_CUDA(cudaMemsetAsync(s->stage, 0, bytes, s->stream));
+	// the next field's copy into the stage is ordered after this kernel on
+	// the same stream; pageable sources are staged by the copy call itself
 	PPC_TRY(launch_unpack_vec(s, dev, static_cast<const double*>(s->stage), r, n));
-	// the stage is reused by the next field: keep copies ordered
-	PPC_CUDA(cudaStreamSynchronize(s->stream));
 	return PPC_OK;
 }
 
@@ -175,7 +177,6 @@ int get_vec(ppc_state* s, double* host, const double4* dev, int32_t r, int32_t n
 	PPC_TRY(ensure_stage(s, bytes));
 	PPC_TRY(launch_pack_vec(s, static_cast<double*>(s->stage), dev, r, n));
 	PPC_CUDA(cudaMemcpyAsync(host, s->stage, bytes, cudaMemcpyDeviceToHost, s->stream));
-	PPC_CUDA(cudaStreamSynchronize(s->stream));
 	return PPC_OK;
 }
 
@@ -193,7 +194,6 @@ int put_prm(ppc_state* s, int field, const double* host, int32_t r, int32_t n, b
 		PPC_CUDA(cudaMemcpyAsync(s->stage, tmp.data(), bytes, cudaMemcpyHostToDevice, s->stream));
 	}
 	PPC_TRY(launch_unpack_prm(s, field, static_cast<const double*>(s->stage), r, n));
-	PPC_CUDA(cudaStreamSynchronize(s->stream));
 	return PPC_OK;
 }
 
@@ -205,7 +205,6 @@ int get_prm(ppc_state* s, int field, double* host, int32_t r, int32_t n)
 	PPC_TRY(ensure_stage(s, bytes));
 	PPC_TRY(launch_pack_prm(s, field, static_cast<double*>(s->stage), r, n));
 	PPC_CUDA(cudaMemcpyAsync(host, s->stage, bytes, cudaMemcpyDeviceToHost, s->stream));
-	PPC_CUDA(cudaStreamSynchronize(s->stream));
 	return PPC_OK;
 }
 
@@ -301,6 +300,7 @@ int transfer_in(ppc_state* s, int32_t r, const ppc_agents* a, bool defaults)
 		PPC_CUDA(cudaMemsetAsync(v.ncnt + base, 0, sizeof(int32_t) * std::max(n, 1), s->stream));
 		int32_t cnt[2] = { n, n };
 		PPC_CUDA(cudaMemcpyAsync(&v.ctr[r].count, cnt, sizeof(int32_t) * 2, cudaMemcpyHostToDevice, s->stream));
+		s->host_count[r] = n;
 	}
 
 	// host flags that pick kernel variants
@@ -320,14 +320,10 @@ int transfer_in(ppc_state* s, int32_t r, const ppc_agents* a, bool defaults)
 	return PPC_OK;
 }
 
-int transfer_out(ppc_state* s, int32_t r, ppc_agents* a)
+// queues the copies of the first n agents of replicate r into the host view
+// (no synchronisation)
+int copy_out(ppc_state* s, int32_t r, ppc_agents* a, int32_t n)
 {
-	std::vector<rep_counters> c;
-	PPC_TRY(read_counters(s, c));
-	const int32_t n = c[r].count;
-	a->count = n;
-	if (n > a->capacity)
-		return fail(PPC_ERR_CAPACITY, "host arrays are smaller than the agent count");
 	const int32_t base = s->reps[r].base;
 	const int D = s->ndefs;
 	view& v = s->v;
@@ -355,6 +351,31 @@ int transfer_out(ppc_state* s, int32_t r, ppc_agents* a)
 	PPC_TRY(get_scalar(s, a->is_movable, v.movable, base, n, 1));
 	PPC_TRY(get_scalar(s, a->flags, v.flags, base, n, 1));
 	PPC_TRY(get_scalar(s, a->agent_ids, v.ids, base, n, 1));
+	return PPC_OK;
+}
+
+int transfer_out(ppc_state* s, int32_t r, ppc_agents* a)
+{
+	// Copies as many agents as this host last saw in the replicate, together
+	// with the counters, and synchronises once; if the device count turns out
+	// larger (divisions since), the copies are redone with the true count.
+	// Rows between the device count and the previous count, within the host
+	// capacity, may be overwritten.
+	const int32_t guess = std::max(0, std::min(s->host_count[r], std::min(a->capacity, s->reps[r].cap)));
+	PPC_CUDA(cudaMemcpyAsync(s->pinned_ctr, s->v.ctr, sizeof(rep_counters) * s->nreps, cudaMemcpyDeviceToHost,
+							 s->stream));
+	PPC_TRY(copy_out(s, r, a, guess));
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	for (int32_t k = 0; k < s->nreps; k++)
+		s->host_count[k] = s->pinned_ctr[k].count;
+	const int32_t n = s->host_count[r];
+	a->count = n;
+	if (n > a->capacity)
+		return fail(PPC_ERR_CAPACITY, "host arrays are smaller than the agent count");
+	if (n > guess)
+		PPC_TRY(copy_out(s, r, a, n));
+	const int32_t base = s->reps[r].base;
+	view& v = s->v;
 	if (a->spring_counts)
 	{
 		PPC_TRY(get_scalar(s, a->spring_counts, v.scnt, base, n, 1));
@@ -653,6 +674,12 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.moves, 2 * C));
 	try_(alloc(s, v.nmoves, replicates));
 	try_(alloc(s, v.draw_epoch, replicates));
+	s->host_count.assign(replicates, 0);
+	if (rc == PPC_OK
+		&& cudaHostAlloc(reinterpret_cast<void**>(&s->pinned_ctr), sizeof(rep_counters) * replicates,
+						 cudaHostAllocDefault)
+			   != cudaSuccess)
+		rc = fail(PPC_ERR_CUDA, "cudaHostAlloc failed");
 	if (rc == PPC_OK)
 	{
 		std::vector<int32_t> rid(C, 0);
@@ -690,6 +717,8 @@ int ppc_destroy(ppc_state* s)
 		cudaFree(b.p);
 	if (s->stage)
 		cudaFree(s->stage);
+	if (s->pinned_ctr)
+		cudaFreeHost(s->pinned_ctr);
 	if (s->own_stream)
 		cudaStreamDestroy(s->own_stream);
 	delete s;

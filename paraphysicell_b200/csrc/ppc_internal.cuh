@@ -189,6 +189,9 @@ struct ppc_state
 	// (default), or warp-cooperative pair work with candidates read from
 	// global memory or from the block's ranges staged in shared memory;
 	// threads per block; staging bytes per block
+	// host copies of the replicate counts as last read (a download's first guess)
+	std::vector<int32_t> host_count;
+	ppc::rep_counters* pinned_ctr = nullptr; // pinned landing area of the counters
 	bool staged = false;
 	bool coop = false;
 	int tile_threads = 128;
