@@ -317,19 +317,29 @@ def ensemble_form(args, flush):
     from paraphysicell_b200 import workloads as wl
     from paraphysicell_b200.device import Simulation
 
+    from paraphysicell_b200.abi import PPC_FP32_FORCE
+
     meshes, params, sets = wl.config4()
-    sim = Simulation(meshes, params, [a.capacity for a in sets], seed=1)
-    stream = torch.cuda.Stream()
-    sim.set_stream(stream.cuda_stream)
-    for r, a in enumerate(sets):
-        sim.upload(a, replicate=r)
-    sim.update_mechanics_mesh()
     total = sum(a.count for a in sets)
-    with torch.cuda.stream(stream):
-        shape = sim.autotune(steps=5)
-    out = _timed_steps(sim, stream, sim.step, lambda: total, args.steps, args.warmup, flush)
-    out["launch_shape"] = {"tile_edge": shape[0], "threads": shape[1], "chosen_by": "ppc_autotune"}
-    sim.close()
+
+    def run(precision):
+        sim = Simulation(meshes, params, [a.capacity for a in sets], seed=1)
+        stream = torch.cuda.Stream()
+        sim.set_stream(stream.cuda_stream)
+        if precision:
+            sim.set_precision(precision)
+        for r, a in enumerate(sets):
+            sim.upload(a, replicate=r)
+        sim.update_mechanics_mesh()
+        with torch.cuda.stream(stream):
+            shape = sim.autotune(steps=5)
+        res = _timed_steps(sim, stream, sim.step, lambda: total, args.steps, args.warmup, flush)
+        res["launch_shape"] = {"tile_edge": shape[0], "threads": shape[1], "chosen_by": "ppc_autotune"}
+        sim.close()
+        return res
+
+    out = run(0)
+    out["fp32_force"] = run(PPC_FP32_FORCE)
     out.update({"workload": "config4", "replicates": len(sets), "agents": total,
                 "description": ENSEMBLE})
     return out
