@@ -304,12 +304,14 @@ __global__ void k_bin_scatter(view v)
 __global__ void k_bin_fixup(view v, int cur)
 {
 	grid_wait();
-	int s = blockIdx.x * blockDim.x + threadIdx.x;
-	if (s >= v.total_cap)
+	// thread tp takes the agent the scatter put at provisional position tp;
+	// its final position is in the same voxel's range, so the stores of
+	// neighbouring threads land close together
+	const int tp = blockIdx.x * blockDim.x + threadIdx.x;
+	if (tp >= *v.cursor)
 		return;
-	int r, local;
-	if (!live(v, s, r, local))
-		return;
+	const int s = v.tmp[tp];
+	const int r = rep_of(v, s);
 	const int32_t key = v.key[s];
 	const int2 sc = v.vsc[s];
 	const double4 prm = v.prm[s];
