@@ -252,14 +252,18 @@ def test_springs_survive_removals_like_oracle():
     gu.assert_same_state(gd, go)
 
 
-def test_batch_replicates_match_independent_oracles():
+@pytest.mark.parametrize("shape", [(-1, 128, 0), (-2, 128, 0), (0, 128, 32 * 1024), (0, 64, 16 * 1024)],
+                         ids=lambda s: "edge%d_t%d" % s[:2])
+def test_batch_replicates_match_independent_oracles(shape):
     """Ensemble form: each replicate of one batched state evolves exactly
-    like its own single simulation in the oracle."""
+    like its own single simulation in the oracle, in every launch shape
+    (blocks of the key-ordered array span replicate boundaries)."""
     meshes, params, sets = wl.config4(seed=61, replicates=6, n_min=200, n_max=3000)
     from oracle.oracle import Oracle
     from paraphysicell_b200.device import Simulation
     gu.build.ensure_built()
     d = Simulation(meshes, params, [s.capacity for s in sets])
+    d.set_launch_shape(*shape)
     oracles = []
     for r, (m, s) in enumerate(zip(meshes, sets)):
         d.upload(s, replicate=r)
