@@ -256,11 +256,13 @@ int ppc_update_motility(ppc_state* s);
 /* position_solver::update_basement_membrane_interactions (reference: src/solver/host/position_solver.cpp:316-335). */
 int ppc_update_basement_membrane_interactions(ppc_state* s);
 
-/* position_solver::update_spring_attachments (reference: src/solver/host/position_solver.cpp:451-479).
- * Spring contraction over the stored springs. Stochastic attachment and
- * detachment with non-zero rates is not implemented on the device and returns
- * PPC_ERR_UNSUPPORTED; with all rates zero it leaves the springs unchanged,
- * as the reference does. */
+/* position_solver::update_spring_attachments (reference: src/solver/host/position_solver.cpp:372-479).
+ * Stochastic detachment and attachment (update_spring_attachments_internal)
+ * with counter-based draws — agent i's k-th draw of the n-th spring update of
+ * a replicate is uniform(seed, n, replicate, i, k) — in the reference's
+ * serial order and capacity checks, then spring contraction. Needs the
+ * neighbour lists (computed here if stale). ppc_step takes the same route
+ * (through these separate entry points) while any rate is non-zero. */
 int ppc_update_spring_attachments(ppc_state* s);
 
 /* position_solver::update_positions (reference: src/solver/host/position_solver.cpp:481-520). */

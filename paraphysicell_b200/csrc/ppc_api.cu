@@ -407,7 +407,7 @@ int ensure_bins(ppc_state* s)
 	return PPC_OK;
 }
 
-bool springs_unsupported(ppc_state* s) { return s->params.automated_spring_adhesion && s->rates_nonzero; }
+bool stochastic_springs(ppc_state* s) { return s->params.automated_spring_adhesion && s->rates_nonzero; }
 
 // The fused step recomputes neighbours inside its force pass and does not
 // store them; the lists the reference would hold after the step are built
@@ -440,15 +440,49 @@ int enqueue_step(ppc_state* s, bool phenotype, double p_divide, double p_death)
 	return PPC_OK;
 }
 
+// one step through the separate entry points, for stochastic spring
+// attachment: the spring update needs every agent's neighbour list and its
+// attachments must be settled before the springs pull, so the step runs the
+// reference's sequence (simulator::simulate_mechanics, src/simulator.cpp:173-192)
+int enqueue_step_separate(ppc_state* s, bool phenotype, double p_divide, double p_death)
+{
+	PPC_TRY(launch_neighbors(s));
+	PPC_TRY(launch_forces(s));
+	if (s->params.virtual_wall_at_domain_edges)
+		PPC_TRY(launch_membrane(s));
+	PPC_TRY(launch_spring_updates(s));
+	PPC_TRY(launch_springs(s));
+	PPC_TRY(launch_positions(s));
+	PPC_TRY(launch_mark_remove(s));
+	PPC_TRY(launch_compact(s, false, !phenotype));
+	if (phenotype)
+	{
+		PPC_TRY(launch_flag_by_draws(s, p_divide, p_death));
+		PPC_TRY(launch_divide(s));
+		PPC_TRY(launch_mark_remove(s));
+		PPC_TRY(launch_compact(s, true, true));
+	}
+	PPC_TRY(launch_bin(s));
+	return PPC_OK;
+}
+
 constexpr int kGraphSteps = 10; // even, so a replay leaves the position buffer parity unchanged
 
 int run_steps(ppc_state* s, int32_t steps, bool phenotype, double p_divide, double p_death)
 {
 	if (steps < 0)
 		return fail(PPC_ERR_ARG, "negative step count");
-	if (springs_unsupported(s))
-		return fail(PPC_ERR_UNSUPPORTED, "stochastic spring attachment with non-zero rates is not on the device path");
 	PPC_TRY(ensure_bins(s));
+	if (stochastic_springs(s))
+	{
+		// non-zero attachment or detachment rates
+		s->has_springs = true;
+		for (int32_t k = 0; k < steps; k++)
+			PPC_TRY(enqueue_step_separate(s, phenotype, p_divide, p_death));
+		s->bins_valid = true;
+		s->lists_stale = steps > 0 || s->lists_stale;
+		return PPC_OK;
+	}
 	int32_t done = 0;
 	// the first step after an upload may read non-zero velocities
 	while (done < steps && s->vel_dirty)
@@ -614,6 +648,7 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	v.ncap = s->ncap;
 	v.dt = params->mechanics_time_step;
 	v.walls = params->virtual_wall_at_domain_edges;
+	v.auto_springs = params->automated_spring_adhesion != 0;
 	rep_info* reps = nullptr;
 	try_(alloc(s, reps, replicates));
 	v.reps = reps;
@@ -657,6 +692,7 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.vsc, C));
 	try_(alloc(s, v.order_valid, 1));
 	try_(alloc(s, v.move_src, C)); // -1: no pending move into the slot
+	try_(alloc(s, v.sdel, C * s->scap));
 	if (rc == PPC_OK && cudaMemset(v.move_src, 0xff, sizeof(int32_t) * std::max<size_t>(C, 1)) != cudaSuccess)
 		rc = fail(PPC_ERR_CUDA, "cudaMemset failed");
 	try_(alloc(s, v.sorted, C));
@@ -930,11 +966,13 @@ int ppc_update_spring_attachments(ppc_state* s)
 		return fail(PPC_ERR_ARG, "null state");
 	if (!s->params.automated_spring_adhesion)
 		return PPC_OK;
-	if (springs_unsupported(s))
-		return fail(PPC_ERR_UNSUPPORTED, "stochastic spring attachment with non-zero rates is not on the device path");
-	if (!s->has_springs)
-		return PPC_OK;
-	PPC_TRY(launch_springs(s));
+	// detachment and attachment draws (they advance the draw epoch even when
+	// every rate is zero, as the reference's loop does), then the pull
+	PPC_TRY(ensure_lists(s));
+	PPC_TRY(launch_spring_updates(s));
+	s->has_springs = s->has_springs || s->rates_nonzero;
+	if (s->has_springs)
+		PPC_TRY(launch_springs(s));
 	return finish(s);
 }
 

@@ -65,6 +65,9 @@ struct rep_counters
 	int64_t divisions;	 // environment::divisions_count
 	int64_t deaths;		 // environment::deaths_count
 	int64_t next_id;	 // id of the next created agent
+	int32_t nattach;	 // entries in the spring-attachment candidate list
+	int32_t pad;
+	int64_t spring_epoch; // spring updates so far: epoch of their counter-based draws
 };
 
 // everything a kernel needs, passed by value
@@ -73,6 +76,7 @@ struct view
 	int32_t dims, ndefs, nreps, total_cap, scap, ncap;
 	double dt;
 	int32_t walls;
+	int32_t auto_springs; // automated_spring_adhesion: every step updates springs
 	const rep_info* reps;
 	rep_counters* ctr;
 	int32_t* err;
@@ -114,6 +118,7 @@ struct view
 	int2* vsc;		// [C] voxel start and count of each slot's voxel, from the scatter to the fixup
 	int32_t* order_valid; // 1 while `sorted` lists exactly the live slots (set by the fixup)
 	int32_t* move_src;	  // [C] tail slot whose agent the next k_bin_count moves into this hole, or -1
+	uint8_t* sdel;		  // [C*S] spring marked for detachment this step
 	int32_t* sorted;
 	int32_t* skey;
 	double4* spos4;
@@ -230,6 +235,7 @@ int launch_neighbors(ppc_state* s);
 int launch_forces(ppc_state* s);
 int launch_membrane(ppc_state* s);
 int launch_springs(ppc_state* s);
+int launch_spring_updates(ppc_state* s);
 int launch_positions(ppc_state* s);
 int launch_fused(ppc_state* s);
 int launch_compact(ppc_state* s, bool phenotype_pass, bool fold = false);

@@ -25,6 +25,15 @@ constexpr int kTileItems = 16;
 // visible. Launched without the attribute, the wait returns at once.
 __device__ __forceinline__ void grid_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// a fused step's spring update with all rates zero changes no spring but
+// still advances the draw epoch, as the reference's loop does
+__device__ __forceinline__ void bump_spring_epochs(const view& v)
+{
+	if (blockIdx.x == 0 && v.auto_springs)
+		for (int r = threadIdx.x; r < v.nreps; r += blockDim.x)
+			v.ctr[r].spring_epoch++;
+}
+
 __device__ __forceinline__ int rep_of(const view& v, int s) { return v.nreps == 1 ? 0 : v.rid[s]; }
 
 __device__ __forceinline__ double comp(const double4& p, int d) { return d == 0 ? p.x : (d == 1 ? p.y : p.z); }
@@ -695,6 +704,7 @@ template <int DIMS, bool WALLS, bool SPRINGS, bool VEL>
 __global__ void __launch_bounds__(kFusedThreads, 5) k_fused(view v, int cur)
 {
 	grid_wait();
+	bump_spring_epochs(v);
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= *v.cursor)
 		return;
@@ -790,6 +800,7 @@ template <int DIMS, bool WALLS, bool SPRINGS, bool VEL>
 __global__ void __launch_bounds__(kFusedThreads, 5) k_fused_f32(view v, int cur)
 {
 	grid_wait();
+	bump_spring_epochs(v);
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= *v.cursor)
 		return;
@@ -980,6 +991,7 @@ template <int DIMS, bool WALLS, bool SPRINGS, bool VEL, bool F32>
 __global__ void __launch_bounds__(kStageThreads, PPC_STAGE_MINB) k_fused_staged(view v, int cur, int cap)
 {
 	grid_wait();
+	bump_spring_epochs(v);
 	constexpr int NR = DIMS == 3 ? 9 : (DIMS == 2 ? 3 : 1);
 	extern __shared__ float4 stage[]; // cap staged positions, then the neighbour lists
 	__shared__ int s_a[NR], s_o[NR + 1];
@@ -1701,6 +1713,191 @@ __global__ void k_compact_apply(view v, int cur)
 		move_agent(v, cur, base + moves[2 * k], base + moves[2 * k + 1]);
 }
 
+// ---------------------------------------------------------------------------
+// stochastic spring attachment and detachment
+// (update_spring_attachments_internal, reference: position_solver.cpp:372-449)
+// with counter-based draws: agent i's k-th draw of a spring update is
+// uniform(seed, spring epoch, replicate, i, k); detachment uses k = 1024 +
+// position in i's row, attachment k = 4096 + 2 (neighbour position) and the
+// next one.
+// ---------------------------------------------------------------------------
+
+// The reference walks agents in order; when the draw for position k of the
+// walking agent's row passes and that entry is not yet erased, it erases it
+// and the first not-yet-erased entry naming the walker in the partner's row.
+// Entries of one pair of agents are touched only while one of the two walks,
+// so each agent replays that for each of its partners — the lower index
+// first, then the higher — from both rows and the draws of both ends, and
+// marks its own erased entries. Each agent writes only its own row.
+constexpr int kMaxSpringCopies = 16; // copies of one pair an agent can hold
+
+__global__ void k_spring_detach(view v)
+{
+	grid_wait();
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= v.total_cap)
+		return;
+	int r, li;
+	if (!live(v, s, r, li))
+		return;
+	const int n = v.scnt[s];
+	const int base = v.reps[r].base;
+	const uint64_t ep = (uint64_t)v.ctr[r].spring_epoch;
+	const int32_t* row = v.springs + (int64_t)s * v.scap;
+	for (int k = 0; k < n; k++)
+		v.sdel[(int64_t)s * v.scap + k] = 0;
+	for (int k = 0; k < n; k++)
+	{
+		const int j = row[k];
+		bool seen = false; // pair handled at its first entry
+		for (int q = 0; q < k && !seen; q++)
+			seen = row[q] == j;
+		if (seen)
+			continue;
+		const int32_t* rowj = v.springs + (int64_t)j * v.scap;
+		const int nj = v.scnt[j];
+		int P[kMaxSpringCopies], Q[kMaxSpringCopies];
+		int np = 0, nq = 0;
+		for (int q = k; q < n && np < kMaxSpringCopies; q++)
+			if (row[q] == j)
+				P[np++] = q;
+		for (int q = 0; q < nj && nq < kMaxSpringCopies; q++)
+			if (rowj[q] == s)
+				Q[nq++] = q;
+		// a walks first: its entries A name b, b's entries B name a
+		const bool s_first = li < j - base;
+		const int la = s_first ? li : j - base, lb = s_first ? j - base : li;
+		const double ra = (s_first ? v.drate[s] : v.drate[j]) * v.dt;
+		const double rb = (s_first ? v.drate[j] : v.drate[s]) * v.dt;
+		const int* A = s_first ? P : Q;
+		const int* B = s_first ? Q : P;
+		const int na = s_first ? np : nq, nb = s_first ? nq : np;
+		bool ea[kMaxSpringCopies], eb[kMaxSpringCopies];
+		for (int q = 0; q < kMaxSpringCopies; q++)
+			ea[q] = eb[q] = false;
+		for (int q = 0; q < na; q++)
+			if (ppc_uniform(v.seed, ep, (uint64_t)r, (uint64_t)la, 1024u + (uint64_t)A[q]) <= ra)
+			{
+				ea[q] = true;
+				int f = 0;
+				while (f < nb && eb[f])
+					f++;
+				if (f < nb)
+					eb[f] = true;
+			}
+		for (int q = 0; q < nb; q++)
+			if (!eb[q] && ppc_uniform(v.seed, ep, (uint64_t)r, (uint64_t)lb, 1024u + (uint64_t)B[q]) <= rb)
+			{
+				eb[q] = true;
+				int f = 0;
+				while (f < na && ea[f])
+					f++;
+				if (f < na)
+					ea[f] = true;
+			}
+		const bool* mine = s_first ? ea : eb;
+		for (int q = 0; q < np; q++)
+			v.sdel[(int64_t)s * v.scap + P[q]] = mine[q] ? 1 : 0;
+	}
+}
+
+// removes the marked springs from each row, keeping the order of the rest
+__global__ void k_spring_compact_rows(view v)
+{
+	grid_wait();
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= v.total_cap)
+		return;
+	int r, li;
+	if (!live(v, s, r, li))
+		return;
+	const int n = v.scnt[s];
+	int m = 0;
+	for (int k = 0; k < n; k++)
+		if (!v.sdel[(int64_t)s * v.scap + k])
+			v.springs[(int64_t)s * v.scap + m++] = v.springs[(int64_t)s * v.scap + k];
+	v.scnt[s] = m;
+}
+
+// attachment draws for every neighbour j > i of i (neighbour lists from
+// k_neighbors, in the reference's order); the passing (i, position) pairs
+// go to the replicate's candidate list, encoded as i * ncap + position
+__global__ void k_spring_attach_draws(view v)
+{
+	grid_wait();
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= v.total_cap)
+		return;
+	int r, li;
+	if (!live(v, s, r, li))
+		return;
+	const int base = v.reps[r].base;
+	const uint64_t ep = (uint64_t)v.ctr[r].spring_epoch;
+	const int D = v.ndefs;
+	const int nn = min(v.ncnt[s], v.ncap);
+	for (int k = 0; k < nn; k++)
+	{
+		const int j = v.nidx[(int64_t)s * v.ncap + k];
+		if (j - base < li)
+			continue;
+		const double prob_l = v.arate[s] * v.dt * v.aff[(int64_t)s * D + v.def[j]];
+		const double prob_r = v.arate[j] * v.dt * v.aff[(int64_t)j * D + v.def[s]];
+		if (ppc_uniform(v.seed, ep, (uint64_t)r, (uint64_t)li, 4096u + 2u * (uint64_t)k) <= prob_l
+			|| ppc_uniform(v.seed, ep, (uint64_t)r, (uint64_t)li, 4096u + 2u * (uint64_t)k + 1u) <= prob_r)
+		{
+			const int q = atomicAdd(&v.ctr[r].nattach, 1);
+			if (q < v.reps[r].cap)
+				v.divl[base + q] = li * v.ncap + k;
+			else
+				atomicOr(v.err, ERR_LIST_CAPACITY);
+		}
+	}
+}
+
+// one block per replicate: the candidates in the reference's order (agent,
+// then neighbour position), attached while both rows are below their
+// maximum_number_of_attachments; then the replicate's spring epoch advances
+__global__ void k_spring_attach_apply(view v)
+{
+	grid_wait();
+	__shared__ int32_t sh[kSortCap];
+	const int r = blockIdx.x;
+	rep_counters& C = v.ctr[r];
+	const int base = v.reps[r].base;
+	const int nc = min(C.nattach, v.reps[r].cap);
+	if (nc > kSortCap)
+	{
+		if (threadIdx.x == 0)
+			atomicOr(v.err, ERR_LIST_CAPACITY);
+	}
+	else
+		block_sort(v.divl + base, nc, sh);
+	if (threadIdx.x != 0)
+		return;
+	if (nc <= kSortCap)
+		for (int q = 0; q < nc; q++)
+		{
+			const int code = v.divl[base + q];
+			const int s = base + code / v.ncap;
+			const int j = v.nidx[(int64_t)s * v.ncap + code % v.ncap];
+			const int ns = v.scnt[s], nj = v.scnt[j];
+			if (ns < v.maxatt[s] && nj < v.maxatt[j])
+			{
+				if (ns >= v.scap || nj >= v.scap)
+				{
+					atomicOr(v.err, ERR_SPRING_CAPACITY);
+					continue;
+				}
+				v.springs[(int64_t)s * v.scap + ns] = j;
+				v.springs[(int64_t)j * v.scap + nj] = s;
+				v.scnt[s] = ns + 1;
+				v.scnt[j] = nj + 1;
+			}
+		}
+	C.nattach = 0;
+	C.spring_epoch++;
+}
+
 // stand-in for the phenotype models: death with p_death, else division with
 // p_divide, from the counter-based draws of (seed, epoch, replicate, index)
 __global__ void k_flag_by_draws(view v, double p_divide, double p_death)
@@ -2051,6 +2248,17 @@ int launch_springs(ppc_state* s)
 		pdl(k_springs<2>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	else
 		pdl(k_springs<3>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+int launch_spring_updates(ppc_state* s)
+{
+	const int b = blocks_for(s->total_cap, kThreads);
+	pdl(k_spring_detach, b, kThreads, 0, PPC_LAUNCH(s), s->v);
+	pdl(k_spring_compact_rows, b, kThreads, 0, PPC_LAUNCH(s), s->v);
+	pdl(k_spring_attach_draws, b, kThreads, 0, PPC_LAUNCH(s), s->v);
+	pdl(k_spring_attach_apply, s->nreps, kThreads, 0, PPC_LAUNCH(s), s->v);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
