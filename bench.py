@@ -358,6 +358,31 @@ def ensemble_form(args, flush):
     return out
 
 
+def stochastic_springs_form(args, flush):
+    """Config 3 with non-zero spring attachment (0.8 /min) and detachment
+    (0.3 /min) rates and at most 3 springs per agent: the step runs the
+    separate kernels with the stochastic spring update."""
+    import torch
+
+    from paraphysicell_b200 import workloads as wl
+    from paraphysicell_b200.device import Simulation
+
+    mesh, params, a = wl.config3()
+    a.arrays["attachment_rate"][: a.count] = 0.8
+    a.arrays["detachment_rate"][: a.count] = 0.3
+    a.arrays["maximum_number_of_attachments"][: a.count] = 3
+    sim = Simulation(mesh, params, a.capacity, seed=1)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    sim.upload(a)
+    sim.update_mechanics_mesh()
+    out = _timed_steps(sim, stream, sim.step, lambda: a.count, args.steps, args.warmup, flush)
+    sim.close()
+    out.update({"workload": "config3 + spring rates", "agents": a.count,
+                "note": "attachment 0.8/min, detachment 0.3/min, max 3 springs; separate kernels per step"})
+    return out
+
+
 def config5_form(args, flush):
     """Config 5: 1,000,000 agents with division and death every step."""
     import torch
@@ -548,6 +573,7 @@ def run_ours(args, rank, world, local_rank):
         if args.workload == "config3":
             line["forms"]["batched_ensemble"] = ensemble_form(args, flush)
             line["forms"]["config5_division_death"] = config5_form(args, flush)
+            line["forms"]["stochastic_springs"] = stochastic_springs_form(args, flush)
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(args.workload)
     print(json.dumps(line), flush=True)

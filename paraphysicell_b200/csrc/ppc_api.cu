@@ -693,6 +693,9 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.order_valid, 1));
 	try_(alloc(s, v.move_src, C)); // -1: no pending move into the slot
 	try_(alloc(s, v.sdel, C * s->scap));
+	try_(alloc(s, v.first_end, C));
+	if (rc == PPC_OK && cudaMemset(v.first_end, 0x7f, sizeof(int32_t) * std::max<size_t>(C, 1)) != cudaSuccess)
+		rc = fail(PPC_ERR_CUDA, "cudaMemset failed");
 	if (rc == PPC_OK && cudaMemset(v.move_src, 0xff, sizeof(int32_t) * std::max<size_t>(C, 1)) != cudaSuccess)
 		rc = fail(PPC_ERR_CUDA, "cudaMemset failed");
 	try_(alloc(s, v.sorted, C));

@@ -119,6 +119,7 @@ struct view
 	int32_t* order_valid; // 1 while `sorted` lists exactly the live slots (set by the fixup)
 	int32_t* move_src;	  // [C] tail slot whose agent the next k_bin_count moves into this hole, or -1
 	uint8_t* sdel;		  // [C*S] spring marked for detachment this step
+	int32_t* first_end;	  // [C] INT32_MAX between spring attachment passes
 	int32_t* sorted;
 	int32_t* skey;
 	double4* spos4;

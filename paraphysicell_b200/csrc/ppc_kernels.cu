@@ -1854,48 +1854,130 @@ __global__ void k_spring_attach_draws(view v)
 	}
 }
 
-// one block per replicate: the candidates in the reference's order (agent,
+// One block per replicate: the candidates in the reference's order (agent,
 // then neighbour position), attached while both rows are below their
-// maximum_number_of_attachments; then the replicate's spring epoch advances
-__global__ void k_spring_attach_apply(view v)
+// maximum_number_of_attachments; then the replicate's spring epoch advances.
+// Up to kAttachCap candidates the block stages them in shared memory: each
+// endpoint's agent, maximum and row length, and the first endpoint of the
+// list that names the same agent (found with a per-slot atomicMin), whose
+// count slot all its endpoints share;
+// the in-order pass then touches only shared memory apart from the row
+// writes. Longer lists take the same pass over global memory.
+constexpr int kAttachCap = 4096;
+constexpr int kAttachThreads = 1024;
+constexpr size_t kAttachSmem = (size_t)kAttachCap * (2 * 4 + 2 * 4 + 2 * 2 + 2 * 2) + (size_t)kAttachCap * 4;
+
+__global__ void __launch_bounds__(kAttachThreads) k_spring_attach_apply(view v)
 {
 	grid_wait();
-	__shared__ int32_t sh[kSortCap];
+	extern __shared__ int32_t dyn[];
+	int32_t* sh = dyn;						   // [kAttachCap] sort buffer
+	int32_t* agent = sh + kAttachCap;		   // [2 cap] endpoint agents (slots): 2q = i, 2q+1 = j
+	int32_t* cnt = agent + 2 * kAttachCap;	   // [2 cap] row length, kept at each agent's first endpoint
+	int16_t* mx = reinterpret_cast<int16_t*>(cnt + 2 * kAttachCap); // [2 cap] maximum_number_of_attachments
+	int16_t* rep = mx + 2 * kAttachCap;		   // [2 cap] first endpoint naming the same agent
 	const int r = blockIdx.x;
 	rep_counters& C = v.ctr[r];
 	const int base = v.reps[r].base;
 	const int nc = min(C.nattach, v.reps[r].cap);
-	if (nc > kSortCap)
+	int32_t* codes = v.divl + base;
+	block_sort(codes, nc, sh); // nc > kSortCap sorts through global memory
+	if (nc <= kAttachCap)
 	{
+		const int ne = 2 * nc;
+		for (int e = threadIdx.x; e < ne; e += blockDim.x)
+		{
+			const int code = codes[e >> 1];
+			const int i = base + code / v.ncap;
+			const int a = (e & 1) ? v.nidx[(int64_t)i * v.ncap + code % v.ncap] : i;
+			agent[e] = a;
+			cnt[e] = v.scnt[a];
+			mx[e] = (int16_t)min(v.maxatt[a], 32767);
+		}
+		// first endpoint of each agent: atomicMin on a per-slot word (large
+		// between uses), read back, then restored
+		for (int e = threadIdx.x; e < ne; e += blockDim.x)
+			atomicMin(v.first_end + agent[e], e);
+		__syncthreads();
+		for (int e = threadIdx.x; e < ne; e += blockDim.x)
+			rep[e] = (int16_t)__ldcg(v.first_end + agent[e]);
+		__syncthreads();
+		for (int e = threadIdx.x; e < ne; e += blockDim.x)
+			v.first_end[agent[e]] = INT32_MAX;
+		__syncthreads();
+		// a candidate whose agents appear in no earlier candidate sees the
+		// initial row lengths whatever came before: those are settled in
+		// parallel, the rest in order
+		for (int q = threadIdx.x; q < nc; q += blockDim.x)
+			if (rep[2 * q] == 2 * q && rep[2 * q + 1] == 2 * q + 1)
+			{
+				const int ni = cnt[2 * q], nj = cnt[2 * q + 1];
+				if (ni < mx[2 * q] && nj < mx[2 * q + 1])
+				{
+					if (ni >= v.scap || nj >= v.scap)
+					{
+						atomicOr(v.err, ERR_SPRING_CAPACITY);
+						continue;
+					}
+					const int i = agent[2 * q], j = agent[2 * q + 1];
+					v.springs[(int64_t)i * v.scap + ni] = j;
+					v.springs[(int64_t)j * v.scap + nj] = i;
+					cnt[2 * q] = ni + 1;
+					cnt[2 * q + 1] = nj + 1;
+				}
+			}
+		__syncthreads();
 		if (threadIdx.x == 0)
-			atomicOr(v.err, ERR_LIST_CAPACITY);
+			for (int q = 0; q < nc; q++)
+			{
+				const int ri = rep[2 * q], rj = rep[2 * q + 1];
+				if (ri == 2 * q && rj == 2 * q + 1)
+					continue; // settled above
+				const int ni = cnt[ri], nj = cnt[rj];
+				if (ni < mx[2 * q] && nj < mx[2 * q + 1])
+				{
+					if (ni >= v.scap || nj >= v.scap)
+					{
+						atomicOr(v.err, ERR_SPRING_CAPACITY);
+						continue;
+					}
+					const int i = agent[2 * q], j = agent[2 * q + 1];
+					v.springs[(int64_t)i * v.scap + ni] = j;
+					v.springs[(int64_t)j * v.scap + nj] = i;
+					cnt[ri] = ni + 1;
+					cnt[rj] = nj + 1;
+				}
+			}
+		__syncthreads();
+		for (int e = threadIdx.x; e < ne; e += blockDim.x)
+			if (rep[e] == e)
+				v.scnt[agent[e]] = cnt[e];
 	}
-	else
-		block_sort(v.divl + base, nc, sh);
-	if (threadIdx.x != 0)
-		return;
-	if (nc <= kSortCap)
+	else if (threadIdx.x == 0)
 		for (int q = 0; q < nc; q++)
 		{
-			const int code = v.divl[base + q];
-			const int s = base + code / v.ncap;
-			const int j = v.nidx[(int64_t)s * v.ncap + code % v.ncap];
-			const int ns = v.scnt[s], nj = v.scnt[j];
-			if (ns < v.maxatt[s] && nj < v.maxatt[j])
+			const int code = codes[q];
+			const int i = base + code / v.ncap;
+			const int j = v.nidx[(int64_t)i * v.ncap + code % v.ncap];
+			const int ni = v.scnt[i], nj = v.scnt[j];
+			if (ni < v.maxatt[i] && nj < v.maxatt[j])
 			{
-				if (ns >= v.scap || nj >= v.scap)
+				if (ni >= v.scap || nj >= v.scap)
 				{
 					atomicOr(v.err, ERR_SPRING_CAPACITY);
 					continue;
 				}
-				v.springs[(int64_t)s * v.scap + ns] = j;
-				v.springs[(int64_t)j * v.scap + nj] = s;
-				v.scnt[s] = ns + 1;
+				v.springs[(int64_t)i * v.scap + ni] = j;
+				v.springs[(int64_t)j * v.scap + nj] = i;
+				v.scnt[i] = ni + 1;
 				v.scnt[j] = nj + 1;
 			}
 		}
-	C.nattach = 0;
-	C.spring_epoch++;
+	if (threadIdx.x == 0)
+	{
+		C.nattach = 0;
+		C.spring_epoch++;
+	}
 }
 
 // stand-in for the phenotype models: death with p_death, else division with
@@ -2258,7 +2340,9 @@ int launch_spring_updates(ppc_state* s)
 	pdl(k_spring_detach, b, kThreads, 0, PPC_LAUNCH(s), s->v);
 	pdl(k_spring_compact_rows, b, kThreads, 0, PPC_LAUNCH(s), s->v);
 	pdl(k_spring_attach_draws, b, kThreads, 0, PPC_LAUNCH(s), s->v);
-	pdl(k_spring_attach_apply, s->nreps, kThreads, 0, PPC_LAUNCH(s), s->v);
+	PPC_CUDA(cudaFuncSetAttribute(k_spring_attach_apply, cudaFuncAttributeMaxDynamicSharedMemorySize,
+								  (int)kAttachSmem));
+	pdl(k_spring_attach_apply, s->nreps, kAttachThreads, kAttachSmem, PPC_LAUNCH(s), s->v);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
