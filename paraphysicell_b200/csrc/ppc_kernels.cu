@@ -933,15 +933,9 @@ __global__ void __launch_bounds__(kFusedThreads, 5) k_fused_f32(view v, int cur)
 // ---------------------------------------------------------------------------
 
 constexpr int kStageThreads = 128;
-#ifndef PPC_STAGE_SCAN
-#define PPC_STAGE_SCAN 4
-#endif
-constexpr int kStageScan = PPC_STAGE_SCAN; // candidates a lane tests per scan iteration, loads issued together
+constexpr int kStageScan = 4; // candidates a lane tests per scan iteration, loads issued together
 static_assert(kStageScan >= 1 && kStageScan <= kList, "a scan iteration must fit in the neighbour list");
-constexpr size_t kStageStatic = 10 * 1024; // bound on the staged kernel's static shared memory
-#ifndef PPC_STAGE_MINB
-#define PPC_STAGE_MINB 4
-#endif
+constexpr size_t kStageStatic = 16 * 1024; // bound on the staged kernel's static shared memory
 
 // array bounds [lo[k], hi[k]) of the stencil rows of the agent in voxel
 // `key`: rows z outer then y, each the voxels x-1..x+1, which are consecutive
@@ -988,7 +982,7 @@ __device__ __forceinline__ bool filter_keep(const float4& pf, const float4& c, f
 }
 
 template <int DIMS, bool WALLS, bool SPRINGS, bool VEL, bool F32>
-__global__ void __launch_bounds__(kStageThreads, PPC_STAGE_MINB) k_fused_staged(view v, int cur, int cap)
+__global__ void __launch_bounds__(kStageThreads, 4) k_fused_staged(view v, int cur, int cap)
 {
 	grid_wait();
 	bump_spring_epochs(v);
