@@ -151,12 +151,28 @@ int get_scalar(ppc_state* s, T* host, const T* dev, int32_t base, int32_t n, siz
 	return PPC_OK;
 }
 
+// the device address of a pinned, mapped host buffer (kernels then read or
+// write it directly over the bus, without a staging copy), or null
+const void* mapped(const void* host)
+{
+	cudaPointerAttributes at {};
+	if (cudaPointerGetAttributes(&at, host) != cudaSuccess)
+	{
+		cudaGetLastError();
+		return nullptr;
+	}
+	return at.type == cudaMemoryTypeHost ? at.devicePointer : nullptr;
+}
+
 int put_vec(ppc_state* s, double4* dev, const double* host, int32_t r, int32_t n, bool defaults)
 {
 	if (!host && !defaults)
 		return PPC_OK;
 	if (n == 0)
 		return PPC_OK;
+	if (host)
+		if (const void* d = mapped(host))
+			return launch_unpack_vec(s, dev, static_cast<const double*>(d), r, n);
 	const size_t bytes = (size_t)n * s->dims * sizeof(double);
 	PPC_TRY(ensure_stage(s, bytes));
 	if (host)
@@ -173,6 +189,8 @@ int get_vec(ppc_state* s, double* host, const double4* dev, int32_t r, int32_t n
 {
 	if (!host || n == 0)
 		return PPC_OK;
+	if (const void* d = mapped(host))
+		return launch_pack_vec(s, static_cast<double*>(const_cast<void*>(d)), dev, r, n);
 	const size_t bytes = (size_t)n * s->dims * sizeof(double);
 	PPC_TRY(ensure_stage(s, bytes));
 	PPC_TRY(launch_pack_vec(s, static_cast<double*>(s->stage), dev, r, n));

@@ -2155,27 +2155,28 @@ __global__ void k_divide_finish(view v)
 // host layout <-> device layout
 // ---------------------------------------------------------------------------
 
+// host layout (dims doubles per agent) <-> double4 rows, one thread per
+// double so that reads of the flat array (device staging or, for pinned host
+// buffers, host memory read over the bus) are contiguous across a warp
 __global__ void k_unpack_vec(view v, double4* dst, const double* src, int base, int n)
 {
 	grid_wait();
-	const int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= n)
+	const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (e >= (int64_t)n * 4)
 		return;
-	double4 x = make_double4(0, 0, 0, 0);
-	for (int d = 0; d < v.dims; d++)
-		set_comp(x, d, src[(int64_t)i * v.dims + d]);
-	dst[base + i] = x;
+	const int i = (int)(e >> 2), d = (int)(e & 3);
+	double* row = reinterpret_cast<double*>(dst + base + i);
+	row[d] = d < v.dims ? src[(int64_t)i * v.dims + d] : 0.0;
 }
 
 __global__ void k_pack_vec(view v, double* dst, const double4* src, int base, int n)
 {
 	grid_wait();
-	const int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= n)
+	const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (e >= (int64_t)n * v.dims)
 		return;
-	const double4 x = src[base + i];
-	for (int d = 0; d < v.dims; d++)
-		dst[(int64_t)i * v.dims + d] = comp(x, d);
+	const int i = (int)(e / v.dims), d = (int)(e % v.dims);
+	dst[e] = reinterpret_cast<const double*>(src + base + i)[d];
 }
 
 __global__ void k_unpack_prm(view v, int field, const double* src, int base, int n)
@@ -2516,7 +2517,7 @@ int launch_unpack_vec(ppc_state* s, double4* dst, const double* src, int32_t r, 
 {
 	if (n == 0)
 		return PPC_OK;
-	pdl(k_unpack_vec, blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s), s->v, dst, src, s->reps[r].base, n);
+	pdl(k_unpack_vec, blocks_for(n * 4, kThreads), kThreads, 0, PPC_LAUNCH(s), s->v, dst, src, s->reps[r].base, n);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -2525,7 +2526,8 @@ int launch_pack_vec(ppc_state* s, double* dst, const double4* src, int32_t r, in
 {
 	if (n == 0)
 		return PPC_OK;
-	pdl(k_pack_vec, blocks_for(n, kThreads), kThreads, 0, PPC_LAUNCH(s), s->v, dst, src, s->reps[r].base, n);
+	pdl(k_pack_vec, blocks_for(n * s->dims, kThreads), kThreads, 0, PPC_LAUNCH(s), s->v, dst, src, s->reps[r].base,
+		n);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
