@@ -213,7 +213,11 @@ int ppc_download(ppc_state* s, int32_t replicate, ppc_agents* agents);
 /* Overwrites only the fields whose pointers are non-NULL, keeping every other
  * device field; agents->count must equal the device count. This is the
  * per-step host sync of a caller that keeps cell_data authoritative on the
- * host. Synchronises the stream. */
+ * host. When the view carries only positions, velocities, previous
+ * velocities, pressure and orientation, and the positions are bit-identical
+ * to the resident ones, the mechanics mesh is kept (no rebuild before the
+ * next step). Pinned host buffers (ppc_host_alloc) are read directly by the
+ * device. Synchronises the stream. */
 int ppc_upload_fields(ppc_state* s, int32_t replicate, const ppc_agents* agents);
 
 int ppc_get_count(ppc_state* s, int32_t replicate, int32_t* count);

@@ -164,7 +164,8 @@ const void* mapped(const void* host)
 	return at.type == cudaMemoryTypeHost ? at.devicePointer : nullptr;
 }
 
-int put_vec(ppc_state* s, double4* dev, const double* host, int32_t r, int32_t n, bool defaults)
+int put_vec(ppc_state* s, double4* dev, const double* host, int32_t r, int32_t n, bool defaults,
+			int32_t* changed = nullptr)
 {
 	if (!host && !defaults)
 		return PPC_OK;
@@ -172,7 +173,7 @@ int put_vec(ppc_state* s, double4* dev, const double* host, int32_t r, int32_t n
 		return PPC_OK;
 	if (host)
 		if (const void* d = mapped(host))
-			return launch_unpack_vec(s, dev, static_cast<const double*>(d), r, n);
+			return launch_unpack_vec(s, dev, static_cast<const double*>(d), r, n, changed);
 	const size_t bytes = (size_t)n * s->dims * sizeof(double);
 	PPC_TRY(ensure_stage(s, bytes));
 	if (host)
@@ -181,7 +182,7 @@ int put_vec(ppc_state* s, double4* dev, const double* host, int32_t r, int32_t n
 		PPC_CUDA(cudaMemsetAsync(s->stage, 0, bytes, s->stream));
 	// the next field's copy into the stage is ordered after this kernel on
 	// the same stream; pageable sources are staged by the copy call itself
-	PPC_TRY(launch_unpack_vec(s, dev, static_cast<const double*>(s->stage), r, n));
+	PPC_TRY(launch_unpack_vec(s, dev, static_cast<const double*>(s->stage), r, n, changed));
 	return PPC_OK;
 }
 
@@ -229,6 +230,22 @@ int get_prm(ppc_state* s, int field, double* host, int32_t r, int32_t n)
 // reference defaults (src/data_storage_phenotype.cpp:62-125,194-214, src/cell.cpp:47-61)
 constexpr double kRadius = 8.412710547954228, kNuclearRadius = 5.051670902881889, kSurface = 889.3685284131693;
 
+// true when the view carries no field but positions, velocities, previous
+// velocities, pressure and orientation
+bool only_kinematic(const ppc_agents* a)
+{
+	const void* others[] = { a->radius, a->cell_cell_repulsion_strength, a->cell_cell_adhesion_strength,
+							 a->relative_maximum_adhesion_distance, a->cell_BM_repulsion_strength,
+							 a->attachment_elastic_constant, a->attachment_rate, a->detachment_rate,
+							 a->maximum_number_of_attachments, a->cell_adhesion_affinities, a->cell_definition_indices,
+							 a->is_movable, a->flags, a->agent_ids, a->total_volume, a->nuclear_volume,
+							 a->nuclear_radius, a->surface_area, a->polarity, a->spring_counts, a->springs };
+	for (const void* p : others)
+		if (p)
+			return false;
+	return true;
+}
+
 int transfer_in(ppc_state* s, int32_t r, const ppc_agents* a, bool defaults)
 {
 	const rep_info& R = s->reps[r];
@@ -242,7 +259,13 @@ int transfer_in(ppc_state* s, int32_t r, const ppc_agents* a, bool defaults)
 			if (a->cell_definition_indices[i] < 0 || a->cell_definition_indices[i] >= D)
 				return fail(PPC_ERR_ARG, "cell definition index out of range");
 
-	PPC_TRY(put_vec(s, v.pos[s->cur], a->positions, r, n, defaults));
+	// an upload of kinematic fields only (positions, velocities, previous
+	// velocities, pressure, orientation) keeps the mesh when the positions it
+	// brings are bit-identical to the resident ones
+	const bool kinematic = !defaults && only_kinematic(a);
+	if (kinematic && a->positions)
+		PPC_CUDA(cudaMemsetAsync(v.pos_changed, 0, sizeof(int32_t), s->stream));
+	PPC_TRY(put_vec(s, v.pos[s->cur], a->positions, r, n, defaults, kinematic ? v.pos_changed : nullptr));
 	PPC_TRY(put_vec(s, v.vel, a->velocities, r, n, defaults));
 	PPC_TRY(put_vec(s, v.vprev, a->previous_velocities, r, n, defaults));
 	PPC_TRY(put_vec(s, v.orient, a->orientation, r, n, defaults));
@@ -331,6 +354,16 @@ int transfer_in(ppc_state* s, int32_t r, const ppc_agents* a, bool defaults)
 		if (rate)
 			for (int32_t i = 0; i < n && !s->rates_nonzero; i++)
 				s->rates_nonzero = rate[i] != 0.0;
+	if (kinematic)
+	{
+		*s->pinned_flag = 0;
+		if (a->positions)
+			PPC_CUDA(cudaMemcpyAsync(s->pinned_flag, v.pos_changed, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
+		PPC_CUDA(cudaStreamSynchronize(s->stream));
+		if (*s->pinned_flag)
+			s->bins_valid = false; // the slots still hold the same agents
+		return PPC_OK;
+	}
 	s->bins_valid = false;
 	// slots were rewritten: the next rebuild counts by slot
 	PPC_CUDA(cudaMemsetAsync(v.order_valid, 0, sizeof(int32_t), s->stream));
@@ -712,6 +745,7 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.move_src, C)); // -1: no pending move into the slot
 	try_(alloc(s, v.sdel, C * s->scap));
 	try_(alloc(s, v.first_end, C));
+	try_(alloc(s, v.pos_changed, 1));
 	if (rc == PPC_OK && cudaMemset(v.first_end, 0x7f, sizeof(int32_t) * std::max<size_t>(C, 1)) != cudaSuccess)
 		rc = fail(PPC_ERR_CUDA, "cudaMemset failed");
 	if (rc == PPC_OK && cudaMemset(v.move_src, 0xff, sizeof(int32_t) * std::max<size_t>(C, 1)) != cudaSuccess)
@@ -733,10 +767,12 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.draw_epoch, replicates));
 	s->host_count.assign(replicates, 0);
 	if (rc == PPC_OK
-		&& cudaHostAlloc(reinterpret_cast<void**>(&s->pinned_ctr), sizeof(rep_counters) * replicates,
+		&& cudaHostAlloc(reinterpret_cast<void**>(&s->pinned_ctr), sizeof(rep_counters) * (replicates + 1),
 						 cudaHostAllocDefault)
 			   != cudaSuccess)
 		rc = fail(PPC_ERR_CUDA, "cudaHostAlloc failed");
+	if (rc == PPC_OK)
+		s->pinned_flag = reinterpret_cast<int32_t*>(s->pinned_ctr + replicates);
 	if (rc == PPC_OK)
 	{
 		std::vector<int32_t> rid(C, 0);
@@ -863,11 +899,13 @@ int ppc_upload(ppc_state* s, int32_t r, const ppc_agents* a)
 	if (a->count > s->reps[r].cap)
 		return fail(PPC_ERR_CAPACITY, "agent count exceeds the replicate's capacity");
 	// a fresh upload resets the replicate's counters except the event totals
+	// and the spring-draw epoch
 	std::vector<rep_counters> all;
 	PPC_TRY(read_counters(s, all));
 	rep_counters c {};
 	c.divisions = all[r].divisions;
 	c.deaths = all[r].deaths;
+	c.spring_epoch = all[r].spring_epoch; // the draw streams continue, as in the reference's generator
 	PPC_CUDA(cudaMemcpy(&s->v.ctr[r], &c, sizeof c, cudaMemcpyHostToDevice));
 	s->lists_stale = false;
 	return transfer_in(s, r, a, true);

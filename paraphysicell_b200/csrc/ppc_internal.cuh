@@ -120,6 +120,7 @@ struct view
 	int32_t* move_src;	  // [C] tail slot whose agent the next k_bin_count moves into this hole, or -1
 	uint8_t* sdel;		  // [C*S] spring marked for detachment this step
 	int32_t* first_end;	  // [C] INT32_MAX between spring attachment passes
+	int32_t* pos_changed; // set by an upload whose positions differ from the resident ones
 	int32_t* sorted;
 	int32_t* skey;
 	double4* spos4;
@@ -198,6 +199,7 @@ struct ppc_state
 	// host copies of the replicate counts as last read (a download's first guess)
 	std::vector<int32_t> host_count;
 	ppc::rep_counters* pinned_ctr = nullptr; // pinned landing area of the counters
+	int32_t* pinned_flag = nullptr;			 // pinned landing area of pos_changed
 	bool staged = false;
 	bool coop = false;
 	int tile_threads = 128;
@@ -245,7 +247,7 @@ int launch_divide(ppc_state* s);
 int launch_flag_by_draws(ppc_state* s, double p_divide, double p_death);
 
 // packing between host-layout staging buffers and device arrays
-int launch_unpack_vec(ppc_state* s, double4* dst, const double* src, int32_t r, int32_t n);
+int launch_unpack_vec(ppc_state* s, double4* dst, const double* src, int32_t r, int32_t n, int32_t* changed = nullptr);
 int launch_pack_vec(ppc_state* s, double* dst, const double4* src, int32_t r, int32_t n);
 int launch_unpack_prm(ppc_state* s, int field, const double* src, int32_t r, int32_t n);
 int launch_pack_prm(ppc_state* s, int field, double* dst, int32_t r, int32_t n);

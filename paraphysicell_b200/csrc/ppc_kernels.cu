@@ -2158,7 +2158,8 @@ __global__ void k_divide_finish(view v)
 // host layout (dims doubles per agent) <-> double4 rows, one thread per
 // double so that reads of the flat array (device staging or, for pinned host
 // buffers, host memory read over the bus) are contiguous across a warp
-__global__ void k_unpack_vec(view v, double4* dst, const double* src, int base, int n)
+// `changed`, when given, is set when any value differs from the one it replaces
+__global__ void k_unpack_vec(view v, double4* dst, const double* src, int base, int n, int32_t* changed)
 {
 	grid_wait();
 	const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -2166,7 +2167,10 @@ __global__ void k_unpack_vec(view v, double4* dst, const double* src, int base, 
 		return;
 	const int i = (int)(e >> 2), d = (int)(e & 3);
 	double* row = reinterpret_cast<double*>(dst + base + i);
-	row[d] = d < v.dims ? src[(int64_t)i * v.dims + d] : 0.0;
+	const double x = d < v.dims ? src[(int64_t)i * v.dims + d] : 0.0;
+	if (changed && __double_as_longlong(row[d]) != __double_as_longlong(x))
+		*changed = 1;
+	row[d] = x;
 }
 
 __global__ void k_pack_vec(view v, double* dst, const double4* src, int base, int n)
@@ -2513,11 +2517,12 @@ int launch_flag_by_draws(ppc_state* s, double p_divide, double p_death)
 	return PPC_OK;
 }
 
-int launch_unpack_vec(ppc_state* s, double4* dst, const double* src, int32_t r, int32_t n)
+int launch_unpack_vec(ppc_state* s, double4* dst, const double* src, int32_t r, int32_t n, int32_t* changed)
 {
 	if (n == 0)
 		return PPC_OK;
-	pdl(k_unpack_vec, blocks_for(n * 4, kThreads), kThreads, 0, PPC_LAUNCH(s), s->v, dst, src, s->reps[r].base, n);
+	pdl(k_unpack_vec, blocks_for(n * 4, kThreads), kThreads, 0, PPC_LAUNCH(s), s->v, dst, src, s->reps[r].base, n,
+		changed);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
