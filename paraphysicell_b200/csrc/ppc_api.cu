@@ -742,6 +742,9 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.tmp, C));
 	try_(alloc(s, v.vsc, C));
 	try_(alloc(s, v.order_valid, 1));
+	try_(alloc(s, v.binned, replicates));
+	try_(alloc(s, v.moves_pending, 1));
+	try_(alloc(s, v.appended, 1));
 	try_(alloc(s, v.move_src, C)); // -1: no pending move into the slot
 	try_(alloc(s, v.sdel, C * s->scap));
 	try_(alloc(s, v.first_end, C));

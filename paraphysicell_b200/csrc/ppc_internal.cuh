@@ -116,8 +116,11 @@ struct view
 	int32_t* vrank;
 	int32_t* tmp;
 	int2* vsc;		// [C] voxel start and count of each slot's voxel, from the scatter to the fixup
-	int32_t* order_valid; // 1 while `sorted` lists exactly the live slots (set by the fixup)
+	int32_t* order_valid; // 1 once a rebuild has set `sorted` (cleared by uploads)
+	int32_t* binned;	  // [replicates] live count at the last rebuild (the slots `sorted` lists)
 	int32_t* move_src;	  // [C] tail slot whose agent the next k_bin_count moves into this hole, or -1
+	int32_t* moves_pending; // a folded compaction left moves for the next k_bin_count
+	int32_t* appended;		// agents were appended (division) since the last rebuild
 	uint8_t* sdel;		  // [C*S] spring marked for detachment this step
 	int32_t* first_end;	  // [C] INT32_MAX between spring attachment passes
 	int32_t* pos_changed; // set by an upload whose positions differ from the resident ones

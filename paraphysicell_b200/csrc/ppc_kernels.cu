@@ -155,32 +155,13 @@ __device__ __forceinline__ void move_agent(const view& v, int cur, int d, int s)
 	v.ncnt[d] = v.ncnt[s];
 }
 
-// Voxel key and provisional rank of every live agent, and the per-tile
-// totals the scan needs. When the previous rebuild's key-ordered array still
-// lists exactly the live slots (nothing removed, divided or uploaded since),
-// thread t takes the agent at position t of that order: agents rarely change
-// voxel between steps, so a warp's agents share voxels and tiles, and one
-// atomic per distinct voxel and per distinct tile of the warp suffices.
-// Otherwise thread t takes slot t. The provisional rank only has to be a
-// permutation of 0..count-1 inside the voxel; k_bin_fixup sets the final one.
-__global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur)
+// Voxel key and provisional rank of one agent (s < 0: an idle lane), with
+// one atomic per distinct voxel and per distinct scan tile of the warp.
+// A hole the compaction plan filled gets its tail agent first.
+__device__ __forceinline__ void count_agent(const view& v, int cur, int s, int r, int lane, bool moves)
 {
-	grid_wait();
-	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	const int lane = threadIdx.x & 31;
-	int s = -1, r = 0, local = 0;
-	if (*v.order_valid)
+	if (s >= 0 && moves)
 	{
-		if (t < *v.cursor)
-		{
-			s = v.sorted[t];
-			r = rep_of(v, s);
-		}
-	}
-	else if (t < v.total_cap && live(v, t, r, local))
-	{
-		s = t;
-		// a hole that the compaction plan filled with a tail agent
 		const int src = v.move_src[s];
 		if (src >= 0)
 		{
@@ -213,6 +194,40 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur)
 		v.key[s] = key;
 		v.vrank[s] = base + __popc(same & ((1u << lane) - 1));
 	}
+}
+
+// Voxel key and provisional rank of every live agent, and the per-tile
+// totals the scan needs. The previous rebuild's key order lists the slots
+// that were live then; those still live are taken in that order — agents
+// rarely change voxel between steps, so a warp's agents share voxels and
+// tiles and the atomics aggregate — and the slots appended since (division
+// daughters past the previous count) by slot. Without a previous order
+// (after an upload) every live slot is taken by slot. The provisional rank
+// only has to be a permutation of 0..count-1 inside the voxel; k_bin_fixup
+// sets the final one.
+__global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur)
+{
+	grid_wait();
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	const int lane = threadIdx.x & 31;
+	const bool ordered = *v.order_valid != 0;
+	const bool moves = *v.moves_pending != 0;
+	const bool appended = *v.appended != 0;
+	// both candidates first, so that their loads overlap
+	int sa = -1, ra = 0, sb = -1, rb = 0, local = 0;
+	if ((!ordered || appended) && t < v.total_cap && live(v, t, rb, local)
+		&& local >= (ordered ? v.binned[rb] : 0))
+		sb = t;
+	if (ordered && t < *v.cursor)
+	{
+		const int q = v.sorted[t];
+		if (live(v, q, ra, local))
+			sa = q;
+	}
+	if (__any_sync(0xffffffffu, sa >= 0))
+		count_agent(v, cur, sa, ra, lane, moves);
+	if (__any_sync(0xffffffffu, sb >= 0))
+		count_agent(v, cur, sb, rb, lane, moves);
 }
 
 // Exclusive scan of the per-voxel counts into vstart (one block per tile of
@@ -292,8 +307,17 @@ __global__ void k_bin_scatter(view v)
 	grid_wait();
 	int s = blockIdx.x * blockDim.x + threadIdx.x;
 	if (blockIdx.x == 0)
+	{
 		for (int k = threadIdx.x; k < v.ntiles; k += blockDim.x)
 			v.tile_sum[k] = 0; // ready for the next rebuild's k_bin_count
+		for (int k = threadIdx.x; k < v.nreps; k += blockDim.x)
+			v.binned[k] = v.ctr[k].count; // the slots this rebuild's order lists
+		if (threadIdx.x == 0)
+		{
+			*v.moves_pending = 0; // applied by this rebuild's k_bin_count
+			*v.appended = 0;	  // counted by it too
+		}
+	}
 	if (s >= v.total_cap)
 		return;
 	int r, local;
@@ -1684,15 +1708,17 @@ __global__ void k_compact_plan(view v, int phenotype_pass, int springs, int fold
 			moves[2 * nm + 1] = occ;
 			nm++;
 			if (fold)
+			{
 				v.move_src[base + h] = base + occ; // applied by the next k_bin_count
+				*v.moves_pending = 1;
+			}
 		}
 	}
 	C.count = cnt;
 	C.deaths += deaths;
 	C.nbad = 0;
 	v.nmoves[r] = nm;
-	if (cnt != cnt0 || nm > 0)
-		*v.order_valid = 0; // the live slots changed: the next count goes by slot
+
 }
 
 // the planned moves, one thread per move
@@ -2044,7 +2070,7 @@ __global__ void k_divide_plan(view v, int springs)
 		C.ndiv = 0;
 		return;
 	}
-	*v.order_valid = 0; // daughters are appended: the next count goes by slot
+	*v.appended = 1; // daughters go past the count: the next k_bin_count takes new slots too
 	if (springs)
 		for (int k = 0; k < nd; k++)
 		{
