@@ -164,6 +164,9 @@ int ppc_destroy(ppc_state* s);
  * work of this state; NULL selects the state's own stream. */
 int ppc_set_stream(ppc_state* s, void* cuda_stream);
 
+/* Arithmetic of the fused force pass (enum ppc_precision). Steps with
+ * non-zero spring attachment or detachment rates run the separate FP64
+ * kernels whatever the setting. */
 int ppc_set_precision(ppc_state* s, int32_t precision);
 
 /* Seed of the counter-based random stream that replaces the reference's
