@@ -336,6 +336,69 @@ def test_batch_replicates_match_independent_oracles(shape):
         gu.assert_same_state(out, gu.fetch(o, s))
 
 
+@pytest.mark.parametrize("shape", [(-1, 128, 0), (-2, 128, 0), (0, 128, 32 * 1024)], ids=lambda s: "edge%d" % s[0])
+def test_empty_and_tiny_simulations(shape):
+    """No agents, one agent, and every agent removed: the step, the mesh and
+    the downloads behave like the oracle's."""
+    from paraphysicell_b200.abi import AgentArrays
+    mesh, params, a = wl.scaled(wl.config2, 300, seed=95)
+    for n in (0, 1):
+        b = AgentArrays(n, a.dims, a.ndefs, capacity=4)
+        for k in b.arrays:
+            width = b.arrays[k].size // b.capacity
+            b.arrays[k][: n * width] = a.arrays[k][: n * width]
+        o, d = gu.make_pair(mesh, params, b)
+        d.set_launch_shape(*shape)
+        o.update_mechanics_mesh()
+        o.update_cell_neighbors()
+        d.update_mechanics_mesh()
+        o.step(3, 0, 0.0, 0.0)
+        d.step(3)
+        gu.assert_same_state(gu.fetch(d, b), gu.fetch(o, b))
+    gone = a.copy()
+    gone.arrays["flags"][: gone.count] = FLAG_TO_REMOVE  # every agent removed
+    o, d = gu.make_pair(mesh, params, gone)
+    d.set_launch_shape(*shape)
+    o.update_cell_container_for_mechanics()
+    d.update_cell_container_for_mechanics()
+    assert d.count() == gu.fetch(o, gone).count == 0
+    o.update_mechanics_mesh()
+    d.update_mechanics_mesh()
+    o.step(2, 0, 0.0, 0.0)
+    d.step(2)
+    assert d.count() == gu.fetch(o, gone).count == 0
+
+
+@pytest.mark.parametrize("shape", [(-1, 128, 0), (-2, 128, 0), (0, 128, 32 * 1024)], ids=lambda s: "edge%d" % s[0])
+def test_batch_with_an_empty_replicate(shape):
+    """A batched state whose middle replicate has no agents steps the others
+    exactly like their own oracles."""
+    meshes, params, sets = wl.config4(seed=63, replicates=3, n_min=300, n_max=1200)
+    from oracle.oracle import Oracle
+    from paraphysicell_b200.abi import AgentArrays
+    from paraphysicell_b200.device import Simulation
+    gu.build.ensure_built()
+    sets[1] = AgentArrays(0, sets[1].dims, sets[1].ndefs, capacity=sets[1].capacity)
+    d = Simulation(meshes, params, [s.capacity for s in sets])
+    d.set_launch_shape(*shape)
+    oracles = []
+    for r, (m, s_) in enumerate(zip(meshes, sets)):
+        d.upload(s_, replicate=r)
+        o = Oracle(m, params)
+        o.upload(s_)
+        o.update_mechanics_mesh()
+        o.update_cell_neighbors()
+        oracles.append(o)
+    d.update_mechanics_mesh()
+    d.step(12)
+    for r, (o, s_) in enumerate(zip(oracles, sets)):
+        o.step(12, 0, 0.0, 0.0)
+        out = gu.AgentArrays(0, s_.dims, s_.ndefs, s_.capacity)
+        out.count = out.capacity
+        d.download(out, replicate=r)
+        gu.assert_same_state(out, gu.fetch(o, s_))
+
+
 def test_errors_are_reported():
     """Device-detected failures come back as status codes, not faults."""
     from paraphysicell_b200.abi import PPCError, PPC_ERR_CAPACITY, PPC_ERR_NONFINITE
