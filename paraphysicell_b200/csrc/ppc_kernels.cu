@@ -1947,12 +1947,24 @@ __global__ void __launch_bounds__(kAttachThreads) k_spring_attach_apply(view v)
 				}
 			}
 		__syncthreads();
+		// the others, listed in order (the sort buffer is free now)
+		int ndep = 0;
+		for (int q0 = 0; q0 < nc; q0 += blockDim.x)
+		{
+			const int q = q0 + threadIdx.x;
+			const int dep = q < nc && !(rep[2 * q] == 2 * q && rep[2 * q + 1] == 2 * q + 1);
+			int total;
+			const int off = block_exclusive_scan(dep, total);
+			if (dep)
+				sh[ndep + off] = q;
+			ndep += total;
+		}
+		__syncthreads();
 		if (threadIdx.x == 0)
-			for (int q = 0; q < nc; q++)
+			for (int w = 0; w < ndep; w++)
 			{
+				const int q = sh[w];
 				const int ri = rep[2 * q], rj = rep[2 * q + 1];
-				if (ri == 2 * q && rj == 2 * q + 1)
-					continue; // settled above
 				const int ni = cnt[ri], nj = cnt[rj];
 				if (ni < mx[2 * q] && nj < mx[2 * q + 1])
 				{
