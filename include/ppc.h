@@ -291,6 +291,63 @@ int ppc_update_cell_container_for_phenotype(ppc_state* s);
  * src/original/core/standard_models.cpp:478-540). */
 int ppc_flag_by_draws(ppc_state* s, double p_divide, double p_death);
 
+/*
+ * Phenotype fields of one replicate that cell-cell interactions read or write
+ * and that the mechanics state does not hold (reference: cell_data
+ * interactions.*, deaths.dead, states.damage/total_attack_time/number_of_nuclei,
+ * volumes.*, agent_data.internalized_substrates). Host memory, one row per
+ * agent in the state's current agent order (`count` = the replicate's count).
+ * Per-definition rows have cell_definitions_count entries; substrate rows have
+ * `substrates` entries. The resident total volume, nuclear volume, radius,
+ * nuclear radius, surface area, positions and flags are the state's own.
+ */
+typedef struct ppc_interactions
+{
+	int32_t count;
+	int32_t substrates;
+
+	/* read */
+	const uint8_t* dead;						/* [count] deaths.dead */
+	const double* dead_phagocytosis_rate;		/* [count] */
+	const double* damage_rate;					/* [count] */
+	const double* live_phagocytosis_rates;		/* [count*definitions] */
+	const double* attack_rates;					/* [count*definitions] */
+	const double* fusion_rates;					/* [count*definitions] */
+	const double* immunogenicities;				/* [count*definitions] */
+	const double* fraction_transferred_when_ingested; /* [count*substrates] */
+
+	/* read and written */
+	double* damage;				/* [count] states.damage */
+	double* total_attack_time;	/* [count] states.total_attack_time */
+	int32_t* number_of_nuclei;	/* [count] states.number_of_nuclei */
+	double* fluid;				/* [count] volumes.* */
+	double* solid;
+	double* cytoplasmic;
+	double* cytoplasmic_fluid;
+	double* cytoplasmic_solid;
+	double* nuclear_fluid;
+	double* nuclear_solid;
+	double* fluid_fraction;
+	double* cytoplasmic_to_nuclear_ratio;
+	double* target_solid_cytoplasmic;
+	double* target_solid_nuclear;
+	double* internalized_substrates; /* [count*substrates] */
+} ppc_interactions;
+
+/* interactions_solver::update_cell_cell_interactions (reference:
+ * src/solver/host/interactions_solver.cpp:143-265): each live agent walks its
+ * neighbour list and, with one uniform draw per neighbour, may ingest a dead
+ * neighbour, ingest a live one, attack it or fuse with it (at most one live
+ * ingestion, attack and fusion per agent). Draw k of agent i at the n-th call
+ * for a replicate is uniform(seed, n, replicate, i, PPC_DRAW_INTERACTION + k).
+ * Ingested and fused neighbours get PPC_FLAG_TO_REMOVE; the ingesting or fusing
+ * agent's volumes, geometry (and, when fusing, position) change in the
+ * resident state and in `fields`, which is uploaded and written back. The
+ * outcome is that of the reference run on one thread (agents in index order).
+ * Uses the neighbour lists of the last ppc_update_cell_neighbors (rebuilt
+ * here if a fused step ran since). Synchronizes. */
+int ppc_update_cell_cell_interactions(ppc_state* s, int32_t replicate, ppc_interactions* fields);
+
 /* ---- fused step ----------------------------------------------------------- */
 /* ppc_step returns once the work is queued (device errors surface at the
  * next ppc_synchronize or syncing call). Blocks of steps are captured once in

@@ -66,6 +66,7 @@
 #define PPC_DRAW_WALK 16u		 /* 2 per attempt, up to PPC_DRAW_ATTEMPTS attempts */
 #define PPC_DRAW_ORIENTATION 96u /* 2 per attempt */
 #define PPC_DRAW_ATTEMPTS 32u
+#define PPC_DRAW_INTERACTION 1048576u /* + neighbour position, cell-cell interactions */
 
 PPC_HD uint64_t ppc_mix64(uint64_t z)
 {

@@ -10,7 +10,7 @@ import ctypes as C
 import os
 import subprocess
 
-from paraphysicell_b200.abi import Agents, Mesh, Params, PPCError
+from paraphysicell_b200.abi import Agents, Interactions, Mesh, Params, PPCError
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libppc_oracle.so")
@@ -48,6 +48,7 @@ def lib():
         L.orc_step.argtypes = [vp, C.c_int32, C.c_int32, C.c_double, C.c_double]
         L.orc_time_steps.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double]
         L.orc_time_steps.restype = C.c_double
+        L.orc_update_cell_cell_interactions.argtypes = [vp, C.POINTER(Interactions)]
         L.orc_get_neighbors.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_int32]
         L.orc_get_mesh_bins.argtypes = [vp, C.c_void_p, C.c_void_p]
         L.orc_get_mesh_position.argtypes = [vp, C.c_void_p, C.c_void_p]
@@ -106,6 +107,13 @@ class Oracle:
         if fn is None:
             raise AttributeError(name)
         return lambda *a: fn(self.h, *a)
+
+    def update_cell_cell_interactions(self, fields):
+        """`fields` (abi.InteractionArrays) is read and written back in place."""
+        st = fields.struct()
+        rc = self.L.orc_update_cell_cell_interactions(self.h, C.byref(st))
+        if rc != 0:
+            raise PPCError(rc, "orc_update_cell_cell_interactions")
 
     def time_steps(self, steps, threads, with_phenotype=False, p_divide=0.0, p_death=0.0):
         return self.L.orc_time_steps(self.h, steps, threads, int(with_phenotype), p_divide, p_death)

@@ -68,6 +68,7 @@ struct world
 	// draw epochs: `epoch` for phenotype draws (flags, division), advanced
 	// once per draw-consuming call; `spring_epoch` for the attachment loop
 	uint64_t seed = 0, epoch = 0, spring_epoch = 0;
+	uint64_t ix_epoch = 0; // cell-cell interaction calls so far
 	bool timed = false; // timed mode draws from thread_local mt19937
 
 	std::mutex removal_mtx;
@@ -734,6 +735,143 @@ void flag_by_draws(world& w, double p_divide, double p_death)
 	w.epoch++;
 }
 
+/* ---- cell-cell interactions (reference: src/solver/host/interactions_solver.cpp:1-265) ---- */
+
+constexpr real_t ix_zero_threshold = 1e-16; // reference: src/solver/host/solver_helper.h:12
+
+// physicell::update_geometry (interactions_solver.cpp:89-96)
+void ix_geometry(world& w, index_t i)
+{
+	const real_t four_thirds_pi = M_PI * 4.0 / 3.0;
+	w.radius[i] = ppc_cbrt(w.vol[i] / four_thirds_pi);
+	w.nrad[i] = ppc_cbrt(w.nvol[i] / four_thirds_pi);
+	w.sarea[i] = 4.0 * M_PI * w.radius[i] * w.radius[i];
+}
+
+// ingest (interactions_solver.cpp:6-26,64-74,98-112)
+void ix_ingest(world& w, ppc_interactions& f, index_t l, index_t r)
+{
+	f.cytoplasmic_fluid[l] += f.fluid[r];
+	f.cytoplasmic_solid[l] += f.solid[r];
+	f.fluid[l] += f.fluid[r];
+	f.solid[l] += f.solid[r];
+	f.cytoplasmic[l] += f.fluid[r] + f.solid[r];
+	w.vol[l] += f.fluid[r] + f.solid[r];
+	f.fluid_fraction[l] = f.fluid[l] / (w.vol[l] + ix_zero_threshold);
+	f.cytoplasmic_to_nuclear_ratio[l] = f.cytoplasmic_solid[l] / (f.nuclear_solid[l] + ix_zero_threshold);
+	const index_t S = f.substrates;
+	for (index_t q = 0; q < S; q++)
+		f.internalized_substrates[(size_t)l * S + q] +=
+			f.internalized_substrates[(size_t)r * S + q] * f.fraction_transferred_when_ingested[(size_t)r * S + q];
+	ix_geometry(w, l);
+	w.flags[r] = PPC_FLAG_TO_REMOVE;
+}
+
+// fuse (interactions_solver.cpp:28-53,76-87,114-131)
+void ix_fuse(world& w, ppc_interactions& f, index_t l, index_t r)
+{
+	const int dims = w.mesh.dims;
+	const real_t both = w.vol[l] + w.vol[r];
+	for (int d = 0; d < dims; d++)
+		w.pos[(size_t)l * dims + d] =
+			(w.pos[(size_t)l * dims + d] * w.vol[l] + w.pos[(size_t)r * dims + d] * w.vol[r]) / both;
+
+	f.cytoplasmic_fluid[l] += f.cytoplasmic_fluid[r];
+	f.nuclear_fluid[l] += f.nuclear_fluid[r];
+	f.cytoplasmic_solid[l] += f.cytoplasmic_solid[r];
+	f.nuclear_solid[l] += f.nuclear_solid[r];
+	f.target_solid_cytoplasmic[l] += f.target_solid_cytoplasmic[r];
+	f.target_solid_nuclear[l] += f.target_solid_nuclear[r];
+	f.fluid[l] = f.nuclear_fluid[l] + f.cytoplasmic_fluid[l];
+	f.solid[l] = f.nuclear_solid[l] + f.cytoplasmic_solid[l];
+	w.nvol[l] = f.nuclear_fluid[l] + f.nuclear_solid[l];
+	f.cytoplasmic[l] = f.cytoplasmic_fluid[l] + f.cytoplasmic_solid[l];
+	w.vol[l] = w.nvol[l] + f.cytoplasmic[l];
+	f.fluid_fraction[l] = f.fluid[l] / (w.vol[l] + ix_zero_threshold);
+	f.cytoplasmic_to_nuclear_ratio[l] = f.cytoplasmic_solid[l] / (f.nuclear_solid[l] + ix_zero_threshold);
+
+	const index_t S = f.substrates;
+	for (index_t q = 0; q < S; q++)
+		f.internalized_substrates[(size_t)l * S + q] += f.internalized_substrates[(size_t)r * S + q];
+	ix_geometry(w, l);
+	f.number_of_nuclei[l] += f.number_of_nuclei[r];
+	w.flags[r] = PPC_FLAG_TO_REMOVE;
+}
+
+// update_cell_cell_interactions_internal (interactions_solver.cpp:143-251),
+// serial; the mutex-guarded flag checks become plain checks. Draw k of agent
+// i is uniform(seed, call, 0, i, PPC_DRAW_INTERACTION + k) instead of the
+// shared generator's next number.
+void cell_cell_interactions(world& w, ppc_interactions& f)
+{
+	const uint64_t epoch = w.ix_epoch++;
+	const index_t n = w.n;
+	const index_t D = w.ndefs;
+	const real_t dt = w.params.mechanics_time_step;
+	for (index_t i = 0; i < n; i++)
+	{
+		bool attacked_once = false;
+		bool phagocytosed_once = false;
+		bool fused_once = false;
+		if (f.dead[i] == 1)
+			continue;
+		for (size_t k = 0; k < w.neighbors[i].size(); k++)
+		{
+			const index_t j = w.neighbors[i][k];
+			const index_t dj = w.def[j];
+			const real_t r = ppc_uniform(w.seed, epoch, 0, (uint64_t)i, PPC_DRAW_INTERACTION + (uint64_t)k);
+			if (f.dead[j] == 1)
+			{
+				if (r < f.dead_phagocytosis_rate[i] * dt)
+				{
+					if (w.flags[i] == PPC_FLAG_TO_REMOVE)
+						break;
+					if (w.flags[j] == PPC_FLAG_TO_REMOVE)
+						continue;
+					ix_ingest(w, f, i, j);
+				}
+				continue;
+			}
+			if (!phagocytosed_once && r < f.live_phagocytosis_rates[(size_t)i * D + dj] * dt)
+			{
+				if (w.flags[i] == PPC_FLAG_TO_REMOVE)
+					break;
+				if (w.flags[j] == PPC_FLAG_TO_REMOVE)
+					continue;
+				ix_ingest(w, f, i, j);
+				phagocytosed_once = true;
+				continue;
+			}
+			{
+				const real_t attack_r = f.attack_rates[(size_t)i * D + dj];
+				const real_t immuno_r = f.immunogenicities[(size_t)j * D + w.def[i]];
+				if (!attacked_once && r < attack_r * immuno_r * dt)
+				{
+					if (w.flags[i] == PPC_FLAG_TO_REMOVE)
+						break;
+					if (w.flags[j] == PPC_FLAG_TO_REMOVE)
+						continue;
+					// attack (interactions_solver.cpp:133-141)
+					f.damage[j] += f.damage_rate[i] * dt;
+					f.total_attack_time[j] += dt;
+					attacked_once = true;
+					continue;
+				}
+			}
+			if (!fused_once && r < f.fusion_rates[(size_t)i * D + dj] * dt)
+			{
+				if (w.flags[i] == PPC_FLAG_TO_REMOVE)
+					break;
+				if (w.flags[j] == PPC_FLAG_TO_REMOVE)
+					continue;
+				ix_fuse(w, f, i, j);
+				fused_once = true;
+				continue;
+			}
+		}
+	}
+}
+
 // simulator::simulate_mechanics (reference: src/simulator.cpp:157-196) and,
 // optionally, simulator::simulate_phenotype (src/simulator.cpp:198-220)
 void step_body(world& w, bool with_phenotype, double p_divide, double p_death)
@@ -908,6 +1046,13 @@ void orc_update_positions(orc_state* s) { update_positions(s->w); }
 void orc_update_cell_container_for_mechanics(orc_state* s) { compact_mechanics(s->w); }
 void orc_flag_by_draws(orc_state* s, double p_divide, double p_death) { flag_by_draws(s->w, p_divide, p_death); }
 void orc_update_cell_container_for_phenotype(orc_state* s) { compact_phenotype(s->w); }
+int orc_update_cell_cell_interactions(orc_state* s, ppc_interactions* f)
+{
+	if (!f || f->count != s->w.n || f->substrates < 0)
+		return PPC_ERR_ARG;
+	cell_cell_interactions(s->w, *f);
+	return PPC_OK;
+}
 
 void orc_step(orc_state* s, int32_t steps, int32_t with_phenotype, double p_divide, double p_death)
 {

@@ -3,7 +3,8 @@
  *
  * This library restates the reference's mechanics solver
  * (reference: src/solver/host/{common_solver,position_solver,containers_solver}.cpp,
- * solver_helper.h, src/cell_data.cpp:262-313, src/cell.cpp:108-163) on the CPU.
+ * solver_helper.h, interactions_solver.cpp, src/cell_data.cpp:262-313,
+ * src/cell.cpp:108-163) on the CPU.
  * It exists only to check the CUDA implementation and to time the reference's
  * OpenMP structure as the CPU baseline. Only the tests, the smoke check and
  * the benchmark's CPU-baseline leg may load it; the product never does.
@@ -57,6 +58,9 @@ void orc_update_positions(orc_state* s);
 void orc_update_cell_container_for_mechanics(orc_state* s);
 void orc_flag_by_draws(orc_state* s, double p_divide, double p_death);
 void orc_update_cell_container_for_phenotype(orc_state* s);
+/* interactions_solver::update_cell_cell_interactions; `fields` rows follow
+   the oracle's agent order */
+int orc_update_cell_cell_interactions(orc_state* s, ppc_interactions* fields);
 
 /* one mechanics step in simulator::simulate_mechanics order, `steps` times;
    with_phenotype adds flag_by_draws + the phenotype container update +

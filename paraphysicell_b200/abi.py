@@ -234,6 +234,108 @@ class AgentArrays:
         return [list(rows[i, : cnt[i]]) for i in range(self.count)]
 
 
+class Interactions(C.Structure):
+    """ppc_interactions (include/ppc.h)."""
+    _fields_ = [
+        ("count", C.c_int32),
+        ("substrates", C.c_int32),
+        ("dead", _U8),
+        ("dead_phagocytosis_rate", _D),
+        ("damage_rate", _D),
+        ("live_phagocytosis_rates", _D),
+        ("attack_rates", _D),
+        ("fusion_rates", _D),
+        ("immunogenicities", _D),
+        ("fraction_transferred_when_ingested", _D),
+        ("damage", _D),
+        ("total_attack_time", _D),
+        ("number_of_nuclei", _I32),
+        ("fluid", _D),
+        ("solid", _D),
+        ("cytoplasmic", _D),
+        ("cytoplasmic_fluid", _D),
+        ("cytoplasmic_solid", _D),
+        ("nuclear_fluid", _D),
+        ("nuclear_solid", _D),
+        ("fluid_fraction", _D),
+        ("cytoplasmic_to_nuclear_ratio", _D),
+        ("target_solid_cytoplasmic", _D),
+        ("target_solid_nuclear", _D),
+        ("internalized_substrates", _D),
+    ]
+
+
+def _volume_defaults():
+    """volume_t::set_defaults (reference: src/data_storage_phenotype.cpp:62-95)."""
+    ff = 0.75
+    total = 2494.0
+    fluid = ff * total
+    nuclear = 540.0
+    nf = ff * nuclear
+    cyto = total - nuclear
+    cf = ff * cyto
+    return {"fluid": fluid, "solid": total - fluid, "cytoplasmic": cyto, "cytoplasmic_fluid": cf,
+            "cytoplasmic_solid": cyto - cf, "nuclear_fluid": nf, "nuclear_solid": nuclear - nf,
+            "fluid_fraction": ff, "cytoplasmic_to_nuclear_ratio": cyto / (1e-16 + nuclear),
+            "target_solid_cytoplasmic": cyto - cf, "target_solid_nuclear": nuclear - nf}
+
+
+# (field, dtype, per-agent multiplicity: "defs", "subs" or 1, default); the
+# interaction defaults are interactions_t::set_defaults and cell_state_t's
+# (reference: src/data_storage_phenotype.cpp:320-328, src/cell.cpp:40-45)
+INTERACTION_FIELDS = [
+    ("dead", np.uint8, 1, 0),
+    ("dead_phagocytosis_rate", np.float64, 1, 0.0),
+    ("damage_rate", np.float64, 1, 1.0),
+    ("live_phagocytosis_rates", np.float64, "defs", 0.0),
+    ("attack_rates", np.float64, "defs", 0.0),
+    ("fusion_rates", np.float64, "defs", 0.0),
+    ("immunogenicities", np.float64, "defs", 1.0),
+    ("fraction_transferred_when_ingested", np.float64, "subs", 0.0),
+    ("damage", np.float64, 1, 0.0),
+    ("total_attack_time", np.float64, 1, 0.0),
+    ("number_of_nuclei", np.int32, 1, 1),
+] + [(k, np.float64, 1, v) for k, v in _volume_defaults().items()] + [
+    ("internalized_substrates", np.float64, "subs", 0.0),
+]
+
+
+class InteractionArrays:
+    """Host arrays of the phenotype fields cell-cell interactions use, one row
+    per agent, with the reference's defaults."""
+
+    def __init__(self, count, ndefs, substrates=0):
+        self.count = int(count)
+        self.ndefs = int(ndefs)
+        self.substrates = int(substrates)
+        self.arrays = {}
+        for name, dt, mult, dflt in INTERACTION_FIELDS:
+            width = {"defs": self.ndefs, "subs": self.substrates}.get(mult, 1)
+            self.arrays[name] = np.full(max(self.count * width, 1), dflt, dtype=dt)
+
+    def __getitem__(self, name):
+        arr = self.arrays[name]
+        mult = next(m for f, _, m, _ in INTERACTION_FIELDS if f == name)
+        if mult == 1:
+            return arr[: self.count]
+        width = self.ndefs if mult == "defs" else self.substrates
+        return arr[: self.count * width].reshape(self.count, width)
+
+    def struct(self):
+        s = Interactions()
+        s.count = self.count
+        s.substrates = self.substrates
+        for name, dt, _, _ in INTERACTION_FIELDS:
+            setattr(s, name, self.arrays[name].ctypes.data_as(_PTR[dt]))
+        return s
+
+    def copy(self):
+        out = InteractionArrays(self.count, self.ndefs, self.substrates)
+        for k, v in self.arrays.items():
+            out.arrays[k][:] = v
+        return out
+
+
 def status_name(rc):
     return STATUS_NAMES.get(rc, f"status {rc}")
 

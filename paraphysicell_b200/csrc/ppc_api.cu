@@ -1078,6 +1078,138 @@ int ppc_flag_by_draws(ppc_state* s, double p_divide, double p_death)
 	return finish(s);
 }
 
+int ppc_update_cell_cell_interactions(ppc_state* s, int32_t r, ppc_interactions* f)
+{
+	if (!valid(s, r) || !f || f->substrates < 0)
+		return fail(PPC_ERR_ARG, "invalid arguments");
+	std::vector<rep_counters> c;
+	PPC_TRY(read_counters(s, c));
+	const int32_t n = c[r].count;
+	if (f->count != n)
+		return fail(PPC_ERR_ARG, "fields.count differs from the replicate's agent count");
+	if ((int32_t)s->ix_epoch.size() < s->nreps)
+		s->ix_epoch.resize(s->nreps, 0);
+	const uint64_t epoch = s->ix_epoch[r]++;
+	if (n == 0)
+		return PPC_OK;
+	const int32_t D = s->ndefs, S = f->substrates;
+	const double* reads[] = { f->dead_phagocytosis_rate, f->damage_rate };
+	const double* reads_d[] = { f->live_phagocytosis_rates, f->attack_rates, f->fusion_rates, f->immunogenicities };
+	double* rw[] = { f->damage, f->total_attack_time, f->fluid, f->solid, f->cytoplasmic, f->cytoplasmic_fluid,
+					 f->cytoplasmic_solid, f->nuclear_fluid, f->nuclear_solid, f->fluid_fraction,
+					 f->cytoplasmic_to_nuclear_ratio, f->target_solid_cytoplasmic, f->target_solid_nuclear };
+	if (!f->dead || !f->number_of_nuclei || (S > 0 && (!f->internalized_substrates || !f->fraction_transferred_when_ingested)))
+		return fail(PPC_ERR_ARG, "a ppc_interactions field is NULL");
+	for (auto* p : reads)
+		if (!p)
+			return fail(PPC_ERR_ARG, "a ppc_interactions field is NULL");
+	for (auto* p : reads_d)
+		if (!p)
+			return fail(PPC_ERR_ARG, "a ppc_interactions field is NULL");
+	for (auto* p : rw)
+		if (!p)
+			return fail(PPC_ERR_ARG, "a ppc_interactions field is NULL");
+	PPC_TRY(ensure_lists(s));
+
+	// one device block: per-agent doubles, per-definition rows, substrate rows,
+	// nuclei, candidates, dead flags
+	const size_t nd = (size_t)n;
+	const size_t doubles = nd * (2 + 13) + nd * D * 4 + nd * S * 2;
+	const size_t ints = nd * 2 + nd * s->ncap;
+	const size_t bytes = doubles * sizeof(double) + ints * sizeof(int32_t) + nd;
+	char* d = nullptr;
+	PPC_CUDA(cudaMalloc(&d, bytes));
+	double* dp = reinterpret_cast<double*>(d);
+	auto take = [&](size_t count) { double* q = dp; dp += count; return q; };
+	ix_fields x {};
+	x.n = n;
+	x.substrates = S;
+	x.replicate = r;
+	x.base = s->reps[r].base;
+	x.dt = s->params.mechanics_time_step;
+	x.epoch = epoch;
+	double* dr[2];
+	for (int k = 0; k < 2; k++)
+		dr[k] = take(nd);
+	double* dd[4];
+	for (int k = 0; k < 4; k++)
+		dd[k] = take(nd * D);
+	double* dw[13];
+	for (int k = 0; k < 13; k++)
+		dw[k] = take(nd);
+	double* dfrac = take(nd * S);
+	double* disub = take(nd * S);
+	int32_t* ip = reinterpret_cast<int32_t*>(dp);
+	x.nuclei = ip;
+	x.ncand = ip + nd;
+	x.cand = ip + 2 * nd;
+	uint8_t* ddead = reinterpret_cast<uint8_t*>(ip + 2 * nd + nd * s->ncap);
+	x.dead = ddead;
+	x.dead_phago = dr[0];
+	x.damage_rate = dr[1];
+	x.live_phago = dd[0];
+	x.attack = dd[1];
+	x.fusion = dd[2];
+	x.immuno = dd[3];
+	x.damage = dw[0];
+	x.attack_time = dw[1];
+	x.fluid = dw[2];
+	x.solid = dw[3];
+	x.cyto = dw[4];
+	x.cyto_fluid = dw[5];
+	x.cyto_solid = dw[6];
+	x.nuc_fluid = dw[7];
+	x.nuc_solid = dw[8];
+	x.fluid_fraction = dw[9];
+	x.c2n = dw[10];
+	x.target_cyto = dw[11];
+	x.target_nuc = dw[12];
+	x.frac = dfrac;
+	x.isub = disub;
+
+	auto h2d = [&](void* dst, const void* src, size_t b) {
+		return cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, s->stream);
+	};
+	auto d2h = [&](void* dst, const void* src, size_t b) {
+		return cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, s->stream);
+	};
+	cudaError_t e = cudaSuccess;
+	for (int k = 0; k < 2 && e == cudaSuccess; k++)
+		e = h2d(dr[k], reads[k], nd * sizeof(double));
+	for (int k = 0; k < 4 && e == cudaSuccess; k++)
+		e = h2d(dd[k], reads_d[k], nd * D * sizeof(double));
+	for (int k = 0; k < 13 && e == cudaSuccess; k++)
+		e = h2d(dw[k], rw[k], nd * sizeof(double));
+	if (e == cudaSuccess && S > 0)
+		e = h2d(dfrac, f->fraction_transferred_when_ingested, nd * S * sizeof(double));
+	if (e == cudaSuccess && S > 0)
+		e = h2d(disub, f->internalized_substrates, nd * S * sizeof(double));
+	if (e == cudaSuccess)
+		e = h2d(x.nuclei, f->number_of_nuclei, nd * sizeof(int32_t));
+	if (e == cudaSuccess)
+		e = h2d(ddead, f->dead, nd);
+	int rc = e == cudaSuccess ? launch_interactions(s, x) : ppc::cuda_fail(e, "interaction field upload");
+	e = cudaSuccess;
+	for (int k = 0; k < 13 && e == cudaSuccess && rc == PPC_OK; k++)
+		e = d2h(rw[k], dw[k], nd * sizeof(double));
+	if (e == cudaSuccess && rc == PPC_OK && S > 0)
+		e = d2h(f->internalized_substrates, disub, nd * S * sizeof(double));
+	if (e == cudaSuccess && rc == PPC_OK)
+		e = d2h(f->number_of_nuclei, x.nuclei, nd * sizeof(int32_t));
+	const cudaError_t es = cudaStreamSynchronize(s->stream);
+	cudaFree(d);
+	if (rc != PPC_OK)
+		return rc;
+	if (e != cudaSuccess)
+		return ppc::cuda_fail(e, "interaction field download");
+	if (es != cudaSuccess)
+		return ppc::cuda_fail(es, "cudaStreamSynchronize");
+	// positions and radii changed: the next mesh update rebuilds the bins; the
+	// neighbour lists stay those the interactions used, as in the reference
+	s->bins_valid = false;
+	return finish(s);
+}
+
 int ppc_step(ppc_state* s, int32_t steps)
 {
 	if (!s)

@@ -1,0 +1,244 @@
+// Cell-cell interactions on the device: phagocytosis of dead and live
+// neighbours, attack and fusion (reference:
+// src/solver/host/interactions_solver.cpp:1-265).
+//
+// The reference walks every live agent's neighbour list under a mutex; each
+// neighbour costs one uniform draw, and an action re-checks the removal flags
+// of both agents before it changes anything. The outcome therefore depends on
+// the order in which agents act. This implementation fixes the order of a
+// one-thread run (agents in index order, neighbours in list order) and splits
+// the work in two passes:
+//  1. k_ix_candidates, one thread per agent: draws every neighbour's number and
+//     keeps the neighbours for which some action's threshold passes (the draw
+//     and the rates do not depend on any other agent's actions);
+//  2. k_ix_resolve, one block: lists the agents that have candidates, in index
+//     order, and one thread replays the reference's loop over those
+//     candidates only, with the flag checks and the at-most-once rules.
+// With the small rates of a real model only a few neighbours per step become
+// candidates, so the serial pass is short.
+
+#include <cuda_runtime.h>
+
+#include "../../include/ppc_draws.h"
+#include "ppc_internal.cuh"
+
+namespace ppc {
+namespace {
+
+constexpr int kIxThreads = 256;
+constexpr int kIxResolveThreads = 1024;
+constexpr double kZeroThreshold = 1e-16; // reference: solver_helper.h:12
+constexpr double kPi = 3.141592653589793;
+
+__global__ void __launch_bounds__(kIxThreads) k_ix_candidates(view v, ix_fields x)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= x.n)
+		return;
+	int m = 0;
+	if (x.dead[i] != 1)
+	{
+		const int s = x.base + i;
+		const int nn = min(v.ncnt[s], v.ncap);
+		const int D = v.ndefs;
+		const double dt = x.dt;
+		const int di = v.def[s];
+		for (int k = 0; k < nn; k++)
+		{
+			const int j = v.nidx[(int64_t)s * v.ncap + k] - x.base;
+			if ((unsigned)j >= (unsigned)x.n)
+				continue; // a list older than the last removal: skip, never read past the rows
+			const double r
+				= ppc_uniform(v.seed, x.epoch, (uint64_t)x.replicate, (uint64_t)i, PPC_DRAW_INTERACTION + (uint64_t)k);
+			bool any;
+			if (x.dead[j] == 1)
+				any = r < x.dead_phago[i] * dt;
+			else
+			{
+				const int dj = v.def[x.base + j];
+				any = r < x.live_phago[(int64_t)i * D + dj] * dt
+					  || r < x.attack[(int64_t)i * D + dj] * x.immuno[(int64_t)j * D + di] * dt
+					  || r < x.fusion[(int64_t)i * D + dj] * dt;
+			}
+			if (any)
+				x.cand[(int64_t)i * v.ncap + m++] = k;
+		}
+	}
+	x.ncand[i] = m;
+}
+
+__device__ void ix_geometry(const view& v, int s)
+{
+	// interactions_solver.cpp:89-96 (update_geometry)
+	const double four_thirds_pi = kPi * 4.0 / 3.0;
+	double4 prm = v.prm[s];
+	prm.x = ppc_cbrt(v.vol[s] / four_thirds_pi);
+	v.prm[s] = prm;
+	v.nrad[s] = ppc_cbrt(v.nvol[s] / four_thirds_pi);
+	v.sarea[s] = 4.0 * kPi * prm.x * prm.x;
+}
+
+// ingest_volume + ingest_internalized + update_geometry (interactions_solver.cpp:6-26,64-74,98-112)
+__device__ void ix_ingest(const view& v, const ix_fields& x, int l, int r)
+{
+	const int sl = x.base + l, sr = x.base + r;
+	x.cyto_fluid[l] += x.fluid[r];
+	x.cyto_solid[l] += x.solid[r];
+	x.fluid[l] += x.fluid[r];
+	x.solid[l] += x.solid[r];
+	x.cyto[l] += x.fluid[r] + x.solid[r];
+	v.vol[sl] += x.fluid[r] + x.solid[r];
+	x.fluid_fraction[l] = x.fluid[l] / (v.vol[sl] + kZeroThreshold);
+	x.c2n[l] = x.cyto_solid[l] / (x.nuc_solid[l] + kZeroThreshold);
+	const int S = x.substrates;
+	for (int q = 0; q < S; q++)
+		x.isub[(int64_t)l * S + q] += x.isub[(int64_t)r * S + q] * x.frac[(int64_t)r * S + q];
+	ix_geometry(v, sl);
+	v.flags[sr] = PPC_FLAG_TO_REMOVE;
+}
+
+// fuse_position + fuse_volume + fuse_internalized + update_geometry
+// (interactions_solver.cpp:28-53,76-87,114-131)
+template <int DIMS>
+__device__ void ix_fuse(const view& v, const ix_fields& x, int cur, int l, int r)
+{
+	const int sl = x.base + l, sr = x.base + r;
+	const double vl = v.vol[sl], vr = v.vol[sr];
+	const double both = vl + vr;
+	double4 pl = v.pos[cur][sl];
+	const double4 pr = v.pos[cur][sr];
+	pl.x = (pl.x * vl + pr.x * vr) / both;
+	if (DIMS >= 2)
+		pl.y = (pl.y * vl + pr.y * vr) / both;
+	if (DIMS >= 3)
+		pl.z = (pl.z * vl + pr.z * vr) / both;
+	v.pos[cur][sl] = pl;
+
+	x.cyto_fluid[l] += x.cyto_fluid[r];
+	x.nuc_fluid[l] += x.nuc_fluid[r];
+	x.cyto_solid[l] += x.cyto_solid[r];
+	x.nuc_solid[l] += x.nuc_solid[r];
+	x.target_cyto[l] += x.target_cyto[r];
+	x.target_nuc[l] += x.target_nuc[r];
+	x.fluid[l] = x.nuc_fluid[l] + x.cyto_fluid[l];
+	x.solid[l] = x.nuc_solid[l] + x.cyto_solid[l];
+	v.nvol[sl] = x.nuc_fluid[l] + x.nuc_solid[l];
+	x.cyto[l] = x.cyto_fluid[l] + x.cyto_solid[l];
+	v.vol[sl] = v.nvol[sl] + x.cyto[l];
+	x.fluid_fraction[l] = x.fluid[l] / (v.vol[sl] + kZeroThreshold);
+	x.c2n[l] = x.cyto_solid[l] / (x.nuc_solid[l] + kZeroThreshold);
+
+	const int S = x.substrates;
+	for (int q = 0; q < S; q++)
+		x.isub[(int64_t)l * S + q] += x.isub[(int64_t)r * S + q];
+	ix_geometry(v, sl);
+	x.nuclei[l] += x.nuclei[r];
+	v.flags[sr] = PPC_FLAG_TO_REMOVE;
+}
+
+// update_cell_cell_interactions_internal (interactions_solver.cpp:143-251)
+// for one agent, over its candidate neighbours in list order
+template <int DIMS>
+__device__ void ix_agent(const view& v, const ix_fields& x, int cur, int i)
+{
+	bool attacked_once = false, phagocytosed_once = false, fused_once = false;
+	const int s = x.base + i;
+	const int D = v.ndefs;
+	const double dt = x.dt;
+	const int di = v.def[s];
+	const int m = x.ncand[i];
+	for (int c = 0; c < m; c++)
+	{
+		const int k = x.cand[(int64_t)i * v.ncap + c];
+		const int j = v.nidx[(int64_t)s * v.ncap + k] - x.base;
+		const int sj = x.base + j;
+		const double r
+			= ppc_uniform(v.seed, x.epoch, (uint64_t)x.replicate, (uint64_t)i, PPC_DRAW_INTERACTION + (uint64_t)k);
+		if (x.dead[j] == 1)
+		{
+			if (r < x.dead_phago[i] * dt)
+			{
+				if (v.flags[s] == PPC_FLAG_TO_REMOVE)
+					break;
+				if (v.flags[sj] == PPC_FLAG_TO_REMOVE)
+					continue;
+				ix_ingest(v, x, i, j);
+			}
+			continue;
+		}
+		const int dj = v.def[sj];
+		if (!phagocytosed_once && r < x.live_phago[(int64_t)i * D + dj] * dt)
+		{
+			if (v.flags[s] == PPC_FLAG_TO_REMOVE)
+				break;
+			if (v.flags[sj] == PPC_FLAG_TO_REMOVE)
+				continue;
+			ix_ingest(v, x, i, j);
+			phagocytosed_once = true;
+			continue;
+		}
+		const double attack_r = x.attack[(int64_t)i * D + dj];
+		const double immuno_r = x.immuno[(int64_t)j * D + di];
+		if (!attacked_once && r < attack_r * immuno_r * dt)
+		{
+			if (v.flags[s] == PPC_FLAG_TO_REMOVE)
+				break;
+			if (v.flags[sj] == PPC_FLAG_TO_REMOVE)
+				continue;
+			// attack (interactions_solver.cpp:133-141)
+			x.damage[j] += x.damage_rate[i] * dt;
+			x.attack_time[j] += dt;
+			attacked_once = true;
+			continue;
+		}
+		if (!fused_once && r < x.fusion[(int64_t)i * D + dj] * dt)
+		{
+			if (v.flags[s] == PPC_FLAG_TO_REMOVE)
+				break;
+			if (v.flags[sj] == PPC_FLAG_TO_REMOVE)
+				continue;
+			ix_fuse<DIMS>(v, x, cur, i, j);
+			fused_once = true;
+			continue;
+		}
+	}
+}
+
+template <int DIMS>
+__global__ void __launch_bounds__(kIxResolveThreads) k_ix_resolve(view v, ix_fields x, int cur)
+{
+	__shared__ int list[kIxResolveThreads];
+	for (int i0 = 0; i0 < x.n; i0 += blockDim.x)
+	{
+		const int i = i0 + threadIdx.x;
+		const int has = i < x.n && x.ncand[i] > 0;
+		int total;
+		const int off = block_exclusive_scan(has, total);
+		if (has)
+			list[off] = i;
+		__syncthreads();
+		if (threadIdx.x == 0)
+			for (int w = 0; w < total; w++)
+				ix_agent<DIMS>(v, x, cur, list[w]);
+		__syncthreads();
+	}
+}
+
+} // namespace
+
+int launch_interactions(ppc_state* s, const ix_fields& x)
+{
+	if (x.n == 0)
+		return PPC_OK;
+	k_ix_candidates<<<blocks_for(x.n, kIxThreads), kIxThreads, 0, PPC_LAUNCH(s)>>>(s->v, x);
+	if (s->dims == 1)
+		k_ix_resolve<1><<<1, kIxResolveThreads, 0, PPC_LAUNCH(s)>>>(s->v, x, s->cur);
+	else if (s->dims == 2)
+		k_ix_resolve<2><<<1, kIxResolveThreads, 0, PPC_LAUNCH(s)>>>(s->v, x, s->cur);
+	else
+		k_ix_resolve<3><<<1, kIxResolveThreads, 0, PPC_LAUNCH(s)>>>(s->v, x, s->cur);
+	PPC_CUDA(cudaGetLastError());
+	return PPC_OK;
+}
+
+} // namespace ppc

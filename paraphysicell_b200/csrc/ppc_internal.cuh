@@ -201,6 +201,7 @@ struct ppc_state
 	// threads per block; staging bytes per block
 	// host copies of the replicate counts as last read (a download's first guess)
 	std::vector<int32_t> host_count;
+	std::vector<uint64_t> ix_epoch; // cell-cell interaction calls so far, per replicate
 	ppc::rep_counters* pinned_ctr = nullptr; // pinned landing area of the counters
 	int32_t* pinned_flag = nullptr;			 // pinned landing area of pos_changed
 	bool staged = false;
@@ -257,4 +258,56 @@ int launch_pack_prm(ppc_state* s, int field, double* dst, int32_t r, int32_t n);
 int launch_neighbors_local(ppc_state* s, int32_t r, int32_t n, int32_t* counts, int32_t* lists, int32_t cap);
 int launch_springs_local(ppc_state* s, int32_t r, int32_t n, int32_t* rows, int32_t cap, int to_device);
 
+// device copies of the ppc_interactions fields of one replicate (local rows)
+struct ix_fields
+{
+	int32_t n, substrates, replicate, base;
+	double dt;
+	uint64_t epoch;
+	const uint8_t* dead;
+	const double *dead_phago, *damage_rate, *live_phago, *attack, *fusion, *immuno, *frac;
+	double *damage, *attack_time;
+	int32_t* nuclei;
+	double *fluid, *solid, *cyto, *cyto_fluid, *cyto_solid, *nuc_fluid, *nuc_solid, *fluid_fraction, *c2n, *target_cyto,
+		*target_nuc, *isub;
+	int32_t* ncand; // [n] candidate neighbours of each agent
+	int32_t* cand;	// [n*ncap] their positions in the agent's neighbour list
+};
+int launch_interactions(ppc_state* s, const ix_fields& x);
+
 } // namespace ppc
+
+// block-wide exclusive scan of one int per thread; returns the block total
+__device__ __forceinline__ int block_exclusive_scan(int x, int& total)
+{
+	__shared__ int warp_sums[32];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	int incl = x;
+	for (int o = 1; o < 32; o <<= 1)
+	{
+		int y = __shfl_up_sync(0xffffffffu, incl, o);
+		if (lane >= o)
+			incl += y;
+	}
+	if (lane == 31)
+		warp_sums[warp] = incl;
+	__syncthreads();
+	const int nwarps = blockDim.x >> 5;
+	if (warp == 0)
+	{
+		int w = lane < nwarps ? warp_sums[lane] : 0;
+		for (int o = 1; o < 32; o <<= 1)
+		{
+			int y = __shfl_up_sync(0xffffffffu, w, o);
+			if (lane >= o)
+				w += y;
+		}
+		if (lane < nwarps)
+			warp_sums[lane] = w;
+	}
+	__syncthreads();
+	total = warp_sums[nwarps - 1];
+	int excl = incl - x + (warp > 0 ? warp_sums[warp - 1] : 0);
+	__syncthreads();
+	return excl;
+}

@@ -88,41 +88,6 @@ __device__ __forceinline__ int axis_coord(double x, const rep_info& R, int d, in
 	return (int)q;
 }
 
-// block-wide exclusive scan of one int per thread; returns the block total
-__device__ __forceinline__ int block_exclusive_scan(int x, int& total)
-{
-	__shared__ int warp_sums[32];
-	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	int incl = x;
-	for (int o = 1; o < 32; o <<= 1)
-	{
-		int y = __shfl_up_sync(0xffffffffu, incl, o);
-		if (lane >= o)
-			incl += y;
-	}
-	if (lane == 31)
-		warp_sums[warp] = incl;
-	__syncthreads();
-	const int nwarps = blockDim.x >> 5;
-	if (warp == 0)
-	{
-		int w = lane < nwarps ? warp_sums[lane] : 0;
-		for (int o = 1; o < 32; o <<= 1)
-		{
-			int y = __shfl_up_sync(0xffffffffu, w, o);
-			if (lane >= o)
-				w += y;
-		}
-		if (lane < nwarps)
-			warp_sums[lane] = w;
-	}
-	__syncthreads();
-	total = warp_sums[nwarps - 1];
-	int excl = incl - x + (warp > 0 ? warp_sums[warp - 1] : 0);
-	__syncthreads();
-	return excl;
-}
-
 // copies every per-agent field of slot s into slot d (cell_data::remove,
 // reference: src/cell_data.cpp:285-313); spring rows were moved by the plan
 __device__ __forceinline__ void move_agent(const view& v, int cur, int d, int s)

@@ -14,7 +14,7 @@ import os
 
 import numpy as np
 
-from .abi import Agents, Mesh, Params, PPCError
+from .abi import Agents, Interactions, Mesh, Params, PPCError
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libppc.so")
@@ -35,6 +35,7 @@ EXPORTS = (
     "ppc_get_neighbors", "ppc_get_mesh_bins", "ppc_get_voxel_count", "ppc_get_mesh_position",
     "ppc_get_mesh_index", "ppc_get_launch_count", "ppc_last_error", "ppc_abi_version",
     "ppc_set_profiling", "ppc_get_profile", "ppc_set_launch_shape", "ppc_autotune",
+    "ppc_update_cell_cell_interactions",
 ) + tuple("ppc_" + e for e in ENTRY_POINTS)
 
 
@@ -79,6 +80,7 @@ def lib():
         L.ppc_last_error.restype = C.c_char_p
         for e in ENTRY_POINTS:
             getattr(L, "ppc_" + e).argtypes = [vp]
+        L.ppc_update_cell_cell_interactions.argtypes = [vp, C.c_int32, C.POINTER(Interactions)]
         _lib = L
     return _lib
 
@@ -212,6 +214,13 @@ class Simulation:
 
     def flag_by_draws(self, p_divide, p_death):
         _check(lib().ppc_flag_by_draws(self.h, p_divide, p_death), "ppc_flag_by_draws")
+
+    def update_cell_cell_interactions(self, fields, replicate=0):
+        """interactions_solver::update_cell_cell_interactions on one replicate;
+        `fields` (abi.InteractionArrays) is read and written back in place."""
+        st = fields.struct()
+        _check(lib().ppc_update_cell_cell_interactions(self.h, replicate, C.byref(st)),
+               "ppc_update_cell_cell_interactions")
 
     # ---- readback ----
     def neighbors(self, replicate=0, capacity=None):

@@ -105,3 +105,58 @@ def test_bins_descending_index_order():
         seg = list(agents[off: off + c])
         assert seg == sorted(seg, reverse=True)
         off += c
+
+
+def _check_interaction_asserts(case, flags, damage):
+    names = {"none": 0, "to_remove": FLAG_TO_REMOVE}
+    for a in case["asserts"]:
+        got = flags[a["cell"]] if a["field"] == "flag" else damage[a["cell"]]
+        want = names[a["value"]] if a["field"] == "flag" else a["value"]
+        assert (got == want) == (a["op"] == "EQ"), a
+
+
+@pytest.mark.parametrize("name", ["attack", "dead_phagocytosis", "phagocytosis", "fusion"])
+def test_interactions_known_answers(name):
+    """host_interactions_solver.{attack,dead_phagocytosis,phagocytosis,fusion}
+    (reference: test/test.cpp:402-560): who is damaged or flagged for
+    removal after the test's interaction calls."""
+    mesh, params, a, f, case = sc.interaction_case(name)
+    o = Oracle(mesh, params)
+    o.upload(a)
+    o.update_mechanics_mesh()
+    o.update_cell_neighbors()
+    for _ in range(case["calls"]):
+        o.update_cell_cell_interactions(f)
+    o.download(a)
+    _check_interaction_asserts(case, a["flags"], f["damage"])
+
+
+def test_interactions_ingest_and_fuse_volumes():
+    """The ingesting agent gains the prey's fluid and solid volume, the fused
+    agent the partner's compartments and nuclei, and both take the
+    volume-weighted position and new radius (interactions_solver.cpp:6-131)."""
+    mesh, params, a, f, case = sc.interaction_case("fusion")
+    o = Oracle(mesh, params)
+    before = f.copy()
+    vol0 = a["total_volume"].copy()
+    o.upload(a)
+    o.update_mechanics_mesh()
+    o.update_cell_neighbors()
+    o.update_cell_cell_interactions(f)
+    o.download(a)
+    assert f["number_of_nuclei"][0] == 2
+    assert a["total_volume"][0] == a["nuclear_volume"][0] + f["cytoplasmic"][0]
+    assert a["total_volume"][0] == vol0[0] + vol0[1]
+    assert f["nuclear_solid"][0] == before["nuclear_solid"][0] + before["nuclear_solid"][1]
+    r = (a["total_volume"][0] / (np.pi * 4.0 / 3.0)) ** (1.0 / 3.0)
+    assert abs(a["radius"][0] - r) <= 1e-12 * r
+    assert a["flags"][1] == FLAG_TO_REMOVE
+
+
+def test_interactions_rejects_wrong_count():
+    mesh, params, a, f, case = sc.interaction_case("attack")
+    o = Oracle(mesh, params)
+    o.upload(a)
+    from paraphysicell_b200.abi import InteractionArrays, PPCError
+    with pytest.raises(PPCError):
+        o.update_cell_cell_interactions(InteractionArrays(a.count + 1, 3))
