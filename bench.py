@@ -383,6 +383,46 @@ def stochastic_springs_form(args, flush):
     return out
 
 
+def interactions_form(args):
+    """Config 3 (88,700 agents) through ppc_update_cell_cell_interactions
+    with page-locked phenotype fields: each call uploads the fields, runs the
+    candidate and ordered-resolution kernels and writes the fields back
+    (synchronous, so timed on the host clock around the call). Rates give
+    per-neighbour action probabilities of a few per mille."""
+    import time
+
+    import numpy as np
+
+    from paraphysicell_b200 import workloads as wl
+    from paraphysicell_b200.abi import FLAG_TO_REMOVE, AgentArrays
+    from paraphysicell_b200.device import PinnedPool, Simulation
+
+    mesh, params, a = wl.config3()
+    pool = PinnedPool()
+    f = wl.interaction_fields(a, params.cell_definitions_count, seed=9, scale=0.02, pinned=pool)
+    sim = Simulation(mesh, params, a.capacity, seed=1)
+    sim.upload(a)
+    sim.update_mechanics_mesh()
+    sim.update_cell_neighbors()
+    for _ in range(args.warmup):
+        sim.update_cell_cell_interactions(f)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        sim.update_cell_cell_interactions(f)
+        times.append(time.perf_counter() - t0)
+    out_a = AgentArrays(a.count, a.dims, a.ndefs, a.capacity)
+    sim.download(out_a)
+    flags = out_a["flags"]
+    sim.close()
+    pool.free()
+    ms = 1e3 * float(np.median(times))
+    return {"workload": "config3 cell-cell interactions", "agents": a.count, "calls": args.steps,
+            "ms_per_call_median": ms, "agents_per_s": a.count / (ms * 1e-3),
+            "flagged_for_removal": int(np.count_nonzero(flags == FLAG_TO_REMOVE)),
+            "note": "host clock around each synchronous call; includes the field copies in and out"}
+
+
 def config5_form(args, flush):
     """Config 5: 1,000,000 agents with division and death every step."""
     import torch
@@ -574,6 +614,7 @@ def run_ours(args, rank, world, local_rank):
             line["forms"]["batched_ensemble"] = ensemble_form(args, flush)
             line["forms"]["config5_division_death"] = config5_form(args, flush)
             line["forms"]["stochastic_springs"] = stochastic_springs_form(args, flush)
+            line["forms"]["cell_cell_interactions"] = interactions_form(args)
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(args.workload)
     print(json.dumps(line), flush=True)

@@ -304,14 +304,17 @@ class InteractionArrays:
     """Host arrays of the phenotype fields cell-cell interactions use, one row
     per agent, with the reference's defaults."""
 
-    def __init__(self, count, ndefs, substrates=0):
+    def __init__(self, count, ndefs, substrates=0, pinned=None):
         self.count = int(count)
         self.ndefs = int(ndefs)
         self.substrates = int(substrates)
         self.arrays = {}
         for name, dt, mult, dflt in INTERACTION_FIELDS:
             width = {"defs": self.ndefs, "subs": self.substrates}.get(mult, 1)
-            self.arrays[name] = np.full(max(self.count * width, 1), dflt, dtype=dt)
+            n = max(self.count * width, 1)
+            arr = pinned(n, dt) if pinned is not None else np.empty(n, dtype=dt)
+            arr[:] = dflt
+            self.arrays[name] = arr
 
     def __getitem__(self, name):
         arr = self.arrays[name]
@@ -329,8 +332,8 @@ class InteractionArrays:
             setattr(s, name, self.arrays[name].ctypes.data_as(_PTR[dt]))
         return s
 
-    def copy(self):
-        out = InteractionArrays(self.count, self.ndefs, self.substrates)
+    def copy(self, pinned=None):
+        out = InteractionArrays(self.count, self.ndefs, self.substrates, pinned)
         for k, v in self.arrays.items():
             out.arrays[k][:] = v
         return out

@@ -813,6 +813,8 @@ int ppc_destroy(ppc_state* s)
 		cudaFree(b.p);
 	if (s->stage)
 		cudaFree(s->stage);
+	if (s->ix_scratch)
+		cudaFree(s->ix_scratch);
 	if (s->pinned_ctr)
 		cudaFreeHost(s->pinned_ctr);
 	if (s->own_stream)
@@ -1117,8 +1119,19 @@ int ppc_update_cell_cell_interactions(ppc_state* s, int32_t r, ppc_interactions*
 	const size_t doubles = nd * (2 + 13) + nd * D * 4 + nd * S * 2;
 	const size_t ints = nd * 2 + nd * s->ncap;
 	const size_t bytes = doubles * sizeof(double) + ints * sizeof(int32_t) + nd;
-	char* d = nullptr;
-	PPC_CUDA(cudaMalloc(&d, bytes));
+	if (bytes > s->ix_scratch_bytes)
+	{
+		if (s->ix_scratch)
+		{
+			PPC_CUDA(cudaStreamSynchronize(s->stream));
+			PPC_CUDA(cudaFree(s->ix_scratch));
+			s->ix_scratch = nullptr;
+			s->ix_scratch_bytes = 0;
+		}
+		PPC_CUDA(cudaMalloc(&s->ix_scratch, bytes));
+		s->ix_scratch_bytes = bytes;
+	}
+	char* d = static_cast<char*>(s->ix_scratch);
 	double* dp = reinterpret_cast<double*>(d);
 	auto take = [&](size_t count) { double* q = dp; dp += count; return q; };
 	ix_fields x {};
@@ -1197,7 +1210,6 @@ int ppc_update_cell_cell_interactions(ppc_state* s, int32_t r, ppc_interactions*
 	if (e == cudaSuccess && rc == PPC_OK)
 		e = d2h(f->number_of_nuclei, x.nuclei, nd * sizeof(int32_t));
 	const cudaError_t es = cudaStreamSynchronize(s->stream);
-	cudaFree(d);
 	if (rc != PPC_OK)
 		return rc;
 	if (e != cudaSuccess)

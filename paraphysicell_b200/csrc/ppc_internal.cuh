@@ -202,6 +202,8 @@ struct ppc_state
 	// host copies of the replicate counts as last read (a download's first guess)
 	std::vector<int32_t> host_count;
 	std::vector<uint64_t> ix_epoch; // cell-cell interaction calls so far, per replicate
+	void* ix_scratch = nullptr;		// device copies of the interaction fields, kept between calls
+	size_t ix_scratch_bytes = 0;
 	ppc::rep_counters* pinned_ctr = nullptr; // pinned landing area of the counters
 	int32_t* pinned_flag = nullptr;			 // pinned landing area of pos_changed
 	bool staged = false;

@@ -198,3 +198,35 @@ def _rescale_ball(mesh, params, a, radius, seed):
     n = a.count
     a.arrays["positions"][: 3 * n] = _ball(rng, n, radius, np.zeros(3)).ravel()
     return mesh, params, a
+
+
+def interaction_fields(a, ndefs, seed, substrates=2, scale=1.0, pinned=None):
+    """Phenotype fields for cell-cell interactions over the agents of `a`:
+    15 % dead agents; per-neighbour action probabilities up to 0.2 (dead
+    ingestion), 0.06 (live ingestion), 0.2 x immunogenicity (attack) and 0.05
+    (fusion) at scale 1 and dt 0.1; volume compartments around the reference
+    defaults; `substrates` internalized substrates. Also sets the agents'
+    total and nuclear volume to the compartments' sums."""
+    from .abi import InteractionArrays
+    rng = np.random.default_rng(seed)
+    n = a.count
+    f = InteractionArrays(n, ndefs, substrates, pinned)
+    f["dead"][:] = (rng.random(n) < 0.15).astype(np.uint8)
+    f["dead_phagocytosis_rate"][:] = rng.random(n) * 2.0 * scale
+    f["damage_rate"][:] = 0.5 + rng.random(n)
+    f["live_phagocytosis_rates"][:] = rng.random((n, ndefs)) * 0.6 * scale
+    f["attack_rates"][:] = rng.random((n, ndefs)) * 2.0 * scale
+    f["immunogenicities"][:] = rng.random((n, ndefs))
+    f["fusion_rates"][:] = rng.random((n, ndefs)) * 0.5 * scale
+    f["damage"][:] = rng.random(n)
+    f["number_of_nuclei"][:] = 1 + (rng.random(n) < 0.1)
+    for k in ("fluid", "solid", "cytoplasmic", "cytoplasmic_fluid", "cytoplasmic_solid", "nuclear_fluid",
+              "nuclear_solid", "target_solid_cytoplasmic", "target_solid_nuclear"):
+        f[k][:] *= 0.5 + rng.random(n)
+    if substrates:
+        f["internalized_substrates"][:] = rng.random((n, substrates)) * 10.0
+        f["fraction_transferred_when_ingested"][:] = rng.random((n, substrates))
+    vol = a.arrays["total_volume"]
+    vol[:n] = f["fluid"] + f["solid"]
+    a.arrays["nuclear_volume"][:n] = f["nuclear_fluid"] + f["nuclear_solid"]
+    return f

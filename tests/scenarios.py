@@ -191,26 +191,5 @@ def random_interaction_fields(a, ndefs, seed, substrates=2, scale=1.0):
     """Interaction fields for a dense agent set with rates high enough that
     agents ingest, attack and fuse neighbours that have already acted or
     been removed in the same call (the order-dependent paths)."""
-    from paraphysicell_b200.abi import InteractionArrays
-    rng = np.random.default_rng(seed)
-    n = a.count
-    f = InteractionArrays(n, ndefs, substrates)
-    f["dead"][:] = (rng.random(n) < 0.15).astype(np.uint8)
-    f["dead_phagocytosis_rate"][:] = rng.random(n) * 2.0 * scale
-    f["damage_rate"][:] = 0.5 + rng.random(n)
-    f["live_phagocytosis_rates"][:] = rng.random((n, ndefs)) * 0.6 * scale
-    f["attack_rates"][:] = rng.random((n, ndefs)) * 2.0 * scale
-    f["immunogenicities"][:] = rng.random((n, ndefs))
-    f["fusion_rates"][:] = rng.random((n, ndefs)) * 0.5 * scale
-    f["damage"][:] = rng.random(n)
-    f["number_of_nuclei"][:] = 1 + (rng.random(n) < 0.1)
-    for k in ("fluid", "solid", "cytoplasmic", "cytoplasmic_fluid", "cytoplasmic_solid", "nuclear_fluid",
-              "nuclear_solid", "target_solid_cytoplasmic", "target_solid_nuclear"):
-        f[k][:] *= 0.5 + rng.random(n)
-    if substrates:
-        f["internalized_substrates"][:] = rng.random((n, substrates)) * 10.0
-        f["fraction_transferred_when_ingested"][:] = rng.random((n, substrates))
-    vol = a.arrays["total_volume"]
-    vol[:n] = f["fluid"] + f["solid"]
-    a.arrays["nuclear_volume"][:n] = f["nuclear_fluid"] + f["nuclear_solid"]
-    return f
+    from paraphysicell_b200 import workloads as wl
+    return wl.interaction_fields(a, ndefs, seed, substrates=substrates, scale=scale)
