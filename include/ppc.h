@@ -255,10 +255,38 @@ int ppc_update_cell_neighbors(ppc_state* s);
  * Uses the neighbour lists of the last ppc_update_cell_neighbors. */
 int ppc_update_cell_forces(ppc_state* s);
 
-/* position_solver::update_motility (reference: src/solver/host/position_solver.cpp:288-314).
- * No-op when no agent is motile; motile agents are not supported on the device
- * (the host view carries no motility fields), so this always succeeds. */
+/* position_solver::update_motility (reference: src/solver/host/position_solver.cpp:288-314)
+ * for a state whose agents carry no motility fields: a no-op that always
+ * succeeds. Motile agents go through ppc_update_motility_fields. */
 int ppc_update_motility(ppc_state* s);
+
+/* Motility fields of one replicate (reference: cell_data motilities.*,
+ * defaults src/data_storage_phenotype.cpp:245-256), host memory, one row per
+ * agent in the state's agent order (`count` = the replicate's count). */
+typedef struct ppc_motility
+{
+	int32_t count;
+	int32_t reserved;
+	const uint8_t* is_motile;				 /* [count] */
+	const uint8_t* restrict_to_2d;			 /* [count] */
+	const double* persistence_time;			 /* [count] */
+	const double* migration_speed;			 /* [count] */
+	const double* migration_bias;			 /* [count] */
+	const double* migration_bias_direction;	 /* [count*dims] */
+	double* motility_vector;				 /* [count*dims], read and written */
+} ppc_motility;
+
+/* position_solver::update_motility with motile agents (reference:
+ * src/solver/host/position_solver.cpp:115-145,198-212,288-314,
+ * solver_helper.h:82-101,160-182,250-287). A motile agent redraws its
+ * direction with probability dt/persistence_time — draw 0 of agent i at the
+ * n-th call for a replicate is uniform(seed, n, replicate, i,
+ * PPC_DRAW_MOTILITY), the direction comes from the draws after it — mixes it
+ * with migration_bias_direction by migration_bias, scales it to
+ * migration_speed, and adds its motility vector to its resident velocity.
+ * The reference's per-agent direction-update callbacks (chemotaxis) are not
+ * run: the caller sets migration_bias_direction. Synchronizes. */
+int ppc_update_motility_fields(ppc_state* s, int32_t replicate, ppc_motility* fields);
 
 /* position_solver::update_basement_membrane_interactions (reference: src/solver/host/position_solver.cpp:316-335). */
 int ppc_update_basement_membrane_interactions(ppc_state* s);

@@ -67,6 +67,7 @@
 #define PPC_DRAW_ORIENTATION 96u /* 2 per attempt */
 #define PPC_DRAW_ATTEMPTS 32u
 #define PPC_DRAW_INTERACTION 1048576u /* + neighbour position, cell-cell interactions */
+#define PPC_DRAW_MOTILITY 2097152u	/* persistence draw; the direction's draws follow */
 
 PPC_HD uint64_t ppc_mix64(uint64_t z)
 {

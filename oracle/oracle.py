@@ -10,7 +10,7 @@ import ctypes as C
 import os
 import subprocess
 
-from paraphysicell_b200.abi import Agents, Interactions, Mesh, Params, PPCError
+from paraphysicell_b200.abi import Agents, Interactions, Mesh, Motility, Params, PPCError
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libppc_oracle.so")
@@ -49,6 +49,7 @@ def lib():
         L.orc_time_steps.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double]
         L.orc_time_steps.restype = C.c_double
         L.orc_update_cell_cell_interactions.argtypes = [vp, C.POINTER(Interactions)]
+        L.orc_update_motility_fields.argtypes = [vp, C.POINTER(Motility)]
         L.orc_get_neighbors.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_int32]
         L.orc_get_mesh_bins.argtypes = [vp, C.c_void_p, C.c_void_p]
         L.orc_get_mesh_position.argtypes = [vp, C.c_void_p, C.c_void_p]
@@ -107,6 +108,13 @@ class Oracle:
         if fn is None:
             raise AttributeError(name)
         return lambda *a: fn(self.h, *a)
+
+    def update_motility_fields(self, fields):
+        """`fields` (abi.MotilityArrays): motility vectors are written back."""
+        st = fields.struct()
+        rc = self.L.orc_update_motility_fields(self.h, C.byref(st))
+        if rc != 0:
+            raise PPCError(rc, "orc_update_motility_fields")
 
     def update_cell_cell_interactions(self, fields):
         """`fields` (abi.InteractionArrays) is read and written back in place."""

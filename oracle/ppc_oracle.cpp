@@ -69,6 +69,7 @@ struct world
 	// once per draw-consuming call; `spring_epoch` for the attachment loop
 	uint64_t seed = 0, epoch = 0, spring_epoch = 0;
 	uint64_t ix_epoch = 0; // cell-cell interaction calls so far
+	uint64_t mot_epoch = 0; // motility calls so far
 	bool timed = false; // timed mode draws from thread_local mt19937
 
 	std::mutex removal_mtx;
@@ -739,6 +740,46 @@ void flag_by_draws(world& w, double p_divide, double p_death)
 
 constexpr real_t ix_zero_threshold = 1e-16; // reference: src/solver/host/solver_helper.h:12
 
+/* ---- motility (reference: src/solver/host/position_solver.cpp:115-145,198-212,288-314,
+        solver_helper.h:82-101,160-182,250-287) ---- */
+
+// update_motility_single for every agent; the random walk is the
+// counter-based unit vector instead of the angle-based draw, the
+// direction-update callbacks are not run
+void motility(world& w, ppc_motility& f)
+{
+	const uint64_t epoch = w.mot_epoch++;
+	const int dims = w.mesh.dims;
+	const real_t dt = w.params.mechanics_time_step;
+	for (index_t i = 0; i < w.n; i++)
+	{
+		if (f.is_motile[i] == 0)
+			continue;
+		real_t* mv = f.motility_vector + (size_t)i * dims;
+		if (ppc_uniform(w.seed, epoch, 0, (uint64_t)i, PPC_DRAW_MOTILITY) < dt / f.persistence_time[i])
+		{
+			real_t walk[3] = { 0, 0, 0 };
+			const int wd = (dims == 3 && f.restrict_to_2d[i]) ? 2 : dims;
+			ppc_unit_vector(wd, w.seed, epoch, 0, (uint64_t)i, PPC_DRAW_MOTILITY + 1u, walk);
+			const real_t bias = f.migration_bias[i];
+			for (int d = 0; d < dims; d++)
+				mv[d] = (1 - bias) * walk[d] + bias * f.migration_bias_direction[(size_t)i * dims + d];
+			real_t length;
+			if (dims == 1)
+				length = std::abs(mv[0]);
+			else if (dims == 2)
+				length = std::sqrt(mv[0] * mv[0] + mv[1] * mv[1]);
+			else
+				length = std::sqrt(mv[0] * mv[0] + mv[1] * mv[1] + mv[2] * mv[2]);
+			const real_t scale = f.migration_speed[i];
+			for (int d = 0; d < dims; d++)
+				mv[d] = length > ix_zero_threshold ? mv[d] * scale / length : 0;
+		}
+		for (int d = 0; d < dims; d++)
+			w.vel[(size_t)i * dims + d] += mv[d];
+	}
+}
+
 // physicell::update_geometry (interactions_solver.cpp:89-96)
 void ix_geometry(world& w, index_t i)
 {
@@ -1046,6 +1087,13 @@ void orc_update_positions(orc_state* s) { update_positions(s->w); }
 void orc_update_cell_container_for_mechanics(orc_state* s) { compact_mechanics(s->w); }
 void orc_flag_by_draws(orc_state* s, double p_divide, double p_death) { flag_by_draws(s->w, p_divide, p_death); }
 void orc_update_cell_container_for_phenotype(orc_state* s) { compact_phenotype(s->w); }
+int orc_update_motility_fields(orc_state* s, ppc_motility* f)
+{
+	if (!f || f->count != s->w.n)
+		return PPC_ERR_ARG;
+	motility(s->w, *f);
+	return PPC_OK;
+}
 int orc_update_cell_cell_interactions(orc_state* s, ppc_interactions* f)
 {
 	if (!f || f->count != s->w.n || f->substrates < 0)

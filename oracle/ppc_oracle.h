@@ -61,6 +61,8 @@ void orc_update_cell_container_for_phenotype(orc_state* s);
 /* interactions_solver::update_cell_cell_interactions; `fields` rows follow
    the oracle's agent order */
 int orc_update_cell_cell_interactions(orc_state* s, ppc_interactions* fields);
+/* position_solver::update_motility with motile agents */
+int orc_update_motility_fields(orc_state* s, ppc_motility* fields);
 
 /* one mechanics step in simulator::simulate_mechanics order, `steps` times;
    with_phenotype adds flag_by_draws + the phenotype container update +

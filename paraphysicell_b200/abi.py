@@ -339,6 +339,68 @@ class InteractionArrays:
         return out
 
 
+class Motility(C.Structure):
+    """ppc_motility (include/ppc.h)."""
+    _fields_ = [
+        ("count", C.c_int32),
+        ("reserved", C.c_int32),
+        ("is_motile", _U8),
+        ("restrict_to_2d", _U8),
+        ("persistence_time", _D),
+        ("migration_speed", _D),
+        ("migration_bias", _D),
+        ("migration_bias_direction", _D),
+        ("motility_vector", _D),
+    ]
+
+
+# motility_t::set_defaults (reference: src/data_storage_phenotype.cpp:245-256)
+MOTILITY_FIELDS = [
+    ("is_motile", np.uint8, 1, 0),
+    ("restrict_to_2d", np.uint8, 1, 0),
+    ("persistence_time", np.float64, 1, 1.0),
+    ("migration_speed", np.float64, 1, 1.0),
+    ("migration_bias", np.float64, 1, 0.0),
+    ("migration_bias_direction", np.float64, "dims", 0.0),
+    ("motility_vector", np.float64, "dims", 0.0),
+]
+
+
+class MotilityArrays:
+    """Host arrays of the motility fields, one row per agent, with the
+    reference's defaults."""
+
+    def __init__(self, count, dims, pinned=None):
+        self.count = int(count)
+        self.dims = int(dims)
+        self.arrays = {}
+        for name, dt, mult, dflt in MOTILITY_FIELDS:
+            n = max(self.count * (self.dims if mult == "dims" else 1), 1)
+            arr = pinned(n, dt) if pinned is not None else np.empty(n, dtype=dt)
+            arr[:] = dflt
+            self.arrays[name] = arr
+
+    def __getitem__(self, name):
+        arr = self.arrays[name]
+        mult = next(m for f, _, m, _ in MOTILITY_FIELDS if f == name)
+        if mult == 1:
+            return arr[: self.count]
+        return arr[: self.count * self.dims].reshape(self.count, self.dims)
+
+    def struct(self):
+        s = Motility()
+        s.count = self.count
+        for name, dt, _, _ in MOTILITY_FIELDS:
+            setattr(s, name, self.arrays[name].ctypes.data_as(_PTR[dt]))
+        return s
+
+    def copy(self, pinned=None):
+        out = MotilityArrays(self.count, self.dims, pinned)
+        for k, v in self.arrays.items():
+            out.arrays[k][:] = v
+        return out
+
+
 def status_name(rc):
     return STATUS_NAMES.get(rc, f"status {rc}")
 

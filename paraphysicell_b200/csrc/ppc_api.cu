@@ -1080,6 +1080,86 @@ int ppc_flag_by_draws(ppc_state* s, double p_divide, double p_death)
 	return finish(s);
 }
 
+// device scratch for the phenotype fields of a per-call entry point, kept
+// between calls
+static int ensure_field_scratch(ppc_state* s, size_t bytes)
+{
+	if (bytes <= s->ix_scratch_bytes)
+		return PPC_OK;
+	if (s->ix_scratch)
+	{
+		PPC_CUDA(cudaStreamSynchronize(s->stream));
+		PPC_CUDA(cudaFree(s->ix_scratch));
+		s->ix_scratch = nullptr;
+		s->ix_scratch_bytes = 0;
+	}
+	PPC_CUDA(cudaMalloc(&s->ix_scratch, bytes));
+	s->ix_scratch_bytes = bytes;
+	return PPC_OK;
+}
+
+int ppc_update_motility_fields(ppc_state* s, int32_t r, ppc_motility* f)
+{
+	if (!valid(s, r) || !f)
+		return fail(PPC_ERR_ARG, "invalid arguments");
+	if (!f->is_motile || !f->restrict_to_2d || !f->persistence_time || !f->migration_speed || !f->migration_bias
+		|| !f->migration_bias_direction || !f->motility_vector)
+		return fail(PPC_ERR_ARG, "a ppc_motility field is NULL");
+	std::vector<rep_counters> c;
+	PPC_TRY(read_counters(s, c));
+	const int32_t n = c[r].count;
+	if (f->count != n)
+		return fail(PPC_ERR_ARG, "fields.count differs from the replicate's agent count");
+	if ((int32_t)s->mot_epoch.size() < s->nreps)
+		s->mot_epoch.resize(s->nreps, 0);
+	const uint64_t epoch = s->mot_epoch[r]++;
+	if (n == 0)
+		return PPC_OK;
+	const size_t nd = (size_t)n, dims = (size_t)s->dims;
+	const size_t bytes = sizeof(double) * (3 * nd + 2 * nd * dims) + 2 * nd;
+	PPC_TRY(ensure_field_scratch(s, bytes));
+	double* dp = static_cast<double*>(s->ix_scratch);
+	mot_fields m {};
+	m.n = n;
+	m.replicate = r;
+	m.base = s->reps[r].base;
+	m.dt = s->params.mechanics_time_step;
+	m.epoch = epoch;
+	double* persistence = dp;
+	double* speed = dp + nd;
+	double* bias = dp + 2 * nd;
+	double* direction = dp + 3 * nd;
+	double* vec = dp + 3 * nd + nd * dims;
+	uint8_t* motile = reinterpret_cast<uint8_t*>(dp + 3 * nd + 2 * nd * dims);
+	uint8_t* restrict2d = motile + nd;
+	m.persistence = persistence;
+	m.speed = speed;
+	m.bias = bias;
+	m.direction = direction;
+	m.vector = vec;
+	m.motile = motile;
+	m.restrict2d = restrict2d;
+	struct copy
+	{
+		void* dst;
+		const void* src;
+		size_t bytes;
+	} in[] = { { persistence, f->persistence_time, nd * sizeof(double) },
+			   { speed, f->migration_speed, nd * sizeof(double) },
+			   { bias, f->migration_bias, nd * sizeof(double) },
+			   { direction, f->migration_bias_direction, nd * dims * sizeof(double) },
+			   { vec, f->motility_vector, nd * dims * sizeof(double) },
+			   { motile, f->is_motile, nd },
+			   { restrict2d, f->restrict_to_2d, nd } };
+	for (auto& k : in)
+		PPC_CUDA(cudaMemcpyAsync(k.dst, k.src, k.bytes, cudaMemcpyHostToDevice, s->stream));
+	PPC_TRY(launch_motility(s, m));
+	PPC_CUDA(cudaMemcpyAsync(f->motility_vector, vec, nd * dims * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	s->vel_dirty = true; // the next fused step reads the velocities
+	return finish(s);
+}
+
 int ppc_update_cell_cell_interactions(ppc_state* s, int32_t r, ppc_interactions* f)
 {
 	if (!valid(s, r) || !f || f->substrates < 0)
@@ -1119,18 +1199,7 @@ int ppc_update_cell_cell_interactions(ppc_state* s, int32_t r, ppc_interactions*
 	const size_t doubles = nd * (2 + 13) + nd * D * 4 + nd * S * 2;
 	const size_t ints = nd * 2 + nd * s->ncap;
 	const size_t bytes = doubles * sizeof(double) + ints * sizeof(int32_t) + nd;
-	if (bytes > s->ix_scratch_bytes)
-	{
-		if (s->ix_scratch)
-		{
-			PPC_CUDA(cudaStreamSynchronize(s->stream));
-			PPC_CUDA(cudaFree(s->ix_scratch));
-			s->ix_scratch = nullptr;
-			s->ix_scratch_bytes = 0;
-		}
-		PPC_CUDA(cudaMalloc(&s->ix_scratch, bytes));
-		s->ix_scratch_bytes = bytes;
-	}
+	PPC_TRY(ensure_field_scratch(s, bytes));
 	char* d = static_cast<char*>(s->ix_scratch);
 	double* dp = reinterpret_cast<double*>(d);
 	auto take = [&](size_t count) { double* q = dp; dp += count; return q; };

@@ -202,6 +202,7 @@ struct ppc_state
 	// host copies of the replicate counts as last read (a download's first guess)
 	std::vector<int32_t> host_count;
 	std::vector<uint64_t> ix_epoch; // cell-cell interaction calls so far, per replicate
+	std::vector<uint64_t> mot_epoch; // motility calls so far, per replicate
 	void* ix_scratch = nullptr;		// device copies of the interaction fields, kept between calls
 	size_t ix_scratch_bytes = 0;
 	ppc::rep_counters* pinned_ctr = nullptr; // pinned landing area of the counters
@@ -276,6 +277,18 @@ struct ix_fields
 	int32_t* cand;	// [n*ncap] their positions in the agent's neighbour list
 };
 int launch_interactions(ppc_state* s, const ix_fields& x);
+
+// device copies of the ppc_motility fields of one replicate (local rows)
+struct mot_fields
+{
+	int32_t n, replicate, base;
+	double dt;
+	uint64_t epoch;
+	const uint8_t *motile, *restrict2d;
+	const double *persistence, *speed, *bias, *direction; // direction: [n*dims]
+	double* vector;										  // [n*dims]
+};
+int launch_motility(ppc_state* s, const mot_fields& m);
 
 } // namespace ppc
 

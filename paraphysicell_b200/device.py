@@ -14,7 +14,7 @@ import os
 
 import numpy as np
 
-from .abi import Agents, Interactions, Mesh, Params, PPCError
+from .abi import Agents, Interactions, Mesh, Motility, Params, PPCError
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libppc.so")
@@ -35,7 +35,7 @@ EXPORTS = (
     "ppc_get_neighbors", "ppc_get_mesh_bins", "ppc_get_voxel_count", "ppc_get_mesh_position",
     "ppc_get_mesh_index", "ppc_get_launch_count", "ppc_last_error", "ppc_abi_version",
     "ppc_set_profiling", "ppc_get_profile", "ppc_set_launch_shape", "ppc_autotune",
-    "ppc_update_cell_cell_interactions",
+    "ppc_update_cell_cell_interactions", "ppc_update_motility_fields",
 ) + tuple("ppc_" + e for e in ENTRY_POINTS)
 
 
@@ -81,6 +81,7 @@ def lib():
         for e in ENTRY_POINTS:
             getattr(L, "ppc_" + e).argtypes = [vp]
         L.ppc_update_cell_cell_interactions.argtypes = [vp, C.c_int32, C.POINTER(Interactions)]
+        L.ppc_update_motility_fields.argtypes = [vp, C.c_int32, C.POINTER(Motility)]
         _lib = L
     return _lib
 
@@ -214,6 +215,12 @@ class Simulation:
 
     def flag_by_draws(self, p_divide, p_death):
         _check(lib().ppc_flag_by_draws(self.h, p_divide, p_death), "ppc_flag_by_draws")
+
+    def update_motility_fields(self, fields, replicate=0):
+        """position_solver::update_motility with motile agents; `fields`
+        (abi.MotilityArrays) is read and its motility vectors written back."""
+        st = fields.struct()
+        _check(lib().ppc_update_motility_fields(self.h, replicate, C.byref(st)), "ppc_update_motility_fields")
 
     def update_cell_cell_interactions(self, fields, replicate=0):
         """interactions_solver::update_cell_cell_interactions on one replicate;

@@ -1,0 +1,129 @@
+"""Motility (position_solver::update_motility, reference:
+src/solver/host/position_solver.cpp:115-145,288-314, solver_helper.h:82-101,
+160-182,250-287): properties of the oracle's restatement on the CPU, and the
+device path bit-exact against it on the GPU. The reference's unit tests have
+no motility case, so these properties stand in for known answers."""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from paraphysicell_b200 import workloads as wl
+from paraphysicell_b200.abi import AgentArrays, Mesh, MotilityArrays, Params
+
+
+def _agents(dims, n, seed):
+    if dims == 3:
+        mesh, params, a = wl.scaled(wl.config3, n, seed=seed, capacity=n + 16)
+    elif dims == 2:
+        mesh, params, a = wl.config1(seed=seed, n=n, capacity=n + 16)
+    else:
+        # one agent per ~6 um of line on average
+        rng = np.random.default_rng(seed)
+        mesh = Mesh.make(1, (-1000, 0, 0), (1000, 0, 0))
+        params = Params.make(dt=0.1, ndefs=1)
+        a = AgentArrays(n, 1, 1, n + 16)
+        a.arrays["positions"][:n] = rng.uniform(-6.0 * n / 2, 6.0 * n / 2, n)
+    return mesh, params, a
+
+
+def _fields(n, dims, seed, persistence=(0.05, 5.0)):
+    rng = np.random.default_rng(seed)
+    m = MotilityArrays(n, dims)
+    m["is_motile"][:] = (rng.random(n) < 0.7).astype(np.uint8)
+    m["restrict_to_2d"][:] = (rng.random(n) < 0.3).astype(np.uint8)
+    m["persistence_time"][:] = rng.uniform(*persistence, n)
+    m["migration_speed"][:] = rng.uniform(0.1, 2.0, n)
+    m["migration_bias"][:] = rng.random(n) * (rng.random(n) < 0.6)
+    d = rng.normal(size=(n, dims))
+    m["migration_bias_direction"][:] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    m["motility_vector"][:] = rng.normal(size=(n, dims)) * 0.1
+    return m
+
+
+def _velocities(x, a):
+    out = AgentArrays(0, a.dims, a.ndefs, a.capacity)
+    out.count = out.capacity
+    x.download(out)
+    return out["velocities"].copy()
+
+
+@pytest.mark.parametrize("dims", [1, 2, 3])
+def test_motility_oracle_properties(dims):
+    """Non-motile agents keep their velocity; a redraw gives a motility vector
+    of length migration_speed (the bias direction when fully biased; z = 0
+    when restricted to 2-D; a direction uniform on the sphere otherwise);
+    without a redraw the stored vector is added unchanged."""
+    n = 300 if dims == 1 else 4000
+    mesh, params, a = _agents(dims, n, seed=11)
+    o = Oracle(mesh, params)
+    o.upload(a)
+    m = _fields(n, dims, seed=12, persistence=(0.001, 0.001))  # dt / p = 100: always redraw
+    m["migration_bias"][: n // 2] = 0.0
+    m["migration_bias"][n // 2:] = 1.0
+    before = m.copy()
+    v0 = _velocities(o, a)
+    o.update_motility_fields(m)
+    v1 = _velocities(o, a)
+    motile = m["is_motile"] == 1
+    assert np.array_equal(v1[~motile], v0[~motile])
+    assert np.array_equal(m["motility_vector"][~motile], before["motility_vector"][~motile])
+    lengths = np.linalg.norm(m["motility_vector"], axis=1)
+    np.testing.assert_allclose(lengths[motile], m["migration_speed"][motile], rtol=1e-14)
+    np.testing.assert_array_equal(v1[motile], v0[motile] + m["motility_vector"][motile])
+    biased = motile & (np.arange(n) >= n // 2)
+    want = m["migration_bias_direction"] * m["migration_speed"][:, None]
+    np.testing.assert_allclose(m["motility_vector"][biased], want[biased], rtol=1e-13, atol=1e-15)
+    if dims == 3:
+        flat = motile & (m["restrict_to_2d"] == 1) & (np.arange(n) < n // 2)
+        assert np.all(m["motility_vector"][flat][:, 2] == 0.0)
+        free = motile & (m["restrict_to_2d"] == 0) & (np.arange(n) < n // 2)
+        unit = m["motility_vector"][free] / m["migration_speed"][free][:, None]
+        assert np.all(np.abs(unit.mean(axis=0)) < 0.08)
+    if dims == 1:
+        unbiased = motile & (np.arange(n) < n // 2)
+        assert set(np.unique(np.sign(m["motility_vector"][unbiased, 0]))) == {-1.0, 1.0}
+
+    # no redraw: persistence far above dt keeps the stored vector
+    m2 = _fields(n, dims, seed=13, persistence=(1e30, 1e30))
+    keep = m2.copy()
+    o.update_motility_fields(m2)
+    v2 = _velocities(o, a)
+    assert np.array_equal(m2["motility_vector"], keep["motility_vector"])
+    mot2 = m2["is_motile"] == 1
+    np.testing.assert_array_equal(v2[mot2], v1[mot2] + keep["motility_vector"][mot2])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [1, 2, 3])
+def test_motility_matches_oracle(dims):
+    """The device's motility pass equals the oracle's bit for bit over three
+    calls, and a fused step after it starts from the moved velocities."""
+    from tests import gpu_util as gu
+    n = 300 if dims == 1 else 3000
+    mesh, params, a = _agents(dims, n, seed=21 + dims)
+    o, d = gu.make_pair(mesh, params, a, seed=5)
+    mo, md = _fields(n, dims, seed=31), _fields(n, dims, seed=31)
+    for _ in range(3):
+        o.update_motility_fields(mo)
+        d.update_motility_fields(md)
+        assert np.array_equal(md["motility_vector"], mo["motility_vector"])
+        assert np.array_equal(_velocities(d, a), _velocities(o, a))
+    o.update_mechanics_mesh()
+    d.update_mechanics_mesh()
+    o.step(1, 0, 0.0, 0.0)
+    d.step(1)
+    gu.assert_same_state(gu.fetch(d, a), gu.fetch(o, a))
+
+
+@pytest.mark.gpu
+def test_motility_argument_errors():
+    from paraphysicell_b200.abi import PPCError
+    from tests import gpu_util as gu
+    mesh, params, a = _agents(2, 100, seed=3)
+    o, d = gu.make_pair(mesh, params, a)
+    with pytest.raises(PPCError):
+        d.update_motility_fields(MotilityArrays(99, 2))
+    with pytest.raises(PPCError):
+        d.update_motility_fields(MotilityArrays(100, 2), replicate=3)
+    d.update_motility_fields(MotilityArrays(100, 2))  # defaults: nobody is motile
+    assert np.all(_velocities(d, a)[:100] == 0.0)
