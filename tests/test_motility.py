@@ -109,6 +109,7 @@ def test_motility_matches_oracle(dims):
         assert np.array_equal(md["motility_vector"], mo["motility_vector"])
         assert np.array_equal(_velocities(d, a), _velocities(o, a))
     o.update_mechanics_mesh()
+    o.update_cell_neighbors()  # the oracle's force pass reads the stored lists
     d.update_mechanics_mesh()
     o.step(1, 0, 0.0, 0.0)
     d.step(1)
