@@ -174,26 +174,31 @@ int ppc_set_precision(ppc_state* s, int32_t precision);
 int ppc_set_random_seed(ppc_state* s, uint64_t seed);
 
 /* Launch shape of the fused force pass, one thread per agent in every shape:
- *  -1 (the default): each thread reads its candidates from global memory and
- *     runs its own pair code — best where agents are sparse (well under one
- *     per voxel);
+ *  -3 (the default): each thread numbers its candidates in the reference's
+ *     order and fetches their single-precision positions ten at a time into
+ *     shared memory with asynchronous copies, then the FP64 data of the kept
+ *     ones two at a time — best where agents are sparse (well under one per
+ *     voxel); `threads` and `smem_bytes` are ignored (128 threads);
+ *  -1: each thread reads its candidates one at a time from global memory and
+ *     runs its own pair code;
  *  -2: the pair code of a warp's kept candidates is spread over the warp's
- *     32 lanes, candidates read from global memory;
+ *     32 lanes, candidates read from global memory — best where agents are
+ *     dense (several per voxel);
  *   0: as -2, with each block's candidate ranges staged in `smem_bytes` of
  *     shared memory (32 KiB is a good budget; a block whose ranges do not fit
- *     reads global memory) — best where agents are dense.
+ *     reads global memory).
  * `threads` per block 32..256, a multiple of 32 (the fused pass uses at most
  * 128). Results do not depend on the shape; ppc_autotune picks one. */
 int ppc_set_launch_shape(ppc_state* s, int32_t tile_edge, int32_t threads, int32_t smem_bytes);
 
 /* Autotuner of the launch shape (no counterpart in the reference, whose
  * OpenMP loops have no launch shape): runs 2 x `steps` mechanics steps
- * (ppc_step) with each candidate shape — -1 and -2 with 128 threads, 0 with
- * 128 threads / 32 KiB and with 64 threads / 16 KiB — times the second half
- * of each on the state's stream,
- * and keeps the fastest. The simulation advances by 8 x `steps` steps (the
- * trajectory does not depend on the shape). Writes the chosen shape to
- * `tile_edge` and `threads` when they are not NULL. */
+ * (ppc_step) with each candidate shape — -3, -1 and -2 with 128 threads, 0
+ * with 128 threads / 32 KiB and with 64 threads / 16 KiB — times the second
+ * half of each on the state's stream, and keeps the fastest. The simulation
+ * advances by 10 x `steps` steps (the trajectory does not depend on the
+ * shape). Writes the chosen shape to `tile_edge` and `threads` when they are
+ * not NULL. */
 int ppc_autotune(ppc_state* s, int32_t steps, int32_t* tile_edge, int32_t* threads);
 
 /* Neighbour-list capacity per agent for ppc_update_cell_neighbors (default 64). */
@@ -266,7 +271,11 @@ int ppc_update_motility(ppc_state* s);
 typedef struct ppc_motility
 {
 	int32_t count;
-	int32_t reserved;
+	/* 0: as the reference, every 3-D walk lies in the xy-plane (its
+	   random_walk receives the restrict_to_2d array pointer as a bool,
+	   src/solver/host/position_solver.cpp:131, which is always true);
+	   1: each agent's restrict_to_2d flag decides */
+	int32_t restrict_per_agent;
 	const uint8_t* is_motile;				 /* [count] */
 	const uint8_t* restrict_to_2d;			 /* [count] */
 	const double* persistence_time;			 /* [count] */
@@ -281,8 +290,8 @@ typedef struct ppc_motility
  * solver_helper.h:82-101,160-182,250-287). A motile agent redraws its
  * direction with probability dt/persistence_time — draw 0 of agent i at the
  * n-th call for a replicate is uniform(seed, n, replicate, i,
- * PPC_DRAW_MOTILITY), the direction comes from the draws after it — mixes it
- * with migration_bias_direction by migration_bias, scales it to
+ * PPC_DRAW_MOTILITY); the walk's angle and z are the next two draws — mixes
+ * it with migration_bias_direction by migration_bias, scales it to
  * migration_speed, and adds its motility vector to its resident velocity.
  * The reference's per-agent direction-update callbacks (chemotaxis) are not
  * run: the caller sets migration_bias_direction. Synchronizes. */

@@ -14,13 +14,16 @@
  * "Fast splittable pseudorandom number generators", OOPSLA 2014), applied in
  * a chain over the counter words.
  *
- * Unit vectors: Marsaglia's rejection method for points on the sphere
- * (G. Marsaglia, "Choosing a point from the surface of a sphere", Ann. Math.
- * Statist. 43, 1972) in 3-D and the same rejection square for the circle in
- * 2-D; they replace the reference's angle-based random walk
- * (src/solver/host/solver_helper.h:82-86,160-165,250-267), which needs cos/sin
- * whose last bit differs between libm and CUDA. Both give directions uniform
- * on the sphere/circle.
+ * Random walks: the reference's own construction (src/solver/host/
+ * solver_helper.h:82-86,160-165,250-267): in 1-D a sign from one uniform
+ * draw; in 2-D an angle theta = 2 pi u and the direction (cos theta,
+ * sin theta); in 3-D theta as in 2-D, z = 2 u' - 1 and the direction
+ * (cos theta sqrt(1 - z^2), sin theta sqrt(1 - z^2), z). The draws are mapped
+ * to their ranges with the operations of std::uniform_real_distribution
+ * (u (b - a) + a). cos and sin are this file's own ppc_sincos (Cody-Waite
+ * reduction and Taylor polynomials, below), so host and device produce the
+ * same bits; libm and CUDA differ from each other, and from it, in the last
+ * bit now and then.
  *
  * Cube root: Newton's iteration for y^3 = t on a range-reduced argument, with
  * a last step whose residual uses exact FMA products. The reference uses
@@ -63,11 +66,10 @@
 /* draw slots k used by the mechanics path */
 #define PPC_DRAW_DEATH 0u
 #define PPC_DRAW_DIVIDE 1u
-#define PPC_DRAW_WALK 16u		 /* 2 per attempt, up to PPC_DRAW_ATTEMPTS attempts */
-#define PPC_DRAW_ORIENTATION 96u /* 2 per attempt */
-#define PPC_DRAW_ATTEMPTS 32u
+#define PPC_DRAW_WALK 16u		 /* division offset: theta, then z (3-D) */
+#define PPC_DRAW_ORIENTATION 96u /* daughter orientation: theta, then z (3-D) */
 #define PPC_DRAW_INTERACTION 1048576u /* + neighbour position, cell-cell interactions */
-#define PPC_DRAW_MOTILITY 2097152u	/* persistence draw; the direction's draws follow */
+#define PPC_DRAW_MOTILITY 2097152u	/* persistence draw; the walk's theta and z follow */
 
 PPC_HD uint64_t ppc_mix64(uint64_t z)
 {
@@ -93,47 +95,106 @@ PPC_HD double ppc_uniform(uint64_t seed, uint64_t epoch, uint64_t replicate, uin
 	return (double)(ppc_hash(seed, epoch, replicate, slot, k) >> 11) * (1.0 / 9007199254740992.0);
 }
 
-/* Uniform random direction in `dims` dimensions written to w[0..dims-1],
- * from draws k0, k0+1, ... of (seed, epoch, replicate, slot). */
-PPC_HD void ppc_unit_vector(int dims, uint64_t seed, uint64_t epoch, uint64_t replicate, uint64_t slot, uint64_t k0,
+/* Sine and cosine of theta for |theta| <= 2^19 (the random walks pass
+ * theta in [0, 2 pi)).
+ *
+ * Reduction: k = floor(theta 2/pi + 1/2), r = theta - k pi/2 with pi/2 split
+ * into three parts (W. J. Cody and W. Waite, "Software Manual for the
+ * Elementary Functions", 1980): P1 and P2 are pi/2 and the remainder rounded
+ * to 33 significant bits, so k P1 and k P2 are exact for |k| < 2^20, and P3 is
+ * the next remainder rounded to 53 bits; all three were derived from the
+ * decimal expansion of pi in exact rational arithmetic. |r| <= pi/4 plus an
+ * ulp.
+ * Polynomials: the Taylor series of sin and cos about 0 through the terms in
+ * r^19 and r^18, whose truncation error on |r| <= pi/4 is below 1e-19;
+ * coefficients 1/n! (n! is exact in double for n <= 22, the quotients are
+ * correctly rounded), evaluated by Horner's rule.
+ * Result: sin/cos(r) mapped to theta's quadrant k mod 4. Accurate to about
+ * one ulp; every operation is a correctly rounded IEEE operation, so the host
+ * and the device agree bit for bit. */
+PPC_HD void ppc_sincos(double theta, double* sn, double* cs)
+{
+	const double two_over_pi = 0x1.45f306dc9c883p-1;
+	const double P1 = 0x1.921fb544p+0;
+	const double P2 = 0x1.0b4611a6p-34;
+	const double P3 = 0x1.3198a2e037073p-69;
+	const double kd = floor(PPC_ADD(PPC_MUL(theta, two_over_pi), 0.5));
+	const double r = PPC_SUB(PPC_SUB(PPC_SUB(theta, PPC_MUL(kd, P1)), PPC_MUL(kd, P2)), PPC_MUL(kd, P3));
+	const double r2 = PPC_MUL(r, r);
+	/* sin r = r + r r2 (-1/3! + r2 (1/5! - ...)) */
+	double ps = -1.0 / 121645100408832000.0; /* -1/19! */
+	ps = PPC_ADD(PPC_MUL(ps, r2), 1.0 / 355687428096000.0);
+	ps = PPC_ADD(PPC_MUL(ps, r2), -1.0 / 1307674368000.0);
+	ps = PPC_ADD(PPC_MUL(ps, r2), 1.0 / 6227020800.0);
+	ps = PPC_ADD(PPC_MUL(ps, r2), -1.0 / 39916800.0);
+	ps = PPC_ADD(PPC_MUL(ps, r2), 1.0 / 362880.0);
+	ps = PPC_ADD(PPC_MUL(ps, r2), -1.0 / 5040.0);
+	ps = PPC_ADD(PPC_MUL(ps, r2), 1.0 / 120.0);
+	ps = PPC_ADD(PPC_MUL(ps, r2), -1.0 / 6.0);
+	const double s = PPC_ADD(r, PPC_MUL(PPC_MUL(r, r2), ps));
+	/* cos r = 1 + r2 (-1/2! + r2 (1/4! - ...)) */
+	double pc = -1.0 / 6402373705728000.0; /* -1/18! */
+	pc = PPC_ADD(PPC_MUL(pc, r2), 1.0 / 20922789888000.0);
+	pc = PPC_ADD(PPC_MUL(pc, r2), -1.0 / 87178291200.0);
+	pc = PPC_ADD(PPC_MUL(pc, r2), 1.0 / 479001600.0);
+	pc = PPC_ADD(PPC_MUL(pc, r2), -1.0 / 3628800.0);
+	pc = PPC_ADD(PPC_MUL(pc, r2), 1.0 / 40320.0);
+	pc = PPC_ADD(PPC_MUL(pc, r2), -1.0 / 720.0);
+	pc = PPC_ADD(PPC_MUL(pc, r2), 1.0 / 24.0);
+	pc = PPC_ADD(PPC_MUL(pc, r2), -0.5);
+	const double c = PPC_ADD(1.0, PPC_MUL(r2, pc));
+	switch ((int)((long long)kd & 3))
+	{
+	case 0:
+		*sn = s;
+		*cs = c;
+		break;
+	case 1:
+		*sn = c;
+		*cs = -s;
+		break;
+	case 2:
+		*sn = -s;
+		*cs = -c;
+		break;
+	default:
+		*sn = -c;
+		*cs = s;
+		break;
+	}
+}
+
+/* position_helper<dims>::random_walk (reference: src/solver/host/
+ * solver_helper.h:82-86,160-165,250-267) with draws k0 (the sign, or theta)
+ * and k0 + 1 (z, 3-D only) of (seed, epoch, replicate, slot); writes
+ * w[0..dims-1]. The 3-D walk restricted to the plane is the 2-D walk with
+ * w[2] = 0, as in the reference. */
+PPC_HD void ppc_random_walk(int dims, uint64_t seed, uint64_t epoch, uint64_t replicate, uint64_t slot, uint64_t k0,
 							double* w)
 {
+	const double two_pi = 6.283185307179586; /* 2 std::numbers::pi_v<double>, exact */
+	const double u = ppc_uniform(seed, epoch, replicate, slot, k0);
 	if (dims == 1)
 	{
-		/* reference: solver_helper.h:82-86, walk = rand < 0.5 ? -1 : 1 */
-		double u = ppc_uniform(seed, epoch, replicate, slot, k0);
 		w[0] = u < 0.5 ? -1.0 : 1.0;
 		return;
 	}
-	for (uint32_t t = 0; t < PPC_DRAW_ATTEMPTS; t++)
+	/* uniform(0, 2 pi) = u (2 pi - 0) + 0 */
+	const double theta = PPC_ADD(PPC_MUL(u, PPC_SUB(two_pi, 0.0)), 0.0);
+	double sn, cs;
+	ppc_sincos(theta, &sn, &cs);
+	if (dims == 2)
 	{
-		double a = PPC_SUB(PPC_MUL(2.0, ppc_uniform(seed, epoch, replicate, slot, k0 + 2 * t)), 1.0);
-		double b = PPC_SUB(PPC_MUL(2.0, ppc_uniform(seed, epoch, replicate, slot, k0 + 2 * t + 1)), 1.0);
-		double s = PPC_ADD(PPC_MUL(a, a), PPC_MUL(b, b));
-		if (s >= 1.0 || s == 0.0)
-			continue;
-		if (dims == 2)
-		{
-			double l = PPC_SQRT(s);
-			w[0] = PPC_DIV(a, l);
-			w[1] = PPC_DIV(b, l);
-		}
-		else
-		{
-			double f = PPC_MUL(2.0, PPC_SQRT(PPC_SUB(1.0, s)));
-			w[0] = PPC_MUL(a, f);
-			w[1] = PPC_MUL(b, f);
-			w[2] = PPC_SUB(1.0, PPC_MUL(2.0, s));
-		}
+		w[0] = cs;
+		w[1] = sn;
 		return;
 	}
-	/* probability of reaching here is (1 - pi/4)^32 < 1e-21 */
-	w[0] = 0.0;
-	w[1] = 0.0;
-	if (dims == 3)
-		w[2] = 1.0;
-	else
-		w[0] = 1.0;
+	/* uniform(-1, 1) = u' (1 - (-1)) + (-1) */
+	const double z = PPC_ADD(PPC_MUL(ppc_uniform(seed, epoch, replicate, slot, k0 + 1u), 2.0), -1.0);
+	const double rr = PPC_SQRT(PPC_SUB(1.0, PPC_MUL(z, z)));
+	w[0] = PPC_MUL(cs, rr);
+	w[1] = PPC_MUL(sn, rr);
+	w[2] = z;
 }
 
 PPC_HD uint64_t ppc_d2u(double x)

@@ -50,6 +50,11 @@ def lib():
         L.orc_time_steps.restype = C.c_double
         L.orc_update_cell_cell_interactions.argtypes = [vp, C.POINTER(Interactions)]
         L.orc_update_motility_fields.argtypes = [vp, C.POINTER(Motility)]
+        L.orc_sincos.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
+        L.orc_random_walk.argtypes = [C.c_int32, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64,
+                                      C.c_void_p]
+        L.orc_uniform.argtypes = [C.c_uint64] * 5
+        L.orc_uniform.restype = C.c_double
         L.orc_get_neighbors.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_int32]
         L.orc_get_mesh_bins.argtypes = [vp, C.c_void_p, C.c_void_p]
         L.orc_get_mesh_position.argtypes = [vp, C.c_void_p, C.c_void_p]
@@ -147,3 +152,25 @@ class Oracle:
         agents = np.zeros(max(self.count, 1), np.int32)
         self.L.orc_get_mesh_bins(self.h, counts.ctypes.data, agents.ctypes.data)
         return counts, agents[: self.count]
+
+
+def sincos(theta):
+    """ppc_sincos of include/ppc_draws.h over an array of angles."""
+    import numpy as np
+    th = np.ascontiguousarray(theta, dtype=np.float64)
+    sn, cs = np.empty_like(th), np.empty_like(th)
+    lib().orc_sincos(th.ctypes.data, th.size, sn.ctypes.data, cs.ctypes.data)
+    return sn, cs
+
+
+def random_walk(dims, seed, epoch, replicate, slot, k0):
+    """ppc_random_walk of include/ppc_draws.h: the reference's random walk
+    from the counter-based draws."""
+    import numpy as np
+    w = np.zeros(3)
+    lib().orc_random_walk(dims, seed, epoch, replicate, slot, k0, w.ctypes.data)
+    return w[:dims]
+
+
+def uniform(seed, epoch, replicate, slot, k):
+    return lib().orc_uniform(seed, epoch, replicate, slot, k)

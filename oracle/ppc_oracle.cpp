@@ -651,7 +651,7 @@ void divide(world& w, index_t p, index_t c, uint64_t epoch)
 	w.springs[p].clear();
 
 	real_t walk[3];
-	ppc_unit_vector(dims, w.seed, epoch, 0, (uint64_t)p, PPC_DRAW_WALK, walk);
+	ppc_random_walk(dims, w.seed, epoch, 0, (uint64_t)p, PPC_DRAW_WALK, walk);
 	{
 		real_t tmp = 0;
 		for (int d = 0; d < dims; d++)
@@ -677,7 +677,7 @@ void divide(world& w, index_t p, index_t c, uint64_t epoch)
 	w.maxatt[c] = w.maxatt[p];
 	w.def[c] = w.def[p];
 	// assign_orientation() of the new cell draws a fresh direction
-	ppc_unit_vector(dims, w.seed, epoch, 0, (uint64_t)p, PPC_DRAW_ORIENTATION, w.orient.data() + (size_t)c * dims);
+	ppc_random_walk(dims, w.seed, epoch, 0, (uint64_t)p, PPC_DRAW_ORIENTATION, w.orient.data() + (size_t)c * dims);
 
 	for (int d = 0; d < dims; d++)
 	{
@@ -743,9 +743,12 @@ constexpr real_t ix_zero_threshold = 1e-16; // reference: src/solver/host/solver
 /* ---- motility (reference: src/solver/host/position_solver.cpp:115-145,198-212,288-314,
         solver_helper.h:82-101,160-182,250-287) ---- */
 
-// update_motility_single for every agent; the random walk is the
-// counter-based unit vector instead of the angle-based draw, the
-// direction-update callbacks are not run
+// update_motility_single for every agent, with the reference's random walk
+// from counter-based draws; the direction-update callbacks are not run. The
+// reference passes the whole restrict_to_2d array to random_walk, whose bool
+// parameter is then always true (position_solver.cpp:131), so every 3-D walk
+// lies in the xy-plane; fields.restrict_per_agent = 1 reads each agent's flag
+// instead.
 void motility(world& w, ppc_motility& f)
 {
 	const uint64_t epoch = w.mot_epoch++;
@@ -759,8 +762,8 @@ void motility(world& w, ppc_motility& f)
 		if (ppc_uniform(w.seed, epoch, 0, (uint64_t)i, PPC_DRAW_MOTILITY) < dt / f.persistence_time[i])
 		{
 			real_t walk[3] = { 0, 0, 0 };
-			const int wd = (dims == 3 && f.restrict_to_2d[i]) ? 2 : dims;
-			ppc_unit_vector(wd, w.seed, epoch, 0, (uint64_t)i, PPC_DRAW_MOTILITY + 1u, walk);
+			const bool planar = dims == 3 && (f.restrict_per_agent ? f.restrict_to_2d[i] != 0 : true);
+			ppc_random_walk(planar ? 2 : dims, w.seed, epoch, 0, (uint64_t)i, PPC_DRAW_MOTILITY + 1u, walk);
 			const real_t bias = f.migration_bias[i];
 			for (int d = 0; d < dims; d++)
 				mv[d] = (1 - bias) * walk[d] + bias * f.migration_bias_direction[(size_t)i * dims + d];
@@ -1126,6 +1129,23 @@ double orc_time_steps(orc_state* s, int32_t steps, int32_t threads, int32_t with
 	auto t1 = std::chrono::high_resolution_clock::now();
 	w.timed = false;
 	return std::chrono::duration<double>(t1 - t0).count();
+}
+
+void orc_sincos(const double* theta, int32_t n, double* sn, double* cs)
+{
+	for (int32_t i = 0; i < n; i++)
+		ppc_sincos(theta[i], sn + i, cs + i);
+}
+
+void orc_random_walk(int32_t dims, uint64_t seed, uint64_t epoch, uint64_t replicate, uint64_t slot, uint64_t k0,
+					 double* w)
+{
+	ppc_random_walk(dims, seed, epoch, replicate, slot, k0, w);
+}
+
+double orc_uniform(uint64_t seed, uint64_t epoch, uint64_t replicate, uint64_t slot, uint64_t k)
+{
+	return ppc_uniform(seed, epoch, replicate, slot, k);
 }
 
 int orc_get_neighbors(orc_state* s, int32_t* counts, int32_t* lists, int32_t list_capacity)

@@ -74,6 +74,13 @@ void orc_step(orc_state* s, int32_t steps, int32_t with_phenotype, double p_divi
 double orc_time_steps(orc_state* s, int32_t steps, int32_t threads, int32_t with_phenotype, double p_divide,
 					  double p_death);
 
+/* the draws header's sine/cosine and random walk evaluated on the host, for
+   the tests that pin them against libm and the reference's construction */
+void orc_sincos(const double* theta, int32_t n, double* sn, double* cs);
+void orc_random_walk(int32_t dims, uint64_t seed, uint64_t epoch, uint64_t replicate, uint64_t slot, uint64_t k0,
+					 double* w);
+double orc_uniform(uint64_t seed, uint64_t epoch, uint64_t replicate, uint64_t slot, uint64_t k);
+
 /* readback */
 int orc_get_neighbors(orc_state* s, int32_t* counts, int32_t* lists, int32_t list_capacity);
 int orc_get_mesh_bins(orc_state* s, int32_t* voxel_counts, int32_t* agents);

@@ -343,7 +343,7 @@ class Motility(C.Structure):
     """ppc_motility (include/ppc.h)."""
     _fields_ = [
         ("count", C.c_int32),
-        ("reserved", C.c_int32),
+        ("restrict_per_agent", C.c_int32),
         ("is_motile", _U8),
         ("restrict_to_2d", _U8),
         ("persistence_time", _D),
@@ -370,9 +370,12 @@ class MotilityArrays:
     """Host arrays of the motility fields, one row per agent, with the
     reference's defaults."""
 
-    def __init__(self, count, dims, pinned=None):
+    def __init__(self, count, dims, pinned=None, restrict_per_agent=False):
         self.count = int(count)
         self.dims = int(dims)
+        # False: every 3-D walk in the xy-plane, as the reference; True: each
+        # agent's restrict_to_2d flag decides
+        self.restrict_per_agent = bool(restrict_per_agent)
         self.arrays = {}
         for name, dt, mult, dflt in MOTILITY_FIELDS:
             n = max(self.count * (self.dims if mult == "dims" else 1), 1)
@@ -390,12 +393,13 @@ class MotilityArrays:
     def struct(self):
         s = Motility()
         s.count = self.count
+        s.restrict_per_agent = int(self.restrict_per_agent)
         for name, dt, _, _ in MOTILITY_FIELDS:
             setattr(s, name, self.arrays[name].ctypes.data_as(_PTR[dt]))
         return s
 
     def copy(self, pinned=None):
-        out = MotilityArrays(self.count, self.dims, pinned)
+        out = MotilityArrays(self.count, self.dims, pinned, self.restrict_per_agent)
         for k, v in self.arrays.items():
             out.arrays[k][:] = v
         return out

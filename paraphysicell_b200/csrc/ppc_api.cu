@@ -861,13 +861,14 @@ int ppc_set_launch_shape(ppc_state* s, int32_t tile_edge, int32_t threads, int32
 {
 	if (!s)
 		return fail(PPC_ERR_ARG, "null state");
-	if ((tile_edge != 0 && tile_edge != -1 && tile_edge != -2) || threads < 32 || threads > 256 || threads % 32 != 0 || smem_bytes < 0
+	if (tile_edge < -3 || tile_edge > 0 || threads < 32 || threads > 256 || threads % 32 != 0 || smem_bytes < 0
 		|| smem_bytes > 160 * 1024)
-		return fail(PPC_ERR_ARG, "tile edge 0, -1 or -2, threads 32..256 (multiple of 32), smem <= 160 KiB");
+		return fail(PPC_ERR_ARG, "tile edge 0, -1, -2 or -3, threads 32..256 (multiple of 32), smem <= 160 KiB");
 	PPC_CUDA(cudaStreamSynchronize(s->stream));
 	release_graph(s);
+	s->flat = tile_edge == -3;
 	s->staged = tile_edge == 0;
-	s->coop = tile_edge != -1;
+	s->coop = tile_edge == 0 || tile_edge == -2;
 	s->tile_threads = threads;
 	s->tile_smem = smem_bytes;
 	return PPC_OK;
@@ -1124,6 +1125,7 @@ int ppc_update_motility_fields(ppc_state* s, int32_t r, ppc_motility* f)
 	m.replicate = r;
 	m.base = s->reps[r].base;
 	m.dt = s->params.mechanics_time_step;
+	m.per_agent = f->restrict_per_agent != 0;
 	m.epoch = epoch;
 	double* persistence = dp;
 	double* speed = dp + nd;
@@ -1306,14 +1308,15 @@ int ppc_autotune(ppc_state* s, int32_t steps, int32_t* tile_edge, int32_t* threa
 	{
 		int edge, threads, smem;
 	};
-	const shape cand[] = { { -1, 128, 0 }, { -2, 128, 0 }, { 0, 128, 32 * 1024 }, { 0, 64, 16 * 1024 } };
+	const shape cand[] = { { -3, 128, 0 }, { -1, 128, 0 }, { -2, 128, 0 }, { 0, 128, 32 * 1024 }, { 0, 64, 16 * 1024 } };
+	const int ncand = (int)(sizeof cand / sizeof cand[0]);
 	cudaEvent_t e0 = nullptr, e1 = nullptr;
 	PPC_CUDA(cudaEventCreate(&e0));
 	PPC_CUDA(cudaEventCreate(&e1));
 	int best = -1;
 	float best_ms = 0.f;
 	int rc = PPC_OK;
-	for (int k = 0; k < 4 && rc == PPC_OK; k++)
+	for (int k = 0; k < ncand && rc == PPC_OK; k++)
 	{
 		rc = ppc_set_launch_shape(s, cand[k].edge, cand[k].threads, cand[k].smem);
 		if (rc == PPC_OK)

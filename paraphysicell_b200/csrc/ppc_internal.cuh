@@ -209,6 +209,7 @@ struct ppc_state
 	int32_t* pinned_flag = nullptr;			 // pinned landing area of pos_changed
 	bool staged = false;
 	bool coop = false;
+	bool flat = true; // per-thread pass with batched candidate fetches (shape -3, the default)
 	int tile_threads = 128;
 	int tile_smem = 32 * 1024;
 
@@ -281,7 +282,7 @@ int launch_interactions(ppc_state* s, const ix_fields& x);
 // device copies of the ppc_motility fields of one replicate (local rows)
 struct mot_fields
 {
-	int32_t n, replicate, base;
+	int32_t n, replicate, base, per_agent;
 	double dt;
 	uint64_t epoch;
 	const uint8_t *motile, *restrict2d;

@@ -316,7 +316,7 @@ __global__ void k_bin_fixup(view v, int cur)
 	double4 p = v.pos[cur][s];
 	const double rmad = v.rmad[s];
 	const long long bits = (long long)(uint32_t)v.def[s] | ((long long)(v.movable[s] != 0) << 32)
-						   | ((long long)min(v.scnt[s], 255) << 40);
+						   | ((long long)min(v.scnt[s], 255) << 40) | ((long long)(r & 0xffff) << 48);
 	const int D = v.ndefs;
 	double aff[4];
 #pragma unroll
@@ -515,7 +515,8 @@ struct pair_fp64
 	}
 };
 
-// bits of sprm4.w: definition index (0..31), movable (32), spring count (40..47)
+// bits of sprm4.w: definition index (0..31), movable (32), spring count (40..47),
+// replicate (48..63, its low 16 bits)
 __device__ __forceinline__ void unpack_bits(double w, int& def, bool& mov)
 {
 	const long long b = __double_as_longlong(w);
@@ -1322,6 +1323,369 @@ __global__ void __launch_bounds__(kStageThreads, 4) k_fused_staged(view v, int c
 }
 
 // ---------------------------------------------------------------------------
+// fused step, one thread per agent, candidates fetched in batches.
+//
+// The per-thread pass above walks each stencil row's candidates one load at a
+// time, and a warp runs as many iterations per row as its longest row among
+// 32 agents, so a sparse tissue costs a warp some thirty dependent loads. Here
+// a thread numbers its candidates in the reference's order (rows z, y; in a
+// row the key-ordered range of its three voxels) and fetches them
+// kFlatBatch at a time into shared memory with asynchronous copies, which
+// keep no registers while they are in flight; the single-precision positions
+// go through the filter of the cooperative passes (it never rejects a pair the
+// FP64 test accepts), and the candidates it keeps fetch their FP64 position,
+// parameters and affinity entry kFlatHits at a time, again as one round trip,
+// before the exact test and the pair code run in candidate order. The
+// epilogue's per-agent rows and the first two spring partners are prefetched
+// into L2 while the scan runs.
+// ---------------------------------------------------------------------------
+
+constexpr int kFlatThreads = 128;
+constexpr int kFlatBatch = 10; // candidates a thread fetches per round
+constexpr int kFlatHits = 2;   // kept candidates whose FP64 data a round fetches (5 slots each)
+static_assert(5 * kFlatHits <= kFlatBatch, "a kept candidate's data takes five slots of its thread's column");
+
+// Each thread owns one column [.][tid] of the slot arrays. A round first
+// holds up to kFlatBatch single-precision candidate positions; once the
+// filter has read them, the same slots take the kept candidates' data: FP64
+// position (slots 5h, 5h+1), parameters (5h+2, 5h+3; the FP32 form's float4 in
+// 5h+2) and affinity entry (5h+4).
+struct flat_smem
+{
+	float4 slot[kFlatBatch][kFlatThreads];
+	int32_t cu[kFlatBatch][kFlatThreads]; // array positions of the round's candidates
+	int2 rows[9][kFlatThreads];			  // per stencil row: first candidate number, array position - number
+};
+
+__device__ __forceinline__ double4 slots_double4(const float4& a, const float4& b)
+{
+	const double2 x = *reinterpret_cast<const double2*>(&a);
+	const double2 y = *reinterpret_cast<const double2*>(&b);
+	return make_double4(x.x, x.y, y.x, y.y);
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src)
+{
+	const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async_small(void* dst, const void* src)
+{
+	const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+	asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(BYTES) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+	asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+enum : int
+{
+	FUSED_WALLS = 1,
+	FUSED_SPRINGS = 2,
+	FUSED_VEL = 4
+};
+
+template <int DIMS, bool F32>
+__global__ void __launch_bounds__(kFlatThreads, 5) k_fused_flat(view v, int cur, int opts)
+{
+	grid_wait();
+	bump_spring_epochs(v);
+	extern __shared__ __align__(16) unsigned char flat_raw[];
+	flat_smem& sm = *reinterpret_cast<flat_smem*>(flat_raw);
+	constexpr int NR = DIMS == 3 ? 9 : (DIMS == 2 ? 3 : 1);
+	const bool walls_on = (opts & FUSED_WALLS) != 0;
+	const bool springs_on = (opts & FUSED_SPRINGS) != 0;
+	const bool vel_on = (opts & FUSED_VEL) != 0;
+	const int tid = threadIdx.x;
+	const int t = blockIdx.x * kFlatThreads + tid;
+	if (t >= v.total_cap)
+		return;
+	// the agent's key-ordered rows, issued before the count is known (t is
+	// below the capacity, so the loads stay in bounds)
+	const int s = v.sorted[t];
+	const int32_t key = v.skey[t];
+	const double4 pi = v.spos4[t];
+	const float4 pf = v.sposf[t];
+	const double4 qi = v.sprm4[t];
+	if (t >= *v.cursor)
+		return;
+	int def_i;
+	bool mov_i;
+	unpack_bits(qi.w, def_i, mov_i);
+	const long long bits_i = __double_as_longlong(qi.w);
+	const int r = v.nreps == 1 ? 0 : (v.nreps <= 65536 ? (int)((bits_i >> 48) & 0xffff) : v.rid[s]);
+	const rep_info& R = v.reps[r];
+	const int D = v.ndefs;
+	// this agent's affinity row: read per neighbour by definition index
+	if (F32)
+		prefetch_l1(v.safff + (int64_t)t * D);
+	else
+		prefetch_l1(v.saff + (int64_t)t * D);
+
+	// stencil rows and the candidate numbering
+	const int32_t lk = key - (int32_t)R.vox_base;
+	const int g0 = R.grid[0], g1 = R.grid[1], g2 = R.grid[2];
+	const int cx = lk % g0, cy = (lk / g0) % g1, cz = lk / (g0 * g1);
+	const int xlo = cx > 0 ? cx - 1 : 0;
+	const int xhi = cx + 1 < g0 ? cx + 1 : g0 - 1;
+	int lo[NR], hi[NR];
+#pragma unroll
+	for (int k = 0; k < NR; k++)
+	{
+		const int dz = DIMS == 3 ? k / 3 - 1 : 0;
+		const int dy = DIMS >= 2 ? k % 3 - 1 : 0;
+		const int z = cz + dz, y = cy + dy;
+		const bool ok = z >= 0 && z < g2 && y >= 0 && y < g1;
+		const int64_t row = R.vox_base + (int64_t)g0 * (y + (int64_t)g1 * z);
+		lo[k] = ok ? v.vstart[row + xlo] : 0;
+		hi[k] = ok ? v.vstart[row + xhi + 1] : 0;
+	}
+	// the epilogue's per-agent rows are read after the scan: ask L2 for them
+	// now, with the indices of the first two spring partners
+	const int nspr = (springs_on && mov_i) ? unpack_springs(qi.w) : 0;
+	prefetch_l2(v.flags + s);
+	int j0 = -1, j1 = -1;
+	if (mov_i)
+	{
+		prefetch_l2(v.vprev + s);
+		if (walls_on)
+			prefetch_l2(&v.prm[s].w);
+		if (nspr > 0)
+		{
+			prefetch_l2(v.ec + s);
+			j0 = v.springs[(int64_t)s * v.scap];
+			if (nspr > 1)
+				j1 = v.springs[(int64_t)s * v.scap + 1];
+		}
+	}
+	// the scan adds its terms to the velocity the agent enters the step with
+	double vx = 0.0, vy = 0.0, vz = 0.0, pressure = 0.0;
+	if (vel_on && mov_i)
+	{
+		const double4 v0 = v.vel[s];
+		vx = v0.x;
+		vy = v0.y;
+		vz = v0.z;
+	}
+	int C = 0;
+#pragma unroll
+	for (int k = 0; k < NR; k++)
+	{
+		sm.rows[k][tid] = make_int2(C, lo[k] - C);
+		C += hi[k] - lo[k];
+	}
+
+	nsum fx, fy, fz, fp;
+	const float margin = R.fmargin;
+	int k = 0;								 // row of the next candidate
+	int knext = NR > 1 ? sm.rows[1][tid].x : C; // first candidate number of row k + 1
+	bool partners = false;
+	for (int c0 = 0; c0 < C; c0 += kFlatBatch)
+	{
+		const int nb = min(kFlatBatch, C - c0);
+#pragma unroll
+		for (int j = 0; j < kFlatBatch; j++)
+			if (j < nb)
+			{
+				const int c = c0 + j;
+				while (c >= knext)
+				{
+					k++;
+					knext = k + 1 < NR ? sm.rows[k + 1][tid].x : C;
+				}
+				const int u = sm.rows[k][tid].y + c;
+				sm.cu[j][tid] = u;
+				cp_async16(&sm.slot[j][tid], v.sposf + u);
+			}
+		if (!partners)
+		{
+			// the partner indices have arrived by now: their rows to L2
+			partners = true;
+			if (j0 >= 0)
+			{
+				prefetch_l2(v.pos[cur] + j0);
+				prefetch_l2(v.def + j0);
+				prefetch_l2(v.ec + j0);
+				prefetch_l2(v.aff + (int64_t)j0 * D + def_i);
+			}
+			if (j1 >= 0)
+			{
+				prefetch_l2(v.pos[cur] + j1);
+				prefetch_l2(v.def + j1);
+				prefetch_l2(v.ec + j1);
+				prefetch_l2(v.aff + (int64_t)j1 * D + def_i);
+			}
+		}
+		cp_async_wait_all();
+		unsigned hm = 0;
+#pragma unroll
+		for (int j = 0; j < kFlatBatch; j++)
+			if (j < nb && sm.cu[j][tid] != t && filter_keep<DIMS>(pf, sm.slot[j][tid], margin))
+				hm |= 1u << j;
+		while (hm)
+		{
+			// FP64 position, parameters and affinity of up to kFlatHits kept
+			// candidates in one round trip
+			int hu[kFlatHits];
+#pragma unroll
+			for (int h = 0; h < kFlatHits; h++)
+			{
+				hu[h] = -1;
+				if (hm)
+				{
+					const int j = __ffs(hm) - 1;
+					hm &= hm - 1;
+					const int u = sm.cu[j][tid];
+					hu[h] = u;
+					const char* gp = reinterpret_cast<const char*>(v.spos4 + u);
+					cp_async16(&sm.slot[5 * h][tid], gp);
+					cp_async16(&sm.slot[5 * h + 1][tid], gp + 16);
+					if (F32)
+					{
+						cp_async16(&sm.slot[5 * h + 2][tid], v.sprmf + u);
+						cp_async_small<4>(&sm.slot[5 * h + 4][tid], v.safff + (int64_t)u * D + def_i);
+					}
+					else
+					{
+						const char* gq = reinterpret_cast<const char*>(v.sprm4 + u);
+						cp_async16(&sm.slot[5 * h + 2][tid], gq);
+						cp_async16(&sm.slot[5 * h + 3][tid], gq + 16);
+						cp_async_small<8>(&sm.slot[5 * h + 4][tid], v.saff + (int64_t)u * D + def_i);
+					}
+				}
+			}
+			cp_async_wait_all();
+#pragma unroll
+			for (int h = 0; h < kFlatHits; h++)
+			{
+				if (hu[h] < 0)
+					continue;
+				// exact FP64 neighbour test: distance <= rmad_i r_i + rmad_j r_j
+				const double4 q = slots_double4(sm.slot[5 * h][tid], sm.slot[5 * h + 1][tid]);
+				const double ddx = pi.x - q.x;
+				const double ddy = DIMS >= 2 ? pi.y - q.y : 0.0;
+				const double ddz = DIMS >= 3 ? pi.z - q.z : 0.0;
+				double d2 = ddx * ddx;
+				if (DIMS >= 2)
+					d2 = d2 + ddy * ddy;
+				if (DIMS >= 3)
+					d2 = d2 + ddz * ddz;
+				const double ad = pi.w + q.w;
+				const double dist = DIMS == 1 ? fabs(ddx) : sqrt(d2);
+				if (!(dist <= ad))
+					continue;
+				if (F32)
+				{
+					// pair_fp32::add with this agent's values
+					const float4 qj = sm.slot[5 * h + 2][tid];
+					const float afj = sm.slot[5 * h + 4][tid].x;
+					int def_j, spr_j;
+					bool mov_j;
+					unpack_fbits(qj.w, def_j, mov_j, spr_j);
+					const float dx = (float)ddx, dy = (float)ddy, dz = (float)ddz;
+					float d2f = dx * dx;
+					if (DIMS >= 2)
+						d2f = d2f + dy * dy;
+					if (DIMS >= 3)
+						d2f = d2f + dz * dz;
+					const float distf = DIMS == 1 ? fabsf(dx) : sqrtf(d2f);
+					const float d = distf < 0.00001f ? 0.00001f : distf;
+					float rep = 1.f - d / ((float)qi.x + qj.x);
+					rep = rep < 0.f ? 0.f : rep;
+					rep = rep * rep;
+					const float term = rep * 36.64504274775163f;
+					if (mov_i)
+						fp.add(term);
+					if (mov_j)
+						fp.add(term);
+					if (mov_i)
+					{
+						rep = rep * sqrtf((float)qi.y * qj.y);
+						float adh = 1.f - d / (pf.w + (float)q.w);
+						adh = adh * adh;
+						adh = adh * sqrtf((float)qi.z * qj.z * v.safff[(int64_t)t * D + def_j] * afj);
+						const float force = (rep - adh) / d;
+						fx.add(force * dx);
+						fy.add(force * dy);
+						fz.add(force * dz);
+					}
+				}
+				else
+				{
+					// pair_fp64::add_pair with this agent's values
+					const double4 pr = slots_double4(sm.slot[5 * h + 2][tid], sm.slot[5 * h + 3][tid]);
+					int def_j;
+					bool mov_j;
+					unpack_bits(pr.w, def_j, mov_j);
+					const double d = dist < 0.00001 ? 0.00001 : dist;
+					double rep = 1.0 - d / (qi.x + pr.x);
+					rep = rep < 0 ? 0 : rep;
+					rep = rep * rep;
+					const double term = rep * simple_pressure_coefficient;
+					if (mov_i)
+						pressure = pressure + term;
+					if (mov_j)
+						pressure = pressure + term;
+					if (mov_i)
+					{
+						rep = rep * sqrt(qi.y * pr.y);
+						double adh = 1.0 - d / ad;
+						adh = adh * adh;
+						const double afj = *reinterpret_cast<const double*>(&sm.slot[5 * h + 4][tid]);
+						adh = adh * sqrt(qi.z * pr.z * v.saff[(int64_t)t * D + def_j] * afj);
+						const double force = (rep - adh) / d;
+						vx = vx + force * ddx;
+						vy = vy + force * ddy;
+						vz = vz + force * ddz;
+					}
+				}
+			}
+		}
+	}
+	if (F32)
+	{
+		vx = vx + fx.value();
+		vy = vy + fy.value();
+		vz = vz + fz.value();
+		pressure = fp.value();
+	}
+
+	// membrane, springs, Adams-Bashforth, then the agent's stores
+	double4 p = make_double4(pi.x, pi.y, pi.z, 0.0);
+	double4 vp = make_double4(0, 0, 0, 0);
+	const uint8_t flag = v.flags[s];
+	if (mov_i)
+	{
+		vp = v.vprev[s];
+		double4 vel = make_double4(vx, vy, vz, 0.0);
+		if (walls_on)
+			walls<DIMS>(v, R, p, qi.x, v.prm[s].w, vel);
+		if (nspr > 0)
+			spring_contract<DIMS>(v, cur, s, nspr, p, def_i, vel);
+		ab2<DIMS>(v.dt, p, vel, vp);
+	}
+	v.pressure[s] = pressure;
+	if (mov_i)
+	{
+		v.vprev[s] = vp;
+		if (vel_on)
+			v.vel[s] = make_double4(0, 0, 0, 0);
+	}
+	v.pos[cur ^ 1][s] = p;
+	if (!(p.x == p.x && p.y == p.y && p.z == p.z))
+		atomicOr(v.err, ERR_NONFINITE);
+	if (to_remove<DIMS>(R, p, flag))
+		append_bad(v, r, s - R.base);
+}
+
+// ---------------------------------------------------------------------------
 // separate reference entry points
 // ---------------------------------------------------------------------------
 
@@ -2077,7 +2441,7 @@ __global__ void k_divide_apply(view v, int cur)
 		// random direction, projected against the orientation by polarity and
 		// scaled by the parent's radius (reference: src/cell.cpp:129-150)
 		double w[3] = { 0, 0, 0 };
-		ppc_unit_vector(DIMS, v.seed, ep, (uint64_t)r, (uint64_t)lp, PPC_DRAW_WALK, w);
+		ppc_random_walk(DIMS, v.seed, ep, (uint64_t)r, (uint64_t)lp, PPC_DRAW_WALK, w);
 		double4 prm = v.prm[p];
 		const double4 o = v.orient[p];
 		const double pol = v.polarity[p];
@@ -2125,7 +2489,7 @@ __global__ void k_divide_apply(view v, int cur)
 		v.scnt[c] = 0;
 		v.ncnt[c] = 0;
 		double ow[3] = { 0, 0, 0 };
-		ppc_unit_vector(DIMS, v.seed, ep, (uint64_t)r, (uint64_t)lp, PPC_DRAW_ORIENTATION, ow);
+		ppc_random_walk(DIMS, v.seed, ep, (uint64_t)r, (uint64_t)lp, PPC_DRAW_ORIENTATION, ow);
 		v.orient[c] = make_double4(ow[0], ow[1], ow[2], 0.0);
 
 		double4 pp = v.pos[cur][p];
@@ -2428,6 +2792,28 @@ static int staged_dispatch(ppc_state* s)
 	return PPC_OK;
 }
 
+template <int DIMS>
+static int flat_dispatch(ppc_state* s)
+{
+	const int opts = (s->params.virtual_wall_at_domain_edges ? FUSED_WALLS : 0)
+					 | ((s->has_springs && s->params.automated_spring_adhesion) ? FUSED_SPRINGS : 0)
+					 | (s->vel_dirty ? FUSED_VEL : 0);
+	const int b = blocks_for(s->total_cap, kFlatThreads);
+	cudaStream_t st = PPC_LAUNCH(s);
+	const int dyn = (int)sizeof(flat_smem);
+	if (s->precision == PPC_FP32_FORCE)
+	{
+		PPC_CUDA(cudaFuncSetAttribute(k_fused_flat<DIMS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+		pdl(k_fused_flat<DIMS, true>, b, kFlatThreads, dyn, st, s->v, s->cur, opts);
+	}
+	else
+	{
+		PPC_CUDA(cudaFuncSetAttribute(k_fused_flat<DIMS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+		pdl(k_fused_flat<DIMS, false>, b, kFlatThreads, dyn, st, s->v, s->cur, opts);
+	}
+	return PPC_OK;
+}
+
 int launch_fused(ppc_state* s)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
@@ -2447,7 +2833,13 @@ int launch_fused(ppc_state* s)
 		ev_end = s->prof_events[s->prof_used + 1];
 		s->prof_used += 2;
 	}
-	if (s->staged || s->coop)
+	if (s->flat)
+	{
+		int rc = s->dims == 1 ? flat_dispatch<1>(s) : (s->dims == 2 ? flat_dispatch<2>(s) : flat_dispatch<3>(s));
+		if (rc != PPC_OK)
+			return rc;
+	}
+	else if (s->staged || s->coop)
 	{
 		int rc = s->dims == 1 ? staged_dispatch<1>(s) : (s->dims == 2 ? staged_dispatch<2>(s) : staged_dispatch<3>(s));
 		if (rc != PPC_OK)

@@ -2,9 +2,8 @@
 // src/solver/host/solver_helper.h:82-101,160-182,250-287). One thread per agent: a motile agent
 // redraws its direction with probability dt / persistence_time, mixes it with its migration
 // bias direction, scales the result to its migration speed and adds it to its velocity. The
-// reference draws the direction from angles (cos/sin of a uniform angle, and a uniform z in
-// 3-D); here it comes from the counter-based unit vector of ppc_draws.h, uniform on the
-// circle/sphere like the reference's, and bit-identical on host and device.
+// direction is the reference's random walk (an angle, and z in 3-D) from counter-based draws,
+// with the sine and cosine of ppc_draws.h, bit-identical on host and device.
 
 #include <cuda_runtime.h>
 
@@ -31,8 +30,12 @@ __global__ void __launch_bounds__(kMotThreads) k_motility(view v, mot_fields m)
 	if (ppc_uniform(v.seed, m.epoch, (uint64_t)m.replicate, (uint64_t)i, PPC_DRAW_MOTILITY) < m.dt / m.persistence[i])
 	{
 		double walk[3] = { 0, 0, 0 };
-		const int wd = (DIMS == 3 && m.restrict2d[i]) ? 2 : DIMS;
-		ppc_unit_vector(wd, v.seed, m.epoch, (uint64_t)m.replicate, (uint64_t)i, PPC_DRAW_MOTILITY + 1u, walk);
+		// the reference's walk is planar for every 3-D agent (its bool
+		// parameter receives the restrict_to_2d array pointer,
+		// position_solver.cpp:131); per_agent reads each agent's flag instead
+		const bool planar = DIMS == 3 && (m.per_agent ? m.restrict2d[i] != 0 : true);
+		ppc_random_walk(planar ? 2 : DIMS, v.seed, m.epoch, (uint64_t)m.replicate, (uint64_t)i, PPC_DRAW_MOTILITY + 1u,
+						walk);
 		const double bias = m.bias[i];
 		for (int d = 0; d < DIMS; d++)
 			mv[d] = (1 - bias) * walk[d] + bias * m.direction[(int64_t)i * DIMS + d];

@@ -47,17 +47,21 @@ def _velocities(x, a):
     return out["velocities"].copy()
 
 
-@pytest.mark.parametrize("dims", [1, 2, 3])
-def test_motility_oracle_properties(dims):
+@pytest.mark.parametrize("dims,per_agent", [(1, False), (2, False), (3, False), (3, True)])
+def test_motility_oracle_properties(dims, per_agent):
     """Non-motile agents keep their velocity; a redraw gives a motility vector
-    of length migration_speed (the bias direction when fully biased; z = 0
-    when restricted to 2-D; a direction uniform on the sphere otherwise);
-    without a redraw the stored vector is added unchanged."""
+    of length migration_speed (the bias direction when fully biased). In 3-D
+    the reference's walk lies in the xy-plane for every agent (its bool
+    parameter receives the restrict_to_2d array pointer,
+    position_solver.cpp:131); with restrict_per_agent the flagged agents stay
+    in the plane and the others get directions uniform on the sphere. Without
+    a redraw the stored vector is added unchanged."""
     n = 300 if dims == 1 else 4000
     mesh, params, a = _agents(dims, n, seed=11)
     o = Oracle(mesh, params)
     o.upload(a)
     m = _fields(n, dims, seed=12, persistence=(0.001, 0.001))  # dt / p = 100: always redraw
+    m.restrict_per_agent = per_agent
     m["migration_bias"][: n // 2] = 0.0
     m["migration_bias"][n // 2:] = 1.0
     before = m.copy()
@@ -73,12 +77,16 @@ def test_motility_oracle_properties(dims):
     biased = motile & (np.arange(n) >= n // 2)
     want = m["migration_bias_direction"] * m["migration_speed"][:, None]
     np.testing.assert_allclose(m["motility_vector"][biased], want[biased], rtol=1e-13, atol=1e-15)
-    if dims == 3:
+    if dims == 3 and not per_agent:
+        unbiased = motile & (np.arange(n) < n // 2)
+        assert np.all(m["motility_vector"][unbiased][:, 2] == 0.0)
+    if dims == 3 and per_agent:
         flat = motile & (m["restrict_to_2d"] == 1) & (np.arange(n) < n // 2)
         assert np.all(m["motility_vector"][flat][:, 2] == 0.0)
         free = motile & (m["restrict_to_2d"] == 0) & (np.arange(n) < n // 2)
         unit = m["motility_vector"][free] / m["migration_speed"][free][:, None]
         assert np.all(np.abs(unit.mean(axis=0)) < 0.08)
+        assert np.count_nonzero(unit[:, 2]) == len(unit)
     if dims == 1:
         unbiased = motile & (np.arange(n) < n // 2)
         assert set(np.unique(np.sign(m["motility_vector"][unbiased, 0]))) == {-1.0, 1.0}
@@ -93,9 +101,40 @@ def test_motility_oracle_properties(dims):
     np.testing.assert_array_equal(v2[mot2], v1[mot2] + keep["motility_vector"][mot2])
 
 
+def test_motility_walk_is_the_references():
+    """A redrawn, unbiased motility vector is migration_speed times the
+    reference's random walk built from the agent's draws: theta = 2 pi u1 and,
+    in 3-D with restrict_per_agent, z = 2 u2 - 1 (solver_helper.h:160-165,
+    250-267); compared with libm's cos and sin to within 2 ulp."""
+    from oracle import oracle as orc
+    for dims, per_agent in ((2, False), (3, False), (3, True)):
+        n = 2000
+        mesh, params, a = _agents(dims, n, seed=41)
+        o = Oracle(mesh, params, seed=17)
+        o.upload(a)
+        m = _fields(n, dims, seed=42, persistence=(0.001, 0.001))
+        m.restrict_per_agent = per_agent
+        m["migration_bias"][:] = 0.0
+        m["migration_speed"][:] = 1.0
+        o.update_motility_fields(m)
+        for i in np.nonzero(m["is_motile"] == 1)[0][:400]:
+            u1 = orc.uniform(17, 0, 0, int(i), 2097152 + 1)
+            theta = u1 * (2 * np.pi)
+            want = np.zeros(dims)
+            if dims == 3 and per_agent and m["restrict_to_2d"][i] == 0:
+                z = orc.uniform(17, 0, 0, int(i), 2097152 + 2) * 2.0 - 1.0
+                r = np.sqrt(1 - z * z)
+                want[:] = (np.cos(theta) * r, np.sin(theta) * r, z)
+            else:
+                want[:2] = (np.cos(theta), np.sin(theta))
+            got = m["motility_vector"][i]
+            # unit vector scaled by 1 / length: a few ulp from the walk itself
+            np.testing.assert_allclose(got, want, rtol=0, atol=4e-16)
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("dims", [1, 2, 3])
-def test_motility_matches_oracle(dims):
+@pytest.mark.parametrize("dims,per_agent", [(1, False), (2, False), (3, False), (3, True)])
+def test_motility_matches_oracle(dims, per_agent):
     """The device's motility pass equals the oracle's bit for bit over three
     calls, and a fused step after it starts from the moved velocities."""
     from tests import gpu_util as gu
@@ -103,6 +142,7 @@ def test_motility_matches_oracle(dims):
     mesh, params, a = _agents(dims, n, seed=21 + dims)
     o, d = gu.make_pair(mesh, params, a, seed=5)
     mo, md = _fields(n, dims, seed=31), _fields(n, dims, seed=31)
+    mo.restrict_per_agent = md.restrict_per_agent = per_agent
     for _ in range(3):
         o.update_motility_fields(mo)
         d.update_motility_fields(md)
