@@ -52,8 +52,8 @@ WORKLOADS = {
 }
 
 
-ENSEMBLE = ("256 independent 3-D replicates, N_r log-uniform in [500, 50000], cube side 20 ceil(N_r^(1/3)) um, "
-            "one type, FP64, one batched state")
+ENSEMBLE = ("256 independent 3-D replicates, N_r log-uniform in [500, 50000], cube side (8000 N_r)^(1/3) um "
+            "(one agent per 8000 um^3), one type, FP64, one batched state")
 
 
 def make_workload(name):
@@ -130,9 +130,62 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def error_vs_oracle(name, steps=3):
+    """The device's FP64 step against the oracle's serial restatement of the
+    reference on the same workload, outside the timed region: `steps` steps
+    from the same state, then the largest relative difference of the step's
+    velocity (previous_velocities after update_positions) over agents, the
+    largest position difference, the number of agents whose neighbour list
+    (as the reference orders it) differs, and whether the voxel bins agree."""
+    from oracle.oracle import Oracle
+    from paraphysicell_b200.abi import AgentArrays
+    from paraphysicell_b200.device import Simulation
+
+    mesh, params, a = make_workload(name)
+    ph = phenotype_args(name)
+    o = Oracle(mesh, params, seed=1)
+    o.upload(a)
+    o.update_mechanics_mesh()
+    o.update_cell_neighbors()
+    d = Simulation(mesh, params, a.capacity, seed=1)
+    d.upload(a)
+    d.update_mechanics_mesh()
+    if ph:
+        o.step(steps, 1, ph[0], ph[1])
+        d.step_with_phenotype(steps, ph[0], ph[1])
+    else:
+        o.step(steps, 0, 0.0, 0.0)
+        d.step(steps)
+
+    def fetch(x):
+        out = AgentArrays(0, a.dims, a.ndefs, a.capacity, a.spring_capacity)
+        out.count = out.capacity
+        x.download(out)
+        return out
+
+    go, gd = fetch(o), fetch(d)
+    res = {"steps": steps, "agents": int(go.count), "same_count": go.count == gd.count,
+           "same_ids": bool(go.count == gd.count and np.array_equal(go["agent_ids"], gd["agent_ids"]))}
+    if res["same_ids"]:
+        vo, vd = go["previous_velocities"], gd["previous_velocities"]
+        scale = max(float(np.max(np.linalg.norm(vo, axis=1))), 1e-300)
+        res["max_rel_velocity_err_vs_oracle"] = float(np.max(np.linalg.norm(vd - vo, axis=1)) / scale)
+        res["max_abs_position_diff_um"] = float(np.max(np.abs(gd["positions"] - go["positions"])))
+        res["velocity_bit_exact"] = bool(np.array_equal(vo, vd))
+        no, nd = o.neighbors(), d.neighbors()
+        res["neighbor_mismatches"] = int(sum(1 for x, y in zip(no, nd) if x != y))
+        co, ao = o.mesh_bins()
+        cd, ad = d.mesh_bins()
+        res["bins_equal"] = bool(np.array_equal(co, cd) and np.array_equal(ao, ad))
+    d.close()
+    return res
+
+
 def cpu_baseline(name, budget_s=8.0, max_steps=400):
     """Times the oracle's OpenMP restatement of the reference on all host
-    threads for a bounded number of steps of the workload."""
+    threads for a bounded number of steps of the workload, then checks the
+    device's FP64 step against the oracle's serial form of the same
+    workload (error_vs_oracle)."""
     from oracle.oracle import Oracle
 
     threads = len(os.sched_getaffinity(0))
@@ -148,7 +201,8 @@ def cpu_baseline(name, budget_s=8.0, max_steps=400):
     t = o.time_steps(steps, threads, **kw)
     return {"value": a.count * steps / t, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{steps} steps of the full {a.count}-agent workload, OpenMP over {threads} threads, "
-                      f"std::chrono around the step loop ({t:.2f} s)"}
+                      f"std::chrono around the step loop ({t:.2f} s)",
+            "error_vs_oracle": error_vs_oracle(name)}
 
 
 def max_over_ranks(x, device):
@@ -265,6 +319,72 @@ def fp32_form(args, mesh, params, a, ph, flush):
             "velocity_rel_err_vs_fp64": err,
             "note": "pair forces in FP32 (Neumaier-compensated sums), exact FP64 neighbour predicate, FP64 "
                     "positions/binning/integration; same L2-flushed protocol as value"}
+
+
+def e2e_form(sim, host, step, K, world, mode):
+    """End to end through the C ABI: every step uploads positions and previous
+    velocities from pinned host rows, steps, and downloads positions, previous
+    velocities and pressure (the step's result: update_positions leaves the
+    step's velocity in previous_velocities and zeroes velocities,
+    src/solver/host/position_solver.cpp:481-504). Host clock and CUDA events
+    around the loop; the larger is reported."""
+    import torch
+
+    sim.set_host_transfer(mode)
+    sim.upload(host)
+    sim.update_mechanics_mesh()
+    up_fields = ("positions", "previous_velocities")
+    down_fields = ("positions", "previous_velocities", "simple_pressure")
+    d = host.dims
+    sim.download(host, fields=down_fields)
+    torch.cuda.synchronize()
+    counts = []
+    E = max(3, min(K, 50))
+    stream = torch.cuda.current_stream()
+    t0 = time.perf_counter()
+    for k in range(E):
+        sim.upload_fields(host, up_fields)
+        step(1)
+        sim.download(host, fields=down_fields)
+        counts.append(host.count)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    del stream
+    ms = wall * 1e3
+    n = float(sum(counts))
+    sim.set_host_transfer(0)
+    return {"value": n / (ms / 1e3) * world, "unit": UNIT,
+            "h2d_bytes_per_step": int(np.mean(counts) * 2 * 8 * d),
+            "d2h_bytes_per_step": int(np.mean(counts) * (2 * 8 * d + 8)),
+            "steps": E, "ms_per_step": ms / E,
+            "transfer": "copy engine + (un)pack kernels" if mode == 0 else "zero-copy (un)pack kernels"}
+
+
+def host_link_peak(h2d_bytes, d2h_bytes, reps=5):
+    """Plain pinned cudaMemcpyAsync of the e2e step's byte counts, one copy
+    per direction, best of `reps` (CUDA events): the host link's ceiling for
+    the e2e leg."""
+    import torch
+
+    out = {}
+    for name, nbytes, h2d in (("h2d_gbs", h2d_bytes, True), ("d2h_gbs", d2h_bytes, False)):
+        hbuf = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        dbuf = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+        best = None
+        for _ in range(reps + 1):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            if h2d:
+                dbuf.copy_(hbuf, non_blocking=True)
+            else:
+                hbuf.copy_(dbuf, non_blocking=True)
+            e1.record()
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        out[name] = nbytes / (best * 1e-3) / 1e9
+    out["note"] = "pinned cudaMemcpyAsync of the e2e step's bytes, one copy per direction, best of 5"
+    return out
 
 
 def fused_pass_time(sim, stream, step, flush, n):
@@ -452,7 +572,7 @@ def run_ours(args, rank, world, local_rank):
     import torch
 
     from paraphysicell_b200 import build
-    from paraphysicell_b200.abi import AgentArrays
+    from paraphysicell_b200.abi import PPC_TRANSFER_COPY_ENGINE, PPC_TRANSFER_ZERO_COPY, AgentArrays
     from paraphysicell_b200.device import PinnedPool, Simulation
 
     if not torch.cuda.is_available():
@@ -533,37 +653,16 @@ def run_ours(args, rank, world, local_rank):
     host = AgentArrays(n0, a.dims, a.ndefs, a.capacity, a.spring_capacity, pinned=pool)
     for k_, v_ in a.arrays.items():
         host.arrays[k_][:] = v_
-    sim.upload(host)
-    sim.update_mechanics_mesh()
-    # inputs the step reads from the host's copy: positions and the previous
-    # velocities (Adams-Bashforth); its result: new positions, the step's
-    # velocity (which update_positions moves into previous_velocities and
-    # clears from velocities, src/solver/host/position_solver.cpp:481-504)
-    # and pressure
-    up_fields = ("positions", "previous_velocities")
-    down_fields = ("positions", "previous_velocities", "simple_pressure")
-    d = a.dims
-    sim.download(host, fields=down_fields)
-    torch.cuda.synchronize()
-    e2e_counts = []
-    E = max(3, min(K, 50))
-    t0 = time.perf_counter()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for k in range(E):
-        sim.upload_fields(host, up_fields)
-        step(1)
-        sim.download(host, fields=down_fields)
-        e2e_counts.append(host.count)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - t0
-    e2e_ms = max(ev0.elapsed_time(ev1), wall * 1e3)
-    n_e2e = float(sum(e2e_counts))
-    e2e = {"value": n_e2e / (e2e_ms / 1e3) * world, "unit": UNIT,
-           "h2d_bytes_per_step": int(np.mean(e2e_counts) * 2 * 8 * d),
-           "d2h_bytes_per_step": int(np.mean(e2e_counts) * (2 * 8 * d + 8)),
-           "steps": E, "wall_s": wall}
+    e2e = e2e_form(sim, host, step, K, world, PPC_TRANSFER_COPY_ENGINE)
+    e2e["zero_copy"] = e2e_form(sim, host, step, K, world, PPC_TRANSFER_ZERO_COPY)["value"]
+    link = host_link_peak(e2e["h2d_bytes_per_step"], e2e["d2h_bytes_per_step"])
+    e2e["host_link"] = link
+    device_us = total_ms / K * 1e3
+    bound_us = (e2e["h2d_bytes_per_step"] / (link["h2d_gbs"] * 1e3) + e2e["d2h_bytes_per_step"] / (link["d2h_gbs"] * 1e3)
+                + device_us)
+    e2e["bound_us_per_step"] = bound_us
+    e2e["us_per_step"] = e2e["ms_per_step"] * 1e3
+    e2e["vs_bound"] = e2e["us_per_step"] / bound_us
     pool_free = pool.free
 
     if rank != 0:
@@ -581,7 +680,7 @@ def run_ours(args, rank, world, local_rank):
         peak = 6650.0
         peak_src = "fallback"
     spring_counts = a.arrays["spring_counts"][:n0]
-    per_agent = algorithmic_bytes_per_agent(d, a.ndefs, bool(params.virtual_wall_at_domain_edges),
+    per_agent = algorithmic_bytes_per_agent(a.dims, a.ndefs, bool(params.virtual_wall_at_domain_edges),
                                             float(spring_counts.mean()), float((spring_counts > 0).mean()))
     fused_avg_ms = fused_ms / max(fused_launches, 1)
     achieved = (per_agent * n0) / (fused_avg_ms / 1e3) / 1e9
@@ -617,6 +716,7 @@ def run_ours(args, rank, world, local_rank):
             line["forms"]["cell_cell_interactions"] = interactions_form(args)
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(args.workload)
+        line["error_vs_oracle"] = line["cpu_baseline"].pop("error_vs_oracle")
     print(json.dumps(line), flush=True)
     sim.close()
     del host

@@ -219,13 +219,17 @@ int ppc_upload(ppc_state* s, int32_t replicate, const ppc_agents* agents);
 int ppc_download(ppc_state* s, int32_t replicate, ppc_agents* agents);
 
 /* Overwrites only the fields whose pointers are non-NULL, keeping every other
- * device field; agents->count must equal the device count. This is the
- * per-step host sync of a caller that keeps cell_data authoritative on the
- * host. When the view carries only positions, velocities, previous
- * velocities, pressure and orientation, and the positions are bit-identical
- * to the resident ones, the mechanics mesh is kept (no rebuild before the
- * next step). Pinned host buffers (ppc_host_alloc) are read directly by the
- * device. Synchronises the stream. */
+ * device field; agents->count must equal the device count (read from the
+ * device unless a download or upload since the last count-changing call
+ * already told it). This is the per-step host sync of a caller that keeps
+ * cell_data authoritative on the host. When the view carries only positions,
+ * velocities, previous velocities, pressure and orientation (the kinematic
+ * fields), the device compares the positions with the resident ones and the
+ * next step rebuilds the mechanics mesh only if some differ; if in addition
+ * every one of those rows is page-locked (ppc_host_alloc), the call returns
+ * once the copies are queued, and the rows must stay unchanged until the next
+ * call that synchronises the stream (ppc_download, ppc_synchronize, ...).
+ * Otherwise it synchronises the stream. */
 int ppc_upload_fields(ppc_state* s, int32_t replicate, const ppc_agents* agents);
 
 int ppc_get_count(ppc_state* s, int32_t replicate, int32_t* count);
@@ -234,6 +238,18 @@ int ppc_get_count(ppc_state* s, int32_t replicate, int32_t* count);
  * kernel reported since the last check (e.g. PPC_ERR_NONFINITE from
  * ppc_step, which itself returns as soon as the work is queued). */
 int ppc_synchronize(ppc_state* s);
+
+/* How page-locked host rows (ppc_host_alloc) travel in ppc_upload,
+ * ppc_upload_fields and ppc_download (pageable rows always take the copy
+ * engine through a staging buffer). */
+enum ppc_host_transfer
+{
+	PPC_TRANSFER_COPY_ENGINE = 0, /* the default: DMA copies into a device staging
+									 buffer, then a (un)pack kernel */
+	PPC_TRANSFER_ZERO_COPY = 1	  /* the (un)pack kernels read and write the host rows
+									 over the bus */
+};
+int ppc_set_host_transfer(ppc_state* s, int32_t mode);
 
 /* Page-locked host memory for fast host <-> device copies (cudaHostAlloc);
  * NULL on failure. */
@@ -285,6 +301,17 @@ typedef struct ppc_motility
 	double* motility_vector;				 /* [count*dims], read and written */
 } ppc_motility;
 
+/* Makes the motility fields of replicate r resident on the device (rows in
+ * the state's agent order, `count` = the replicate's count): from then on
+ * they move with their agent when the container is compacted, a dividing
+ * agent's daughter copies them (phenotype_t::copy_to, src/phenotype.cpp:18-30),
+ * and ppc_update_motility_fields(s, r, NULL) uses them without any copy.
+ * Synchronises. */
+int ppc_upload_motility(ppc_state* s, int32_t r, const ppc_motility* fields);
+/* Copies the resident motility fields of replicate r to the host rows and
+ * sets fields->count. Synchronises. */
+int ppc_download_motility(ppc_state* s, int32_t r, ppc_motility* fields);
+
 /* position_solver::update_motility with motile agents (reference:
  * src/solver/host/position_solver.cpp:115-145,198-212,288-314,
  * solver_helper.h:82-101,160-182,250-287). A motile agent redraws its
@@ -294,7 +321,10 @@ typedef struct ppc_motility
  * it with migration_bias_direction by migration_bias, scales it to
  * migration_speed, and adds its motility vector to its resident velocity.
  * The reference's per-agent direction-update callbacks (chemotaxis) are not
- * run: the caller sets migration_bias_direction. Synchronizes. */
+ * run: the caller sets migration_bias_direction. With `fields` NULL the
+ * resident fields (ppc_upload_motility) are used and nothing is copied;
+ * otherwise `fields` is uploaded (and becomes the resident copy), and the
+ * motility vectors are written back to it. Synchronizes. */
 int ppc_update_motility_fields(ppc_state* s, int32_t replicate, ppc_motility* fields);
 
 /* position_solver::update_basement_membrane_interactions (reference: src/solver/host/position_solver.cpp:316-335). */
@@ -371,6 +401,22 @@ typedef struct ppc_interactions
 	double* internalized_substrates; /* [count*substrates] */
 } ppc_interactions;
 
+/* Makes the interaction fields of replicate r resident on the device (rows
+ * in the state's agent order): from then on they move with their agent when
+ * the container is compacted, and division treats them as cell::divide does
+ * (src/cell.cpp:108-163): the parent's damage and total attack time are
+ * cleared, every volume compartment is halved, the internalized substrates
+ * are halved when `compute_internalized_substrates` is non-zero (the
+ * reference's e.m.compute_internalized_substrates), and the daughter copies
+ * the parent's phenotype with a fresh state (no damage or attack time, one
+ * nucleus). ppc_update_cell_cell_interactions(s, r, NULL) then uses them with
+ * no copy. All replicates share one substrate count. Synchronises. */
+int ppc_upload_interactions(ppc_state* s, int32_t r, const ppc_interactions* fields,
+							int32_t compute_internalized_substrates);
+/* Copies the resident interaction fields of replicate r to the host rows and
+ * sets fields->count. Synchronises. */
+int ppc_download_interactions(ppc_state* s, int32_t r, ppc_interactions* fields);
+
 /* interactions_solver::update_cell_cell_interactions (reference:
  * src/solver/host/interactions_solver.cpp:143-265): each live agent walks its
  * neighbour list and, with one uniform draw per neighbour, may ingest a dead
@@ -379,10 +425,14 @@ typedef struct ppc_interactions
  * for a replicate is uniform(seed, n, replicate, i, PPC_DRAW_INTERACTION + k).
  * Ingested and fused neighbours get PPC_FLAG_TO_REMOVE; the ingesting or fusing
  * agent's volumes, geometry (and, when fusing, position) change in the
- * resident state and in `fields`, which is uploaded and written back. The
- * outcome is that of the reference run on one thread (agents in index order).
- * Uses the neighbour lists of the last ppc_update_cell_neighbors (rebuilt
- * here if a fused step ran since). Synchronizes. */
+ * resident state. With `fields` NULL the resident interaction fields
+ * (ppc_upload_interactions) are used and nothing is copied; otherwise
+ * `fields` is uploaded (becoming the resident copy) and written back after
+ * the call. The outcome is that of the reference run on one thread (agents in
+ * index order). Uses the neighbour lists of the last
+ * ppc_update_cell_neighbors (rebuilt here if a fused step ran since); if one
+ * of the replicate's lists was cut at the neighbour capacity, nothing changes
+ * and PPC_ERR_CAPACITY is returned. Synchronizes. */
 int ppc_update_cell_cell_interactions(ppc_state* s, int32_t replicate, ppc_interactions* fields);
 
 /* ---- fused step ----------------------------------------------------------- */

@@ -55,6 +55,10 @@ def lib():
                                       C.c_void_p]
         L.orc_uniform.argtypes = [C.c_uint64] * 5
         L.orc_uniform.restype = C.c_double
+        L.orc_upload_interactions.argtypes = [vp, C.POINTER(Interactions), C.c_int32]
+        L.orc_download_interactions.argtypes = [vp, C.POINTER(Interactions)]
+        L.orc_upload_motility.argtypes = [vp, C.POINTER(Motility)]
+        L.orc_download_motility.argtypes = [vp, C.POINTER(Motility)]
         L.orc_get_neighbors.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_int32]
         L.orc_get_mesh_bins.argtypes = [vp, C.c_void_p, C.c_void_p]
         L.orc_get_mesh_position.argtypes = [vp, C.c_void_p, C.c_void_p]
@@ -114,19 +118,47 @@ class Oracle:
             raise AttributeError(name)
         return lambda *a: fn(self.h, *a)
 
-    def update_motility_fields(self, fields):
-        """`fields` (abi.MotilityArrays): motility vectors are written back."""
-        st = fields.struct()
-        rc = self.L.orc_update_motility_fields(self.h, C.byref(st))
+    def update_motility_fields(self, fields=None):
+        """`fields` (abi.MotilityArrays): motility vectors are written back;
+        None uses the resident fields."""
+        st = fields.struct() if fields is not None else None
+        rc = self.L.orc_update_motility_fields(self.h, C.byref(st) if st is not None else None)
         if rc != 0:
             raise PPCError(rc, "orc_update_motility_fields")
 
-    def update_cell_cell_interactions(self, fields):
-        """`fields` (abi.InteractionArrays) is read and written back in place."""
-        st = fields.struct()
-        rc = self.L.orc_update_cell_cell_interactions(self.h, C.byref(st))
+    def update_cell_cell_interactions(self, fields=None):
+        """`fields` (abi.InteractionArrays) is read and written back in place;
+        None uses the resident fields."""
+        st = fields.struct() if fields is not None else None
+        rc = self.L.orc_update_cell_cell_interactions(self.h, C.byref(st) if st is not None else None)
         if rc != 0:
             raise PPCError(rc, "orc_update_cell_cell_interactions")
+
+    def upload_interactions(self, fields, compute_internalized_substrates=False):
+        rc = self.L.orc_upload_interactions(self.h, C.byref(fields.struct()), int(compute_internalized_substrates))
+        if rc != 0:
+            raise PPCError(rc, "orc_upload_interactions")
+
+    def download_interactions(self, fields):
+        st = fields.struct()
+        rc = self.L.orc_download_interactions(self.h, C.byref(st))
+        fields.count = st.count
+        if rc != 0:
+            raise PPCError(rc, "orc_download_interactions")
+        return fields
+
+    def upload_motility(self, fields):
+        rc = self.L.orc_upload_motility(self.h, C.byref(fields.struct()))
+        if rc != 0:
+            raise PPCError(rc, "orc_upload_motility")
+
+    def download_motility(self, fields):
+        st = fields.struct()
+        rc = self.L.orc_download_motility(self.h, C.byref(st))
+        fields.count = st.count
+        if rc != 0:
+            raise PPCError(rc, "orc_download_motility")
+        return fields
 
     def time_steps(self, steps, threads, with_phenotype=False, p_divide=0.0, p_death=0.0):
         return self.L.orc_time_steps(self.h, steps, threads, int(with_phenotype), p_divide, p_death)

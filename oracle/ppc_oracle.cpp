@@ -71,9 +71,87 @@ struct world
 	uint64_t ix_epoch = 0; // cell-cell interaction calls so far
 	uint64_t mot_epoch = 0; // motility calls so far
 	bool timed = false; // timed mode draws from thread_local mt19937
+	bool mot_per_agent = false; // resident motility: restrict_per_agent of the last upload
 
 	std::mutex removal_mtx;
 	std::shared_mutex division_mtx;
+
+	// Phenotype columns held beside the mechanics fields once a caller makes
+	// them resident (orc_upload_interactions / orc_upload_motility): they
+	// move with their agent on removal, and division halves, copies and
+	// resets them as cell::divide does (src/cell.cpp:108-163).
+	struct ix_store
+	{
+		bool on = false;
+		int S = 0;
+		bool halve_substrates = false; // e.m.compute_internalized_substrates
+		std::vector<uint8_t> dead;
+		std::vector<real_t> dead_phago, damage_rate, live_phago, attack, fusion, immuno, frac, damage, attack_time,
+			fluid, solid, cyto, cyto_fluid, cyto_solid, nuc_fluid, nuc_solid, fluid_fraction, c2n, target_cyto,
+			target_nuc, isub;
+		std::vector<int32_t> nuclei;
+
+		// f(column, values per agent) for every column
+		template <typename F>
+		void each(F&& f, int D)
+		{
+			f(dead, 1);
+			f(dead_phago, 1);
+			f(damage_rate, 1);
+			f(live_phago, D);
+			f(attack, D);
+			f(fusion, D);
+			f(immuno, D);
+			f(frac, S);
+			f(damage, 1);
+			f(attack_time, 1);
+			f(nuclei, 1);
+			for (auto* v : { &fluid, &solid, &cyto, &cyto_fluid, &cyto_solid, &nuc_fluid, &nuc_solid, &fluid_fraction,
+							 &c2n, &target_cyto, &target_nuc })
+				f(*v, 1);
+			f(isub, S);
+		}
+	} ix;
+
+	struct mot_store
+	{
+		bool on = false;
+		std::vector<uint8_t> motile, restrict2d;
+		std::vector<real_t> persistence, speed, bias, direction, vector;
+
+		template <typename F>
+		void each(F&& f, int dims)
+		{
+			f(motile, 1);
+			f(restrict2d, 1);
+			f(persistence, 1);
+			f(speed, 1);
+			f(bias, 1);
+			f(direction, dims);
+			f(vector, dims);
+		}
+	} mot;
+
+	// row `dst` of every resident column takes row `src`'s values
+	void copy_rows(index_t dst, index_t src)
+	{
+		auto cp = [&](auto& col, int width) {
+			std::copy_n(col.begin() + (size_t)src * width, width, col.begin() + (size_t)dst * width);
+		};
+		if (ix.on)
+			ix.each(cp, ndefs);
+		if (mot.on)
+			mot.each(cp, mesh.dims);
+	}
+
+	void grow_stores(index_t rows)
+	{
+		auto rs = [&](auto& col, int width) { col.resize((size_t)rows * width); };
+		if (ix.on)
+			ix.each(rs, ndefs);
+		if (mot.on)
+			mot.each(rs, mesh.dims);
+	}
 
 	void grow(index_t new_cap)
 	{
@@ -96,6 +174,7 @@ struct world
 		neighbors.resize(new_cap);
 		springs.resize(new_cap);
 		cap = new_cap;
+		grow_stores(new_cap);
 	}
 };
 
@@ -578,6 +657,7 @@ void remove_at(world& w, index_t i)
 	w.ids[i] = w.ids[last];
 	w.neighbors[i] = std::move(w.neighbors[last]);
 	w.springs[i] = std::move(w.springs[last]);
+	w.copy_rows(i, last);
 }
 
 // reference: containers_solver.cpp:58-68
@@ -668,6 +748,22 @@ void divide(world& w, index_t p, index_t c, uint64_t epoch)
 	w.nrad[p] = ppc_cbrt(w.nvol[p] / four_thirds_pi);
 	w.sarea[p] = 4.0 * M_PI * w.radius[p] * w.radius[p];
 
+	// resident phenotype columns: molecular.divide() (when substrates are
+	// computed), damage and total attack time cleared, volume.divide() on
+	// every compartment (data_storage_phenotype.cpp:530-560)
+	if (w.ix.on)
+	{
+		auto& x = w.ix;
+		if (x.halve_substrates)
+			for (int q = 0; q < x.S; q++)
+				x.isub[(size_t)p * x.S + q] *= 0.5;
+		x.damage[p] = 0;
+		x.attack_time[p] = 0;
+		for (auto* v : { &x.fluid, &x.solid, &x.cyto, &x.cyto_fluid, &x.cyto_solid, &x.nuc_fluid, &x.nuc_solid,
+						 &x.target_cyto, &x.target_nuc })
+			(*v)[p] *= 0.5;
+	}
+
 	// new_cell.copy_from(*this): phenotype and definition index; state
 	// (velocities, pressure, springs, is_movable) keeps the new-cell defaults
 	for (auto* v : { &w.radius, &w.rep, &w.adh, &w.rmad, &w.bm, &w.ec, &w.arate, &w.drate, &w.vol, &w.nvol, &w.nrad,
@@ -676,6 +772,16 @@ void divide(world& w, index_t p, index_t c, uint64_t epoch)
 	std::memcpy(w.aff.data() + (size_t)c * w.ndefs, w.aff.data() + (size_t)p * w.ndefs, sizeof(real_t) * w.ndefs);
 	w.maxatt[c] = w.maxatt[p];
 	w.def[c] = w.def[p];
+	// the resident phenotype columns are copied (phenotype_t::copy_to); the
+	// new cell's state keeps its constructor's defaults (no damage, no
+	// attack time, one nucleus: cell_state::set_defaults, src/cell.cpp:36-45)
+	w.copy_rows(c, p);
+	if (w.ix.on)
+	{
+		w.ix.damage[c] = 0;
+		w.ix.attack_time[c] = 0;
+		w.ix.nuclei[c] = 1;
+	}
 	// assign_orientation() of the new cell draws a fresh direction
 	ppc_random_walk(dims, w.seed, epoch, 0, (uint64_t)p, PPC_DRAW_ORIENTATION, w.orient.data() + (size_t)c * dims);
 
@@ -955,6 +1061,103 @@ void get(std::vector<T>& dst, const T* src, size_t count, T dflt)
 
 } // namespace
 
+// ppc_interactions / ppc_motility views of the resident columns
+ppc_interactions ix_view(world& w)
+{
+	auto& x = w.ix;
+	ppc_interactions v {};
+	v.count = w.n;
+	v.substrates = x.S;
+	v.dead = x.dead.data();
+	v.dead_phagocytosis_rate = x.dead_phago.data();
+	v.damage_rate = x.damage_rate.data();
+	v.live_phagocytosis_rates = x.live_phago.data();
+	v.attack_rates = x.attack.data();
+	v.fusion_rates = x.fusion.data();
+	v.immunogenicities = x.immuno.data();
+	v.fraction_transferred_when_ingested = x.frac.data();
+	v.damage = x.damage.data();
+	v.total_attack_time = x.attack_time.data();
+	v.number_of_nuclei = x.nuclei.data();
+	v.fluid = x.fluid.data();
+	v.solid = x.solid.data();
+	v.cytoplasmic = x.cyto.data();
+	v.cytoplasmic_fluid = x.cyto_fluid.data();
+	v.cytoplasmic_solid = x.cyto_solid.data();
+	v.nuclear_fluid = x.nuc_fluid.data();
+	v.nuclear_solid = x.nuc_solid.data();
+	v.fluid_fraction = x.fluid_fraction.data();
+	v.cytoplasmic_to_nuclear_ratio = x.c2n.data();
+	v.target_solid_cytoplasmic = x.target_cyto.data();
+	v.target_solid_nuclear = x.target_nuc.data();
+	v.internalized_substrates = x.isub.data();
+	return v;
+}
+
+ppc_motility mot_view(world& w, int32_t per_agent)
+{
+	auto& m = w.mot;
+	ppc_motility v {};
+	v.count = w.n;
+	v.restrict_per_agent = per_agent ? 1 : (w.mot_per_agent ? 1 : 0);
+	v.is_motile = m.motile.data();
+	v.restrict_to_2d = m.restrict2d.data();
+	v.persistence_time = m.persistence.data();
+	v.migration_speed = m.speed.data();
+	v.migration_bias = m.bias.data();
+	v.migration_bias_direction = m.direction.data();
+	v.motility_vector = m.vector.data();
+	return v;
+}
+
+template <typename T>
+void copy_col(T* dst, const T* src, size_t count)
+{
+	if (dst && src && count)
+		std::memcpy(dst, src, count * sizeof(T));
+}
+
+// every column of `src` into `dst` (rows 0..n-1)
+void copy_ix(const ppc_interactions& dst, const ppc_interactions& src, index_t n, index_t D)
+{
+	const size_t N = (size_t)n, S = (size_t)src.substrates;
+	copy_col(const_cast<uint8_t*>(dst.dead), src.dead, N);
+	copy_col(const_cast<real_t*>(dst.dead_phagocytosis_rate), src.dead_phagocytosis_rate, N);
+	copy_col(const_cast<real_t*>(dst.damage_rate), src.damage_rate, N);
+	copy_col(const_cast<real_t*>(dst.live_phagocytosis_rates), src.live_phagocytosis_rates, N * D);
+	copy_col(const_cast<real_t*>(dst.attack_rates), src.attack_rates, N * D);
+	copy_col(const_cast<real_t*>(dst.fusion_rates), src.fusion_rates, N * D);
+	copy_col(const_cast<real_t*>(dst.immunogenicities), src.immunogenicities, N * D);
+	copy_col(const_cast<real_t*>(dst.fraction_transferred_when_ingested), src.fraction_transferred_when_ingested, N * S);
+	copy_col(dst.damage, src.damage, N);
+	copy_col(dst.total_attack_time, src.total_attack_time, N);
+	copy_col(dst.number_of_nuclei, src.number_of_nuclei, N);
+	copy_col(dst.fluid, src.fluid, N);
+	copy_col(dst.solid, src.solid, N);
+	copy_col(dst.cytoplasmic, src.cytoplasmic, N);
+	copy_col(dst.cytoplasmic_fluid, src.cytoplasmic_fluid, N);
+	copy_col(dst.cytoplasmic_solid, src.cytoplasmic_solid, N);
+	copy_col(dst.nuclear_fluid, src.nuclear_fluid, N);
+	copy_col(dst.nuclear_solid, src.nuclear_solid, N);
+	copy_col(dst.fluid_fraction, src.fluid_fraction, N);
+	copy_col(dst.cytoplasmic_to_nuclear_ratio, src.cytoplasmic_to_nuclear_ratio, N);
+	copy_col(dst.target_solid_cytoplasmic, src.target_solid_cytoplasmic, N);
+	copy_col(dst.target_solid_nuclear, src.target_solid_nuclear, N);
+	copy_col(dst.internalized_substrates, src.internalized_substrates, N * S);
+}
+
+void copy_mot(const ppc_motility& dst, const ppc_motility& src, index_t n, int dims)
+{
+	const size_t N = (size_t)n;
+	copy_col(const_cast<uint8_t*>(dst.is_motile), src.is_motile, N);
+	copy_col(const_cast<uint8_t*>(dst.restrict_to_2d), src.restrict_to_2d, N);
+	copy_col(const_cast<real_t*>(dst.persistence_time), src.persistence_time, N);
+	copy_col(const_cast<real_t*>(dst.migration_speed), src.migration_speed, N);
+	copy_col(const_cast<real_t*>(dst.migration_bias), src.migration_bias, N);
+	copy_col(const_cast<real_t*>(dst.migration_bias_direction), src.migration_bias_direction, N * dims);
+	copy_col(dst.motility_vector, src.motility_vector, N * dims);
+}
+
 struct orc_state
 {
 	world w;
@@ -1092,18 +1295,84 @@ void orc_flag_by_draws(orc_state* s, double p_divide, double p_death) { flag_by_
 void orc_update_cell_container_for_phenotype(orc_state* s) { compact_phenotype(s->w); }
 int orc_update_motility_fields(orc_state* s, ppc_motility* f)
 {
-	if (!f || f->count != s->w.n)
+	if (!f)
+	{
+		if (!s->w.mot.on)
+			return PPC_ERR_ARG;
+		ppc_motility view = mot_view(s->w, 0);
+		motility(s->w, view);
+		return PPC_OK;
+	}
+	if (f->count != s->w.n)
 		return PPC_ERR_ARG;
 	motility(s->w, *f);
 	return PPC_OK;
 }
 int orc_update_cell_cell_interactions(orc_state* s, ppc_interactions* f)
 {
-	if (!f || f->count != s->w.n || f->substrates < 0)
+	if (!f)
+	{
+		if (!s->w.ix.on)
+			return PPC_ERR_ARG;
+		ppc_interactions view = ix_view(s->w);
+		cell_cell_interactions(s->w, view);
+		return PPC_OK;
+	}
+	if (f->count != s->w.n || f->substrates < 0)
 		return PPC_ERR_ARG;
 	cell_cell_interactions(s->w, *f);
 	return PPC_OK;
 }
+
+int orc_upload_interactions(orc_state* s, const ppc_interactions* f, int32_t compute_internalized_substrates)
+{
+	world& w = s->w;
+	if (!f || f->count != w.n || f->substrates < 0 || (w.ix.on && f->substrates != w.ix.S))
+		return PPC_ERR_ARG;
+	w.ix.on = true;
+	w.ix.S = f->substrates;
+	w.ix.halve_substrates = compute_internalized_substrates != 0;
+	w.grow_stores(std::max(w.cap, 1));
+	ppc_interactions v = ix_view(w);
+	copy_ix(v, *f, w.n, w.ndefs);
+	return PPC_OK;
+}
+
+int orc_download_interactions(orc_state* s, ppc_interactions* f)
+{
+	world& w = s->w;
+	if (!f || !w.ix.on || f->substrates != w.ix.S)
+		return PPC_ERR_ARG;
+	f->count = w.n;
+	ppc_interactions v = ix_view(w);
+	copy_ix(*f, v, w.n, w.ndefs);
+	return PPC_OK;
+}
+
+int orc_upload_motility(orc_state* s, const ppc_motility* f)
+{
+	world& w = s->w;
+	if (!f || f->count != w.n)
+		return PPC_ERR_ARG;
+	w.mot.on = true;
+	w.mot_per_agent = f->restrict_per_agent != 0;
+	w.grow_stores(std::max(w.cap, 1));
+	ppc_motility v = mot_view(w, f->restrict_per_agent);
+	copy_mot(v, *f, w.n, w.mesh.dims);
+	return PPC_OK;
+}
+
+int orc_download_motility(orc_state* s, ppc_motility* f)
+{
+	world& w = s->w;
+	if (!f || !w.mot.on)
+		return PPC_ERR_ARG;
+	f->count = w.n;
+	ppc_motility v = mot_view(w, 0);
+	copy_mot(*f, v, w.n, w.mesh.dims);
+	return PPC_OK;
+}
+
 
 void orc_step(orc_state* s, int32_t steps, int32_t with_phenotype, double p_divide, double p_death)
 {

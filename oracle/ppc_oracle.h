@@ -63,6 +63,13 @@ void orc_update_cell_container_for_phenotype(orc_state* s);
 int orc_update_cell_cell_interactions(orc_state* s, ppc_interactions* fields);
 /* position_solver::update_motility with motile agents */
 int orc_update_motility_fields(orc_state* s, ppc_motility* fields);
+/* resident phenotype columns (fields == NULL in the two calls above uses
+   them): they move with their agent on removal and division halves, copies
+   and resets them like cell::divide */
+int orc_upload_interactions(orc_state* s, const ppc_interactions* fields, int32_t compute_internalized_substrates);
+int orc_download_interactions(orc_state* s, ppc_interactions* fields);
+int orc_upload_motility(orc_state* s, const ppc_motility* fields);
+int orc_download_motility(orc_state* s, ppc_motility* fields);
 
 /* one mechanics step in simulator::simulate_mechanics order, `steps` times;
    with_phenotype adds flag_by_draws + the phenotype container update +

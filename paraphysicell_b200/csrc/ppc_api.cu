@@ -55,26 +55,69 @@ int alloc(ppc_state* s, T*& p, size_t count, bool zero = true)
 			return rc_;                                                                                                \
 	} while (0)
 
-int ensure_stage(ppc_state* s, size_t bytes)
+int launch_pending(ppc_state* s);
+
+// Staging arena of one transfer call: stage_reset at the start of the call,
+// then each field takes its own 256-byte aligned region, so the copy and the
+// (un)pack kernel of every field are queued without waiting for the previous
+// field's. Growing the arena waits for the queued work (which still reads the
+// old buffer) before freeing it.
+void stage_reset(ppc_state* s)
 {
-	if (bytes <= s->stage_bytes)
-		return PPC_OK;
-	if (s->stage)
+	s->stage_used = 0;
+	s->pending_unpacks.clear();
+	s->pending_copies.clear();
+}
+
+int stage_take(ppc_state* s, size_t bytes, void** out)
+{
+	size_t off = (s->stage_used + 255) & ~(size_t)255;
+	if (off + bytes > s->stage_bytes)
 	{
-		PPC_CUDA(cudaStreamSynchronize(s->stream));
-		PPC_CUDA(cudaFree(s->stage));
-		s->stage = nullptr;
+		const size_t want = std::max(off + bytes, 2 * s->stage_bytes);
+		if (s->stage)
+		{
+			// the deferred unpacks and copies still read the old buffer
+			PPC_TRY(launch_pending(s));
+			PPC_CUDA(cudaStreamSynchronize(s->stream));
+			PPC_CUDA(cudaFree(s->stage));
+			s->stage = nullptr;
+			s->stage_bytes = 0;
+		}
+		PPC_CUDA(cudaMalloc(&s->stage, want));
+		s->stage_bytes = want;
+		off = 0;
 	}
-	PPC_CUDA(cudaMalloc(&s->stage, bytes));
-	s->stage_bytes = bytes;
+	*out = static_cast<char*>(s->stage) + off;
+	s->stage_used = off + bytes;
 	return PPC_OK;
 }
 
-int device_errors(ppc_state* s)
+int flush_unpacks(ppc_state* s)
 {
-	int32_t err = 0;
-	PPC_CUDA(cudaMemcpyAsync(&err, s->v.err, sizeof err, cudaMemcpyDeviceToHost, s->stream));
-	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	for (const auto& u : s->pending_unpacks)
+		PPC_TRY(launch_unpack_vec(s, u.dev, u.src, u.r, u.n, u.changed));
+	s->pending_unpacks.clear();
+	return PPC_OK;
+}
+
+int flush_copies(ppc_state* s)
+{
+	for (const auto& c : s->pending_copies)
+		PPC_CUDA(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, s->stream));
+	s->pending_copies.clear();
+	return PPC_OK;
+}
+
+int launch_pending(ppc_state* s)
+{
+	PPC_TRY(flush_unpacks(s));
+	return flush_copies(s);
+}
+
+// status of the device error bits `err`; clears the device word when set
+int map_errors(ppc_state* s, int32_t err)
+{
 	if (err == 0)
 		return PPC_OK;
 	PPC_CUDA(cudaMemsetAsync(s->v.err, 0, sizeof(int32_t), s->stream));
@@ -94,6 +137,20 @@ int device_errors(ppc_state* s)
 	return fail(PPC_ERR_CUDA, "unknown device error");
 }
 
+int device_errors(ppc_state* s)
+{
+	PPC_CUDA(cudaMemcpyAsync(s->pinned_err, s->v.err, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	return map_errors(s, *s->pinned_err);
+}
+
+// the bins no longer match the positions: the next step rebuilds them
+void invalidate_bins(ppc_state* s)
+{
+	s->bins_valid = false;
+	s->bins_cond = false;
+}
+
 int finish(ppc_state* s)
 {
 	PPC_CUDA(cudaGetLastError());
@@ -109,16 +166,16 @@ int read_counters(ppc_state* s, std::vector<rep_counters>& c)
 	PPC_CUDA(cudaStreamSynchronize(s->stream));
 	for (int32_t k = 0; k < s->nreps; k++)
 		s->host_count[k] = c[k].count;
+	s->counts_known = true;
 	return PPC_OK;
 }
 
 int release_graph(ppc_state* s)
 {
-	if (s->graph)
-	{
-		cudaGraphExecDestroy(s->graph);
-		s->graph = nullptr;
-	}
+	for (auto& e : s->graphs)
+		if (e.exec)
+			cudaGraphExecDestroy(e.exec);
+	s->graphs.clear();
 	return PPC_OK;
 }
 
@@ -164,6 +221,10 @@ const void* mapped(const void* host)
 	return at.type == cudaMemoryTypeHost ? at.devicePointer : nullptr;
 }
 
+// Host rows (dims doubles per agent) into the double4 device rows. Pinned
+// host buffers go through the copy engine into the staging arena (or, in the
+// zero-copy transfer mode, are read by the unpack kernel over the bus);
+// pageable ones are staged by the copy call itself.
 int put_vec(ppc_state* s, double4* dev, const double* host, int32_t r, int32_t n, bool defaults,
 			int32_t* changed = nullptr)
 {
@@ -171,18 +232,19 @@ int put_vec(ppc_state* s, double4* dev, const double* host, int32_t r, int32_t n
 		return PPC_OK;
 	if (n == 0)
 		return PPC_OK;
-	if (host)
+	if (host && s->zero_copy)
 		if (const void* d = mapped(host))
 			return launch_unpack_vec(s, dev, static_cast<const double*>(d), r, n, changed);
 	const size_t bytes = (size_t)n * s->dims * sizeof(double);
-	PPC_TRY(ensure_stage(s, bytes));
+	void* st = nullptr;
+	PPC_TRY(stage_take(s, bytes, &st));
 	if (host)
-		PPC_CUDA(cudaMemcpyAsync(s->stage, host, bytes, cudaMemcpyHostToDevice, s->stream));
+		PPC_CUDA(cudaMemcpyAsync(st, host, bytes, cudaMemcpyHostToDevice, s->stream));
 	else
-		PPC_CUDA(cudaMemsetAsync(s->stage, 0, bytes, s->stream));
-	// the next field's copy into the stage is ordered after this kernel on
-	// the same stream; pageable sources are staged by the copy call itself
-	PPC_TRY(launch_unpack_vec(s, dev, static_cast<const double*>(s->stage), r, n, changed));
+		PPC_CUDA(cudaMemsetAsync(st, 0, bytes, s->stream));
+	// the unpack waits until the call's other copies are queued, so the copy
+	// engine moves the fields back to back
+	s->pending_unpacks.push_back({ dev, static_cast<const double*>(st), r, n, changed });
 	return PPC_OK;
 }
 
@@ -190,12 +252,15 @@ int get_vec(ppc_state* s, double* host, const double4* dev, int32_t r, int32_t n
 {
 	if (!host || n == 0)
 		return PPC_OK;
-	if (const void* d = mapped(host))
-		return launch_pack_vec(s, static_cast<double*>(const_cast<void*>(d)), dev, r, n);
+	if (s->zero_copy)
+		if (const void* d = mapped(host))
+			return launch_pack_vec(s, static_cast<double*>(const_cast<void*>(d)), dev, r, n);
 	const size_t bytes = (size_t)n * s->dims * sizeof(double);
-	PPC_TRY(ensure_stage(s, bytes));
-	PPC_TRY(launch_pack_vec(s, static_cast<double*>(s->stage), dev, r, n));
-	PPC_CUDA(cudaMemcpyAsync(host, s->stage, bytes, cudaMemcpyDeviceToHost, s->stream));
+	void* st = nullptr;
+	PPC_TRY(stage_take(s, bytes, &st));
+	PPC_TRY(launch_pack_vec(s, static_cast<double*>(st), dev, r, n));
+	// the copy waits until the call's other packs are queued
+	s->pending_copies.push_back({ host, st, bytes });
 	return PPC_OK;
 }
 
@@ -204,15 +269,17 @@ int put_prm(ppc_state* s, int field, const double* host, int32_t r, int32_t n, b
 	if ((!host && !defaults) || n == 0)
 		return PPC_OK;
 	const size_t bytes = (size_t)n * sizeof(double);
-	PPC_TRY(ensure_stage(s, bytes));
+	void* st = nullptr;
+	PPC_TRY(stage_take(s, bytes, &st));
 	if (host)
-		PPC_CUDA(cudaMemcpyAsync(s->stage, host, bytes, cudaMemcpyHostToDevice, s->stream));
+		PPC_CUDA(cudaMemcpyAsync(st, host, bytes, cudaMemcpyHostToDevice, s->stream));
 	else
 	{
 		std::vector<double> tmp(n, dflt);
-		PPC_CUDA(cudaMemcpyAsync(s->stage, tmp.data(), bytes, cudaMemcpyHostToDevice, s->stream));
+		PPC_CUDA(cudaMemcpyAsync(st, tmp.data(), bytes, cudaMemcpyHostToDevice, s->stream));
+		PPC_CUDA(cudaStreamSynchronize(s->stream)); // tmp leaves scope
 	}
-	PPC_TRY(launch_unpack_prm(s, field, static_cast<const double*>(s->stage), r, n));
+	PPC_TRY(launch_unpack_prm(s, field, static_cast<const double*>(st), r, n));
 	return PPC_OK;
 }
 
@@ -221,9 +288,10 @@ int get_prm(ppc_state* s, int field, double* host, int32_t r, int32_t n)
 	if (!host || n == 0)
 		return PPC_OK;
 	const size_t bytes = (size_t)n * sizeof(double);
-	PPC_TRY(ensure_stage(s, bytes));
-	PPC_TRY(launch_pack_prm(s, field, static_cast<double*>(s->stage), r, n));
-	PPC_CUDA(cudaMemcpyAsync(host, s->stage, bytes, cudaMemcpyDeviceToHost, s->stream));
+	void* st = nullptr;
+	PPC_TRY(stage_take(s, bytes, &st));
+	PPC_TRY(launch_pack_prm(s, field, static_cast<double*>(st), r, n));
+	PPC_CUDA(cudaMemcpyAsync(host, st, bytes, cudaMemcpyDeviceToHost, s->stream));
 	return PPC_OK;
 }
 
@@ -253,7 +321,7 @@ int transfer_in(ppc_state* s, int32_t r, const ppc_agents* a, bool defaults)
 	const int32_t base = R.base;
 	const int D = s->ndefs;
 	view& v = s->v;
-	PPC_TRY(release_graph(s));
+	stage_reset(s);
 	if (a->cell_definition_indices)
 		for (int32_t i = 0; i < n; i++)
 			if (a->cell_definition_indices[i] < 0 || a->cell_definition_indices[i] >= D)
@@ -262,13 +330,13 @@ int transfer_in(ppc_state* s, int32_t r, const ppc_agents* a, bool defaults)
 	// an upload of kinematic fields only (positions, velocities, previous
 	// velocities, pressure, orientation) keeps the mesh when the positions it
 	// brings are bit-identical to the resident ones
+	// (pos_changed is zero after every rebuild: k_bin_scatter clears it)
 	const bool kinematic = !defaults && only_kinematic(a);
-	if (kinematic && a->positions)
-		PPC_CUDA(cudaMemsetAsync(v.pos_changed, 0, sizeof(int32_t), s->stream));
 	PPC_TRY(put_vec(s, v.pos[s->cur], a->positions, r, n, defaults, kinematic ? v.pos_changed : nullptr));
 	PPC_TRY(put_vec(s, v.vel, a->velocities, r, n, defaults));
 	PPC_TRY(put_vec(s, v.vprev, a->previous_velocities, r, n, defaults));
 	PPC_TRY(put_vec(s, v.orient, a->orientation, r, n, defaults));
+	PPC_TRY(flush_unpacks(s));
 	PPC_TRY(put_prm(s, 0, a->radius, r, n, defaults, kRadius));
 	PPC_TRY(put_prm(s, 1, a->cell_cell_repulsion_strength, r, n, defaults, 10.0));
 	PPC_TRY(put_prm(s, 2, a->cell_cell_adhesion_strength, r, n, defaults, 0.4));
@@ -328,9 +396,10 @@ int transfer_in(ppc_state* s, int32_t r, const ppc_agents* a, bool defaults)
 		if (any)
 		{
 			const size_t bytes = (size_t)n * a->spring_capacity * sizeof(int32_t);
-			PPC_TRY(ensure_stage(s, bytes));
-			PPC_CUDA(cudaMemcpyAsync(s->stage, a->springs, bytes, cudaMemcpyHostToDevice, s->stream));
-			PPC_TRY(launch_springs_local(s, r, n, static_cast<int32_t*>(s->stage), a->spring_capacity, 1));
+			void* st = nullptr;
+			PPC_TRY(stage_take(s, bytes, &st));
+			PPC_CUDA(cudaMemcpyAsync(st, a->springs, bytes, cudaMemcpyHostToDevice, s->stream));
+			PPC_TRY(launch_springs_local(s, r, n, static_cast<int32_t*>(st), a->spring_capacity, 1));
 			PPC_CUDA(cudaStreamSynchronize(s->stream));
 		}
 		s->has_springs = s->has_springs || any;
@@ -356,15 +425,27 @@ int transfer_in(ppc_state* s, int32_t r, const ppc_agents* a, bool defaults)
 				s->rates_nonzero = rate[i] != 0.0;
 	if (kinematic)
 	{
-		*s->pinned_flag = 0;
-		if (a->positions)
-			PPC_CUDA(cudaMemcpyAsync(s->pinned_flag, v.pos_changed, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
-		PPC_CUDA(cudaStreamSynchronize(s->stream));
-		if (*s->pinned_flag)
-			s->bins_valid = false; // the slots still hold the same agents
+		// the slots still hold the same agents; whether the positions moved is
+		// known on the device only: the next rebuild runs there if they did
+		if (a->positions && s->bins_valid)
+		{
+			s->bins_valid = false;
+			s->bins_cond = true;
+		}
+		// page-locked rows are copied by the queued DMA, so the call returns
+		// at once and the next step queues behind the copies; pageable rows
+		// are waited for, so the caller may reuse them on return
+		bool pinned = true;
+		for (const void* p : { (const void*)a->positions, (const void*)a->velocities,
+							   (const void*)a->previous_velocities, (const void*)a->simple_pressure,
+							   (const void*)a->orientation })
+			if (p && !mapped(p))
+				pinned = false;
+		if (!pinned)
+			PPC_CUDA(cudaStreamSynchronize(s->stream));
 		return PPC_OK;
 	}
-	s->bins_valid = false;
+	invalidate_bins(s);
 	// slots were rewritten: the next rebuild counts by slot
 	PPC_CUDA(cudaMemsetAsync(v.order_valid, 0, sizeof(int32_t), s->stream));
 	PPC_CUDA(cudaStreamSynchronize(s->stream));
@@ -382,6 +463,7 @@ int copy_out(ppc_state* s, int32_t r, ppc_agents* a, int32_t n)
 	PPC_TRY(get_vec(s, a->velocities, v.vel, r, n));
 	PPC_TRY(get_vec(s, a->previous_velocities, v.vprev, r, n));
 	PPC_TRY(get_vec(s, a->orientation, v.orient, r, n));
+	PPC_TRY(flush_copies(s));
 	PPC_TRY(get_prm(s, 0, a->radius, r, n));
 	PPC_TRY(get_prm(s, 1, a->cell_cell_repulsion_strength, r, n));
 	PPC_TRY(get_prm(s, 2, a->cell_cell_adhesion_strength, r, n));
@@ -408,17 +490,20 @@ int copy_out(ppc_state* s, int32_t r, ppc_agents* a, int32_t n)
 int transfer_out(ppc_state* s, int32_t r, ppc_agents* a)
 {
 	// Copies as many agents as this host last saw in the replicate, together
-	// with the counters, and synchronises once; if the device count turns out
-	// larger (divisions since), the copies are redone with the true count.
-	// Rows between the device count and the previous count, within the host
-	// capacity, may be overwritten.
+	// with the counters and the device error word, and synchronises once; if
+	// the device count turns out larger (divisions since), the copies are
+	// redone with the true count. Rows between the device count and the
+	// previous count, within the host capacity, may be overwritten.
+	stage_reset(s);
 	const int32_t guess = std::max(0, std::min(s->host_count[r], std::min(a->capacity, s->reps[r].cap)));
-	PPC_CUDA(cudaMemcpyAsync(s->pinned_ctr, s->v.ctr, sizeof(rep_counters) * s->nreps, cudaMemcpyDeviceToHost,
-							 s->stream));
+	PPC_CUDA(cudaMemcpyAsync(s->pinned_ctr, s->v.ctr, sizeof(rep_counters) * (s->nreps + 1), cudaMemcpyDeviceToHost,
+							 s->stream)); // the counters and the error word
 	PPC_TRY(copy_out(s, r, a, guess));
 	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	PPC_TRY(map_errors(s, *s->pinned_err));
 	for (int32_t k = 0; k < s->nreps; k++)
 		s->host_count[k] = s->pinned_ctr[k].count;
+	s->counts_known = true;
 	const int32_t n = s->host_count[r];
 	a->count = n;
 	if (n > a->capacity)
@@ -439,12 +524,14 @@ int transfer_out(ppc_state* s, int32_t r, ppc_agents* a)
 		if (a->springs && n)
 		{
 			const size_t bytes = (size_t)n * a->spring_capacity * sizeof(int32_t);
-			PPC_TRY(ensure_stage(s, bytes));
-			PPC_TRY(launch_springs_local(s, r, n, static_cast<int32_t*>(s->stage), a->spring_capacity, 0));
-			PPC_CUDA(cudaMemcpyAsync(a->springs, s->stage, bytes, cudaMemcpyDeviceToHost, s->stream));
+			void* st = nullptr;
+			PPC_TRY(stage_take(s, bytes, &st));
+			PPC_TRY(launch_springs_local(s, r, n, static_cast<int32_t*>(st), a->spring_capacity, 0));
+			PPC_CUDA(cudaMemcpyAsync(a->springs, st, bytes, cudaMemcpyDeviceToHost, s->stream));
 		}
 	}
-	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	if (n > guess || a->spring_counts)
+		PPC_CUDA(cudaStreamSynchronize(s->stream));
 	return PPC_OK;
 }
 
@@ -452,8 +539,9 @@ int ensure_bins(ppc_state* s)
 {
 	if (!s->bins_valid)
 	{
-		PPC_TRY(launch_bin(s));
+		PPC_TRY(launch_bin(s, s->bins_cond));
 		s->bins_valid = true;
+		s->bins_cond = false;
 	}
 	return PPC_OK;
 }
@@ -487,7 +575,7 @@ int enqueue_step(ppc_state* s, bool phenotype, double p_divide, double p_death)
 		PPC_TRY(launch_mark_remove(s));
 		PPC_TRY(launch_compact(s, true, true));
 	}
-	PPC_TRY(launch_bin(s));
+	PPC_TRY(launch_bin(s, false));
 	return PPC_OK;
 }
 
@@ -513,24 +601,90 @@ int enqueue_step_separate(ppc_state* s, bool phenotype, double p_divide, double 
 		PPC_TRY(launch_mark_remove(s));
 		PPC_TRY(launch_compact(s, true, true));
 	}
-	PPC_TRY(launch_bin(s));
+	PPC_TRY(launch_bin(s, false));
 	return PPC_OK;
 }
 
-constexpr int kGraphSteps = 10; // even, so a replay leaves the position buffer parity unchanged
+constexpr int kGraphSteps = 10; // steps per replay of a long run's graph
+constexpr size_t kGraphCache = 8; // captured graphs kept per state
+
+// Replays `k` fused steps from a captured graph, capturing it on first use.
+// A graph is keyed by everything its kernels' variants and arguments depend
+// on: the step count, the position buffer it starts from, the phenotype
+// update and its probabilities, springs, and whether it starts with the
+// conditional mesh rebuild an upload of positions leaves for the device.
+int replay_steps(ppc_state* s, int k, bool phenotype, double p_divide, double p_death, bool lead_bin)
+{
+	graph_entry* hit = nullptr;
+	for (auto& e : s->graphs)
+		if (e.steps == k && e.cur == s->cur && e.phenotype == phenotype && e.pdiv == p_divide && e.pdeath == p_death
+			&& e.lead_bin == lead_bin && e.springs == s->has_springs)
+			hit = &e;
+	if (!hit)
+	{
+		if (s->graphs.size() >= kGraphCache)
+			PPC_TRY(release_graph(s));
+		graph_entry e {};
+		e.steps = k;
+		e.cur = s->cur;
+		e.phenotype = phenotype;
+		e.pdiv = p_divide;
+		e.pdeath = p_death;
+		e.lead_bin = lead_bin;
+		e.springs = s->has_springs;
+		const int cur0 = s->cur;
+		const int64_t l0 = s->launches;
+		cudaGraph_t g = nullptr;
+		PPC_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+		int rc = lead_bin ? launch_bin(s, true) : PPC_OK;
+		for (int q = 0; q < k && rc == PPC_OK; q++)
+			rc = enqueue_step(s, phenotype, p_divide, p_death);
+		cudaError_t ec = cudaStreamEndCapture(s->stream, &g);
+		s->cur = cur0;
+		if (rc != PPC_OK)
+		{
+			if (g)
+				cudaGraphDestroy(g);
+			return rc;
+		}
+		if (ec != cudaSuccess)
+			return cuda_fail(ec, "cudaStreamEndCapture");
+		ec = cudaGraphInstantiate(&e.exec, g, 0);
+		cudaGraphDestroy(g);
+		if (ec != cudaSuccess)
+			return cuda_fail(ec, "cudaGraphInstantiate");
+		e.launches = s->launches - l0;
+		s->launches = l0;
+		s->graphs.push_back(e);
+		hit = &s->graphs.back();
+	}
+	PPC_CUDA(cudaGraphLaunch(hit->exec, s->stream));
+	s->launches += hit->launches;
+	s->cur ^= k & 1;
+	s->vel_dirty = false;
+	return PPC_OK;
+}
 
 int run_steps(ppc_state* s, int32_t steps, bool phenotype, double p_divide, double p_death)
 {
 	if (steps < 0)
 		return fail(PPC_ERR_ARG, "negative step count");
-	PPC_TRY(ensure_bins(s));
+	if (steps > 0)
+		s->counts_known = false; // compaction and division change the counts
+	const bool graphs = s->use_graphs && !s->profiling;
+	// a rebuild the device decides on (after an upload of positions) rides
+	// at the head of the first replayed graph
+	bool lead_bin = graphs && steps > 0 && !s->bins_valid && s->bins_cond && !s->vel_dirty && !stochastic_springs(s);
+	if (!lead_bin)
+		PPC_TRY(ensure_bins(s));
+	s->bins_valid = true;
+	s->bins_cond = false;
 	if (stochastic_springs(s))
 	{
 		// non-zero attachment or detachment rates
 		s->has_springs = true;
 		for (int32_t k = 0; k < steps; k++)
 			PPC_TRY(enqueue_step_separate(s, phenotype, p_divide, p_death));
-		s->bins_valid = true;
 		s->lists_stale = steps > 0 || s->lists_stale;
 		return PPC_OK;
 	}
@@ -541,42 +695,19 @@ int run_steps(ppc_state* s, int32_t steps, bool phenotype, double p_divide, doub
 		PPC_TRY(enqueue_step(s, phenotype, p_divide, p_death));
 		done++;
 	}
-	if (s->use_graphs && !s->profiling && steps - done >= kGraphSteps)
+	if (graphs)
 	{
-		const bool reuse = s->graph && s->graph_cur == s->cur && s->graph_phenotype == phenotype
-						   && s->graph_pdiv == p_divide && s->graph_pdeath == p_death;
-		if (!reuse)
-		{
-			PPC_TRY(release_graph(s));
-			const int cur0 = s->cur;
-			const int64_t l0 = s->launches;
-			cudaGraph_t g = nullptr;
-			PPC_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-			int rc = PPC_OK;
-			for (int k = 0; k < kGraphSteps && rc == PPC_OK; k++)
-				rc = enqueue_step(s, phenotype, p_divide, p_death);
-			cudaError_t ec = cudaStreamEndCapture(s->stream, &g);
-			if (rc != PPC_OK)
-				return rc;
-			if (ec != cudaSuccess)
-				return cuda_fail(ec, "cudaStreamEndCapture");
-			ec = cudaGraphInstantiate(&s->graph, g, 0);
-			cudaGraphDestroy(g);
-			if (ec != cudaSuccess)
-				return cuda_fail(ec, "cudaGraphInstantiate");
-			s->graph_launches = s->launches - l0;
-			s->launches = l0;
-			s->cur = cur0;
-			s->graph_cur = cur0;
-			s->graph_phenotype = phenotype;
-			s->graph_pdiv = p_divide;
-			s->graph_pdeath = p_death;
-		}
 		while (steps - done >= kGraphSteps)
 		{
-			PPC_CUDA(cudaGraphLaunch(s->graph, s->stream));
-			s->launches += s->graph_launches;
+			PPC_TRY(replay_steps(s, kGraphSteps, phenotype, p_divide, p_death, lead_bin));
+			lead_bin = false;
 			done += kGraphSteps;
+		}
+		while (done < steps)
+		{
+			PPC_TRY(replay_steps(s, 1, phenotype, p_divide, p_death, lead_bin));
+			lead_bin = false;
+			done++;
 		}
 	}
 	while (done < steps)
@@ -584,7 +715,6 @@ int run_steps(ppc_state* s, int32_t steps, bool phenotype, double p_divide, doub
 		PPC_TRY(enqueue_step(s, phenotype, p_divide, p_death));
 		done++;
 	}
-	s->bins_valid = true;
 	s->lists_stale = steps > 0 || s->lists_stale;
 	return PPC_OK;
 }
@@ -703,8 +833,10 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	rep_info* reps = nullptr;
 	try_(alloc(s, reps, replicates));
 	v.reps = reps;
-	try_(alloc(s, v.ctr, replicates));
-	try_(alloc(s, v.err, 1));
+	// the error word sits right after the counters, so one copy brings both
+	try_(alloc(s, v.ctr, (size_t)replicates + 1));
+	if (rc == PPC_OK)
+		v.err = reinterpret_cast<int32_t*>(v.ctr + replicates);
 	try_(alloc(s, v.cursor, 1));
 	v.nvox = (int32_t)vox;
 	v.ntiles = (int32_t)((vox + 4095) / 4096);
@@ -749,6 +881,7 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.sdel, C * s->scap));
 	try_(alloc(s, v.first_end, C));
 	try_(alloc(s, v.pos_changed, 1));
+	try_(alloc(s, v.bin_active, 1));
 	if (rc == PPC_OK && cudaMemset(v.first_end, 0x7f, sizeof(int32_t) * std::max<size_t>(C, 1)) != cudaSuccess)
 		rc = fail(PPC_ERR_CUDA, "cudaMemset failed");
 	if (rc == PPC_OK && cudaMemset(v.move_src, 0xff, sizeof(int32_t) * std::max<size_t>(C, 1)) != cudaSuccess)
@@ -775,7 +908,7 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 			   != cudaSuccess)
 		rc = fail(PPC_ERR_CUDA, "cudaHostAlloc failed");
 	if (rc == PPC_OK)
-		s->pinned_flag = reinterpret_cast<int32_t*>(s->pinned_ctr + replicates);
+		s->pinned_err = reinterpret_cast<int32_t*>(s->pinned_ctr + replicates);
 	if (rc == PPC_OK)
 	{
 		std::vector<int32_t> rid(C, 0);
@@ -842,7 +975,7 @@ int ppc_set_precision(ppc_state* s, int32_t precision)
 	PPC_CUDA(cudaStreamSynchronize(s->stream));
 	s->precision = precision;
 	s->v.f32 = precision == PPC_FP32_FORCE ? 1 : 0;
-	s->bins_valid = false; // the single-precision copies are written by the binning
+	invalidate_bins(s); // the single-precision copies are written by the binning
 	release_graph(s);
 	return PPC_OK;
 }
@@ -871,6 +1004,14 @@ int ppc_set_launch_shape(ppc_state* s, int32_t tile_edge, int32_t threads, int32
 	s->coop = tile_edge == 0 || tile_edge == -2;
 	s->tile_threads = threads;
 	s->tile_smem = smem_bytes;
+	return PPC_OK;
+}
+
+int ppc_set_host_transfer(ppc_state* s, int32_t mode)
+{
+	if (!s || (mode != PPC_TRANSFER_COPY_ENGINE && mode != PPC_TRANSFER_ZERO_COPY))
+		return fail(PPC_ERR_ARG, "mode must be PPC_TRANSFER_COPY_ENGINE or PPC_TRANSFER_ZERO_COPY");
+	s->zero_copy = mode == PPC_TRANSFER_ZERO_COPY;
 	return PPC_OK;
 }
 
@@ -921,9 +1062,14 @@ int ppc_upload_fields(ppc_state* s, int32_t r, const ppc_agents* a)
 {
 	if (!valid(s, r) || !a)
 		return fail(PPC_ERR_ARG, "invalid state, replicate or agents");
-	std::vector<rep_counters> c;
-	PPC_TRY(read_counters(s, c));
-	if (a->count != c[r].count)
+	// the count is read from the device unless no count-changing work was
+	// queued since it was last read (a download, typically)
+	if (!s->counts_known)
+	{
+		std::vector<rep_counters> c;
+		PPC_TRY(read_counters(s, c));
+	}
+	if (a->count != s->host_count[r])
 		return fail(PPC_ERR_ARG, "count differs from the device count");
 	return transfer_in(s, r, a, false);
 }
@@ -932,8 +1078,8 @@ int ppc_download(ppc_state* s, int32_t r, ppc_agents* a)
 {
 	if (!valid(s, r) || !a)
 		return fail(PPC_ERR_ARG, "invalid state, replicate or agents");
-	PPC_TRY(finish(s));
-	return transfer_out(s, r, a);
+	PPC_CUDA(cudaGetLastError());
+	return transfer_out(s, r, a); // reads the device error word with the counters
 }
 
 int ppc_get_count(ppc_state* s, int32_t r, int32_t* count)
@@ -984,8 +1130,9 @@ int ppc_update_mechanics_mesh(ppc_state* s)
 {
 	if (!s)
 		return fail(PPC_ERR_ARG, "null state");
-	PPC_TRY(launch_bin(s));
+	PPC_TRY(launch_bin(s, false));
 	s->bins_valid = true;
+	s->bins_cond = false;
 	return finish(s);
 }
 
@@ -1046,7 +1193,7 @@ int ppc_update_positions(ppc_state* s)
 	if (!s)
 		return fail(PPC_ERR_ARG, "null state");
 	PPC_TRY(launch_positions(s));
-	s->bins_valid = false;
+	invalidate_bins(s);
 	return finish(s);
 }
 
@@ -1054,10 +1201,11 @@ int ppc_update_cell_container_for_mechanics(ppc_state* s)
 {
 	if (!s)
 		return fail(PPC_ERR_ARG, "null state");
+	s->counts_known = false;
 	PPC_TRY(ensure_lists(s));
 	PPC_TRY(launch_mark_remove(s));
 	PPC_TRY(launch_compact(s, false));
-	s->bins_valid = false;
+	invalidate_bins(s);
 	return finish(s);
 }
 
@@ -1065,11 +1213,12 @@ int ppc_update_cell_container_for_phenotype(ppc_state* s)
 {
 	if (!s)
 		return fail(PPC_ERR_ARG, "null state");
+	s->counts_known = false;
 	PPC_TRY(ensure_lists(s));
 	PPC_TRY(launch_divide(s));
 	PPC_TRY(launch_mark_remove(s));
 	PPC_TRY(launch_compact(s, true));
-	s->bins_valid = false;
+	invalidate_bins(s);
 	return finish(s);
 }
 
@@ -1099,197 +1248,378 @@ static int ensure_field_scratch(ppc_state* s, size_t bytes)
 	return PPC_OK;
 }
 
-int ppc_update_motility_fields(ppc_state* s, int32_t r, ppc_motility* f)
+} // extern "C"
+
+namespace ppc {
+namespace {
+
+// one resident column: its device base, the caller's host rows, bytes per
+// value and values per agent
+struct column
 {
-	if (!valid(s, r) || !f)
-		return fail(PPC_ERR_ARG, "invalid arguments");
+	void* dev;
+	const void* host;
+	size_t elem;
+	size_t width;
+};
+
+// the interaction columns of `x` paired with the host rows of `f`, in one order
+std::vector<column> ix_column_list(const ix_columns& x, const ppc_interactions* f, int D)
+{
+	const size_t S = (size_t)x.S, d = (size_t)D, e = sizeof(double);
+	return {
+		{ x.dead, f ? f->dead : nullptr, 1, 1 },
+		{ x.dead_phago, f ? f->dead_phagocytosis_rate : nullptr, e, 1 },
+		{ x.damage_rate, f ? f->damage_rate : nullptr, e, 1 },
+		{ x.live_phago, f ? f->live_phagocytosis_rates : nullptr, e, d },
+		{ x.attack, f ? f->attack_rates : nullptr, e, d },
+		{ x.fusion, f ? f->fusion_rates : nullptr, e, d },
+		{ x.immuno, f ? f->immunogenicities : nullptr, e, d },
+		{ x.frac, f ? f->fraction_transferred_when_ingested : nullptr, e, S },
+		{ x.damage, f ? f->damage : nullptr, e, 1 },
+		{ x.attack_time, f ? f->total_attack_time : nullptr, e, 1 },
+		{ x.nuclei, f ? f->number_of_nuclei : nullptr, sizeof(int32_t), 1 },
+		{ x.fluid, f ? f->fluid : nullptr, e, 1 },
+		{ x.solid, f ? f->solid : nullptr, e, 1 },
+		{ x.cyto, f ? f->cytoplasmic : nullptr, e, 1 },
+		{ x.cyto_fluid, f ? f->cytoplasmic_fluid : nullptr, e, 1 },
+		{ x.cyto_solid, f ? f->cytoplasmic_solid : nullptr, e, 1 },
+		{ x.nuc_fluid, f ? f->nuclear_fluid : nullptr, e, 1 },
+		{ x.nuc_solid, f ? f->nuclear_solid : nullptr, e, 1 },
+		{ x.fluid_fraction, f ? f->fluid_fraction : nullptr, e, 1 },
+		{ x.c2n, f ? f->cytoplasmic_to_nuclear_ratio : nullptr, e, 1 },
+		{ x.target_cyto, f ? f->target_solid_cytoplasmic : nullptr, e, 1 },
+		{ x.target_nuc, f ? f->target_solid_nuclear : nullptr, e, 1 },
+		{ x.isub, f ? f->internalized_substrates : nullptr, e, S },
+	};
+}
+
+std::vector<column> mot_column_list(const mot_columns& m, const ppc_motility* f, int dims)
+{
+	const size_t e = sizeof(double), d = (size_t)dims;
+	return {
+		{ m.motile, f ? f->is_motile : nullptr, 1, 1 },
+		{ m.restrict2d, f ? f->restrict_to_2d : nullptr, 1, 1 },
+		{ m.persistence, f ? f->persistence_time : nullptr, e, 1 },
+		{ m.speed, f ? f->migration_speed : nullptr, e, 1 },
+		{ m.bias, f ? f->migration_bias : nullptr, e, 1 },
+		{ m.direction, f ? f->migration_bias_direction : nullptr, e, d },
+		{ m.vector, f ? f->motility_vector : nullptr, e, d },
+	};
+}
+
+// carves the columns out of one zeroed block of C rows; the view changes, so
+// captured step graphs are released
+int alloc_columns(ppc_state* s, store_block& b, std::vector<std::pair<void**, size_t>> cols)
+{
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	PPC_TRY(release_graph(s));
+	if (b.p)
+	{
+		PPC_CUDA(cudaFree(b.p));
+		b.p = nullptr;
+	}
+	size_t total = 0;
+	for (auto& c : cols)
+		total += (c.second + 255) & ~(size_t)255;
+	PPC_CUDA(cudaMalloc(&b.p, std::max<size_t>(total, 1)));
+	PPC_CUDA(cudaMemset(b.p, 0, std::max<size_t>(total, 1)));
+	b.bytes = total;
+	char* q = static_cast<char*>(b.p);
+	for (auto& c : cols)
+	{
+		*c.first = q;
+		q += (c.second + 255) & ~(size_t)255;
+	}
+	return PPC_OK;
+}
+
+int ensure_ix_store(ppc_state* s, int32_t S)
+{
+	if (s->ix_store.p && s->v.ix.S == S)
+		return PPC_OK;
+	const size_t C = s->total_cap, D = s->ndefs, e = sizeof(double);
+	ix_columns& x = s->v.ix;
+	const int32_t halve = x.halve_sub;
+	x = ix_columns {};
+	x.S = S;
+	x.halve_sub = halve;
+	std::vector<std::pair<void**, size_t>> cols = {
+		{ (void**)&x.dead, C }, { (void**)&x.nuclei, C * 4 }, { (void**)&x.dead_phago, C * e },
+		{ (void**)&x.damage_rate, C * e }, { (void**)&x.live_phago, C * D * e }, { (void**)&x.attack, C * D * e },
+		{ (void**)&x.fusion, C * D * e }, { (void**)&x.immuno, C * D * e }, { (void**)&x.frac, C * S * e },
+		{ (void**)&x.damage, C * e }, { (void**)&x.attack_time, C * e }, { (void**)&x.fluid, C * e },
+		{ (void**)&x.solid, C * e }, { (void**)&x.cyto, C * e }, { (void**)&x.cyto_fluid, C * e },
+		{ (void**)&x.cyto_solid, C * e }, { (void**)&x.nuc_fluid, C * e }, { (void**)&x.nuc_solid, C * e },
+		{ (void**)&x.fluid_fraction, C * e }, { (void**)&x.c2n, C * e }, { (void**)&x.target_cyto, C * e },
+		{ (void**)&x.target_nuc, C * e }, { (void**)&x.isub, C * S * e },
+	};
+	return alloc_columns(s, s->ix_store, cols);
+}
+
+int ensure_mot_store(ppc_state* s)
+{
+	if (s->mot_store.p)
+		return PPC_OK;
+	const size_t C = s->total_cap, d = s->dims, e = sizeof(double);
+	mot_columns& m = s->v.mot;
+	const int32_t per_agent = m.per_agent;
+	m = mot_columns {};
+	m.per_agent = per_agent;
+	std::vector<std::pair<void**, size_t>> cols = {
+		{ (void**)&m.motile, C }, { (void**)&m.restrict2d, C }, { (void**)&m.persistence, C * e },
+		{ (void**)&m.speed, C * e }, { (void**)&m.bias, C * e }, { (void**)&m.direction, C * d * e },
+		{ (void**)&m.vector, C * d * e },
+	};
+	return alloc_columns(s, s->mot_store, cols);
+}
+
+// rows [base, base + n) of the columns from (to_device) or to the host rows
+int move_columns(ppc_state* s, const std::vector<column>& cols, int32_t base, int32_t n, bool to_device)
+{
+	for (const auto& c : cols)
+	{
+		if (!c.host || c.width == 0 || n == 0)
+			continue;
+		char* dev = static_cast<char*>(c.dev) + (size_t)base * c.width * c.elem;
+		const size_t bytes = (size_t)n * c.width * c.elem;
+		if (to_device)
+			PPC_CUDA(cudaMemcpyAsync(dev, c.host, bytes, cudaMemcpyHostToDevice, s->stream));
+		else
+			PPC_CUDA(cudaMemcpyAsync(const_cast<void*>(c.host), dev, bytes, cudaMemcpyDeviceToHost, s->stream));
+	}
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	return PPC_OK;
+}
+
+int check_ix_fields(const ppc_interactions* f)
+{
+	const void* all[] = { f->dead, f->dead_phagocytosis_rate, f->damage_rate, f->live_phagocytosis_rates,
+						  f->attack_rates, f->fusion_rates, f->immunogenicities, f->damage, f->total_attack_time,
+						  f->number_of_nuclei, f->fluid, f->solid, f->cytoplasmic, f->cytoplasmic_fluid,
+						  f->cytoplasmic_solid, f->nuclear_fluid, f->nuclear_solid, f->fluid_fraction,
+						  f->cytoplasmic_to_nuclear_ratio, f->target_solid_cytoplasmic, f->target_solid_nuclear };
+	for (const void* p : all)
+		if (!p)
+			return fail(PPC_ERR_ARG, "a ppc_interactions field is NULL");
+	if (f->substrates > 0 && (!f->internalized_substrates || !f->fraction_transferred_when_ingested))
+		return fail(PPC_ERR_ARG, "a ppc_interactions substrate field is NULL");
+	return PPC_OK;
+}
+
+int check_mot_fields(const ppc_motility* f)
+{
 	if (!f->is_motile || !f->restrict_to_2d || !f->persistence_time || !f->migration_speed || !f->migration_bias
 		|| !f->migration_bias_direction || !f->motility_vector)
 		return fail(PPC_ERR_ARG, "a ppc_motility field is NULL");
+	return PPC_OK;
+}
+
+// the replicate's live count, read from the device unless already known
+int live_count(ppc_state* s, int32_t r, int32_t& n)
+{
+	if (!s->counts_known)
+	{
+		std::vector<rep_counters> c;
+		PPC_TRY(read_counters(s, c));
+	}
+	n = s->host_count[r];
+	return PPC_OK;
+}
+
+} // namespace
+} // namespace ppc
+
+extern "C" {
+
+int ppc_upload_interactions(ppc_state* s, int32_t r, const ppc_interactions* f, int32_t compute_internalized_substrates)
+{
+	if (!valid(s, r) || !f || f->substrates < 0)
+		return fail(PPC_ERR_ARG, "invalid arguments");
+	int32_t n = 0;
+	PPC_TRY(live_count(s, r, n));
+	if (f->count != n)
+		return fail(PPC_ERR_ARG, "fields.count differs from the replicate's agent count");
+	PPC_TRY(check_ix_fields(f));
+	if (s->ix_store.p && f->substrates != s->v.ix.S)
+		return fail(PPC_ERR_ARG, "substrates differ from the resident interaction fields'");
+	PPC_TRY(ensure_ix_store(s, f->substrates));
+	if (s->v.ix.halve_sub != (compute_internalized_substrates != 0))
+	{
+		PPC_CUDA(cudaStreamSynchronize(s->stream));
+		PPC_TRY(release_graph(s));
+		s->v.ix.halve_sub = compute_internalized_substrates != 0;
+	}
+	return move_columns(s, ix_column_list(s->v.ix, f, s->ndefs), s->reps[r].base, n, true);
+}
+
+int ppc_download_interactions(ppc_state* s, int32_t r, ppc_interactions* f)
+{
+	if (!valid(s, r) || !f)
+		return fail(PPC_ERR_ARG, "invalid arguments");
+	if (!s->ix_store.p || f->substrates != s->v.ix.S)
+		return fail(PPC_ERR_ARG, "no resident interaction fields with these substrates");
+	PPC_CUDA(cudaGetLastError());
 	std::vector<rep_counters> c;
 	PPC_TRY(read_counters(s, c));
 	const int32_t n = c[r].count;
+	f->count = n;
+	PPC_TRY(check_ix_fields(f));
+	return move_columns(s, ix_column_list(s->v.ix, f, s->ndefs), s->reps[r].base, n, false);
+}
+
+int ppc_upload_motility(ppc_state* s, int32_t r, const ppc_motility* f)
+{
+	if (!valid(s, r) || !f)
+		return fail(PPC_ERR_ARG, "invalid arguments");
+	int32_t n = 0;
+	PPC_TRY(live_count(s, r, n));
 	if (f->count != n)
 		return fail(PPC_ERR_ARG, "fields.count differs from the replicate's agent count");
+	PPC_TRY(check_mot_fields(f));
+	PPC_TRY(ensure_mot_store(s));
+	if (s->v.mot.per_agent != (f->restrict_per_agent != 0))
+	{
+		PPC_CUDA(cudaStreamSynchronize(s->stream));
+		PPC_TRY(release_graph(s));
+		s->v.mot.per_agent = f->restrict_per_agent != 0;
+	}
+	return move_columns(s, mot_column_list(s->v.mot, f, s->dims), s->reps[r].base, n, true);
+}
+
+int ppc_download_motility(ppc_state* s, int32_t r, ppc_motility* f)
+{
+	if (!valid(s, r) || !f)
+		return fail(PPC_ERR_ARG, "invalid arguments");
+	if (!s->mot_store.p)
+		return fail(PPC_ERR_ARG, "no resident motility fields");
+	PPC_CUDA(cudaGetLastError());
+	std::vector<rep_counters> c;
+	PPC_TRY(read_counters(s, c));
+	const int32_t n = c[r].count;
+	f->count = n;
+	PPC_TRY(check_mot_fields(f));
+	return move_columns(s, mot_column_list(s->v.mot, f, s->dims), s->reps[r].base, n, false);
+}
+
+int ppc_update_motility_fields(ppc_state* s, int32_t r, ppc_motility* f)
+{
+	if (!valid(s, r))
+		return fail(PPC_ERR_ARG, "invalid arguments");
+	if (f)
+		PPC_TRY(ppc_upload_motility(s, r, f)); // fields travel with the call
+	else if (!s->mot_store.p)
+		return fail(PPC_ERR_ARG, "no resident motility fields: upload them or pass fields");
+	int32_t n = 0;
+	PPC_TRY(live_count(s, r, n));
 	if ((int32_t)s->mot_epoch.size() < s->nreps)
 		s->mot_epoch.resize(s->nreps, 0);
 	const uint64_t epoch = s->mot_epoch[r]++;
-	if (n == 0)
-		return PPC_OK;
-	const size_t nd = (size_t)n, dims = (size_t)s->dims;
-	const size_t bytes = sizeof(double) * (3 * nd + 2 * nd * dims) + 2 * nd;
-	PPC_TRY(ensure_field_scratch(s, bytes));
-	double* dp = static_cast<double*>(s->ix_scratch);
-	mot_fields m {};
-	m.n = n;
-	m.replicate = r;
-	m.base = s->reps[r].base;
-	m.dt = s->params.mechanics_time_step;
-	m.per_agent = f->restrict_per_agent != 0;
-	m.epoch = epoch;
-	double* persistence = dp;
-	double* speed = dp + nd;
-	double* bias = dp + 2 * nd;
-	double* direction = dp + 3 * nd;
-	double* vec = dp + 3 * nd + nd * dims;
-	uint8_t* motile = reinterpret_cast<uint8_t*>(dp + 3 * nd + 2 * nd * dims);
-	uint8_t* restrict2d = motile + nd;
-	m.persistence = persistence;
-	m.speed = speed;
-	m.bias = bias;
-	m.direction = direction;
-	m.vector = vec;
-	m.motile = motile;
-	m.restrict2d = restrict2d;
-	struct copy
+	if (n > 0)
 	{
-		void* dst;
-		const void* src;
-		size_t bytes;
-	} in[] = { { persistence, f->persistence_time, nd * sizeof(double) },
-			   { speed, f->migration_speed, nd * sizeof(double) },
-			   { bias, f->migration_bias, nd * sizeof(double) },
-			   { direction, f->migration_bias_direction, nd * dims * sizeof(double) },
-			   { vec, f->motility_vector, nd * dims * sizeof(double) },
-			   { motile, f->is_motile, nd },
-			   { restrict2d, f->restrict_to_2d, nd } };
-	for (auto& k : in)
-		PPC_CUDA(cudaMemcpyAsync(k.dst, k.src, k.bytes, cudaMemcpyHostToDevice, s->stream));
-	PPC_TRY(launch_motility(s, m));
-	PPC_CUDA(cudaMemcpyAsync(f->motility_vector, vec, nd * dims * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
-	PPC_CUDA(cudaStreamSynchronize(s->stream));
-	s->vel_dirty = true; // the next fused step reads the velocities
+		const int32_t base = s->reps[r].base;
+		const mot_columns& mc = s->v.mot;
+		const size_t d = (size_t)s->dims;
+		mot_fields m {};
+		m.n = n;
+		m.replicate = r;
+		m.base = base;
+		m.dt = s->params.mechanics_time_step;
+		m.per_agent = mc.per_agent;
+		m.epoch = epoch;
+		m.motile = mc.motile + base;
+		m.restrict2d = mc.restrict2d + base;
+		m.persistence = mc.persistence + base;
+		m.speed = mc.speed + base;
+		m.bias = mc.bias + base;
+		m.direction = mc.direction + (size_t)base * d;
+		m.vector = mc.vector + (size_t)base * d;
+		PPC_TRY(launch_motility(s, m));
+		s->vel_dirty = true; // the next fused step reads the velocities
+	}
+	if (f)
+		PPC_TRY(move_columns(s, { { s->v.mot.vector, f->motility_vector, sizeof(double), (size_t)s->dims } },
+							 s->reps[r].base, n, false));
 	return finish(s);
 }
 
 int ppc_update_cell_cell_interactions(ppc_state* s, int32_t r, ppc_interactions* f)
 {
-	if (!valid(s, r) || !f || f->substrates < 0)
+	if (!valid(s, r) || (f && f->substrates < 0))
 		return fail(PPC_ERR_ARG, "invalid arguments");
-	std::vector<rep_counters> c;
-	PPC_TRY(read_counters(s, c));
-	const int32_t n = c[r].count;
-	if (f->count != n)
-		return fail(PPC_ERR_ARG, "fields.count differs from the replicate's agent count");
+	if (f)
+	{
+		// fields travel with the call: resident for its duration
+		if (s->ix_store.p && f->substrates != s->v.ix.S)
+			PPC_TRY(ensure_ix_store(s, f->substrates));
+		PPC_TRY(ppc_upload_interactions(s, r, f, s->v.ix.halve_sub));
+	}
+	else if (!s->ix_store.p)
+		return fail(PPC_ERR_ARG, "no resident interaction fields: upload them or pass fields");
+	int32_t n = 0;
+	PPC_TRY(live_count(s, r, n));
 	if ((int32_t)s->ix_epoch.size() < s->nreps)
 		s->ix_epoch.resize(s->nreps, 0);
 	const uint64_t epoch = s->ix_epoch[r]++;
 	if (n == 0)
 		return PPC_OK;
-	const int32_t D = s->ndefs, S = f->substrates;
-	const double* reads[] = { f->dead_phagocytosis_rate, f->damage_rate };
-	const double* reads_d[] = { f->live_phagocytosis_rates, f->attack_rates, f->fusion_rates, f->immunogenicities };
-	double* rw[] = { f->damage, f->total_attack_time, f->fluid, f->solid, f->cytoplasmic, f->cytoplasmic_fluid,
-					 f->cytoplasmic_solid, f->nuclear_fluid, f->nuclear_solid, f->fluid_fraction,
-					 f->cytoplasmic_to_nuclear_ratio, f->target_solid_cytoplasmic, f->target_solid_nuclear };
-	if (!f->dead || !f->number_of_nuclei || (S > 0 && (!f->internalized_substrates || !f->fraction_transferred_when_ingested)))
-		return fail(PPC_ERR_ARG, "a ppc_interactions field is NULL");
-	for (auto* p : reads)
-		if (!p)
-			return fail(PPC_ERR_ARG, "a ppc_interactions field is NULL");
-	for (auto* p : reads_d)
-		if (!p)
-			return fail(PPC_ERR_ARG, "a ppc_interactions field is NULL");
-	for (auto* p : rw)
-		if (!p)
-			return fail(PPC_ERR_ARG, "a ppc_interactions field is NULL");
 	PPC_TRY(ensure_lists(s));
-
-	// one device block: per-agent doubles, per-definition rows, substrate rows,
-	// nuclei, candidates, dead flags
 	const size_t nd = (size_t)n;
-	const size_t doubles = nd * (2 + 13) + nd * D * 4 + nd * S * 2;
-	const size_t ints = nd * 2 + nd * s->ncap;
-	const size_t bytes = doubles * sizeof(double) + ints * sizeof(int32_t) + nd;
-	PPC_TRY(ensure_field_scratch(s, bytes));
-	char* d = static_cast<char*>(s->ix_scratch);
-	double* dp = reinterpret_cast<double*>(d);
-	auto take = [&](size_t count) { double* q = dp; dp += count; return q; };
+	PPC_TRY(ensure_field_scratch(s, sizeof(int32_t) * (2 * nd + nd * s->ncap + 2)));
+	int32_t* ip = static_cast<int32_t*>(s->ix_scratch);
+	const int32_t base = s->reps[r].base;
+	const ix_columns& c = s->v.ix;
+	const size_t D = s->ndefs, S = c.S;
 	ix_fields x {};
 	x.n = n;
-	x.substrates = S;
+	x.substrates = c.S;
 	x.replicate = r;
-	x.base = s->reps[r].base;
+	x.base = base;
 	x.dt = s->params.mechanics_time_step;
 	x.epoch = epoch;
-	double* dr[2];
-	for (int k = 0; k < 2; k++)
-		dr[k] = take(nd);
-	double* dd[4];
-	for (int k = 0; k < 4; k++)
-		dd[k] = take(nd * D);
-	double* dw[13];
-	for (int k = 0; k < 13; k++)
-		dw[k] = take(nd);
-	double* dfrac = take(nd * S);
-	double* disub = take(nd * S);
-	int32_t* ip = reinterpret_cast<int32_t*>(dp);
-	x.nuclei = ip;
-	x.ncand = ip + nd;
-	x.cand = ip + 2 * nd;
-	uint8_t* ddead = reinterpret_cast<uint8_t*>(ip + 2 * nd + nd * s->ncap);
-	x.dead = ddead;
-	x.dead_phago = dr[0];
-	x.damage_rate = dr[1];
-	x.live_phago = dd[0];
-	x.attack = dd[1];
-	x.fusion = dd[2];
-	x.immuno = dd[3];
-	x.damage = dw[0];
-	x.attack_time = dw[1];
-	x.fluid = dw[2];
-	x.solid = dw[3];
-	x.cyto = dw[4];
-	x.cyto_fluid = dw[5];
-	x.cyto_solid = dw[6];
-	x.nuc_fluid = dw[7];
-	x.nuc_solid = dw[8];
-	x.fluid_fraction = dw[9];
-	x.c2n = dw[10];
-	x.target_cyto = dw[11];
-	x.target_nuc = dw[12];
-	x.frac = dfrac;
-	x.isub = disub;
-
-	auto h2d = [&](void* dst, const void* src, size_t b) {
-		return cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, s->stream);
-	};
-	auto d2h = [&](void* dst, const void* src, size_t b) {
-		return cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, s->stream);
-	};
-	cudaError_t e = cudaSuccess;
-	for (int k = 0; k < 2 && e == cudaSuccess; k++)
-		e = h2d(dr[k], reads[k], nd * sizeof(double));
-	for (int k = 0; k < 4 && e == cudaSuccess; k++)
-		e = h2d(dd[k], reads_d[k], nd * D * sizeof(double));
-	for (int k = 0; k < 13 && e == cudaSuccess; k++)
-		e = h2d(dw[k], rw[k], nd * sizeof(double));
-	if (e == cudaSuccess && S > 0)
-		e = h2d(dfrac, f->fraction_transferred_when_ingested, nd * S * sizeof(double));
-	if (e == cudaSuccess && S > 0)
-		e = h2d(disub, f->internalized_substrates, nd * S * sizeof(double));
-	if (e == cudaSuccess)
-		e = h2d(x.nuclei, f->number_of_nuclei, nd * sizeof(int32_t));
-	if (e == cudaSuccess)
-		e = h2d(ddead, f->dead, nd);
-	int rc = e == cudaSuccess ? launch_interactions(s, x) : ppc::cuda_fail(e, "interaction field upload");
-	e = cudaSuccess;
-	for (int k = 0; k < 13 && e == cudaSuccess && rc == PPC_OK; k++)
-		e = d2h(rw[k], dw[k], nd * sizeof(double));
-	if (e == cudaSuccess && rc == PPC_OK && S > 0)
-		e = d2h(f->internalized_substrates, disub, nd * S * sizeof(double));
-	if (e == cudaSuccess && rc == PPC_OK)
-		e = d2h(f->number_of_nuclei, x.nuclei, nd * sizeof(int32_t));
-	const cudaError_t es = cudaStreamSynchronize(s->stream);
-	if (rc != PPC_OK)
-		return rc;
-	if (e != cudaSuccess)
-		return ppc::cuda_fail(e, "interaction field download");
-	if (es != cudaSuccess)
-		return ppc::cuda_fail(es, "cudaStreamSynchronize");
+	x.status = ip;
+	x.ncand = ip + 2;
+	x.dep = ip + 2 + nd;
+	x.cand = ip + 2 + 2 * nd;
+	x.dead = c.dead + base;
+	x.dead_phago = c.dead_phago + base;
+	x.damage_rate = c.damage_rate + base;
+	x.live_phago = c.live_phago + base * D;
+	x.attack = c.attack + base * D;
+	x.fusion = c.fusion + base * D;
+	x.immuno = c.immuno + base * D;
+	x.frac = c.frac + base * S;
+	x.damage = c.damage + base;
+	x.attack_time = c.attack_time + base;
+	x.nuclei = c.nuclei + base;
+	x.fluid = c.fluid + base;
+	x.solid = c.solid + base;
+	x.cyto = c.cyto + base;
+	x.cyto_fluid = c.cyto_fluid + base;
+	x.cyto_solid = c.cyto_solid + base;
+	x.nuc_fluid = c.nuc_fluid + base;
+	x.nuc_solid = c.nuc_solid + base;
+	x.fluid_fraction = c.fluid_fraction + base;
+	x.c2n = c.c2n + base;
+	x.target_cyto = c.target_cyto + base;
+	x.target_nuc = c.target_nuc + base;
+	x.isub = c.isub + base * S;
+	PPC_CUDA(cudaMemsetAsync(x.status, 0, 2 * sizeof(int32_t), s->stream));
+	PPC_TRY(launch_interactions(s, x));
+	PPC_CUDA(cudaMemcpyAsync(s->pinned_err + 1, x.status, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	if (s->pinned_err[1])
+		return fail(PPC_ERR_CAPACITY, "a neighbour list exceeds the neighbour capacity: no interaction ran");
 	// positions and radii changed: the next mesh update rebuilds the bins; the
 	// neighbour lists stay those the interactions used, as in the reference
-	s->bins_valid = false;
+	invalidate_bins(s);
+	if (f)
+	{
+		std::vector<column> back;
+		for (const auto& col : ix_column_list(s->v.ix, f, s->ndefs))
+			back.push_back(col);
+		PPC_TRY(move_columns(s, back, base, n, false));
+	}
 	return finish(s);
 }
 

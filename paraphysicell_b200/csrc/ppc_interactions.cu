@@ -6,16 +6,21 @@
 // neighbour costs one uniform draw, and an action re-checks the removal flags
 // of both agents before it changes anything. The outcome therefore depends on
 // the order in which agents act. This implementation fixes the order of a
-// one-thread run (agents in index order, neighbours in list order) and splits
-// the work in two passes:
+// one-thread run (agents in index order, neighbours in list order) and
+// reaches it in three passes:
 //  1. k_ix_candidates, one thread per agent: draws every neighbour's number and
 //     keeps the neighbours for which some action's threshold passes (the draw
-//     and the rates do not depend on any other agent's actions);
-//  2. k_ix_resolve, one block: lists the agents that have candidates, in index
-//     order, and one thread replays the reference's loop over those
-//     candidates only, with the flag checks and the at-most-once rules.
-// With the small rates of a real model only a few neighbours per step become
-// candidates, so the serial pass is short.
+//     and the rates do not depend on any other agent's actions); it also
+//     checks that no neighbour list was cut at the list capacity;
+//  2. k_ix_independent: an agent's walk reads and writes only itself and its
+//     candidate neighbours, so a walk whose agents appear in no earlier walk
+//     sees the state a one-thread run would show it, whatever runs beside
+//     it. Each such agent (found with a per-slot atomicMin of the first walk
+//     that touches the slot) walks at once, in parallel with the others; the
+//     rest are marked;
+//  3. k_ix_ordered, one block: one thread walks the marked agents in index
+//     order, after every independent walk has finished.
+// With the rates of a real model nearly every walk is independent.
 
 #include <cuda_runtime.h>
 
@@ -36,9 +41,11 @@ __global__ void __launch_bounds__(kIxThreads) k_ix_candidates(view v, ix_fields 
 	if (i >= x.n)
 		return;
 	int m = 0;
+	const int s = x.base + i;
+	if (v.ncnt[s] > v.ncap)
+		atomicOr(x.status, 1); // a cut list: the walks below would miss neighbours
 	if (x.dead[i] != 1)
 	{
-		const int s = x.base + i;
 		const int nn = min(v.ncnt[s], v.ncap);
 		const int D = v.ndefs;
 		const double dt = x.dt;
@@ -65,6 +72,13 @@ __global__ void __launch_bounds__(kIxThreads) k_ix_candidates(view v, ix_fields 
 		}
 	}
 	x.ncand[i] = m;
+	// the first walk that touches each slot (first_end is INT32_MAX between uses)
+	if (m > 0)
+	{
+		atomicMin(v.first_end + s, i);
+		for (int c = 0; c < m; c++)
+			atomicMin(v.first_end + v.nidx[(int64_t)s * v.ncap + x.cand[(int64_t)i * v.ncap + c]], i);
+	}
 }
 
 __device__ void ix_geometry(const view& v, int s)
@@ -204,14 +218,59 @@ __device__ void ix_agent(const view& v, const ix_fields& x, int cur, int i)
 	}
 }
 
+// true when no earlier agent's walk touches this agent or its candidates
+__device__ __forceinline__ bool ix_independent(const view& v, const ix_fields& x, int i)
+{
+	const int s = x.base + i;
+	if (__ldcg(v.first_end + s) != i)
+		return false;
+	const int m = x.ncand[i];
+	for (int c = 0; c < m; c++)
+		if (__ldcg(v.first_end + v.nidx[(int64_t)s * v.ncap + x.cand[(int64_t)i * v.ncap + c]]) != i)
+			return false;
+	return true;
+}
+
 template <int DIMS>
-__global__ void __launch_bounds__(kIxResolveThreads) k_ix_resolve(view v, ix_fields x, int cur)
+__global__ void __launch_bounds__(kIxThreads) k_ix_independent(view v, ix_fields x, int cur)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= x.n)
+		return;
+	int dep = 0;
+	if (x.ncand[i] > 0 && __ldcg(x.status) == 0)
+	{
+		if (ix_independent(v, x, i))
+			ix_agent<DIMS>(v, x, cur, i);
+		else
+			dep = 1;
+	}
+	x.dep[i] = dep;
+}
+
+// the marked agents in index order on one thread, after every independent
+// walk; every thread restores first_end of the slots the walks touched
+template <int DIMS>
+__global__ void __launch_bounds__(kIxResolveThreads) k_ix_ordered(view v, ix_fields x, int cur)
 {
 	__shared__ int list[kIxResolveThreads];
+	const bool ok = __ldcg(x.status) == 0;
+	for (int i = threadIdx.x; i < x.n; i += blockDim.x)
+	{
+		const int m = x.ncand[i];
+		if (m == 0)
+			continue;
+		const int s = x.base + i;
+		v.first_end[s] = INT32_MAX;
+		for (int c = 0; c < m; c++)
+			v.first_end[v.nidx[(int64_t)s * v.ncap + x.cand[(int64_t)i * v.ncap + c]]] = INT32_MAX;
+	}
+	if (!ok)
+		return;
 	for (int i0 = 0; i0 < x.n; i0 += blockDim.x)
 	{
 		const int i = i0 + threadIdx.x;
-		const int has = i < x.n && x.ncand[i] > 0;
+		const int has = i < x.n && x.dep[i] != 0;
 		int total;
 		const int off = block_exclusive_scan(has, total);
 		if (has)
@@ -230,13 +289,23 @@ int launch_interactions(ppc_state* s, const ix_fields& x)
 {
 	if (x.n == 0)
 		return PPC_OK;
-	k_ix_candidates<<<blocks_for(x.n, kIxThreads), kIxThreads, 0, PPC_LAUNCH(s)>>>(s->v, x);
+	const int b = blocks_for(x.n, kIxThreads);
+	k_ix_candidates<<<b, kIxThreads, 0, PPC_LAUNCH(s)>>>(s->v, x);
 	if (s->dims == 1)
-		k_ix_resolve<1><<<1, kIxResolveThreads, 0, PPC_LAUNCH(s)>>>(s->v, x, s->cur);
+	{
+		k_ix_independent<1><<<b, kIxThreads, 0, PPC_LAUNCH(s)>>>(s->v, x, s->cur);
+		k_ix_ordered<1><<<1, kIxResolveThreads, 0, PPC_LAUNCH(s)>>>(s->v, x, s->cur);
+	}
 	else if (s->dims == 2)
-		k_ix_resolve<2><<<1, kIxResolveThreads, 0, PPC_LAUNCH(s)>>>(s->v, x, s->cur);
+	{
+		k_ix_independent<2><<<b, kIxThreads, 0, PPC_LAUNCH(s)>>>(s->v, x, s->cur);
+		k_ix_ordered<2><<<1, kIxResolveThreads, 0, PPC_LAUNCH(s)>>>(s->v, x, s->cur);
+	}
 	else
-		k_ix_resolve<3><<<1, kIxResolveThreads, 0, PPC_LAUNCH(s)>>>(s->v, x, s->cur);
+	{
+		k_ix_independent<3><<<b, kIxThreads, 0, PPC_LAUNCH(s)>>>(s->v, x, s->cur);
+		k_ix_ordered<3><<<1, kIxResolveThreads, 0, PPC_LAUNCH(s)>>>(s->v, x, s->cur);
+	}
 	PPC_CUDA(cudaGetLastError());
 	return PPC_OK;
 }

@@ -70,6 +70,27 @@ struct rep_counters
 	int64_t spring_epoch; // spring updates so far: epoch of their counter-based draws
 };
 
+// Phenotype columns a caller made resident (ppc_upload_interactions,
+// ppc_upload_motility): slot-indexed like the mechanics fields, moved by the
+// compaction and set by division; null pointers until uploaded.
+struct ix_columns
+{
+	uint8_t* dead;
+	double *dead_phago, *damage_rate, *live_phago, *attack, *fusion, *immuno, *frac; // rates: [C], [C*D], [C*S]
+	double *damage, *attack_time, *fluid, *solid, *cyto, *cyto_fluid, *cyto_solid, *nuc_fluid, *nuc_solid,
+		*fluid_fraction, *c2n, *target_cyto, *target_nuc, *isub; // [C], isub [C*S]
+	int32_t* nuclei;
+	int32_t S;		   // internalized substrates per agent
+	int32_t halve_sub; // division halves the internalized substrates (compute_internalized_substrates)
+};
+
+struct mot_columns
+{
+	uint8_t *motile, *restrict2d;
+	double *persistence, *speed, *bias, *direction, *vector; // direction, vector: [C*dims]
+	int32_t per_agent;
+};
+
 // everything a kernel needs, passed by value
 struct view
 {
@@ -124,6 +145,7 @@ struct view
 	uint8_t* sdel;		  // [C*S] spring marked for detachment this step
 	int32_t* first_end;	  // [C] INT32_MAX between spring attachment passes
 	int32_t* pos_changed; // set by an upload whose positions differ from the resident ones
+	int32_t* bin_active;  // the current rebuild runs (a conditional one may find nothing changed)
 	int32_t* sorted;
 	int32_t* skey;
 	double4* spos4;
@@ -145,12 +167,49 @@ struct view
 
 	uint64_t seed;
 	uint64_t* draw_epoch; // per replicate draw epoch
+
+	ix_columns ix;
+	mot_columns mot;
 };
 
 struct buffer
 {
 	void* p = nullptr;
 	size_t bytes = 0;
+};
+
+// one device block holding a set of resident columns
+struct store_block
+{
+	void* p = nullptr;
+	size_t bytes = 0;
+};
+
+// a host-layout unpack or a device-to-host copy queued after the copies or
+// packs of the same transfer call
+struct pending_unpack
+{
+	double4* dev;
+	const double* src;
+	int32_t r, n;
+	int32_t* changed;
+};
+
+struct pending_copy
+{
+	void* dst;
+	const void* src;
+	size_t bytes;
+};
+
+// one captured block of fused steps and what its kernels were captured with
+struct graph_entry
+{
+	cudaGraphExec_t exec = nullptr;
+	int steps = 0, cur = 0;
+	bool phenotype = false, lead_bin = false, springs = false;
+	double pdiv = 0, pdeath = 0;
+	int64_t launches = 0;
 };
 
 } // namespace ppc
@@ -177,6 +236,9 @@ struct ppc_state
 	bool has_springs = false;	  // some agent may have springs
 	bool rates_nonzero = false;	  // some attachment/detachment rate is non-zero
 	bool bins_valid = false;	  // bins match the current positions
+	bool bins_cond = false;		  // ...unless an upload changed them: the device decides (pos_changed)
+	bool counts_known = false;	  // host_count holds the device counts (no count-changing work since)
+	bool zero_copy = false;		  // pinned host rows are read and written by kernels over the bus
 	bool lists_stale = false;	  // a fused step ran since the neighbour lists were built
 	int64_t launches = 0;
 	int max_grid_blocks = 0;
@@ -185,14 +247,12 @@ struct ppc_state
 	// staging for host <-> device copies
 	void* stage = nullptr;
 	size_t stage_bytes = 0;
+	size_t stage_used = 0; // bytes of the arena taken by the current transfer call
+	std::vector<ppc::pending_unpack> pending_unpacks;
+	std::vector<ppc::pending_copy> pending_copies;
 
-	// captured CUDA graph of a block of fused steps
-	cudaGraphExec_t graph = nullptr;
-	int graph_steps = 0;
-	int graph_cur = -1;
-	bool graph_phenotype = false;
-	double graph_pdiv = 0, graph_pdeath = 0;
-	int64_t graph_launches = 0;
+	// captured CUDA graphs of blocks of fused steps (ppc_api.cu: replay_steps)
+	std::vector<ppc::graph_entry> graphs;
 	bool use_graphs = true;
 
 	// fused pass launch shape: one thread per agent with its own pair work
@@ -203,10 +263,11 @@ struct ppc_state
 	std::vector<int32_t> host_count;
 	std::vector<uint64_t> ix_epoch; // cell-cell interaction calls so far, per replicate
 	std::vector<uint64_t> mot_epoch; // motility calls so far, per replicate
-	void* ix_scratch = nullptr;		// device copies of the interaction fields, kept between calls
+	void* ix_scratch = nullptr;		// per-call scratch of the interaction and motility passes
 	size_t ix_scratch_bytes = 0;
+	ppc::store_block ix_store, mot_store; // resident phenotype columns
 	ppc::rep_counters* pinned_ctr = nullptr; // pinned landing area of the counters
-	int32_t* pinned_flag = nullptr;			 // pinned landing area of pos_changed
+	int32_t* pinned_err = nullptr;			 // pinned landing area of the device error word
 	bool staged = false;
 	bool coop = false;
 	bool flat = true; // per-thread pass with batched candidate fetches (shape -3, the default)
@@ -241,7 +302,7 @@ inline int blocks_for(int64_t n, int threads)
 }
 
 // ---- kernel entry points (ppc_kernels.cu) ----
-int launch_bin(ppc_state* s);
+int launch_bin(ppc_state* s, bool conditional);
 int launch_neighbors(ppc_state* s);
 int launch_forces(ppc_state* s);
 int launch_membrane(ppc_state* s);
@@ -276,6 +337,8 @@ struct ix_fields
 		*target_nuc, *isub;
 	int32_t* ncand; // [n] candidate neighbours of each agent
 	int32_t* cand;	// [n*ncap] their positions in the agent's neighbour list
+	int32_t* status; // [2] capacity error found by the candidate pass, count of agents left for the ordered pass
+	int32_t* dep;	 // [n] agents whose interactions depend on an earlier agent's
 };
 int launch_interactions(ppc_state* s, const ix_fields& x);
 

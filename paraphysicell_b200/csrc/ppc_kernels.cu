@@ -88,10 +88,53 @@ __device__ __forceinline__ int axis_coord(double x, const rep_info& R, int d, in
 	return (int)q;
 }
 
+// slot d of every resident phenotype column takes slot s's values
+__device__ __forceinline__ void copy_columns(const view& v, int dims, int d, int s)
+{
+	const ix_columns& x = v.ix;
+	if (x.dead)
+	{
+		const int D = v.ndefs, S = x.S;
+		x.dead[d] = x.dead[s];
+		double* one[] = { x.dead_phago, x.damage_rate, x.damage, x.attack_time, x.fluid, x.solid, x.cyto,
+						  x.cyto_fluid, x.cyto_solid, x.nuc_fluid, x.nuc_solid, x.fluid_fraction, x.c2n,
+						  x.target_cyto, x.target_nuc };
+#pragma unroll
+		for (int k = 0; k < 15; k++)
+			one[k][d] = one[k][s];
+		double* rows_d[] = { x.live_phago, x.attack, x.fusion, x.immuno };
+#pragma unroll
+		for (int k = 0; k < 4; k++)
+			for (int q = 0; q < D; q++)
+				rows_d[k][(int64_t)d * D + q] = rows_d[k][(int64_t)s * D + q];
+		for (int q = 0; q < S; q++)
+		{
+			x.frac[(int64_t)d * S + q] = x.frac[(int64_t)s * S + q];
+			x.isub[(int64_t)d * S + q] = x.isub[(int64_t)s * S + q];
+		}
+		x.nuclei[d] = x.nuclei[s];
+	}
+	const mot_columns& m = v.mot;
+	if (m.motile)
+	{
+		m.motile[d] = m.motile[s];
+		m.restrict2d[d] = m.restrict2d[s];
+		m.persistence[d] = m.persistence[s];
+		m.speed[d] = m.speed[s];
+		m.bias[d] = m.bias[s];
+		for (int q = 0; q < dims; q++)
+		{
+			m.direction[(int64_t)d * dims + q] = m.direction[(int64_t)s * dims + q];
+			m.vector[(int64_t)d * dims + q] = m.vector[(int64_t)s * dims + q];
+		}
+	}
+}
+
 // copies every per-agent field of slot s into slot d (cell_data::remove,
 // reference: src/cell_data.cpp:285-313); spring rows were moved by the plan
 __device__ __forceinline__ void move_agent(const view& v, int cur, int d, int s)
 {
+	copy_columns(v, v.dims, d, s);
 	v.pos[cur][d] = v.pos[cur][s];
 	v.vel[d] = v.vel[s];
 	v.vprev[d] = v.vprev[s];
@@ -170,7 +213,11 @@ __device__ __forceinline__ void count_agent(const view& v, int cur, int s, int r
 // (after an upload) every live slot is taken by slot. The provisional rank
 // only has to be a permutation of 0..count-1 inside the voxel; k_bin_fixup
 // sets the final one.
-__global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur)
+//
+// A conditional rebuild (after an upload of positions) runs only if the
+// upload changed some position; its decision goes to bin_active for the
+// other three kernels.
+__global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur, int conditional)
 {
 	grid_wait();
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -178,6 +225,11 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur)
 	const bool ordered = *v.order_valid != 0;
 	const bool moves = *v.moves_pending != 0;
 	const bool appended = *v.appended != 0;
+	const bool active = !conditional || *v.pos_changed != 0 || moves || appended;
+	if (t == 0)
+		*v.bin_active = active ? 1 : 0;
+	if (!active)
+		return;
 	// both candidates first, so that their loads overlap
 	int sa = -1, ra = 0, sb = -1, rb = 0, local = 0;
 	if ((!ordered || appended) && t < v.total_cap && live(v, t, rb, local)
@@ -202,6 +254,8 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur)
 __global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
 {
 	grid_wait();
+	if (!*v.bin_active)
+		return;
 	const int b = blockIdx.x;
 	// the tile's counts first (counts are padded to whole tiles and zero past
 	// the last voxel), so their loads overlap the predecessor totals' loads
@@ -271,6 +325,10 @@ __global__ void k_bin_scatter(view v)
 {
 	grid_wait();
 	int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s == 0)
+		*v.pos_changed = 0; // read by this rebuild's k_bin_count only
+	if (!*v.bin_active)
+		return;
 	if (blockIdx.x == 0)
 	{
 		for (int k = threadIdx.x; k < v.ntiles; k += blockDim.x)
@@ -302,6 +360,8 @@ __global__ void k_bin_scatter(view v)
 __global__ void k_bin_fixup(view v, int cur)
 {
 	grid_wait();
+	if (!*v.bin_active)
+		return;
 	// thread tp takes the agent the scatter put at provisional position tp;
 	// its final position is in the same voxel's range, so the stores of
 	// neighbouring threads land close together
@@ -2464,6 +2524,24 @@ __global__ void k_divide_apply(view v, int cur)
 		v.prm[p] = prm;
 		v.nrad[p] = nrad;
 		v.sarea[p] = sarea;
+		// resident phenotype columns (src/cell.cpp:119-125,153,
+		// data_storage_phenotype.cpp:530-560): internalized substrates halved
+		// when they are computed, damage and attack time cleared, every
+		// volume compartment halved
+		const ix_columns& x = v.ix;
+		if (x.dead)
+		{
+			if (x.halve_sub)
+				for (int q = 0; q < x.S; q++)
+					x.isub[(int64_t)p * x.S + q] *= 0.5;
+			x.damage[p] = 0;
+			x.attack_time[p] = 0;
+			double* halved[] = { x.fluid, x.solid, x.cyto, x.cyto_fluid, x.cyto_solid, x.nuc_fluid, x.nuc_solid,
+								 x.target_cyto, x.target_nuc };
+#pragma unroll
+			for (int k = 0; k < 9; k++)
+				halved[k][p] *= 0.5;
+		}
 
 		// new cell: defaults of a created cell, then copy_from(parent)
 		v.prm[c] = prm;
@@ -2488,6 +2566,15 @@ __global__ void k_divide_apply(view v, int cur)
 		v.pressure[c] = 0;
 		v.scnt[c] = 0;
 		v.ncnt[c] = 0;
+		// resident columns: the daughter copies the parent's phenotype and
+		// keeps the constructor's state (no damage or attack time, one nucleus)
+		copy_columns(v, DIMS, c, p);
+		if (x.dead)
+		{
+			x.damage[c] = 0;
+			x.attack_time[c] = 0;
+			x.nuclei[c] = 1;
+		}
 		double ow[3] = { 0, 0, 0 };
 		ppc_random_walk(DIMS, v.seed, ep, (uint64_t)r, (uint64_t)lp, PPC_DRAW_ORIENTATION, ow);
 		v.orient[c] = make_double4(ow[0], ow[1], ow[2], 0.0);
@@ -2636,10 +2723,10 @@ static void pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStr
 			return cuda_fail(e_, __func__);                                                                            \
 	} while (0)
 
-int launch_bin(ppc_state* s)
+int launch_bin(ppc_state* s, bool conditional)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
-	pdl(k_bin_count, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
+	pdl(k_bin_count, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur, conditional ? 1 : 0);
 	pdl(k_bin_scan, s->v.ntiles, kThreads, 0, PPC_LAUNCH(s), s->v);
 	pdl(k_bin_scatter, b, kThreads, 0, PPC_LAUNCH(s), s->v);
 	pdl(k_bin_fixup, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);

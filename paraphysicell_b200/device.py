@@ -35,7 +35,9 @@ EXPORTS = (
     "ppc_get_neighbors", "ppc_get_mesh_bins", "ppc_get_voxel_count", "ppc_get_mesh_position",
     "ppc_get_mesh_index", "ppc_get_launch_count", "ppc_last_error", "ppc_abi_version",
     "ppc_set_profiling", "ppc_get_profile", "ppc_set_launch_shape", "ppc_autotune",
-    "ppc_update_cell_cell_interactions", "ppc_update_motility_fields",
+    "ppc_update_cell_cell_interactions", "ppc_update_motility_fields", "ppc_set_host_transfer",
+    "ppc_upload_interactions", "ppc_download_interactions", "ppc_upload_motility", "ppc_download_motility",
+    "ppc_bin_agents_noalloc",
 ) + tuple("ppc_" + e for e in ENTRY_POINTS)
 
 
@@ -75,6 +77,7 @@ def lib():
         L.ppc_get_launch_count.argtypes = [vp, C.POINTER(C.c_int64)]
         L.ppc_set_profiling.argtypes = [vp, C.c_int32]
         L.ppc_set_launch_shape.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32]
+        L.ppc_set_host_transfer.argtypes = [vp, C.c_int32]
         L.ppc_autotune.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.ppc_get_profile.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
         L.ppc_last_error.restype = C.c_char_p
@@ -82,6 +85,10 @@ def lib():
             getattr(L, "ppc_" + e).argtypes = [vp]
         L.ppc_update_cell_cell_interactions.argtypes = [vp, C.c_int32, C.POINTER(Interactions)]
         L.ppc_update_motility_fields.argtypes = [vp, C.c_int32, C.POINTER(Motility)]
+        L.ppc_upload_interactions.argtypes = [vp, C.c_int32, C.POINTER(Interactions), C.c_int32]
+        L.ppc_download_interactions.argtypes = [vp, C.c_int32, C.POINTER(Interactions)]
+        L.ppc_upload_motility.argtypes = [vp, C.c_int32, C.POINTER(Motility)]
+        L.ppc_download_motility.argtypes = [vp, C.c_int32, C.POINTER(Motility)]
         _lib = L
     return _lib
 
@@ -187,6 +194,10 @@ class Simulation:
         _check(lib().ppc_get_launch_count(self.h, C.byref(n)), "ppc_get_launch_count")
         return n.value
 
+    def set_host_transfer(self, mode):
+        """abi.PPC_TRANSFER_COPY_ENGINE (the default) or PPC_TRANSFER_ZERO_COPY."""
+        _check(lib().ppc_set_host_transfer(self.h, mode), "ppc_set_host_transfer")
+
     def set_launch_shape(self, tile_edge, threads, smem_bytes=32 * 1024):
         _check(lib().ppc_set_launch_shape(self.h, tile_edge, threads, smem_bytes), "ppc_set_launch_shape")
 
@@ -216,18 +227,49 @@ class Simulation:
     def flag_by_draws(self, p_divide, p_death):
         _check(lib().ppc_flag_by_draws(self.h, p_divide, p_death), "ppc_flag_by_draws")
 
-    def update_motility_fields(self, fields, replicate=0):
+    def update_motility_fields(self, fields=None, replicate=0):
         """position_solver::update_motility with motile agents; `fields`
-        (abi.MotilityArrays) is read and its motility vectors written back."""
+        (abi.MotilityArrays) is read and its motility vectors written back, or
+        None to use the resident fields (upload_motility)."""
+        if fields is None:
+            _check(lib().ppc_update_motility_fields(self.h, replicate, None), "ppc_update_motility_fields")
+            return
         st = fields.struct()
         _check(lib().ppc_update_motility_fields(self.h, replicate, C.byref(st)), "ppc_update_motility_fields")
 
-    def update_cell_cell_interactions(self, fields, replicate=0):
+    def update_cell_cell_interactions(self, fields=None, replicate=0):
         """interactions_solver::update_cell_cell_interactions on one replicate;
-        `fields` (abi.InteractionArrays) is read and written back in place."""
+        `fields` (abi.InteractionArrays) is read and written back in place, or
+        None to use the resident fields (upload_interactions)."""
+        if fields is None:
+            _check(lib().ppc_update_cell_cell_interactions(self.h, replicate, None),
+                   "ppc_update_cell_cell_interactions")
+            return
         st = fields.struct()
         _check(lib().ppc_update_cell_cell_interactions(self.h, replicate, C.byref(st)),
                "ppc_update_cell_cell_interactions")
+
+    def upload_interactions(self, fields, replicate=0, compute_internalized_substrates=False):
+        st = fields.struct()
+        _check(lib().ppc_upload_interactions(self.h, replicate, C.byref(st), int(compute_internalized_substrates)),
+               "ppc_upload_interactions")
+
+    def download_interactions(self, fields, replicate=0):
+        """Fills `fields` (abi.InteractionArrays, capacity rows) and sets its count."""
+        st = fields.struct()
+        _check(lib().ppc_download_interactions(self.h, replicate, C.byref(st)), "ppc_download_interactions")
+        fields.count = st.count
+        return fields
+
+    def upload_motility(self, fields, replicate=0):
+        st = fields.struct()
+        _check(lib().ppc_upload_motility(self.h, replicate, C.byref(st)), "ppc_upload_motility")
+
+    def download_motility(self, fields, replicate=0):
+        st = fields.struct()
+        _check(lib().ppc_download_motility(self.h, replicate, C.byref(st)), "ppc_download_motility")
+        fields.count = st.count
+        return fields
 
     # ---- readback ----
     def neighbors(self, replicate=0, capacity=None):

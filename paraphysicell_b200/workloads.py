@@ -139,7 +139,9 @@ def config4(seed=4, replicates=256, n_min=500, n_max=50000, spare=1.0):
     params = Params.make(dt=0.1, ndefs=1, walls=False)
     meshes, sets = [], []
     for n in counts:
-        side = 20 * int(np.ceil(n ** (1.0 / 3.0)))
+        # a cube of (8000 N)^(1/3) um (one agent per 8000 um^3), rounded to
+        # whole um: the mesh's bounding box is integer
+        side = max(1, int(np.rint((8000.0 * n) ** (1.0 / 3.0))))
         mesh = Mesh.make(3, (0, 0, 0), (side, side, side))
         a = AgentArrays(int(n), 3, 1, int(np.ceil(n * spare)))
         a.arrays["positions"][: 3 * n] = rng.uniform(0, side, size=(n, 3)).ravel()
