@@ -191,6 +191,24 @@ int ppc_set_random_seed(ppc_state* s, uint64_t seed);
  * 128). Results do not depend on the shape; ppc_autotune picks one. */
 int ppc_set_launch_shape(ppc_state* s, int32_t tile_edge, int32_t threads, int32_t smem_bytes);
 
+/* How ppc_step runs a mechanics step (ppc_step_with_phenotype and steps with
+ * non-zero spring rates always use the separate kernels). */
+enum ppc_step_form
+{
+	PPC_STEP_KERNELS = 0,	 /* the default: the fused pass, the compaction plan and
+								the four mesh-rebuild kernels, six launches */
+	PPC_STEP_PERSISTENT = 1	 /* one cooperative launch: the same phases over all
+								replicates, separated by grid barriers */
+};
+int ppc_set_step_form(ppc_state* s, int32_t form);
+
+/* Bound of every device-side wait (the persistent step's grid barriers), in
+ * polls of about 64 ns each; the default 2^25 is about two seconds. A wait
+ * that runs out leaves the step incomplete: the next synchronising call
+ * returns PPC_ERR_TIMEOUT, later persistent steps do nothing until then, and
+ * ppc_step refuses to run until the state is uploaded again. */
+int ppc_set_wait_limit(ppc_state* s, int64_t polls);
+
 /* Autotuner of the launch shape (no counterpart in the reference, whose
  * OpenMP loops have no launch shape): runs 2 x `steps` mechanics steps
  * (ppc_step) with each candidate shape — -3, -1 and -2 with 128 threads, 0
@@ -352,6 +370,12 @@ int ppc_update_cell_container_for_mechanics(ppc_state* s);
  * PPC_FLAG_TO_DIVIDE (src/cell.cpp:108-163), then removes as above. */
 int ppc_update_cell_container_for_phenotype(ppc_state* s);
 
+/* Number of agents of replicate `replicate` whose flag is `flag` (enum
+ * ppc_flag), counted on the device (no counterpart in the reference: a host
+ * caller sizing the container before a division pass counts this way instead
+ * of downloading every flag). Synchronises. */
+int ppc_count_flags(ppc_state* s, int32_t replicate, int32_t flag, int32_t* count);
+
 /* Sets PPC_FLAG_TO_REMOVE with probability p_death and otherwise
  * PPC_FLAG_TO_DIVIDE with probability p_divide per agent, from the state's
  * counter-based random stream (stand-in for the reference's phenotype models,
@@ -501,7 +525,11 @@ int ppc_get_profile(ppc_state* s, double* fused_ms, int64_t* fused_launches);
  * device buffers; results match ppc_get_mesh_bins: per-voxel counts and the
  * agents grouped by voxel, descending index inside a voxel. Scratch lives in
  * one fixed device array; sizes above PPC_NOALLOC_MAX_AGENTS or
- * PPC_NOALLOC_MAX_VOXELS return PPC_ERR_CAPACITY. Nothing is allocated. The
+ * PPC_NOALLOC_MAX_VOXELS return PPC_ERR_CAPACITY (the grid is sized in 64-bit
+ * arithmetic, so no mesh extent can wrap it). The in-voxel ordering pass costs
+ * c^2 loads for a voxel of c agents: negligible at tissue densities, about a
+ * second of GPU time if all PPC_NOALLOC_MAX_AGENTS agents share one voxel.
+ * Nothing is allocated. The
  * first call on a device looks the array's address up for that device, so
  * make that first call before any stream capture. All calls share the array:
  * calls whose work overlaps on the GPU race. Work is queued on `cuda_stream`

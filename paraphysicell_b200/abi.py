@@ -32,6 +32,7 @@ STATUS_NAMES = {
 FLAG_NONE, FLAG_TO_REMOVE, FLAG_TO_DIVIDE = 0, 1, 2
 PPC_FP64, PPC_FP32_FORCE = 0, 1
 PPC_TRANSFER_COPY_ENGINE, PPC_TRANSFER_ZERO_COPY = 0, 1
+PPC_STEP_KERNELS, PPC_STEP_PERSISTENT = 0, 1
 
 # reference defaults (src/data_storage_phenotype.cpp:62-125,194-214, src/cell.cpp:47-61)
 DEFAULT_RADIUS = 8.412710547954228

@@ -122,6 +122,12 @@ int map_errors(ppc_state* s, int32_t err)
 		return PPC_OK;
 	PPC_CUDA(cudaMemsetAsync(s->v.err, 0, sizeof(int32_t), s->stream));
 	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	if (err & ERR_TIMEOUT)
+	{
+		s->lost = true;
+		return fail(PPC_ERR_TIMEOUT, "a grid barrier of the persistent step gave up waiting; the state must be "
+									 "uploaded again");
+	}
 	if (err & ERR_NONFINITE)
 		return fail(PPC_ERR_NONFINITE, "an agent position is NaN or infinite");
 	if (err & ERR_OUT_OF_MESH)
@@ -565,6 +571,8 @@ int ensure_lists(ppc_state* s)
 // one fused mechanics step (+ phenotype container update)
 int enqueue_step(ppc_state* s, bool phenotype, double p_divide, double p_death)
 {
+	if (s->persistent && !phenotype)
+		return launch_step_persistent(s);
 	// the compaction right before the rebuild leaves its moves to k_bin_count
 	PPC_TRY(launch_fused(s));
 	PPC_TRY(launch_compact(s, false, !phenotype));
@@ -669,6 +677,8 @@ int run_steps(ppc_state* s, int32_t steps, bool phenotype, double p_divide, doub
 {
 	if (steps < 0)
 		return fail(PPC_ERR_ARG, "negative step count");
+	if (s->lost)
+		return fail(PPC_ERR_ARG, "a bounded device wait gave up in an earlier step: upload the state again");
 	if (steps > 0)
 		s->counts_known = false; // compaction and division change the counts
 	const bool graphs = s->use_graphs && !s->profiling;
@@ -719,6 +729,10 @@ int run_steps(ppc_state* s, int32_t steps, bool phenotype, double p_divide, doub
 	return PPC_OK;
 }
 
+// grid of a mesh (validated: positive voxel shapes, maxs >= mins); sizes in
+// 64-bit arithmetic, saturated at INT32_MAX per axis and in the product, so
+// an oversized mesh is rejected by the caller's voxel limit instead of
+// wrapping
 void mesh_info(const ppc_mesh& m, rep_info& R)
 {
 	R.voxels = 1;
@@ -729,11 +743,13 @@ void mesh_info(const ppc_mesh& m, rep_info& R)
 		R.mins_int[d] = m.bounding_box_mins[d];
 		R.maxs_int[d] = m.bounding_box_maxs[d];
 		R.shape[d] = m.voxel_shape[d];
-		int g = 1;
-		if (d < m.dims)
-			g = (m.bounding_box_maxs[d] - m.bounding_box_mins[d] + m.voxel_shape[d] - 1) / m.voxel_shape[d];
-		R.grid[d] = std::max(g, 1);
-		R.voxels *= R.grid[d];
+		int64_t g = 1;
+		if (d < m.dims && m.voxel_shape[d] > 0)
+			g = ((int64_t)m.bounding_box_maxs[d] - (int64_t)m.bounding_box_mins[d] + m.voxel_shape[d] - 1)
+				/ m.voxel_shape[d];
+		g = std::min<int64_t>(std::max<int64_t>(g, 1), INT32_MAX);
+		R.grid[d] = (int32_t)g;
+		R.voxels = std::min<int64_t>(R.voxels * g, (int64_t)INT32_MAX + 1);
 	}
 }
 
@@ -882,6 +898,7 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.first_end, C));
 	try_(alloc(s, v.pos_changed, 1));
 	try_(alloc(s, v.bin_active, 1));
+	try_(alloc(s, v.barrier, 2));
 	if (rc == PPC_OK && cudaMemset(v.first_end, 0x7f, sizeof(int32_t) * std::max<size_t>(C, 1)) != cudaSuccess)
 		rc = fail(PPC_ERR_CUDA, "cudaMemset failed");
 	if (rc == PPC_OK && cudaMemset(v.move_src, 0xff, sizeof(int32_t) * std::max<size_t>(C, 1)) != cudaSuccess)
@@ -1007,6 +1024,30 @@ int ppc_set_launch_shape(ppc_state* s, int32_t tile_edge, int32_t threads, int32
 	return PPC_OK;
 }
 
+int ppc_set_step_form(ppc_state* s, int32_t form)
+{
+	if (!s || (form != PPC_STEP_KERNELS && form != PPC_STEP_PERSISTENT))
+		return fail(PPC_ERR_ARG, "form must be PPC_STEP_KERNELS or PPC_STEP_PERSISTENT");
+	int coop = 0;
+	if (form == PPC_STEP_PERSISTENT
+		&& (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, s->device) != cudaSuccess || !coop))
+		return fail(PPC_ERR_UNSUPPORTED, "the device has no cooperative launch");
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	release_graph(s);
+	s->persistent = form == PPC_STEP_PERSISTENT;
+	return PPC_OK;
+}
+
+int ppc_set_wait_limit(ppc_state* s, int64_t polls)
+{
+	if (!s || polls < 1)
+		return fail(PPC_ERR_ARG, "the wait limit must be at least one poll");
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	release_graph(s);
+	s->wait_limit = polls;
+	return PPC_OK;
+}
+
 int ppc_set_host_transfer(ppc_state* s, int32_t mode)
 {
 	if (!s || (mode != PPC_TRANSFER_COPY_ENGINE && mode != PPC_TRANSFER_ZERO_COPY))
@@ -1055,6 +1096,7 @@ int ppc_upload(ppc_state* s, int32_t r, const ppc_agents* a)
 	c.spring_epoch = all[r].spring_epoch; // the draw streams continue, as in the reference's generator
 	PPC_CUDA(cudaMemcpy(&s->v.ctr[r], &c, sizeof c, cudaMemcpyHostToDevice));
 	s->lists_stale = false;
+	s->lost = false;
 	return transfer_in(s, r, a, true);
 }
 
@@ -1219,6 +1261,19 @@ int ppc_update_cell_container_for_phenotype(ppc_state* s)
 	PPC_TRY(launch_mark_remove(s));
 	PPC_TRY(launch_compact(s, true));
 	invalidate_bins(s);
+	return finish(s);
+}
+
+int ppc_count_flags(ppc_state* s, int32_t r, int32_t flag, int32_t* count)
+{
+	if (!valid(s, r) || !count)
+		return fail(PPC_ERR_ARG, "invalid arguments");
+	int32_t* d = reinterpret_cast<int32_t*>(s->v.err) + 1; // the word after the error word, spare
+	PPC_CUDA(cudaMemsetAsync(d, 0, sizeof(int32_t), s->stream));
+	PPC_TRY(launch_count_flags(s, r, flag, d));
+	PPC_CUDA(cudaMemcpyAsync(s->pinned_err + 1, d, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	*count = s->pinned_err[1];
 	return finish(s);
 }
 

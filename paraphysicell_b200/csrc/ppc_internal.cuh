@@ -41,7 +41,8 @@ enum : int32_t
 	ERR_OUT_OF_MESH = 4,
 	ERR_AGENT_CAPACITY = 8,
 	ERR_SPRING_CAPACITY = 16,
-	ERR_LIST_CAPACITY = 32
+	ERR_LIST_CAPACITY = 32,
+	ERR_TIMEOUT = 64 // a bounded wait of the persistent step gave up
 };
 
 struct rep_info
@@ -146,6 +147,7 @@ struct view
 	int32_t* first_end;	  // [C] INT32_MAX between spring attachment passes
 	int32_t* pos_changed; // set by an upload whose positions differ from the resident ones
 	int32_t* bin_active;  // the current rebuild runs (a conditional one may find nothing changed)
+	unsigned* barrier;	  // [2] grid barrier of the persistent step: arrivals, generation
 	int32_t* sorted;
 	int32_t* skey;
 	double4* spos4;
@@ -271,6 +273,9 @@ struct ppc_state
 	bool staged = false;
 	bool coop = false;
 	bool flat = true; // per-thread pass with batched candidate fetches (shape -3, the default)
+	bool persistent = false;		 // mechanics steps as one cooperative launch each (PPC_STEP_PERSISTENT)
+	long long wait_limit = 1LL << 25; // polls of a bounded device wait before it gives up
+	bool lost = false;				 // a bounded wait gave up: the state needs a fresh upload
 	int tile_threads = 128;
 	int tile_smem = 32 * 1024;
 
@@ -310,10 +315,12 @@ int launch_springs(ppc_state* s);
 int launch_spring_updates(ppc_state* s);
 int launch_positions(ppc_state* s);
 int launch_fused(ppc_state* s);
+int launch_step_persistent(ppc_state* s);
 int launch_compact(ppc_state* s, bool phenotype_pass, bool fold = false);
 int launch_mark_remove(ppc_state* s);
 int launch_divide(ppc_state* s);
 int launch_flag_by_draws(ppc_state* s, double p_divide, double p_death);
+int launch_count_flags(ppc_state* s, int32_t r, int32_t flag, int32_t* count);
 
 // packing between host-layout staging buffers and device arrays
 int launch_unpack_vec(ppc_state* s, double4* dst, const double* src, int32_t r, int32_t n, int32_t* changed = nullptr);

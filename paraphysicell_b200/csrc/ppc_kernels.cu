@@ -217,19 +217,12 @@ __device__ __forceinline__ void count_agent(const view& v, int cur, int s, int r
 // A conditional rebuild (after an upload of positions) runs only if the
 // upload changed some position; its decision goes to bin_active for the
 // other three kernels.
-__global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur, int conditional)
+// the count of the agents at previous key-ordered position t and at slot t
+__device__ __forceinline__ void bin_count_body(const view& v, int cur, int t, int lane)
 {
-	grid_wait();
-	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	const int lane = threadIdx.x & 31;
 	const bool ordered = *v.order_valid != 0;
 	const bool moves = *v.moves_pending != 0;
 	const bool appended = *v.appended != 0;
-	const bool active = !conditional || *v.pos_changed != 0 || moves || appended;
-	if (t == 0)
-		*v.bin_active = active ? 1 : 0;
-	if (!active)
-		return;
 	// both candidates first, so that their loads overlap
 	int sa = -1, ra = 0, sb = -1, rb = 0, local = 0;
 	if ((!ordered || appended) && t < v.total_cap && live(v, t, rb, local)
@@ -247,25 +240,33 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur, int con
 		count_agent(v, cur, sb, rb, lane, moves);
 }
 
-// Exclusive scan of the per-voxel counts into vstart (one block per tile of
-// 4096 voxels); a tile's offset is the sum of the totals of the tiles before
-// it (k_bin_count accumulates them). The counts are cleared at occupied
-// voxels by k_bin_fixup, the tile totals by k_bin_scatter.
-__global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
+__global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur, int conditional)
 {
 	grid_wait();
-	if (!*v.bin_active)
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	const bool active = !conditional || *v.pos_changed != 0 || *v.moves_pending != 0 || *v.appended != 0;
+	if (t == 0)
+		*v.bin_active = active ? 1 : 0;
+	if (!active)
 		return;
-	const int b = blockIdx.x;
+	bin_count_body(v, cur, t, threadIdx.x & 31);
+}
+
+// The scan of one tile of 4096 voxels by a block of THREADS threads.
+template <int THREADS>
+__device__ __forceinline__ void bin_scan_tile(const view& v, int b)
+{
+	constexpr int ITEMS = (1 << kTileShift) / THREADS;
+	static_assert(ITEMS % 4 == 0, "a thread scans whole int4 groups of its tile");
 	// the tile's counts first (counts are padded to whole tiles and zero past
 	// the last voxel), so their loads overlap the predecessor totals' loads
-	const int64_t i0 = ((int64_t)b << kTileShift) + (int64_t)threadIdx.x * kTileItems;
-	int c[kTileItems];
+	const int64_t i0 = ((int64_t)b << kTileShift) + (int64_t)threadIdx.x * ITEMS;
+	int c[ITEMS];
 	int sum = 0;
 	{
 		const int4* q = reinterpret_cast<const int4*>(v.vcnt + i0);
 #pragma unroll
-		for (int k = 0; k < kTileItems / 4; k++)
+		for (int k = 0; k < ITEMS / 4; k++)
 		{
 			int4 x = q[k];
 			c[4 * k] = x.x;
@@ -281,15 +282,15 @@ __global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
 	block_exclusive_scan(part, tile_base);
 
 #pragma unroll
-	for (int k = 0; k < kTileItems; k++)
+	for (int k = 0; k < ITEMS; k++)
 		sum += c[k];
 	int tile_total;
 	int run = tile_base + block_exclusive_scan(sum, tile_total);
-	if (i0 + kTileItems <= v.nvox)
+	if (i0 + ITEMS <= v.nvox)
 	{
 		int4* st = reinterpret_cast<int4*>(v.vstart + i0);
 #pragma unroll
-		for (int k = 0; k < kTileItems / 4; k++)
+		for (int k = 0; k < ITEMS / 4; k++)
 		{
 			int4 x;
 			x.x = run;
@@ -305,42 +306,50 @@ __global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
 	}
 	else
 	{
-		for (int k = 0; k < kTileItems; k++)
+		for (int k = 0; k < ITEMS; k++)
 			if (i0 + k < v.nvox)
 			{
 				v.vstart[i0 + k] = run;
 				run += c[k];
 			}
 	}
-	if (b == gridDim.x - 1 && threadIdx.x == blockDim.x - 1)
+	if (b == v.ntiles - 1 && threadIdx.x == blockDim.x - 1)
 	{
 		v.vstart[v.nvox] = run;
 		*v.cursor = run;
 	}
 }
 
-// provisional scatter; also hands the fixup its voxel's start and count so
-// the fixup need not look them up again
-__global__ void k_bin_scatter(view v)
+// Exclusive scan of the per-voxel counts into vstart (one block per tile of
+// 4096 voxels); a tile's offset is the sum of the totals of the tiles before
+// it (k_bin_count accumulates them). The counts are cleared at occupied
+// voxels by k_bin_fixup, the tile totals by k_bin_scatter.
+__global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
 {
 	grid_wait();
-	int s = blockIdx.x * blockDim.x + threadIdx.x;
-	if (s == 0)
-		*v.pos_changed = 0; // read by this rebuild's k_bin_count only
 	if (!*v.bin_active)
 		return;
-	if (blockIdx.x == 0)
+	bin_scan_tile<kThreads>(v, blockIdx.x);
+}
+
+// provisional scatter; also hands the fixup its voxel's start and count so
+// the fixup need not look them up again
+// block 0 of the scatter readies the counters of the next rebuild
+__device__ __forceinline__ void bin_scatter_resets(const view& v)
+{
+	for (int k = threadIdx.x; k < v.ntiles; k += blockDim.x)
+		v.tile_sum[k] = 0; // ready for the next rebuild's k_bin_count
+	for (int k = threadIdx.x; k < v.nreps; k += blockDim.x)
+		v.binned[k] = v.ctr[k].count; // the slots this rebuild's order lists
+	if (threadIdx.x == 0)
 	{
-		for (int k = threadIdx.x; k < v.ntiles; k += blockDim.x)
-			v.tile_sum[k] = 0; // ready for the next rebuild's k_bin_count
-		for (int k = threadIdx.x; k < v.nreps; k += blockDim.x)
-			v.binned[k] = v.ctr[k].count; // the slots this rebuild's order lists
-		if (threadIdx.x == 0)
-		{
-			*v.moves_pending = 0; // applied by this rebuild's k_bin_count
-			*v.appended = 0;	  // counted by it too
-		}
+		*v.moves_pending = 0; // applied by this rebuild's k_bin_count
+		*v.appended = 0;	  // counted by it too
 	}
+}
+
+__device__ __forceinline__ void bin_scatter_agent(const view& v, int s)
+{
 	if (s >= v.total_cap)
 		return;
 	int r, local;
@@ -350,28 +359,52 @@ __global__ void k_bin_scatter(view v)
 	const int rank = v.vrank[s];
 	const int st = v.vstart[key];
 	const int c = v.vcnt[key];
+	// the bounds hold after every complete count and scan; they guard the
+	// persistent step's phases that still run after another block gave up
+	// on a barrier
+	if ((unsigned)(st + rank) >= (unsigned)v.total_cap)
+	{
+		atomicOr(v.err, ERR_LIST_CAPACITY);
+		return;
+	}
 	v.tmp[st + rank] = s;
 	v.vsc[s] = make_int2(st, c);
+}
+
+__global__ void k_bin_scatter(view v)
+{
+	grid_wait();
+	int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s == 0)
+		*v.pos_changed = 0; // read by this rebuild's k_bin_count only
+	if (!*v.bin_active)
+		return;
+	if (blockIdx.x == 0)
+		bin_scatter_resets(v);
+	bin_scatter_agent(v, s);
 }
 
 // final place inside the voxel: descending slot order, which is the order
 // a serial run of the reference's fetch_sub scatter produces. Affinity rows
 // of up to four definitions are carried in registers.
-__global__ void k_bin_fixup(view v, int cur)
+// thread tp takes the agent the scatter put at provisional position tp;
+// its final position is in the same voxel's range, so the stores of
+// neighbouring threads land close together
+__device__ __forceinline__ void bin_fixup_agent(const view& v, int cur, int tp)
 {
-	grid_wait();
-	if (!*v.bin_active)
-		return;
-	// thread tp takes the agent the scatter put at provisional position tp;
-	// its final position is in the same voxel's range, so the stores of
-	// neighbouring threads land close together
-	const int tp = blockIdx.x * blockDim.x + threadIdx.x;
 	if (tp >= *v.cursor)
 		return;
 	const int s = v.tmp[tp];
+	if ((unsigned)s >= (unsigned)v.total_cap)
+		return;
 	const int r = rep_of(v, s);
 	const int32_t key = v.key[s];
 	const int2 sc = v.vsc[s];
+	if (sc.x < 0 || sc.y < 0 || (int64_t)sc.x + sc.y > v.total_cap)
+	{
+		atomicOr(v.err, ERR_LIST_CAPACITY);
+		return;
+	}
 	const double4 prm = v.prm[s];
 	double4 p = v.pos[cur][s];
 	const double rmad = v.rmad[s];
@@ -388,6 +421,8 @@ __global__ void k_bin_fixup(view v, int cur)
 	for (int u = 0; u < sc.y && sc.y > 1; u++)
 		rank += v.tmp[sc.x + u] > s;
 	const int t = sc.x + rank;
+	if (t >= v.total_cap)
+		return;
 	if (s == 0)
 		*v.order_valid = 1; // `sorted` now lists exactly the live slots
 	p.w = rmad * prm.x; // relative_maximum_adhesion_distance * radius
@@ -420,6 +455,14 @@ __global__ void k_bin_fixup(view v, int cur)
 	}
 }
 
+__global__ void k_bin_fixup(view v, int cur)
+{
+	grid_wait();
+	if (!*v.bin_active)
+		return;
+	bin_fixup_agent(v, cur, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // ---------------------------------------------------------------------------
 // neighbour scan: common_solver::for_each_in_mech_neighborhood +
 // update_cell_neighbors_single (reference: common_solver.h:77-105,
@@ -427,6 +470,15 @@ __global__ void k_bin_fixup(view v, int cur)
 // agents in bin order; calls f for every agent j != i with
 // distance <= rmad_i r_i + rmad_j r_j.
 // ---------------------------------------------------------------------------
+
+// run-time options of the fused passes: basement-membrane walls, springs,
+// a velocity to start the sums from
+enum : int
+{
+	FUSED_WALLS = 1,
+	FUSED_SPRINGS = 2,
+	FUSED_VEL = 4
+};
 
 constexpr int kList = 8; // neighbours recorded per thread before the pair pass runs
 constexpr int kFusedThreads = 128; // block size limit of the fused pass (five blocks per SM resident)
@@ -1031,19 +1083,20 @@ __device__ __forceinline__ bool filter_keep(const float4& pf, const float4& c, f
 	return !(d2f > adf * adf * 1.00001f);
 }
 
-template <int DIMS, bool WALLS, bool SPRINGS, bool VEL, bool F32>
-__global__ void __launch_bounds__(kStageThreads, 4) k_fused_staged(view v, int cur, int cap)
+// the block of agents at key-ordered positions [vb * blockDim, (vb + 1) *
+// blockDim); `stage` holds `cap` staged positions, then the neighbour lists;
+// opts: FUSED_WALLS | FUSED_SPRINGS | FUSED_VEL
+template <int DIMS, bool F32>
+__device__ void fused_staged_block(const view& v, int cur, int cap, int opts, int vb, float4* stage)
 {
-	grid_wait();
-	bump_spring_epochs(v);
+	const bool WALLS = (opts & FUSED_WALLS) != 0, SPRINGS = (opts & FUSED_SPRINGS) != 0, VEL = (opts & FUSED_VEL) != 0;
 	constexpr int NR = DIMS == 3 ? 9 : (DIMS == 2 ? 3 : 1);
-	extern __shared__ float4 stage[]; // cap staged positions, then the neighbour lists
 	__shared__ int s_a[NR], s_o[NR + 1];
 	__shared__ int2 s_rows[NR][kStageThreads]; // each thread's stencil-row bounds
 	int32_t* list = reinterpret_cast<int32_t*>(stage + cap) + threadIdx.x;
 	const int stride = blockDim.x;
 	const int nsorted = *v.cursor;
-	const int t0 = blockIdx.x * blockDim.x;
+	const int t0 = vb * blockDim.x;
 	if (t0 >= nsorted)
 		return;
 	const int tl = min(t0 + (int)blockDim.x, nsorted) - 1;
@@ -1382,6 +1435,15 @@ __global__ void __launch_bounds__(kStageThreads, 4) k_fused_staged(view v, int c
 		append_bad(v, r, s - R.base);
 }
 
+template <int DIMS, bool F32>
+__global__ void __launch_bounds__(kStageThreads, 4) k_fused_staged(view v, int cur, int cap, int opts)
+{
+	grid_wait();
+	bump_spring_epochs(v);
+	extern __shared__ float4 stage_raw[];
+	fused_staged_block<DIMS, F32>(v, cur, cap, opts, blockIdx.x, stage_raw);
+}
+
 // ---------------------------------------------------------------------------
 // fused step, one thread per agent, candidates fetched in batches.
 //
@@ -1445,26 +1507,16 @@ __device__ __forceinline__ void cp_async_wait_all()
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
-enum : int
-{
-	FUSED_WALLS = 1,
-	FUSED_SPRINGS = 2,
-	FUSED_VEL = 4
-};
 
+// the agent at key-ordered position t, with its block's shared slots `sm`
 template <int DIMS, bool F32>
-__global__ void __launch_bounds__(kFlatThreads, 5) k_fused_flat(view v, int cur, int opts)
+__device__ __forceinline__ void fused_flat_agent(const view& v, int cur, int opts, int t, flat_smem& sm)
 {
-	grid_wait();
-	bump_spring_epochs(v);
-	extern __shared__ __align__(16) unsigned char flat_raw[];
-	flat_smem& sm = *reinterpret_cast<flat_smem*>(flat_raw);
 	constexpr int NR = DIMS == 3 ? 9 : (DIMS == 2 ? 3 : 1);
 	const bool walls_on = (opts & FUSED_WALLS) != 0;
 	const bool springs_on = (opts & FUSED_SPRINGS) != 0;
 	const bool vel_on = (opts & FUSED_VEL) != 0;
 	const int tid = threadIdx.x;
-	const int t = blockIdx.x * kFlatThreads + tid;
 	if (t >= v.total_cap)
 		return;
 	// the agent's key-ordered rows, issued before the count is known (t is
@@ -1743,6 +1795,16 @@ __global__ void __launch_bounds__(kFlatThreads, 5) k_fused_flat(view v, int cur,
 		atomicOr(v.err, ERR_NONFINITE);
 	if (to_remove<DIMS>(R, p, flag))
 		append_bad(v, r, s - R.base);
+}
+
+template <int DIMS, bool F32>
+__global__ void __launch_bounds__(kFlatThreads, 5) k_fused_flat(view v, int cur, int opts)
+{
+	grid_wait();
+	bump_spring_epochs(v);
+	extern __shared__ __align__(16) unsigned char flat_raw[];
+	fused_flat_agent<DIMS, F32>(v, cur, opts, blockIdx.x * kFlatThreads + threadIdx.x,
+								*reinterpret_cast<flat_smem*>(flat_raw));
 }
 
 // ---------------------------------------------------------------------------
@@ -2031,11 +2093,8 @@ __device__ void springs_rename_attached(const view& v, int old_slot, int new_slo
 // Produces (hole, source) moves for the agents that end up in holes, the new
 // count and the death count; with springs it also replays every removal on
 // the spring rows in the reference's order.
-__global__ void k_compact_plan(view v, int phenotype_pass, int springs, int fold)
+__device__ void compact_plan_rep(const view& v, int r, int phenotype_pass, int springs, int fold, int32_t* sh)
 {
-	grid_wait();
-	__shared__ int32_t sh[kSortCap];
-	const int r = blockIdx.x;
 	rep_counters& C = v.ctr[r];
 	const int nb = min(C.nbad, v.reps[r].cap);
 	if (nb == 0)
@@ -2107,7 +2166,13 @@ __global__ void k_compact_plan(view v, int phenotype_pass, int springs, int fold
 	C.deaths += deaths;
 	C.nbad = 0;
 	v.nmoves[r] = nm;
+}
 
+__global__ void k_compact_plan(view v, int phenotype_pass, int springs, int fold)
+{
+	grid_wait();
+	__shared__ int32_t sh[kSortCap];
+	compact_plan_rep(v, blockIdx.x, phenotype_pass, springs, fold, sh);
 }
 
 // the planned moves, one thread per move
@@ -2419,6 +2484,18 @@ __global__ void k_flag_by_draws(view v, double p_divide, double p_death)
 		v.flags[s] = PPC_FLAG_TO_DIVIDE;
 }
 
+// agents of replicate r whose flag equals `flag`, added into *count
+__global__ void k_count_flags(view v, int r, int flag, int32_t* count)
+{
+	grid_wait();
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	const int n = v.ctr[r].count;
+	const int hit = i < n && v.flags[v.reps[r].base + i] == flag;
+	const int warp_total = __reduce_add_sync(0xffffffffu, hit);
+	if ((threadIdx.x & 31) == 0 && warp_total)
+		atomicAdd(count, warp_total);
+}
+
 __global__ void k_bump_draw_epoch(view v)
 {
 	grid_wait();
@@ -2692,6 +2769,147 @@ __global__ void k_springs_local(view v, int base, int n, int32_t* rows, int cap,
 	}
 }
 
+// ---------------------------------------------------------------------------
+// persistent step: one cooperative launch per mechanics step
+//
+// The grid stays resident for the whole step and walks its phases — the
+// fused pass, the compaction plan (folded into the count), the count, the
+// scan, the scatter and the fixup of the mesh rebuild — separated by grid
+// barriers, instead of six launches. Every phase is the same device code the
+// separate kernels run, over a grid-stride loop. A barrier waits at most
+// `limit` polls; a block that gives up sets ERR_TIMEOUT and leaves, every
+// block checks the flag after each barrier, and a later persistent launch on
+// the same state does nothing until the host has read the error.
+// ---------------------------------------------------------------------------
+
+constexpr int kPersistThreads = 128;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
+{
+	unsigned x;
+	asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(x) : "l"(p) : "memory");
+	return x;
+}
+
+__device__ __forceinline__ int ld_relaxed_i32(const int32_t* p)
+{
+	int x;
+	asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(x) : "l"(p) : "memory");
+	return x;
+}
+
+// bar[0] arrivals, bar[1] generation (bar[0] is zeroed before every launch)
+__device__ bool grid_barrier(const view& v, unsigned* bar, long long limit)
+{
+	__shared__ int s_ok;
+	__syncthreads();
+	if (threadIdx.x == 0)
+	{
+		int ok = 1;
+		const unsigned gen = ld_acquire_u32(bar + 1);
+		__threadfence();
+		if (atomicAdd(bar, 1u) == gridDim.x - 1)
+		{
+			atomicExch(bar, 0u);
+			__threadfence();
+			atomicAdd(bar + 1, 1u);
+		}
+		else
+		{
+			long long polls = 0;
+			while (ld_acquire_u32(bar + 1) == gen)
+			{
+				if (++polls > limit)
+				{
+					atomicOr(v.err, ERR_TIMEOUT);
+					ok = 0;
+					break;
+				}
+				__nanosleep(64);
+			}
+		}
+		__threadfence();
+		if (ok && (ld_relaxed_i32(v.err) & ERR_TIMEOUT))
+			ok = 0; // another block gave up: the phases after it are incomplete
+		s_ok = ok;
+	}
+	__syncthreads();
+	return s_ok != 0;
+}
+
+struct persist_args
+{
+	unsigned* bar;
+	long long limit;
+	int32_t opts;	// FUSED_* of the fused pass
+	int32_t cap;	// staged pass: staged positions per block (0: global memory)
+	int32_t springs; // the compaction replays removals on the spring rows
+};
+
+template <int DIMS, bool F32, bool STAGED>
+__global__ void __launch_bounds__(kPersistThreads) k_step_persistent(view v, int cur, persist_args pa)
+{
+	extern __shared__ __align__(16) unsigned char smem[];
+	__shared__ int s_skip;
+	if (threadIdx.x == 0)
+		s_skip = (ld_relaxed_i32(v.err) & ERR_TIMEOUT) != 0; // an earlier step gave up: wait for the host
+	__syncthreads();
+	if (s_skip)
+		return;
+	bump_spring_epochs(v);
+	const int nb = gridDim.x;
+	const int nxt = cur ^ 1;
+
+	// fused pass: positions from pos[cur] to pos[nxt]
+	if (STAGED)
+	{
+		const int nvb = (v.total_cap + kPersistThreads - 1) / kPersistThreads;
+		for (int vb = blockIdx.x; vb < nvb; vb += nb)
+		{
+			fused_staged_block<DIMS, F32>(v, cur, pa.cap, pa.opts, vb, reinterpret_cast<float4*>(smem));
+			__syncthreads(); // the block's shared rows are rewritten by the next tile
+		}
+	}
+	else
+		for (int t0 = blockIdx.x * kPersistThreads; t0 < v.total_cap; t0 += nb * kPersistThreads)
+			fused_flat_agent<DIMS, F32>(v, cur, pa.opts, t0 + threadIdx.x, *reinterpret_cast<flat_smem*>(smem));
+	if (!grid_barrier(v, pa.bar, pa.limit))
+		return;
+
+	// compaction plan, one replicate per block; its moves are applied by the count
+	for (int r = blockIdx.x; r < v.nreps; r += nb)
+	{
+		compact_plan_rep(v, r, 0, pa.springs, 1, reinterpret_cast<int32_t*>(smem));
+		__syncthreads(); // thread 0 finishes the serial plan before the next sort
+	}
+	if (!grid_barrier(v, pa.bar, pa.limit))
+		return;
+
+	// mesh rebuild: count, scan, scatter, fixup
+	if (blockIdx.x == 0 && threadIdx.x == 0)
+		*v.bin_active = 1;
+	for (int t0 = blockIdx.x * kPersistThreads; t0 < v.total_cap; t0 += nb * kPersistThreads)
+		bin_count_body(v, nxt, t0 + threadIdx.x, threadIdx.x & 31);
+	if (!grid_barrier(v, pa.bar, pa.limit))
+		return;
+	for (int b = blockIdx.x; b < v.ntiles; b += nb)
+		bin_scan_tile<kPersistThreads>(v, b);
+	if (!grid_barrier(v, pa.bar, pa.limit))
+		return;
+	if (blockIdx.x == 0)
+	{
+		if (threadIdx.x == 0)
+			*v.pos_changed = 0;
+		bin_scatter_resets(v);
+	}
+	for (int t0 = blockIdx.x * kPersistThreads; t0 < v.total_cap; t0 += nb * kPersistThreads)
+		bin_scatter_agent(v, t0 + threadIdx.x);
+	if (!grid_barrier(v, pa.bar, pa.limit))
+		return;
+	for (int t0 = blockIdx.x * kPersistThreads; t0 < v.total_cap; t0 += nb * kPersistThreads)
+		bin_fixup_agent(v, nxt, t0 + threadIdx.x);
+}
+
 } // namespace
 
 // ---------------------------------------------------------------------------
@@ -2842,49 +3060,45 @@ static void fused_dispatch(ppc_state* s, int b)
 #undef PPC_FUSED
 }
 
+// FUSED_WALLS | FUSED_SPRINGS | FUSED_VEL of the state's next fused pass
+static int fused_opts(ppc_state* s)
+{
+	return (s->params.virtual_wall_at_domain_edges ? FUSED_WALLS : 0)
+		   | ((s->has_springs && s->params.automated_spring_adhesion) ? FUSED_SPRINGS : 0)
+		   | (s->vel_dirty ? FUSED_VEL : 0);
+}
+
+// the staged pass's staging capacity (float4 positions) and dynamic shared bytes
+static void staged_shape(ppc_state* s, int& cap, size_t& dyn)
+{
+	const int nt = std::min(s->tile_threads, kStageThreads);
+	const int list_bytes = kList * nt * (int)sizeof(int32_t);
+	cap = s->staged ? std::max(0, (s->tile_smem - list_bytes) / (int)sizeof(float4)) : 0;
+	dyn = (size_t)cap * sizeof(float4) + list_bytes;
+}
+
 template <int DIMS>
 static int staged_dispatch(ppc_state* s)
 {
-	const bool walls = s->params.virtual_wall_at_domain_edges != 0;
-	const bool springs = s->has_springs && s->params.automated_spring_adhesion != 0;
-	const bool vel = s->vel_dirty;
+	const int opts = fused_opts(s);
 	const bool f32 = s->precision == PPC_FP32_FORCE;
 	cudaStream_t st = PPC_LAUNCH(s);
 	const int nt = std::min(s->tile_threads, kStageThreads);
-	const int list_bytes = kList * nt * (int)sizeof(int32_t);
-	const int cap = s->staged ? std::max(0, (s->tile_smem - list_bytes) / (int)sizeof(float4)) : 0;
-	const size_t dyn = (size_t)cap * sizeof(float4) + list_bytes;
+	int cap;
+	size_t dyn;
+	staged_shape(s, cap, dyn);
 	const int b = blocks_for(s->total_cap, nt);
-#define PPC_STAGED(W, S, V, F)                                                                                         \
-	if (walls == W && springs == S && vel == V && f32 == F)                                                            \
-	{                                                                                                                  \
-		auto k = k_fused_staged<DIMS, W, S, V, F>;                                                                     \
-		if (dyn + kStageStatic > 48 * 1024)                                                                            \
-			PPC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));                  \
-		pdl(k, b, nt, dyn, st, s->v, s->cur, cap);                                                                     \
-	}
-#define PPC_STAGED_F(W, S, V)                                                                                          \
-	PPC_STAGED(W, S, V, false)                                                                                         \
-	PPC_STAGED(W, S, V, true)
-	PPC_STAGED_F(false, false, false)
-	PPC_STAGED_F(false, false, true)
-	PPC_STAGED_F(false, true, false)
-	PPC_STAGED_F(false, true, true)
-	PPC_STAGED_F(true, false, false)
-	PPC_STAGED_F(true, false, true)
-	PPC_STAGED_F(true, true, false)
-	PPC_STAGED_F(true, true, true)
-#undef PPC_STAGED_F
-#undef PPC_STAGED
+	auto k = f32 ? k_fused_staged<DIMS, true> : k_fused_staged<DIMS, false>;
+	if (dyn + kStageStatic > 48 * 1024)
+		PPC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+	pdl(k, b, nt, dyn, st, s->v, s->cur, cap, opts);
 	return PPC_OK;
 }
 
 template <int DIMS>
 static int flat_dispatch(ppc_state* s)
 {
-	const int opts = (s->params.virtual_wall_at_domain_edges ? FUSED_WALLS : 0)
-					 | ((s->has_springs && s->params.automated_spring_adhesion) ? FUSED_SPRINGS : 0)
-					 | (s->vel_dirty ? FUSED_VEL : 0);
+	const int opts = fused_opts(s);
 	const int b = blocks_for(s->total_cap, kFlatThreads);
 	cudaStream_t st = PPC_LAUNCH(s);
 	const int dyn = (int)sizeof(flat_smem);
@@ -2898,6 +3112,81 @@ static int flat_dispatch(ppc_state* s)
 		PPC_CUDA(cudaFuncSetAttribute(k_fused_flat<DIMS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
 		pdl(k_fused_flat<DIMS, false>, b, kFlatThreads, dyn, st, s->v, s->cur, opts);
 	}
+	return PPC_OK;
+}
+
+template <int DIMS, bool F32, bool STAGED>
+static int persistent_launch(ppc_state* s, size_t dyn, const persist_args& pa)
+{
+	auto k = k_step_persistent<DIMS, F32, STAGED>;
+	PPC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+	int per_sm = 0;
+	PPC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kPersistThreads, dyn));
+	if (per_sm < 1)
+		return cuda_fail(cudaErrorInvalidConfiguration, "persistent step: no block fits an SM");
+	// every block must be resident at once (the barriers wait for all of them)
+	const int64_t want = ((int64_t)s->total_cap + kPersistThreads - 1) / kPersistThreads;
+	const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)per_sm * s->sm_count,
+																  std::max<int64_t>(want, s->nreps)));
+	cudaLaunchConfig_t cfg {};
+	cfg.gridDim = dim3(grid);
+	cfg.blockDim = dim3(kPersistThreads);
+	cfg.dynamicSmemBytes = dyn;
+	cfg.stream = s->stream;
+	cudaLaunchAttribute at[1];
+	at[0].id = cudaLaunchAttributeCooperative;
+	at[0].val.cooperative = 1;
+	cfg.attrs = at;
+	cfg.numAttrs = 1;
+	PPC_CUDA(cudaLaunchKernelEx(&cfg, k, s->v, s->cur, pa));
+	return PPC_OK;
+}
+
+// one mechanics step (fused pass, folded compaction, mesh rebuild) as one
+// cooperative launch
+int launch_step_persistent(ppc_state* s)
+{
+	persist_args pa {};
+	pa.bar = s->v.barrier;
+	pa.limit = s->wait_limit;
+	pa.opts = fused_opts(s);
+	pa.springs = s->has_springs ? 1 : 0;
+	const bool staged = !s->flat && (s->staged || s->coop);
+	size_t dyn = sizeof(flat_smem);
+	if (staged)
+	{
+		pa.cap = s->staged ? std::max(0, (s->tile_smem - kList * kPersistThreads * (int)sizeof(int32_t))
+											 / (int)sizeof(float4))
+						   : 0;
+		dyn = (size_t)pa.cap * sizeof(float4) + (size_t)kList * kPersistThreads * sizeof(int32_t);
+	}
+	dyn = std::max(dyn, (size_t)kSortCap * sizeof(int32_t)); // the compaction plan's sort buffer
+	PPC_CUDA(cudaMemsetAsync(s->v.barrier, 0, sizeof(unsigned), s->stream));
+	const bool f32 = s->precision == PPC_FP32_FORCE;
+	s->launches++;
+	int rc;
+#define PPC_PERSIST(D)                                                                                                 \
+	if (staged)                                                                                                        \
+		rc = f32 ? persistent_launch<D, true, true>(s, dyn, pa) : persistent_launch<D, false, true>(s, dyn, pa);       \
+	else                                                                                                               \
+		rc = f32 ? persistent_launch<D, true, false>(s, dyn, pa) : persistent_launch<D, false, false>(s, dyn, pa);
+	if (s->dims == 1)
+	{
+		PPC_PERSIST(1)
+	}
+	else if (s->dims == 2)
+	{
+		PPC_PERSIST(2)
+	}
+	else
+	{
+		PPC_PERSIST(3)
+	}
+#undef PPC_PERSIST
+	if (rc != PPC_OK)
+		return rc;
+	s->cur ^= 1;
+	s->vel_dirty = false;
 	return PPC_OK;
 }
 
@@ -2995,6 +3284,14 @@ int launch_flag_by_draws(ppc_state* s, double p_divide, double p_death)
 	const int b = blocks_for(s->total_cap, kThreads);
 	pdl(k_flag_by_draws, b, kThreads, 0, PPC_LAUNCH(s), s->v, p_divide, p_death);
 	pdl(k_bump_draw_epoch, blocks_for(s->nreps, kThreads), kThreads, 0, PPC_LAUNCH(s), s->v);
+	PPC_CHECK_LAUNCH();
+	return PPC_OK;
+}
+
+int launch_count_flags(ppc_state* s, int32_t r, int32_t flag, int32_t* count)
+{
+	pdl(k_count_flags, blocks_for(s->reps[r].cap, kThreads), kThreads, 0, PPC_LAUNCH(s), s->v, (int)r, (int)flag,
+		count);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }

@@ -162,7 +162,10 @@ __global__ void k_na_scatter(int n, int32_t* scratch)
 	scratch[kOffTmp + st + rank] = i;
 }
 
-// final place inside the voxel: descending agent index
+// final place inside the voxel: descending agent index. Each agent counts
+// the larger indices of its voxel, so a voxel of c agents costs c^2 loads:
+// nothing at tissue densities (a few agents per voxel), about 1.7e10 loads
+// for the degenerate case of all PPC_NOALLOC_MAX_AGENTS agents in one voxel.
 __global__ void k_na_order(int n, const int32_t* scratch, int32_t* agents)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -193,13 +196,17 @@ extern "C" int ppc_bin_agents_noalloc(const ppc_mesh* mesh, const double* positi
 	}
 	na_mesh m {};
 	m.dims = mesh->dims;
+	// grid sizes in 64-bit arithmetic, each axis and the running product
+	// checked against the scratch's voxel limit before the next multiply, so
+	// no extent of the 32-bit mesh fields can wrap the voxel count
 	int64_t nvox = 1;
+	bool too_many = false;
 	for (int d = 0; d < 3; d++)
 	{
 		m.mins[d] = mesh->bounding_box_mins[d];
 		m.maxs[d] = mesh->bounding_box_maxs[d];
 		m.shape[d] = mesh->voxel_shape[d];
-		int g = 1;
+		int64_t g = 1;
 		if (d < mesh->dims)
 		{
 			if (mesh->voxel_shape[d] <= 0 || mesh->bounding_box_maxs[d] < mesh->bounding_box_mins[d])
@@ -207,17 +214,21 @@ extern "C" int ppc_bin_agents_noalloc(const ppc_mesh* mesh, const double* positi
 				ppc::set_error("ppc_bin_agents_noalloc: invalid mesh");
 				return PPC_ERR_ARG;
 			}
-			g = (mesh->bounding_box_maxs[d] - mesh->bounding_box_mins[d] + mesh->voxel_shape[d] - 1)
-				/ mesh->voxel_shape[d];
+			const int64_t extent = (int64_t)mesh->bounding_box_maxs[d] - (int64_t)mesh->bounding_box_mins[d];
+			g = (extent + mesh->voxel_shape[d] - 1) / mesh->voxel_shape[d];
 		}
-		m.grid[d] = g < 1 ? 1 : g;
-		nvox *= m.grid[d];
+		g = g < 1 ? 1 : g;
+		too_many = too_many || g > PPC_NOALLOC_MAX_VOXELS;
+		nvox = too_many ? PPC_NOALLOC_MAX_VOXELS + 1 : nvox * g;
+		too_many = too_many || nvox > PPC_NOALLOC_MAX_VOXELS;
+		m.grid[d] = (int32_t)(too_many ? 1 : g);
 	}
-	if (count > PPC_NOALLOC_MAX_AGENTS || nvox > PPC_NOALLOC_MAX_VOXELS)
+	if (count > PPC_NOALLOC_MAX_AGENTS || too_many)
 	{
 		ppc::set_error("ppc_bin_agents_noalloc: at most " + std::to_string(PPC_NOALLOC_MAX_AGENTS) + " agents and "
 					   + std::to_string(PPC_NOALLOC_MAX_VOXELS) + " voxels fit its fixed scratch (asked for "
-					   + std::to_string(count) + " agents, " + std::to_string(nvox) + " voxels)");
+					   + std::to_string(count) + " agents, "
+					   + (too_many ? std::string("more than the limit of") : std::to_string(nvox)) + " voxels)");
 		return PPC_ERR_CAPACITY;
 	}
 	m.nvox = (int32_t)nvox;

@@ -37,6 +37,7 @@ EXPORTS = (
     "ppc_set_profiling", "ppc_get_profile", "ppc_set_launch_shape", "ppc_autotune",
     "ppc_update_cell_cell_interactions", "ppc_update_motility_fields", "ppc_set_host_transfer",
     "ppc_upload_interactions", "ppc_download_interactions", "ppc_upload_motility", "ppc_download_motility",
+    "ppc_count_flags", "ppc_set_step_form", "ppc_set_wait_limit",
     "ppc_bin_agents_noalloc",
 ) + tuple("ppc_" + e for e in ENTRY_POINTS)
 
@@ -67,6 +68,7 @@ def lib():
         L.ppc_host_free.restype = None
         L.ppc_get_event_counts.argtypes = [vp, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         L.ppc_flag_by_draws.argtypes = [vp, C.c_double, C.c_double]
+        L.ppc_count_flags.argtypes = [vp, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]
         L.ppc_step.argtypes = [vp, C.c_int32]
         L.ppc_step_with_phenotype.argtypes = [vp, C.c_int32, C.c_double, C.c_double]
         L.ppc_get_neighbors.argtypes = [vp, C.c_int32, vp, vp, C.c_int32]
@@ -78,6 +80,8 @@ def lib():
         L.ppc_set_profiling.argtypes = [vp, C.c_int32]
         L.ppc_set_launch_shape.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32]
         L.ppc_set_host_transfer.argtypes = [vp, C.c_int32]
+        L.ppc_set_step_form.argtypes = [vp, C.c_int32]
+        L.ppc_set_wait_limit.argtypes = [vp, C.c_int64]
         L.ppc_autotune.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.ppc_get_profile.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
         L.ppc_last_error.restype = C.c_char_p
@@ -175,6 +179,11 @@ class Simulation:
         _check(lib().ppc_get_count(self.h, replicate, C.byref(n)), "ppc_get_count")
         return n.value
 
+    def count_flags(self, flag, replicate=0):
+        n = C.c_int32()
+        _check(lib().ppc_count_flags(self.h, replicate, flag, C.byref(n)), "ppc_count_flags")
+        return n.value
+
     def event_counts(self, replicate=0):
         d, k = C.c_int64(), C.c_int64()
         _check(lib().ppc_get_event_counts(self.h, replicate, C.byref(d), C.byref(k)), "ppc_get_event_counts")
@@ -197,6 +206,13 @@ class Simulation:
     def set_host_transfer(self, mode):
         """abi.PPC_TRANSFER_COPY_ENGINE (the default) or PPC_TRANSFER_ZERO_COPY."""
         _check(lib().ppc_set_host_transfer(self.h, mode), "ppc_set_host_transfer")
+
+    def set_step_form(self, form):
+        """abi.PPC_STEP_KERNELS (the default) or PPC_STEP_PERSISTENT."""
+        _check(lib().ppc_set_step_form(self.h, form), "ppc_set_step_form")
+
+    def set_wait_limit(self, polls):
+        _check(lib().ppc_set_wait_limit(self.h, polls), "ppc_set_wait_limit")
 
     def set_launch_shape(self, tile_edge, threads, smem_bytes=32 * 1024):
         _check(lib().ppc_set_launch_shape(self.h, tile_edge, threads, smem_bytes), "ppc_set_launch_shape")

@@ -16,9 +16,12 @@
 // src/environment.h) for the fields the mechanics path uses.
 //
 // Residency follows the pattern the reference's simulator uses for BioFVM's
-// device solver (src/simulator.cpp:95-118): after a solver call the agents
-// live on the GPU; host code that reads or writes `e.data` calls
-// `e.sync_to_host()` first, and the next solver call uploads the host data.
+// device solver (src/simulator.cpp:95-118), with one state more: after a
+// solver call the agents live on the GPU; host code that reads `e.data` calls
+// `e.sync_to_host(access::read)` first (both copies are then current and the
+// next solver call uploads nothing), host code that also writes it calls
+// `e.sync_to_host()` (access::read_write, the default) or, after a read sync,
+// `e.host_modified()`, and the next solver call uploads the host data.
 //
 // Threading: like the reference, every entry point may be called by all
 // threads of an enclosing `omp parallel` region (src/simulator.cpp:302) or
@@ -154,6 +157,62 @@ struct cell_data
 	int64_t next_id = 0;
 };
 
+// The agents of each mechanics voxel, in bin order, as a contiguous index
+// table: bins[v] is a read-only range with size(), begin(), end() and
+// operator[] like the reference's std::vector<index_t> per voxel
+// (environment::cells_in_mechanics_voxels, src/environment.h:44), without
+// one heap vector per voxel.
+class voxel_bins
+{
+public:
+	struct range
+	{
+		const index_t* b;
+		const index_t* e;
+		size_t size() const { return (size_t)(e - b); }
+		bool empty() const { return b == e; }
+		const index_t* begin() const { return b; }
+		const index_t* end() const { return e; }
+		index_t operator[](size_t k) const { return b[k]; }
+	};
+	struct iterator
+	{
+		const voxel_bins* bins;
+		size_t v;
+		range operator*() const { return (*bins)[v]; }
+		iterator& operator++()
+		{
+			++v;
+			return *this;
+		}
+		bool operator!=(const iterator& o) const { return v != o.v; }
+	};
+
+	size_t size() const { return start.empty() ? 0 : start.size() - 1; }
+	range operator[](size_t v) const { return { agents.data() + start[v], agents.data() + start[v + 1] }; }
+	iterator begin() const { return { this, 0 }; }
+	iterator end() const { return { this, size() }; }
+
+	// voxel_counts[v] agents per voxel, the agents concatenated in voxel order
+	void assign(const std::vector<int32_t>& voxel_counts, std::vector<int32_t>&& concatenated)
+	{
+		start.assign(voxel_counts.size() + 1, 0);
+		for (size_t v = 0; v < voxel_counts.size(); v++)
+			start[v + 1] = start[v] + voxel_counts[v];
+		agents = std::move(concatenated);
+	}
+
+private:
+	std::vector<int64_t> start;
+	std::vector<index_t> agents;
+};
+
+enum class access
+{
+	read,	   // host code only reads e.data: the device copy stays current
+	read_write // host code may change e.data: the next solver call uploads it
+};
+
 // The mechanics part of the reference's environment (src/environment.h:12-60).
 struct environment
 {
@@ -182,14 +241,16 @@ struct environment
 	index_t cell_definitions_count;
 	uint64_t random_seed = 0;
 
-	std::vector<std::vector<index_t>> cells_in_mechanics_voxels; // filled by sync_to_host
+	voxel_bins cells_in_mechanics_voxels; // filled by sync_to_host
 	cell_data data;
 
 	// ---- residency ----
 	ppc_state* device = nullptr;
 	bool device_current = false; // the GPU holds the latest agent data
+	bool host_current = true;	 // e.data holds the latest agent data
 	index_t capacity = 0;
 	int32_t neighbor_capacity = 64; // per-agent list length on the device; grows on demand
+	int64_t divisions_base = 0, deaths_base = 0; // events of device states replaced by a larger one
 
 	// the reference's neighbour lists are unbounded vectors: grow the device
 	// lists until every list fits
@@ -223,6 +284,9 @@ struct environment
 		if (device)
 		{
 			sync_to_host();
+			// the new state's event counters start from zero
+			divisions_base = divisions_count;
+			deaths_base = deaths_count;
 			ppc_destroy(device);
 			device = nullptr;
 		}
@@ -283,24 +347,39 @@ struct environment
 		return a;
 	}
 
-	// host -> device when the host holds the latest data
+	// host -> device when the host holds the latest data; afterwards the device
+	// work makes the host copy stale
 	void sync_to_device()
 	{
 		ensure_state(data.agents_count * 2);
-		if (device_current)
-			return;
-		std::vector<int32_t> counts, rows;
-		ppc_agents a = view(true, counts, rows);
-		check(ppc_upload(device, 0, &a), "ppc_upload");
-		device_current = true;
+		if (!device_current)
+		{
+			std::vector<int32_t> counts, rows;
+			ppc_agents a = view(true, counts, rows);
+			check(ppc_upload(device, 0, &a), "ppc_upload");
+			device_current = true;
+		}
+		host_current = false;
 	}
 
+	// host code changed e.data after a read-only sync: the next solver call
+	// uploads it
+	void host_modified() { device_current = false; }
+
 	// device -> host (counterpart of simulator::sync_data_host); also fills
-	// states.neighbors and cells_in_mechanics_voxels
-	void sync_to_host()
+	// states.neighbors and cells_in_mechanics_voxels. With access::read the
+	// device copy stays current, so the next solver call uploads nothing.
+	void sync_to_host(access mode = access::read_write)
 	{
-		if (!device || !device_current)
-			return;
+		if (device && device_current && !host_current)
+			download_all();
+		if (mode == access::read_write)
+			device_current = false;
+	}
+
+private:
+	void download_all()
+	{
 		int32_t n = 0;
 		check(ppc_get_count(device, 0, &n), "ppc_get_count");
 		data.agents_count = n;
@@ -342,13 +421,12 @@ struct environment
 		check(ppc_get_voxel_count(device, 0, &voxels), "ppc_get_voxel_count");
 		std::vector<int32_t> vc(voxels), va(n > 0 ? n : 1);
 		check(ppc_get_mesh_bins(device, 0, vc.data(), va.data()), "ppc_get_mesh_bins");
-		cells_in_mechanics_voxels.assign(voxels, {});
-		size_t o = 0;
-		for (int64_t v = 0; v < voxels; v++)
-			for (int32_t k = 0; k < vc[v]; k++)
-				cells_in_mechanics_voxels[v].push_back(va[o++]);
+		va.resize(n);
+		cells_in_mechanics_voxels.assign(vc, std::move(va));
 		check(ppc_get_event_counts(device, 0, &divisions_count, &deaths_count), "ppc_get_event_counts");
-		device_current = false;
+		divisions_count += divisions_base;
+		deaths_count += deaths_base;
+		host_current = true;
 	}
 };
 
@@ -415,18 +493,19 @@ public:
 			check(ppc_update_cell_container_for_mechanics(e.device), "ppc_update_cell_container_for_mechanics");
 		});
 	}
-	// without BioFVM's release_internalized_substrates; grows the device
-	// state when divisions would exceed its capacity
+	// without BioFVM's release_internalized_substrates; the dividing agents
+	// are counted on the device, and the state grows (through the host) only
+	// when their daughters would exceed its capacity
 	void update_cell_container_for_phenotype(environment& e)
 	{
 		once_per_team([&] {
 			e.sync_to_device();
-			int64_t dividing = 0;
+			int32_t dividing = 0, n = 0;
+			check(ppc_count_flags(e.device, 0, PPC_FLAG_TO_DIVIDE, &dividing), "ppc_count_flags");
+			check(ppc_get_count(e.device, 0, &n), "ppc_get_count");
+			if (n + dividing + 1 > e.capacity)
 			{
-				e.sync_to_host();
-				for (auto f : e.data.flags)
-					dividing += f == cell_state_flag::to_divide;
-				e.ensure_state(e.data.agents_count + (index_t)dividing + 1);
+				e.ensure_state(n + dividing + 1);
 				e.sync_to_device();
 			}
 			check(ppc_update_cell_container_for_phenotype(e.device), "ppc_update_cell_container_for_phenotype");

@@ -236,6 +236,89 @@ static void fused_equals_separate()
 	report(ok, "solver.simulate_mechanics equals the separate entry points");
 }
 
+static void fill_ball(environment& e, int count, unsigned seed)
+{
+	for (int i = 0; i < count; i++)
+	{
+		const index_t k = e.data.add();
+		for (int d = 0; d < 3; d++)
+		{
+			seed = seed * 1103515245u + 12345u;
+			e.data.agent_data.positions[(size_t)k * 3 + d] = 150 + 300.0 * ((seed >> 8) & 0xffff) / 65536.0;
+		}
+		e.data.geometries.radius[k] = 8.412710547954228;
+		e.data.mechanics.cell_cell_repulsion_strength[k] = 10;
+		e.data.mechanics.cell_cell_adhesion_strength[k] = 0.4;
+		e.data.mechanics.relative_maximum_adhesion_distance[k] = 1.25;
+		e.data.mechanics.cell_adhesion_affinities[k] = 1;
+		e.data.agent_data.volumes[k] = 2494;
+		e.data.volumes.nuclear[k] = 540;
+	}
+}
+
+static int64_t launches(environment& e)
+{
+	int64_t n = 0;
+	check(ppc_get_launch_count(e.device, &n), "ppc_get_launch_count");
+	return n;
+}
+
+// a read-only host sync keeps the device copy current, so the next solver
+// call uploads nothing; a read-write sync makes it upload again; the
+// trajectory is the same either way
+static void residency_read_only()
+{
+	environment a(make_mesh(3, 600, 600, 600), 1), b(make_mesh(3, 600, 600, 600), 1);
+	fill_ball(a, 1500, 11);
+	fill_ball(b, 1500, 11);
+	solver sa, sb;
+	sa.initialize(a);
+	sb.initialize(b);
+	sa.containers.update_mechanics_mesh(a);
+	sb.containers.update_mechanics_mesh(b);
+	sa.simulate_mechanics(a, 3);
+	sb.simulate_mechanics(b, 3);
+	a.sync_to_host(access::read);
+	const int64_t l0 = launches(a);
+	sa.simulate_mechanics(a, 1);
+	const int64_t quiet = launches(a) - l0;
+	a.sync_to_host();
+	const int64_t l1 = launches(a);
+	sa.simulate_mechanics(a, 1);
+	const int64_t uploaded = launches(a) - l1;
+	sb.simulate_mechanics(b, 2);
+	a.sync_to_host(access::read);
+	b.sync_to_host(access::read);
+	const bool same = a.data.agents_count == b.data.agents_count
+					  && std::memcmp(a.data.agent_data.positions.data(), b.data.agent_data.positions.data(),
+									 sizeof(double) * a.data.agent_data.positions.size())
+							 == 0;
+	report(uploaded > quiet && same, "environment.sync_to_host(access::read) keeps the device copy");
+}
+
+// flagged divisions through containers_solver with the count taken on the
+// device; the state grows when the daughters exceed its capacity
+static void phenotype_divisions_grow_the_state()
+{
+	environment e(make_mesh(3, 600, 600, 600), 1);
+	fill_ball(e, 600, 5);
+	solver sv;
+	sv.initialize(e); // capacity 1200: twice the count
+	sv.containers.update_mechanics_mesh(e);
+	e.sync_to_host();
+	for (index_t i = 0; i < 600; i++)
+		e.data.flags[i] = cell_state_flag::to_divide;
+#pragma omp parallel
+	sv.containers.update_cell_container_for_phenotype(e);
+	e.sync_to_host(access::read);
+	bool ok = e.data.agents_count == 1200 && e.divisions_count == 600 && e.capacity > 1200;
+	int64_t max_id = 0;
+	for (index_t i = 0; i < e.data.agents_count; i++)
+		max_id = e.data.agent_data.ids[i] > max_id ? e.data.agent_data.ids[i] : max_id;
+	ok = ok && max_id == 1199;
+	report(ok, "containers_solver.update_cell_container_for_phenotype counts divisions on the device");
+}
+
 int main()
 {
 	try
@@ -251,6 +334,8 @@ int main()
 					neighbors_grid(dims, cells, adhesion);
 		container_remove();
 		fused_equals_separate();
+		residency_read_only();
+		phenotype_divisions_grow_the_state();
 	}
 	catch (const std::exception& x)
 	{

@@ -35,5 +35,5 @@ def test_reference_unit_tests_pass_through_host_layer():
     r = subprocess.run([exe], capture_output=True, text=True, timeout=600, env=dict(os.environ, OMP_NUM_THREADS="4"))
     print(r.stdout)
     lines = [l for l in r.stdout.splitlines() if l.startswith(("PASS", "FAIL"))]
-    assert len(lines) == 26, r.stdout + r.stderr
+    assert len(lines) == 28, r.stdout + r.stderr
     assert r.returncode == 0, r.stdout + r.stderr

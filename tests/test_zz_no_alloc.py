@@ -34,6 +34,36 @@ def _noalloc(L, mesh, pos_dev, n, counts_dev, agents_dev, stream):
                                     C.c_void_p(agents_dev), C.c_void_p(stream))
 
 
+def _line(n, seed):
+    """A 1-D mesh: agents on a 3000 um line (100 voxels)."""
+    from paraphysicell_b200.abi import AgentArrays, Params
+    rng = np.random.default_rng(seed)
+    mesh = Mesh.make(1, (0, 0, 0), (3000, 0, 0))
+    a = AgentArrays(n, 1, 1, n)
+    a.arrays["positions"][:n] = rng.uniform(0, 3000, n)
+    return mesh, Params.make(dt=0.1, ndefs=1), a
+
+
+def _odd_tiles(seed):
+    """4097 voxels (241 x 17 in 2-D, one past a 4096-voxel scan tile), so the
+    scan's last tile is partial and writes the final start entry."""
+    from paraphysicell_b200.abi import AgentArrays, Params
+    rng = np.random.default_rng(seed)
+    mesh = Mesh.make(2, (0, 0, 0), (241 * 30, 17 * 30, 0))
+    assert mesh.voxel_count() == 4097
+    n = 3000
+    a = AgentArrays(n, 2, 1, n)
+    a.arrays["positions"][: 2 * n] = (rng.random((n, 2)) * [241 * 30, 17 * 30]).ravel()
+    return mesh, Params.make(dt=0.1, ndefs=1), a
+
+
+def _empty(case):
+    """No agents: every voxel count must be zeroed, nothing else written."""
+    from paraphysicell_b200.abi import AgentArrays
+    mesh, params, a = case
+    return mesh, params, AgentArrays(0, a.dims, a.ndefs, 4)
+
+
 def test_noalloc_binning_matches_state_bins_on_consecutive_calls():
     import torch
 
@@ -41,7 +71,8 @@ def test_noalloc_binning_matches_state_bins_on_consecutive_calls():
 
     build.ensure_built()
     L = device.lib()
-    cases = [wl.config2(seed=31), wl.config1(seed=32), wl.scaled(wl.config5, 20000, seed=33)]
+    cases = [wl.config2(seed=31), wl.config1(seed=32), wl.scaled(wl.config5, 20000, seed=33), _line(1500, seed=34),
+             _odd_tiles(seed=35), _empty(wl.config2(seed=36))]
     stream = torch.cuda.current_stream().cuda_stream
     for mesh, params, a in cases:
         want_counts, want_agents = _reference_bins(mesh, params, a)
