@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PPC_ABI_VERSION 1
+#define PPC_ABI_VERSION 2
 
 /* Status codes. The reference has no error reporting (all entry points are
  * void); these are new. */
@@ -299,6 +299,22 @@ int ppc_update_cell_forces(ppc_state* s);
  * succeeds. Motile agents go through ppc_update_motility_fields. */
 int ppc_update_motility(ppc_state* s);
 
+/* Standard rules that set an agent's migration bias direction when it
+ * redraws its walk (the reference's update_migration_bias_direction
+ * callbacks, set by the builder from the XML: src/builder.cpp:1184-1232). */
+enum ppc_direction_rule
+{
+	PPC_DIRECTION_NONE = 0,		  /* the direction the caller set */
+	PPC_DIRECTION_CHEMOTAXIS = 1, /* chemotaxis_function: the gradient of substrate
+									 chemotaxis_index times chemotaxis_direction,
+									 normalised (src/original/core/standard_models.cpp:542-555) */
+	PPC_DIRECTION_ADVANCED_CHEMOTAXIS = 2, /* advanced_chemotaxis_function<false>: the
+											  gradients weighted by the chemotactic
+											  sensitivities, normalised (:557-583) */
+	PPC_DIRECTION_ADVANCED_CHEMOTAXIS_NORMALIZED = 3 /* advanced_chemotaxis_function<true>:
+														each gradient normalised first */
+};
+
 /* Motility fields of one replicate (reference: cell_data motilities.*,
  * defaults src/data_storage_phenotype.cpp:245-256), host memory, one row per
  * agent in the state's agent order (`count` = the replicate's count). */
@@ -315,9 +331,35 @@ typedef struct ppc_motility
 	const double* persistence_time;			 /* [count] */
 	const double* migration_speed;			 /* [count] */
 	const double* migration_bias;			 /* [count] */
-	const double* migration_bias_direction;	 /* [count*dims] */
+	double* migration_bias_direction;		 /* [count*dims], read, and written by a direction rule */
 	double* motility_vector;				 /* [count*dims], read and written */
+	/* direction rules (NULL direction_rule: PPC_DIRECTION_NONE for all) */
+	const uint8_t* direction_rule;			 /* [count] enum ppc_direction_rule */
+	const int32_t* chemotaxis_index;		 /* [count] substrate of PPC_DIRECTION_CHEMOTAXIS */
+	const double* chemotaxis_direction;		 /* [count] +1 up the gradient, -1 down */
+	const double* chemotactic_sensitivities; /* [count*substrates] weights of the advanced rules */
+	int32_t substrates;						 /* columns of chemotactic_sensitivities */
+	int32_t reserved;
 } ppc_motility;
+
+/* Substrate gradients of one replicate's diffusion mesh, the input of the
+ * chemotaxis rules (the reference reads them with agent::nearest_gradient of
+ * the absent paraBioFVM library). The diffusion mesh shares the replicate's
+ * bounding box; voxel_shape gives its voxel edges, its grid is
+ * ceil(extent / voxel_shape) per axis like the mechanics mesh, and an agent's
+ * voxel is found by the same truncation. `gradients` holds, per diffusion
+ * voxel (x fastest, then y, then z), per substrate, the x, y and z components
+ * (3 values even in 1-D and 2-D). */
+typedef struct ppc_gradient_field
+{
+	int32_t substrates;
+	int32_t voxel_shape[3];
+	const double* gradients; /* [voxels * substrates * 3] */
+} ppc_gradient_field;
+
+/* Copies replicate r's gradient field to the device, where the motility pass
+ * reads it (replacing any earlier field of that replicate). Synchronises. */
+int ppc_upload_gradients(ppc_state* s, int32_t r, const ppc_gradient_field* field);
 
 /* Makes the motility fields of replicate r resident on the device (rows in
  * the state's agent order, `count` = the replicate's count): from then on
@@ -338,11 +380,13 @@ int ppc_download_motility(ppc_state* s, int32_t r, ppc_motility* fields);
  * PPC_DRAW_MOTILITY); the walk's angle and z are the next two draws — mixes
  * it with migration_bias_direction by migration_bias, scales it to
  * migration_speed, and adds its motility vector to its resident velocity.
- * The reference's per-agent direction-update callbacks (chemotaxis) are not
- * run: the caller sets migration_bias_direction. With `fields` NULL the
+ * Agents with a direction rule (ppc_direction_rule) first set their
+ * migration bias direction from the uploaded gradient field, as the
+ * reference's callback does right after the walk is drawn; the others keep
+ * the direction the caller set. With `fields` NULL the
  * resident fields (ppc_upload_motility) are used and nothing is copied;
  * otherwise `fields` is uploaded (and becomes the resident copy), and the
- * motility vectors are written back to it. Synchronizes. */
+ * motility vectors and bias directions are written back to it. Synchronizes. */
 int ppc_update_motility_fields(ppc_state* s, int32_t replicate, ppc_motility* fields);
 
 /* position_solver::update_basement_membrane_interactions (reference: src/solver/host/position_solver.cpp:316-335). */

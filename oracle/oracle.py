@@ -10,7 +10,7 @@ import ctypes as C
 import os
 import subprocess
 
-from paraphysicell_b200.abi import Agents, Interactions, Mesh, Motility, Params, PPCError
+from paraphysicell_b200.abi import Agents, GradientField, Interactions, Mesh, Motility, Params, PPCError
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libppc_oracle.so")
@@ -58,6 +58,7 @@ def lib():
         L.orc_upload_interactions.argtypes = [vp, C.POINTER(Interactions), C.c_int32]
         L.orc_download_interactions.argtypes = [vp, C.POINTER(Interactions)]
         L.orc_upload_motility.argtypes = [vp, C.POINTER(Motility)]
+        L.orc_upload_gradients.argtypes = [vp, C.POINTER(GradientField)]
         L.orc_download_motility.argtypes = [vp, C.POINTER(Motility)]
         L.orc_get_neighbors.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_int32]
         L.orc_get_mesh_bins.argtypes = [vp, C.c_void_p, C.c_void_p]
@@ -146,6 +147,11 @@ class Oracle:
         if rc != 0:
             raise PPCError(rc, "orc_download_interactions")
         return fields
+
+    def upload_gradients(self, field):
+        rc = self.L.orc_upload_gradients(self.h, C.byref(field))
+        if rc != 0:
+            raise PPCError(rc, "orc_upload_gradients")
 
     def upload_motility(self, fields):
         rc = self.L.orc_upload_motility(self.h, C.byref(fields.struct()))

@@ -116,21 +116,36 @@ struct world
 	struct mot_store
 	{
 		bool on = false;
-		std::vector<uint8_t> motile, restrict2d;
-		std::vector<real_t> persistence, speed, bias, direction, vector;
+		int S = 0; // chemotactic sensitivities per agent
+		std::vector<uint8_t> motile, restrict2d, rule;
+		std::vector<real_t> persistence, speed, bias, direction, vector, chemo_dir, sens;
+		std::vector<int32_t> chemo_index;
 
 		template <typename F>
 		void each(F&& f, int dims)
 		{
 			f(motile, 1);
 			f(restrict2d, 1);
+			f(rule, 1);
 			f(persistence, 1);
 			f(speed, 1);
 			f(bias, 1);
 			f(direction, dims);
 			f(vector, dims);
+			f(chemo_index, 1);
+			f(chemo_dir, 1);
+			f(sens, S);
 		}
 	} mot;
+
+	// substrate gradients of the diffusion mesh (agent::nearest_gradient of
+	// the absent paraBioFVM): per voxel, per substrate, x, y, z
+	struct gradient_field
+	{
+		int S = 0, grid[3] = { 1, 1, 1 };
+		real_t shape[3] = { 1, 1, 1 };
+		std::vector<real_t> g;
+	} grad;
 
 	// row `dst` of every resident column takes row `src`'s values
 	void copy_rows(index_t dst, index_t src)
@@ -849,6 +864,64 @@ constexpr real_t ix_zero_threshold = 1e-16; // reference: src/solver/host/solver
 /* ---- motility (reference: src/solver/host/position_solver.cpp:115-145,198-212,288-314,
         solver_helper.h:82-101,160-182,250-287) ---- */
 
+// normalize (reference: src/solver/host/solver_helper.h:30-45)
+void normalize_vec(real_t* x, int dims)
+{
+	real_t length = 0;
+	for (int d = 0; d < dims; d++)
+		length += x[d] * x[d];
+	length = std::sqrt(length);
+	for (int d = 0; d < dims; d++)
+		x[d] = length > ix_zero_threshold ? x[d] / length : 0;
+}
+
+// the gradient of substrate q in the diffusion voxel holding agent i
+void nearest_gradient(const world& w, index_t i, int q, real_t* g)
+{
+	const int dims = w.mesh.dims;
+	int c[3] = { 0, 0, 0 };
+	for (int d = 0; d < dims; d++)
+	{
+		const real_t f = (w.pos[(size_t)i * dims + d] - w.mesh.mins[d]) / w.grad.shape[d];
+		const int k = f > 0 ? (int)f : 0;
+		c[d] = k < w.grad.grid[d] ? k : w.grad.grid[d] - 1;
+	}
+	const int64_t vox = c[0] + (int64_t)w.grad.grid[0] * (c[1] + (int64_t)w.grad.grid[1] * c[2]);
+	for (int d = 0; d < dims; d++)
+		g[d] = w.grad.g[(size_t)(vox * w.grad.S + q) * 3 + d];
+}
+
+// chemotaxis_function and advanced_chemotaxis_function<normalize>
+// (reference: src/original/core/standard_models.cpp:542-583)
+void direction_rule(const world& w, const ppc_motility& f, index_t i, int rule)
+{
+	const int dims = w.mesh.dims;
+	real_t* dir = f.migration_bias_direction + (size_t)i * dims;
+	if (rule == PPC_DIRECTION_CHEMOTAXIS)
+	{
+		real_t g[3];
+		nearest_gradient(w, i, f.chemotaxis_index[i], g);
+		for (int d = 0; d < dims; d++)
+			dir[d] = g[d] * f.chemotaxis_direction[i];
+	}
+	else
+	{
+		for (int d = 0; d < dims; d++)
+			dir[d] = 0;
+		for (int q = 0; q < w.grad.S; q++)
+		{
+			real_t g[3];
+			nearest_gradient(w, i, q, g);
+			if (rule == PPC_DIRECTION_ADVANCED_CHEMOTAXIS_NORMALIZED)
+				normalize_vec(g, dims);
+			const real_t wgt = q < f.substrates ? f.chemotactic_sensitivities[(size_t)i * f.substrates + q] : 0.0;
+			for (int d = 0; d < dims; d++)
+				dir[d] += g[d] * wgt;
+		}
+	}
+	normalize_vec(dir, dims);
+}
+
 // update_motility_single for every agent, with the reference's random walk
 // from counter-based draws; the direction-update callbacks are not run. The
 // reference passes the whole restrict_to_2d array to random_walk, whose bool
@@ -870,6 +943,11 @@ void motility(world& w, ppc_motility& f)
 			real_t walk[3] = { 0, 0, 0 };
 			const bool planar = dims == 3 && (f.restrict_per_agent ? f.restrict_to_2d[i] != 0 : true);
 			ppc_random_walk(planar ? 2 : dims, w.seed, epoch, 0, (uint64_t)i, PPC_DRAW_MOTILITY + 1u, walk);
+			// update_migration_bias_direction_f runs after the walk is drawn
+			// (position_solver.cpp:133-136)
+			const int rule = f.direction_rule ? (int)f.direction_rule[i] : (int)PPC_DIRECTION_NONE;
+			if (rule != PPC_DIRECTION_NONE && !w.grad.g.empty())
+				direction_rule(w, f, i, rule);
 			const real_t bias = f.migration_bias[i];
 			for (int d = 0; d < dims; d++)
 				mv[d] = (1 - bias) * walk[d] + bias * f.migration_bias_direction[(size_t)i * dims + d];
@@ -1107,6 +1185,11 @@ ppc_motility mot_view(world& w, int32_t per_agent)
 	v.migration_bias = m.bias.data();
 	v.migration_bias_direction = m.direction.data();
 	v.motility_vector = m.vector.data();
+	v.direction_rule = m.rule.data();
+	v.chemotaxis_index = m.chemo_index.data();
+	v.chemotaxis_direction = m.chemo_dir.data();
+	v.chemotactic_sensitivities = m.sens.data();
+	v.substrates = m.S;
 	return v;
 }
 
@@ -1154,8 +1237,13 @@ void copy_mot(const ppc_motility& dst, const ppc_motility& src, index_t n, int d
 	copy_col(const_cast<real_t*>(dst.persistence_time), src.persistence_time, N);
 	copy_col(const_cast<real_t*>(dst.migration_speed), src.migration_speed, N);
 	copy_col(const_cast<real_t*>(dst.migration_bias), src.migration_bias, N);
-	copy_col(const_cast<real_t*>(dst.migration_bias_direction), src.migration_bias_direction, N * dims);
+	copy_col(dst.migration_bias_direction, src.migration_bias_direction, N * dims);
 	copy_col(dst.motility_vector, src.motility_vector, N * dims);
+	copy_col(const_cast<uint8_t*>(dst.direction_rule), src.direction_rule, N);
+	copy_col(const_cast<int32_t*>(dst.chemotaxis_index), src.chemotaxis_index, N);
+	copy_col(const_cast<real_t*>(dst.chemotaxis_direction), src.chemotaxis_direction, N);
+	copy_col(const_cast<real_t*>(dst.chemotactic_sensitivities), src.chemotactic_sensitivities,
+			 N * (size_t)std::min(dst.substrates, src.substrates));
 }
 
 struct orc_state
@@ -1354,11 +1442,45 @@ int orc_upload_motility(orc_state* s, const ppc_motility* f)
 	world& w = s->w;
 	if (!f || f->count != w.n)
 		return PPC_ERR_ARG;
+	const int S = f->direction_rule ? f->substrates : (w.mot.on ? w.mot.S : 0);
+	if (w.mot.on && S != w.mot.S)
+	{
+		w.mot = world::mot_store {};
+	}
 	w.mot.on = true;
+	w.mot.S = S;
 	w.mot_per_agent = f->restrict_per_agent != 0;
 	w.grow_stores(std::max(w.cap, 1));
 	ppc_motility v = mot_view(w, f->restrict_per_agent);
 	copy_mot(v, *f, w.n, w.mesh.dims);
+	if (!f->direction_rule)
+		std::fill(w.mot.rule.begin(), w.mot.rule.begin() + w.n, (uint8_t)PPC_DIRECTION_NONE);
+	return PPC_OK;
+}
+
+int orc_upload_gradients(orc_state* s, const ppc_gradient_field* g)
+{
+	world& w = s->w;
+	if (!g || g->substrates < 0 || (g->substrates > 0 && !g->gradients))
+		return PPC_ERR_ARG;
+	world::gradient_field f;
+	f.S = g->substrates;
+	size_t voxels = 1;
+	for (int d = 0; d < 3; d++)
+	{
+		int n = 1;
+		if (d < w.mesh.dims)
+		{
+			if (g->voxel_shape[d] <= 0)
+				return PPC_ERR_ARG;
+			n = (w.mesh.maxs[d] - w.mesh.mins[d] + g->voxel_shape[d] - 1) / g->voxel_shape[d];
+			f.shape[d] = g->voxel_shape[d];
+		}
+		f.grid[d] = n < 1 ? 1 : n;
+		voxels *= (size_t)f.grid[d];
+	}
+	f.g.assign(g->gradients, g->gradients + voxels * (size_t)f.S * 3);
+	w.grad = std::move(f);
 	return PPC_OK;
 }
 

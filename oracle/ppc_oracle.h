@@ -70,6 +70,8 @@ int orc_upload_interactions(orc_state* s, const ppc_interactions* fields, int32_
 int orc_download_interactions(orc_state* s, ppc_interactions* fields);
 int orc_upload_motility(orc_state* s, const ppc_motility* fields);
 int orc_download_motility(orc_state* s, ppc_motility* fields);
+/* the gradient field the chemotaxis direction rules read */
+int orc_upload_gradients(orc_state* s, const ppc_gradient_field* field);
 
 /* one mechanics step in simulator::simulate_mechanics order, `steps` times;
    with_phenotype adds flag_by_draws + the phenotype container update +

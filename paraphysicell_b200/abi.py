@@ -353,7 +353,39 @@ class Motility(C.Structure):
         ("migration_bias", _D),
         ("migration_bias_direction", _D),
         ("motility_vector", _D),
+        ("direction_rule", _U8),
+        ("chemotaxis_index", _I32),
+        ("chemotaxis_direction", _D),
+        ("chemotactic_sensitivities", _D),
+        ("substrates", C.c_int32),
+        ("reserved", C.c_int32),
     ]
+
+
+PPC_DIRECTION_NONE, PPC_DIRECTION_CHEMOTAXIS = 0, 1
+PPC_DIRECTION_ADVANCED_CHEMOTAXIS, PPC_DIRECTION_ADVANCED_CHEMOTAXIS_NORMALIZED = 2, 3
+
+
+class GradientField(C.Structure):
+    """ppc_gradient_field (include/ppc.h)."""
+    _fields_ = [
+        ("substrates", C.c_int32),
+        ("voxel_shape", C.c_int32 * 3),
+        ("gradients", _D),
+    ]
+
+    @classmethod
+    def make(cls, gradients, voxel_shape):
+        """`gradients`: float64 array [voxels, substrates, 3] (kept alive by the
+        returned struct)."""
+        g = cls()
+        arr = np.ascontiguousarray(gradients, dtype=np.float64)
+        g.substrates = arr.shape[1]
+        for d in range(3):
+            g.voxel_shape[d] = int(voxel_shape[d])
+        g.gradients = arr.ctypes.data_as(_D)
+        g._keep = arr
+        return g
 
 
 # motility_t::set_defaults (reference: src/data_storage_phenotype.cpp:245-256)
@@ -365,6 +397,10 @@ MOTILITY_FIELDS = [
     ("migration_bias", np.float64, 1, 0.0),
     ("migration_bias_direction", np.float64, "dims", 0.0),
     ("motility_vector", np.float64, "dims", 0.0),
+    ("direction_rule", np.uint8, 1, 0),
+    ("chemotaxis_index", np.int32, 1, 0),
+    ("chemotaxis_direction", np.float64, 1, 1.0),
+    ("chemotactic_sensitivities", np.float64, "subs", 0.0),
 ]
 
 
@@ -372,15 +408,17 @@ class MotilityArrays:
     """Host arrays of the motility fields, one row per agent, with the
     reference's defaults."""
 
-    def __init__(self, count, dims, pinned=None, restrict_per_agent=False):
+    def __init__(self, count, dims, pinned=None, restrict_per_agent=False, substrates=0):
         self.count = int(count)
         self.dims = int(dims)
+        self.substrates = int(substrates)
         # False: every 3-D walk in the xy-plane, as the reference; True: each
         # agent's restrict_to_2d flag decides
         self.restrict_per_agent = bool(restrict_per_agent)
         self.arrays = {}
         for name, dt, mult, dflt in MOTILITY_FIELDS:
-            n = max(self.count * (self.dims if mult == "dims" else 1), 1)
+            width = {"dims": self.dims, "subs": self.substrates}.get(mult, 1)
+            n = max(self.count * width, 1)
             arr = pinned(n, dt) if pinned is not None else np.empty(n, dtype=dt)
             arr[:] = dflt
             self.arrays[name] = arr
@@ -390,18 +428,20 @@ class MotilityArrays:
         mult = next(m for f, _, m, _ in MOTILITY_FIELDS if f == name)
         if mult == 1:
             return arr[: self.count]
-        return arr[: self.count * self.dims].reshape(self.count, self.dims)
+        width = self.dims if mult == "dims" else self.substrates
+        return arr[: self.count * width].reshape(self.count, width)
 
     def struct(self):
         s = Motility()
         s.count = self.count
+        s.substrates = self.substrates
         s.restrict_per_agent = int(self.restrict_per_agent)
         for name, dt, _, _ in MOTILITY_FIELDS:
             setattr(s, name, self.arrays[name].ctypes.data_as(_PTR[dt]))
         return s
 
     def copy(self, pinned=None):
-        out = MotilityArrays(self.count, self.dims, pinned, self.restrict_per_agent)
+        out = MotilityArrays(self.count, self.dims, pinned, self.restrict_per_agent, self.substrates)
         for k, v in self.arrays.items():
             out.arrays[k][:] = v
         return out

@@ -965,6 +965,12 @@ int ppc_destroy(ppc_state* s)
 		cudaFree(s->stage);
 	if (s->ix_scratch)
 		cudaFree(s->ix_scratch);
+	for (auto& b : { s->ix_store.p, s->mot_store.p })
+		if (b)
+			cudaFree(b);
+	for (auto& g : s->gradients)
+		if (g.p)
+			cudaFree(g.p);
 	if (s->pinned_ctr)
 		cudaFreeHost(s->pinned_ctr);
 	if (s->own_stream)
@@ -1360,6 +1366,10 @@ std::vector<column> mot_column_list(const mot_columns& m, const ppc_motility* f,
 		{ m.bias, f ? f->migration_bias : nullptr, e, 1 },
 		{ m.direction, f ? f->migration_bias_direction : nullptr, e, d },
 		{ m.vector, f ? f->motility_vector : nullptr, e, d },
+		{ m.rule, f ? f->direction_rule : nullptr, 1, 1 },
+		{ m.chemo_index, f ? f->chemotaxis_index : nullptr, sizeof(int32_t), 1 },
+		{ m.chemo_dir, f ? f->chemotaxis_direction : nullptr, e, 1 },
+		{ m.sens, f ? f->chemotactic_sensitivities : nullptr, e, (size_t)m.S },
 	};
 }
 
@@ -1412,19 +1422,21 @@ int ensure_ix_store(ppc_state* s, int32_t S)
 	return alloc_columns(s, s->ix_store, cols);
 }
 
-int ensure_mot_store(ppc_state* s)
+int ensure_mot_store(ppc_state* s, int32_t S)
 {
-	if (s->mot_store.p)
+	if (s->mot_store.p && s->v.mot.S == S)
 		return PPC_OK;
 	const size_t C = s->total_cap, d = s->dims, e = sizeof(double);
 	mot_columns& m = s->v.mot;
 	const int32_t per_agent = m.per_agent;
 	m = mot_columns {};
 	m.per_agent = per_agent;
+	m.S = S;
 	std::vector<std::pair<void**, size_t>> cols = {
-		{ (void**)&m.motile, C }, { (void**)&m.restrict2d, C }, { (void**)&m.persistence, C * e },
-		{ (void**)&m.speed, C * e }, { (void**)&m.bias, C * e }, { (void**)&m.direction, C * d * e },
-		{ (void**)&m.vector, C * d * e },
+		{ (void**)&m.motile, C }, { (void**)&m.restrict2d, C }, { (void**)&m.rule, C },
+		{ (void**)&m.persistence, C * e }, { (void**)&m.speed, C * e }, { (void**)&m.bias, C * e },
+		{ (void**)&m.direction, C * d * e }, { (void**)&m.vector, C * d * e }, { (void**)&m.chemo_index, C * 4 },
+		{ (void**)&m.chemo_dir, C * e }, { (void**)&m.sens, C * (size_t)S * e },
 	};
 	return alloc_columns(s, s->mot_store, cols);
 }
@@ -1467,6 +1479,11 @@ int check_mot_fields(const ppc_motility* f)
 	if (!f->is_motile || !f->restrict_to_2d || !f->persistence_time || !f->migration_speed || !f->migration_bias
 		|| !f->migration_bias_direction || !f->motility_vector)
 		return fail(PPC_ERR_ARG, "a ppc_motility field is NULL");
+	if (f->substrates < 0)
+		return fail(PPC_ERR_ARG, "negative substrate count");
+	if (f->direction_rule
+		&& (!f->chemotaxis_index || !f->chemotaxis_direction || (f->substrates > 0 && !f->chemotactic_sensitivities)))
+		return fail(PPC_ERR_ARG, "a direction-rule field of ppc_motility is NULL");
 	return PPC_OK;
 }
 
@@ -1532,13 +1549,16 @@ int ppc_upload_motility(ppc_state* s, int32_t r, const ppc_motility* f)
 	if (f->count != n)
 		return fail(PPC_ERR_ARG, "fields.count differs from the replicate's agent count");
 	PPC_TRY(check_mot_fields(f));
-	PPC_TRY(ensure_mot_store(s));
+	const int32_t S = f->direction_rule ? f->substrates : (s->mot_store.p ? s->v.mot.S : 0);
+	PPC_TRY(ensure_mot_store(s, S));
 	if (s->v.mot.per_agent != (f->restrict_per_agent != 0))
 	{
 		PPC_CUDA(cudaStreamSynchronize(s->stream));
 		PPC_TRY(release_graph(s));
 		s->v.mot.per_agent = f->restrict_per_agent != 0;
 	}
+	if (!f->direction_rule && n > 0) // no rules: every agent keeps the caller's direction
+		PPC_CUDA(cudaMemsetAsync(s->v.mot.rule + s->reps[r].base, PPC_DIRECTION_NONE, (size_t)n, s->stream));
 	return move_columns(s, mot_column_list(s->v.mot, f, s->dims), s->reps[r].base, n, true);
 }
 
@@ -1581,21 +1601,80 @@ int ppc_update_motility_fields(ppc_state* s, int32_t r, ppc_motility* f)
 		m.base = base;
 		m.dt = s->params.mechanics_time_step;
 		m.per_agent = mc.per_agent;
+		m.cur = s->cur;
 		m.epoch = epoch;
 		m.motile = mc.motile + base;
 		m.restrict2d = mc.restrict2d + base;
+		m.rule = mc.rule + base;
 		m.persistence = mc.persistence + base;
 		m.speed = mc.speed + base;
 		m.bias = mc.bias + base;
 		m.direction = mc.direction + (size_t)base * d;
 		m.vector = mc.vector + (size_t)base * d;
+		m.chemo_index = mc.chemo_index + base;
+		m.chemo_dir = mc.chemo_dir + base;
+		m.S = mc.S;
+		m.sens = mc.sens + (size_t)base * mc.S;
+		if ((int32_t)s->gradients.size() > r && s->gradients[r].p)
+		{
+			const auto& g = s->gradients[r];
+			m.grad = static_cast<const double*>(g.p);
+			m.gS = g.S;
+			for (int q = 0; q < 3; q++)
+			{
+				m.ggrid[q] = g.grid[q];
+				m.gshape[q] = g.shape[q];
+				m.gmins[q] = s->reps[r].mins[q];
+			}
+		}
 		PPC_TRY(launch_motility(s, m));
 		s->vel_dirty = true; // the next fused step reads the velocities
 	}
 	if (f)
-		PPC_TRY(move_columns(s, { { s->v.mot.vector, f->motility_vector, sizeof(double), (size_t)s->dims } },
+		PPC_TRY(move_columns(s,
+							 { { s->v.mot.vector, f->motility_vector, sizeof(double), (size_t)s->dims },
+							   { s->v.mot.direction, f->migration_bias_direction, sizeof(double), (size_t)s->dims } },
 							 s->reps[r].base, n, false));
 	return finish(s);
+}
+
+int ppc_upload_gradients(ppc_state* s, int32_t r, const ppc_gradient_field* g)
+{
+	if (!valid(s, r) || !g || g->substrates < 0 || (g->substrates > 0 && !g->gradients))
+		return fail(PPC_ERR_ARG, "invalid gradient field");
+	ppc_state::gradient_field f;
+	f.S = g->substrates;
+	int64_t voxels = 1;
+	const ppc_mesh& m = s->meshes[r];
+	for (int d = 0; d < 3; d++)
+	{
+		int64_t n = 1;
+		if (d < m.dims)
+		{
+			if (g->voxel_shape[d] <= 0)
+				return fail(PPC_ERR_ARG, "diffusion voxel edges must be positive");
+			n = ((int64_t)m.bounding_box_maxs[d] - m.bounding_box_mins[d] + g->voxel_shape[d] - 1) / g->voxel_shape[d];
+			f.shape[d] = g->voxel_shape[d];
+		}
+		f.grid[d] = (int32_t)std::max<int64_t>(1, std::min<int64_t>(n, INT32_MAX));
+		voxels *= f.grid[d];
+		if (voxels > ((int64_t)1 << 31))
+			return fail(PPC_ERR_CAPACITY, "the diffusion mesh has too many voxels");
+	}
+	if ((int32_t)s->gradients.size() < s->nreps)
+		s->gradients.resize(s->nreps);
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	if (s->gradients[r].p)
+		PPC_CUDA(cudaFree(s->gradients[r].p));
+	s->gradients[r] = ppc_state::gradient_field {};
+	const size_t bytes = (size_t)voxels * f.S * 3 * sizeof(double);
+	if (bytes)
+	{
+		PPC_CUDA(cudaMalloc(&f.p, bytes));
+		PPC_CUDA(cudaMemcpy(f.p, g->gradients, bytes, cudaMemcpyHostToDevice));
+	}
+	s->gradients[r] = f;
+	return PPC_OK;
 }
 
 int ppc_update_cell_cell_interactions(ppc_state* s, int32_t r, ppc_interactions* f)

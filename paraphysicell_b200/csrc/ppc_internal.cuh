@@ -87,9 +87,12 @@ struct ix_columns
 
 struct mot_columns
 {
-	uint8_t *motile, *restrict2d;
+	uint8_t *motile, *restrict2d, *rule;
 	double *persistence, *speed, *bias, *direction, *vector; // direction, vector: [C*dims]
+	int32_t* chemo_index;
+	double *chemo_dir, *sens; // sens: [C*S]
 	int32_t per_agent;
+	int32_t S; // chemotactic sensitivities per agent
 };
 
 // everything a kernel needs, passed by value
@@ -268,6 +271,13 @@ struct ppc_state
 	void* ix_scratch = nullptr;		// per-call scratch of the interaction and motility passes
 	size_t ix_scratch_bytes = 0;
 	ppc::store_block ix_store, mot_store; // resident phenotype columns
+	struct gradient_field
+	{
+		void* p = nullptr;
+		int32_t S = 0, grid[3] = { 1, 1, 1 };
+		double shape[3] = { 1, 1, 1 };
+	};
+	std::vector<gradient_field> gradients; // per replicate, for the chemotaxis rules
 	ppc::rep_counters* pinned_ctr = nullptr; // pinned landing area of the counters
 	int32_t* pinned_err = nullptr;			 // pinned landing area of the device error word
 	bool staged = false;
@@ -352,12 +362,20 @@ int launch_interactions(ppc_state* s, const ix_fields& x);
 // device copies of the ppc_motility fields of one replicate (local rows)
 struct mot_fields
 {
-	int32_t n, replicate, base, per_agent;
+	int32_t n, replicate, base, per_agent, cur;
 	double dt;
 	uint64_t epoch;
-	const uint8_t *motile, *restrict2d;
-	const double *persistence, *speed, *bias, *direction; // direction: [n*dims]
-	double* vector;										  // [n*dims]
+	const uint8_t *motile, *restrict2d, *rule;
+	const double *persistence, *speed, *bias;
+	double* direction; // [n*dims], written by a direction rule
+	double* vector;	   // [n*dims]
+	const int32_t* chemo_index;
+	const double *chemo_dir, *sens; // sens: [n*S]
+	int32_t S;
+	// the replicate's gradient field (null without one): [voxels * gS * 3]
+	const double* grad;
+	int32_t gS, ggrid[3];
+	double gshape[3], gmins[3];
 };
 int launch_motility(ppc_state* s, const mot_fields& m);
 

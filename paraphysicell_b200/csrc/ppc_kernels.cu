@@ -119,14 +119,19 @@ __device__ __forceinline__ void copy_columns(const view& v, int dims, int d, int
 	{
 		m.motile[d] = m.motile[s];
 		m.restrict2d[d] = m.restrict2d[s];
+		m.rule[d] = m.rule[s];
 		m.persistence[d] = m.persistence[s];
 		m.speed[d] = m.speed[s];
 		m.bias[d] = m.bias[s];
+		m.chemo_index[d] = m.chemo_index[s];
+		m.chemo_dir[d] = m.chemo_dir[s];
 		for (int q = 0; q < dims; q++)
 		{
 			m.direction[(int64_t)d * dims + q] = m.direction[(int64_t)s * dims + q];
 			m.vector[(int64_t)d * dims + q] = m.vector[(int64_t)s * dims + q];
 		}
+		for (int q = 0; q < m.S; q++)
+			m.sens[(int64_t)d * m.S + q] = m.sens[(int64_t)s * m.S + q];
 	}
 }
 

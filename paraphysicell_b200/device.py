@@ -14,7 +14,7 @@ import os
 
 import numpy as np
 
-from .abi import Agents, Interactions, Mesh, Motility, Params, PPCError
+from .abi import Agents, GradientField, Interactions, Mesh, Motility, Params, PPCError
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libppc.so")
@@ -37,7 +37,7 @@ EXPORTS = (
     "ppc_set_profiling", "ppc_get_profile", "ppc_set_launch_shape", "ppc_autotune",
     "ppc_update_cell_cell_interactions", "ppc_update_motility_fields", "ppc_set_host_transfer",
     "ppc_upload_interactions", "ppc_download_interactions", "ppc_upload_motility", "ppc_download_motility",
-    "ppc_count_flags", "ppc_set_step_form", "ppc_set_wait_limit",
+    "ppc_count_flags", "ppc_set_step_form", "ppc_set_wait_limit", "ppc_upload_gradients",
     "ppc_bin_agents_noalloc",
 ) + tuple("ppc_" + e for e in ENTRY_POINTS)
 
@@ -81,6 +81,7 @@ def lib():
         L.ppc_set_launch_shape.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32]
         L.ppc_set_host_transfer.argtypes = [vp, C.c_int32]
         L.ppc_set_step_form.argtypes = [vp, C.c_int32]
+        L.ppc_upload_gradients.argtypes = [vp, C.c_int32, C.POINTER(GradientField)]
         L.ppc_set_wait_limit.argtypes = [vp, C.c_int64]
         L.ppc_autotune.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.ppc_get_profile.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
@@ -276,6 +277,10 @@ class Simulation:
         _check(lib().ppc_download_interactions(self.h, replicate, C.byref(st)), "ppc_download_interactions")
         fields.count = st.count
         return fields
+
+    def upload_gradients(self, field, replicate=0):
+        """`field`: abi.GradientField (the chemotaxis rules' input)."""
+        _check(lib().ppc_upload_gradients(self.h, replicate, C.byref(field)), "ppc_upload_gradients")
 
     def upload_motility(self, fields, replicate=0):
         st = fields.struct()

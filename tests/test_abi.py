@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol():
 def test_abi_version_and_struct_layout():
     build.ensure_built()
     L = device.lib()
-    assert L.ppc_abi_version() == 1
+    assert L.ppc_abi_version() == 2
     # field counts mirror include/ppc.h
     assert len(Agents._fields_) == 29
     assert C.sizeof(Mesh) == 40

@@ -168,3 +168,107 @@ def test_motility_argument_errors():
         d.update_motility_fields(MotilityArrays(100, 2), replicate=3)
     d.update_motility_fields(MotilityArrays(100, 2))  # defaults: nobody is motile
     assert np.all(_velocities(d, a)[:100] == 0.0)
+
+
+def _gradient_field(mesh, substrates, seed, voxel=20):
+    """A gradient field over the diffusion mesh (20 um voxels) whose value
+    differs from voxel to voxel, so a wrong voxel lookup shows."""
+    from paraphysicell_b200.abi import GradientField
+    rng = np.random.default_rng(seed)
+    grid = [max(1, -(-(mesh.bounding_box_maxs[d] - mesh.bounding_box_mins[d]) // voxel)) if d < mesh.dims else 1
+            for d in range(3)]
+    g = rng.normal(size=(grid[0] * grid[1] * grid[2], substrates, 3))
+    return GradientField.make(g, (voxel, voxel, voxel)), g, grid
+
+
+def _voxel_of(mesh, pos, grid, voxel=20):
+    c = np.zeros((len(pos), 3), dtype=np.int64)
+    for d in range(mesh.dims):
+        f = (pos[:, d] - mesh.bounding_box_mins[d]) / voxel
+        c[:, d] = np.minimum(np.maximum(f, 0).astype(np.int64), grid[d] - 1)
+    return c[:, 0] + grid[0] * (c[:, 1] + grid[1] * c[:, 2])
+
+
+def _chemotaxis_fields(n, dims, substrates, seed):
+    from paraphysicell_b200.abi import (PPC_DIRECTION_ADVANCED_CHEMOTAXIS,
+                                        PPC_DIRECTION_ADVANCED_CHEMOTAXIS_NORMALIZED, PPC_DIRECTION_CHEMOTAXIS)
+    rng = np.random.default_rng(seed)
+    m = MotilityArrays(n, dims, substrates=substrates)
+    m["is_motile"][:] = 1
+    m["persistence_time"][:] = 0.001  # dt / persistence = 100: every agent redraws
+    m["migration_speed"][:] = 1.0
+    m["migration_bias"][:] = 1.0  # the direction alone
+    m["direction_rule"][:] = rng.choice([0, PPC_DIRECTION_CHEMOTAXIS, PPC_DIRECTION_ADVANCED_CHEMOTAXIS,
+                                         PPC_DIRECTION_ADVANCED_CHEMOTAXIS_NORMALIZED], size=n)
+    m["chemotaxis_index"][:] = rng.integers(0, substrates, n)
+    m["chemotaxis_direction"][:] = rng.choice([-1.0, 1.0], n)
+    m["chemotactic_sensitivities"][:] = rng.uniform(-1, 2, (n, substrates))
+    d = rng.normal(size=(n, dims))
+    m["migration_bias_direction"][:] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    return m
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_chemotaxis_rules_in_the_oracle(dims):
+    """The standard direction rules (standard_models.cpp:542-583) from the
+    gradient of the agent's diffusion voxel: chemotaxis follows one
+    substrate's gradient times the direction sign, advanced chemotaxis the
+    sensitivity-weighted sum (of normalised gradients in its second form),
+    each normalised; agents without a rule keep the caller's direction."""
+    n, S = 3000, 3
+    mesh, params, a = _agents(dims, n, seed=51)
+    o = Oracle(mesh, params)
+    o.upload(a)
+    field, g, grid = _gradient_field(mesh, S, seed=52)
+    o.upload_gradients(field)
+    m = _chemotaxis_fields(n, dims, S, seed=53)
+    before = m.copy()
+    o.update_motility_fields(m)
+    vox = _voxel_of(mesh, a["positions"].reshape(n, dims), grid)
+    rule = m["direction_rule"]
+
+    def unit(x):
+        length = np.sqrt(np.sum(x * x, axis=-1, keepdims=True))
+        return np.where(length > 1e-16, x / np.where(length > 0, length, 1), 0)
+
+    want = before["migration_bias_direction"].copy()
+    gi = g[vox][:, :, :dims]  # [n, S, dims]
+    chem = rule == 1
+    want[chem] = unit(gi[chem, m["chemotaxis_index"][chem]] * m["chemotaxis_direction"][chem, None])
+    for r, norm in ((2, False), (3, True)):
+        sel = rule == r
+        gg = unit(gi[sel]) if norm else gi[sel]
+        want[sel] = unit(np.sum(gg * m["chemotactic_sensitivities"][sel][:, :, None], axis=1))
+    np.testing.assert_allclose(m["migration_bias_direction"], want, rtol=0, atol=1e-14)
+    # fully biased, unit speed: the motility vector is the direction (normalised again)
+    np.testing.assert_allclose(m["motility_vector"], unit(want), rtol=0, atol=1e-14)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims,resident", [(2, False), (3, False), (3, True)])
+def test_chemotaxis_rules_match_oracle(dims, resident):
+    from tests import gpu_util as gu
+    n, S = 3000, 3
+    mesh, params, a = _agents(dims, n, seed=61)
+    o, d = gu.make_pair(mesh, params, a, seed=9)
+    field, _, _ = _gradient_field(mesh, S, seed=62)
+    o.upload_gradients(field)
+    d.upload_gradients(field)
+    mo, md = _chemotaxis_fields(n, dims, S, seed=63), _chemotaxis_fields(n, dims, S, seed=63)
+    mo["persistence_time"][:] = md["persistence_time"][:] = np.linspace(0.05, 2.0, n)
+    if resident:
+        o.upload_motility(mo)
+        d.upload_motility(md)
+    for _ in range(3):
+        if resident:
+            o.update_motility_fields(None)
+            d.update_motility_fields(None)
+        else:
+            o.update_motility_fields(mo)
+            d.update_motility_fields(md)
+        assert np.array_equal(_velocities(d, a), _velocities(o, a))
+    if resident:
+        mo = o.download_motility(MotilityArrays(a.capacity, dims, substrates=S))
+        md = d.download_motility(MotilityArrays(a.capacity, dims, substrates=S))
+    for k in ("motility_vector", "migration_bias_direction"):
+        assert np.array_equal(md[k], mo[k]), k
