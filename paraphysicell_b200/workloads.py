@@ -14,8 +14,8 @@ shapes, sizes and value distributions:
             three types (rep 8/10/12, adh 0.2/0.4/0.8), 20% of agents draw
             1-3 springs to random neighbours within 1.25 (ri + rj), k = 0.05
   config 4  ensemble of replicates, N_r log-uniform in [500, 50000], cube
-            side 20 * ceil(N_r^(1/3)) um (density ~1 per 8000 um^3),
-            one type, r ~ U[7,10]
+            side (8000 N_r)^(1/3) um rounded to whole um (one agent per
+            8000 um^3), one type, r ~ U[7,10]
   config 5  3-D, 1,000,000 agents in a ball of radius 2900 in an 8000 um
             cube, two types, with division/death draws
 
