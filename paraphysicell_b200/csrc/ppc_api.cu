@@ -808,6 +808,8 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 			std::frexp(ext, &e2);
 			R.fmargin = (float)std::ldexp(16.0, e2 - 24);
 		}
+		R.inv_grid[0] = 1.0 / R.grid[0];
+		R.inv_grid[1] = 1.0 / R.grid[1];
 		R.base = (int32_t)cap;
 		R.cap = capacities[r];
 		R.vox_base = vox;

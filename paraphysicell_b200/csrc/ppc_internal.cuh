@@ -54,6 +54,7 @@ struct rep_info
 	int64_t voxels;
 	int32_t maxs_int[3], mins_int[3];
 	float fmargin;	  // bound on the FP32 distance error of positions relative to mins (um)
+	double inv_grid[2]; // 1 / grid[0], 1 / grid[1]: voxel coordinates of a key without integer division
 };
 
 // per-replicate device counters

@@ -48,6 +48,33 @@ __device__ __forceinline__ void set_comp(double4& p, int d, double x)
 		p.z = x;
 }
 
+// a / b and a % b for 0 <= a < 2^31 through the double reciprocal `inv` of
+// b: the product is within an ulp-sized error of a / b, so the truncated
+// quotient is off by at most one, which the remainder test corrects
+__device__ __forceinline__ void divmod_inv(int32_t a, int32_t b, double inv, int32_t& q, int32_t& r)
+{
+	q = (int32_t)((double)a * inv);
+	r = a - q * b;
+	if (r >= b)
+	{
+		q++;
+		r -= b;
+	}
+	else if (r < 0)
+	{
+		q--;
+		r += b;
+	}
+}
+
+// voxel coordinates of the local key lk (x fastest)
+__device__ __forceinline__ void voxel_coords(const rep_info& R, int32_t lk, int& cx, int& cy, int& cz)
+{
+	int32_t q;
+	divmod_inv(lk, R.grid[0], R.inv_grid[0], q, cx);
+	divmod_inv(q, R.grid[1], R.inv_grid[1], cz, cy);
+}
+
 // slot s is live when its index inside its replicate is below the count
 __device__ __forceinline__ bool live(const view& v, int s, int& r, int& local)
 {
@@ -504,13 +531,13 @@ __device__ __forceinline__ void for_each_neighbor(const view& v, const rep_info&
 {
 	const int32_t lk = (int32_t)(key - R.vox_base);
 	const int g0 = R.grid[0], g1 = R.grid[1], g2 = R.grid[2];
-	const int cx = lk % g0;
-	const int cy = (lk / g0) % g1;
-	const int cz = lk / (g0 * g1);
+	int cx, cy, cz;
+	voxel_coords(R, lk, cx, cy, cz);
 	const int xlo = cx > 0 ? cx - 1 : 0;
 	const int xhi = cx + 1 < g0 ? cx + 1 : g0 - 1;
 	constexpr int NR = DIMS == 3 ? 9 : (DIMS == 2 ? 3 : 1);
 	int lo[NR], hi[NR];
+	const int32_t vb = (int32_t)R.vox_base; // voxel keys fit 31 bits (checked at creation)
 #pragma unroll
 	for (int k = 0; k < NR; k++)
 	{
@@ -518,7 +545,7 @@ __device__ __forceinline__ void for_each_neighbor(const view& v, const rep_info&
 		const int dy = DIMS >= 2 ? k % 3 - 1 : 0;
 		const int z = cz + dz, y = cy + dy;
 		const bool ok = z >= 0 && z < g2 && y >= 0 && y < g1;
-		const int64_t row = R.vox_base + (int64_t)g0 * (y + (int64_t)g1 * z);
+		const int32_t row = ok ? vb + g0 * (y + g1 * z) : 0;
 		lo[k] = ok ? v.vstart[row + xlo] : 0;
 		hi[k] = ok ? v.vstart[row + xhi + 1] : 0;
 	}
@@ -930,7 +957,8 @@ __global__ void __launch_bounds__(kFusedThreads, 5) k_fused_f32(view v, int cur)
 
 	const int32_t lk = v.skey[t] - (int32_t)R.vox_base;
 	const int g0 = R.grid[0], g1 = R.grid[1], g2 = R.grid[2];
-	const int cx = lk % g0, cy = (lk / g0) % g1, cz = lk / (g0 * g1);
+	int cx, cy, cz;
+	voxel_coords(R, lk, cx, cy, cz);
 	const int xlo = cx > 0 ? cx - 1 : 0;
 	const int xhi = cx + 1 < g0 ? cx + 1 : g0 - 1;
 	constexpr int NR = DIMS == 3 ? 9 : (DIMS == 2 ? 3 : 1);
@@ -942,7 +970,7 @@ __global__ void __launch_bounds__(kFusedThreads, 5) k_fused_f32(view v, int cur)
 		const int dy = DIMS >= 2 ? k % 3 - 1 : 0;
 		const int z = cz + dz, y = cy + dy;
 		const bool ok = z >= 0 && z < g2 && y >= 0 && y < g1;
-		const int64_t row = R.vox_base + (int64_t)g0 * (y + (int64_t)g1 * z);
+		const int32_t row = ok ? (int32_t)R.vox_base + g0 * (y + g1 * z) : 0;
 		lo[k] = ok ? v.vstart[row + xlo] : 0;
 		hi[k] = ok ? v.vstart[row + xhi + 1] : 0;
 	}
@@ -1053,12 +1081,12 @@ __device__ __forceinline__ void stencil_bounds(const view& v, const rep_info& R,
 {
 	const int32_t lk = (int32_t)(key - R.vox_base);
 	const int g0 = R.grid[0], g1 = R.grid[1], g2 = R.grid[2];
-	const int cx = lk % g0;
-	const int cy = (lk / g0) % g1;
-	const int cz = lk / (g0 * g1);
+	int cx, cy, cz;
+	voxel_coords(R, lk, cx, cy, cz);
 	const int xlo = cx > 0 ? cx - 1 : 0;
 	const int xhi = cx + 1 < g0 ? cx + 1 : g0 - 1;
 	constexpr int NR = DIMS == 3 ? 9 : (DIMS == 2 ? 3 : 1);
+	const int32_t vb = (int32_t)R.vox_base;
 #pragma unroll
 	for (int k = 0; k < NR; k++)
 	{
@@ -1066,7 +1094,7 @@ __device__ __forceinline__ void stencil_bounds(const view& v, const rep_info& R,
 		const int dy = DIMS >= 2 ? k % 3 - 1 : 0;
 		const int z = cz + dz, y = cy + dy;
 		const bool ok = z >= 0 && z < g2 && y >= 0 && y < g1;
-		const int64_t row = R.vox_base + (int64_t)g0 * (y + (int64_t)g1 * z);
+		const int32_t row = ok ? vb + g0 * (y + g1 * z) : 0;
 		lo[k] = ok ? v.vstart[row + xlo] : 0;
 		hi[k] = ok ? v.vstart[row + xhi + 1] : 0;
 	}
@@ -1549,7 +1577,8 @@ __device__ __forceinline__ void fused_flat_agent(const view& v, int cur, int opt
 	// stencil rows and the candidate numbering
 	const int32_t lk = key - (int32_t)R.vox_base;
 	const int g0 = R.grid[0], g1 = R.grid[1], g2 = R.grid[2];
-	const int cx = lk % g0, cy = (lk / g0) % g1, cz = lk / (g0 * g1);
+	int cx, cy, cz;
+	voxel_coords(R, lk, cx, cy, cz);
 	const int xlo = cx > 0 ? cx - 1 : 0;
 	const int xhi = cx + 1 < g0 ? cx + 1 : g0 - 1;
 	int lo[NR], hi[NR];
@@ -1560,7 +1589,7 @@ __device__ __forceinline__ void fused_flat_agent(const view& v, int cur, int opt
 		const int dy = DIMS >= 2 ? k % 3 - 1 : 0;
 		const int z = cz + dz, y = cy + dy;
 		const bool ok = z >= 0 && z < g2 && y >= 0 && y < g1;
-		const int64_t row = R.vox_base + (int64_t)g0 * (y + (int64_t)g1 * z);
+		const int32_t row = ok ? (int32_t)R.vox_base + g0 * (y + g1 * z) : 0;
 		lo[k] = ok ? v.vstart[row + xlo] : 0;
 		hi[k] = ok ? v.vstart[row + xhi + 1] : 0;
 	}
