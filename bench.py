@@ -14,11 +14,11 @@ seeded synthetic agents (the reference's sample XML setups are not used).
 bracketed by CUDA events on the library's stream with L2 flushed (a 256 MiB
 write) before every timed step. `e2e`: the same steps through the C ABI with
 host buffers: every step uploads positions and previous velocities from
-pinned host memory and downloads positions, velocities, previous velocities
-and pressure. `roofline`: algorithmic bytes of the fused force kernel per
-launch over its event-timed duration. `cpu_baseline`: the CPU restatement of
-the reference's OpenMP path on this host's cores, on a bounded number of
-steps of the same workload.
+pinned host memory and downloads positions, previous velocities and pressure
+(the step leaves velocities at zero). `roofline`: algorithmic bytes of the
+fused force kernel per launch over its event-timed duration.
+`cpu_baseline`: the CPU restatement of the reference's OpenMP path on this
+host's cores, on a bounded number of steps of the same workload.
 
 With torchrun (N > 1) every rank advances its own replica of the workload
 (the single-simulation path does not shard; replicas only) and the max over
@@ -181,11 +181,11 @@ def error_vs_oracle(name, steps=3):
     return res
 
 
-def cpu_baseline(name, budget_s=8.0, max_steps=400):
+def cpu_baseline(name, budget_s=8.0, max_steps=400, with_error=True):
     """Times the oracle's OpenMP restatement of the reference on all host
-    threads for a bounded number of steps of the workload, then checks the
-    device's FP64 step against the oracle's serial form of the same
-    workload (error_vs_oracle)."""
+    threads for a bounded number of steps of the workload, then (with_error)
+    checks the device's FP64 step against the oracle's serial form of the
+    same workload (error_vs_oracle)."""
     from oracle.oracle import Oracle
 
     threads = len(os.sched_getaffinity(0))
@@ -199,10 +199,34 @@ def cpu_baseline(name, budget_s=8.0, max_steps=400):
     t = o.time_steps(2, threads, **kw)  # warm-up and step-time estimate
     steps = int(max(3, min(max_steps, budget_s / max(t / 2, 1e-6))))
     t = o.time_steps(steps, threads, **kw)
-    return {"value": a.count * steps / t, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{steps} steps of the full {a.count}-agent workload, OpenMP over {threads} threads, "
-                      f"std::chrono around the step loop ({t:.2f} s)",
-            "error_vs_oracle": error_vs_oracle(name)}
+    out = {"value": a.count * steps / t, "unit": UNIT, "cores": threads, "kind": "port",
+           "sample": f"{steps} steps of the full {a.count}-agent workload, OpenMP over {threads} threads, "
+                     f"std::chrono around the step loop ({t:.2f} s)"}
+    if with_error:
+        out["error_vs_oracle"] = error_vs_oracle(name)
+    return out
+
+
+def ensemble_cpu_baseline(steps=2):
+    """The ensemble on the host: every replicate in turn through the oracle's
+    OpenMP restatement on all host threads, `steps` steps each (only the
+    step loops are timed)."""
+    from oracle.oracle import Oracle
+    from paraphysicell_b200 import workloads as wl
+
+    threads = len(os.sched_getaffinity(0))
+    meshes, params, sets = wl.config4()
+    total_t, agent_steps = 0.0, 0
+    for m, a in zip(meshes, sets):
+        o = Oracle(m, params, seed=1)
+        o.upload(a)
+        o.update_mechanics_mesh()
+        o.update_cell_neighbors()
+        total_t += o.time_steps(steps, threads)
+        agent_steps += a.count * steps
+    return {"value": agent_steps / total_t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"all {len(sets)} replicates one after another, {steps} steps each, OpenMP over {threads} "
+                      f"threads, std::chrono around each replicate's step loop ({total_t:.2f} s in total)"}
 
 
 def max_over_ranks(x, device):
@@ -450,7 +474,7 @@ def ensemble_form(args, flush):
     from paraphysicell_b200 import workloads as wl
     from paraphysicell_b200.device import Simulation
 
-    from paraphysicell_b200.abi import PPC_FP32_FORCE
+    from paraphysicell_b200.abi import PPC_FP32_FORCE, PPC_STEP_PERSISTENT
 
     meshes, params, sets = wl.config4()
     total = sum(a.count for a in sets)
@@ -468,6 +492,11 @@ def ensemble_form(args, flush):
             shape = sim.autotune(steps=5)
         res = _timed_steps(sim, stream, sim.step, lambda: total, args.steps, args.warmup, flush)
         res["launch_shape"] = {"tile_edge": shape[0], "threads": shape[1], "chosen_by": "ppc_autotune"}
+        # the same steps as one cooperative launch each (ppc_set_step_form)
+        sim.set_step_form(PPC_STEP_PERSISTENT)
+        per = _timed_steps(sim, stream, sim.step, lambda: total, args.steps, args.warmup, flush)
+        res["persistent"] = {"value": per["value"], "ms_per_step": per["ms_per_step"],
+                             "steady_state": per["steady_state"]}
         sim.close()
         return res
 
@@ -475,6 +504,8 @@ def ensemble_form(args, flush):
     out["fp32_force"] = run(PPC_FP32_FORCE)
     out.update({"workload": "config4", "replicates": len(sets), "agents": total,
                 "description": ENSEMBLE})
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = ensemble_cpu_baseline()
     return out
 
 
@@ -504,43 +535,64 @@ def stochastic_springs_form(args, flush):
 
 
 def interactions_form(args):
-    """Config 3 (88,700 agents) through ppc_update_cell_cell_interactions
-    with page-locked phenotype fields: each call uploads the fields, runs the
-    candidate and ordered-resolution kernels and writes the fields back
-    (synchronous, so timed on the host clock around the call). Rates give
-    per-neighbour action probabilities of a few per mille."""
+    """Config 3 (88,700 agents) through ppc_update_cell_cell_interactions at
+    two rate settings (per-neighbour action probabilities of a few per mille,
+    and up to 0.2). `resident`: the phenotype fields are uploaded once
+    (ppc_upload_interactions) and each call works on the device columns;
+    `per_call_fields`: each call copies page-locked fields in and out. Calls
+    are synchronous, so each is timed on the host clock. `cpu` is the
+    oracle's serial restatement of the reference's loop
+    (src/solver/host/interactions_solver.cpp:143-251) on the same first call."""
     import time
 
-    import numpy as np
-
+    from oracle.oracle import Oracle
     from paraphysicell_b200 import workloads as wl
     from paraphysicell_b200.abi import FLAG_TO_REMOVE, AgentArrays
     from paraphysicell_b200.device import PinnedPool, Simulation
 
-    mesh, params, a = wl.config3()
-    pool = PinnedPool()
-    f = wl.interaction_fields(a, params.cell_definitions_count, seed=9, scale=0.02, pinned=pool)
-    sim = Simulation(mesh, params, a.capacity, seed=1)
-    sim.upload(a)
-    sim.update_mechanics_mesh()
-    sim.update_cell_neighbors()
-    for _ in range(args.warmup):
-        sim.update_cell_cell_interactions(f)
-    times = []
-    for _ in range(args.steps):
+    out = {"workload": "config3 cell-cell interactions", "calls": args.steps,
+           "note": "host clock around each synchronous call; median over calls"}
+    for label, scale in (("low_rates", 0.02), ("high_rates", 1.0)):
+        mesh, params, a = wl.config3()
+        pool = PinnedPool()
+        f = wl.interaction_fields(a, params.cell_definitions_count, seed=9, scale=scale, pinned=pool)
+        res = {"rate_scale": scale, "agents": a.count}
+        for form in ("resident", "per_call_fields"):
+            sim = Simulation(mesh, params, a.capacity, seed=1)
+            sim.upload(a)
+            sim.update_mechanics_mesh()
+            sim.update_cell_neighbors()
+            g = f.copy(pinned=pool)
+            if form == "resident":
+                sim.upload_interactions(g)
+                call = lambda: sim.update_cell_cell_interactions(None)  # noqa: E731
+            else:
+                call = lambda: sim.update_cell_cell_interactions(g)  # noqa: E731
+            call()
+            sim.synchronize()
+            times = []
+            for _ in range(max(3, min(args.steps, 50))):
+                t0 = time.perf_counter()
+                call()
+                times.append(time.perf_counter() - t0)
+            res[form + "_ms_per_call"] = 1e3 * float(np.median(times))
+            if form == "resident":
+                b = AgentArrays(a.count, a.dims, a.ndefs, a.capacity)
+                sim.download(b)
+                res["flagged_for_removal_after_calls"] = int(np.count_nonzero(b["flags"][: b.count] == FLAG_TO_REMOVE))
+            sim.close()
+        o = Oracle(mesh, params, seed=1)
+        o.upload(a)
+        o.update_mechanics_mesh()
+        o.update_cell_neighbors()
+        o.upload_interactions(f.copy())
         t0 = time.perf_counter()
-        sim.update_cell_cell_interactions(f)
-        times.append(time.perf_counter() - t0)
-    out_a = AgentArrays(a.count, a.dims, a.ndefs, a.capacity)
-    sim.download(out_a)
-    flags = out_a["flags"]
-    sim.close()
-    pool.free()
-    ms = 1e3 * float(np.median(times))
-    return {"workload": "config3 cell-cell interactions", "agents": a.count, "calls": args.steps,
-            "ms_per_call_median": ms, "agents_per_s": a.count / (ms * 1e-3),
-            "flagged_for_removal": int(np.count_nonzero(flags == FLAG_TO_REMOVE)),
-            "note": "host clock around each synchronous call; includes the field copies in and out"}
+        o.update_cell_cell_interactions(None)
+        res["cpu_ms_per_call"] = 1e3 * (time.perf_counter() - t0)
+        res["cpu_kind"] = "oracle, serial restatement, first call"
+        out[label] = res
+        pool.free()
+    return out
 
 
 def config5_form(args, flush):
@@ -565,6 +617,9 @@ def config5_form(args, flush):
     sim.close()
     out.update({"workload": "config5", "agents": a.count, "divisions": divisions, "deaths": deaths,
                 "description": WORKLOADS["config5"]})
+    out["fp32_force"] = fp32_form(args, mesh, params, a, (wl.P_DIVIDE, wl.P_DEATH), flush)
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline("config5", budget_s=10.0, with_error=False)
     return out
 
 

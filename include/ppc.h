@@ -179,6 +179,10 @@ int ppc_set_random_seed(ppc_state* s, uint64_t seed);
  *     shared memory with asynchronous copies, then the FP64 data of the kept
  *     ones two at a time — best where agents are sparse (well under one per
  *     voxel); `threads` and `smem_bytes` are ignored (128 threads);
+ *  -4: a warp lays its 32 agents' candidates end to end and every lane takes
+ *     every 32nd of them, so the filter and the pair code run on full warps
+ *     however unevenly the candidates fall; each agent's lane adds its own
+ *     pair terms in its candidate order (128 threads);
  *  -1: each thread reads its candidates one at a time from global memory and
  *     runs its own pair code;
  *  -2: the pair code of a warp's kept candidates is spread over the warp's
@@ -196,7 +200,7 @@ int ppc_set_launch_shape(ppc_state* s, int32_t tile_edge, int32_t threads, int32
 enum ppc_step_form
 {
 	PPC_STEP_KERNELS = 0,	 /* the default: the fused pass, the compaction plan and
-								the four mesh-rebuild kernels, six launches */
+								the two mesh-rebuild kernels, four launches */
 	PPC_STEP_PERSISTENT = 1	 /* one cooperative launch: the same phases over all
 								replicates, separated by grid barriers */
 };
@@ -211,10 +215,10 @@ int ppc_set_wait_limit(ppc_state* s, int64_t polls);
 
 /* Autotuner of the launch shape (no counterpart in the reference, whose
  * OpenMP loops have no launch shape): runs 2 x `steps` mechanics steps
- * (ppc_step) with each candidate shape — -3, -1 and -2 with 128 threads, 0
- * with 128 threads / 32 KiB and with 64 threads / 16 KiB — times the second
+ * (ppc_step) with each candidate shape — -3, -4, -1 and -2 with 128 threads,
+ * 0 with 128 threads / 32 KiB and with 64 threads / 16 KiB — times the second
  * half of each on the state's stream, and keeps the fastest. The simulation
- * advances by 10 x `steps` steps (the trajectory does not depend on the
+ * advances by 12 x `steps` steps (the trajectory does not depend on the
  * shape). Writes the chosen shape to `tile_edge` and `threads` when they are
  * not NULL. */
 int ppc_autotune(ppc_state* s, int32_t steps, int32_t* tile_edge, int32_t* threads);

@@ -857,7 +857,13 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 		v.err = reinterpret_cast<int32_t*>(v.ctr + replicates);
 	try_(alloc(s, v.cursor, 1));
 	v.nvox = (int32_t)vox;
-	v.ntiles = (int32_t)((vox + 4095) / 4096);
+	{
+		// rebuild tiles of about 512 agents at full capacity, 64 to 4096 voxels
+		const double want = 512.0 * (double)std::max<int64_t>(vox, 1) / (double)std::max<int64_t>(cap, 1);
+		const int sh = (int)std::lround(std::log2(std::max(want, 1.0)));
+		v.tshift = std::min(12, std::max(6, sh));
+	}
+	v.ntiles = (int32_t)((vox + (1 << v.tshift) - 1) >> v.tshift);
 	try_(alloc(s, v.pos[0], C));
 	try_(alloc(s, v.pos[1], C));
 	try_(alloc(s, v.vel, C));
@@ -883,14 +889,19 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.flags, C));
 	try_(alloc(s, v.ids, C));
 	try_(alloc(s, v.rid, C));
-	// counts padded to whole tiles so the scan can use 16-byte loads
-	try_(alloc(s, v.vcnt, (size_t)v.ntiles * 4096));
-	try_(alloc(s, v.vstart, (size_t)v.ntiles * 4096 + 1));
-	try_(alloc(s, v.tile_sum, (size_t)v.ntiles));
+	try_(alloc(s, v.vstart, (size_t)vox + 1));
 	try_(alloc(s, v.key, C));
-	try_(alloc(s, v.vrank, C));
 	try_(alloc(s, v.tmp, C));
 	try_(alloc(s, v.vsc, C));
+	try_(alloc(s, v.tprev, (size_t)v.ntiles));
+	try_(alloc(s, v.tdelta, (size_t)v.ntiles));
+	try_(alloc(s, v.sdelta, ((size_t)v.ntiles + 1023) / 1024));
+	try_(alloc(s, v.chead, (size_t)v.ntiles * 32));
+	try_(alloc(s, v.cnext, C));
+	try_(alloc(s, v.porder, C));
+	try_(alloc(s, v.tdone, 1));
+	if (rc == PPC_OK && cudaMemset(v.chead, 0xff, sizeof(int32_t) * (size_t)v.ntiles * 32) != cudaSuccess)
+		rc = fail(PPC_ERR_CUDA, "cudaMemset failed");
 	try_(alloc(s, v.order_valid, 1));
 	try_(alloc(s, v.binned, replicates));
 	try_(alloc(s, v.moves_pending, 1));
@@ -1019,12 +1030,13 @@ int ppc_set_launch_shape(ppc_state* s, int32_t tile_edge, int32_t threads, int32
 {
 	if (!s)
 		return fail(PPC_ERR_ARG, "null state");
-	if (tile_edge < -3 || tile_edge > 0 || threads < 32 || threads > 256 || threads % 32 != 0 || smem_bytes < 0
+	if (tile_edge < -4 || tile_edge > 0 || threads < 32 || threads > 256 || threads % 32 != 0 || smem_bytes < 0
 		|| smem_bytes > 160 * 1024)
-		return fail(PPC_ERR_ARG, "tile edge 0, -1, -2 or -3, threads 32..256 (multiple of 32), smem <= 160 KiB");
+		return fail(PPC_ERR_ARG, "tile edge 0, -1, -2, -3 or -4, threads 32..256 (multiple of 32), smem <= 160 KiB");
 	PPC_CUDA(cudaStreamSynchronize(s->stream));
 	release_graph(s);
 	s->flat = tile_edge == -3;
+	s->queue = tile_edge == -4;
 	s->staged = tile_edge == 0;
 	s->coop = tile_edge == 0 || tile_edge == -2;
 	s->tile_threads = threads;
@@ -1774,7 +1786,8 @@ int ppc_autotune(ppc_state* s, int32_t steps, int32_t* tile_edge, int32_t* threa
 	{
 		int edge, threads, smem;
 	};
-	const shape cand[] = { { -3, 128, 0 }, { -1, 128, 0 }, { -2, 128, 0 }, { 0, 128, 32 * 1024 }, { 0, 64, 16 * 1024 } };
+	const shape cand[] = { { -3, 128, 0 }, { -4, 128, 0 }, { -1, 128, 0 }, { -2, 128, 0 }, { 0, 128, 32 * 1024 },
+							 { 0, 64, 16 * 1024 } };
 	const int ncand = (int)(sizeof cand / sizeof cand[0]);
 	cudaEvent_t e0 = nullptr, e1 = nullptr;
 	PPC_CUDA(cudaEventCreate(&e0));

@@ -108,7 +108,8 @@ struct view
 	int32_t* err;
 	int32_t* cursor;	// number of binned agents (length of `sorted`)
 	int32_t nvox;		// voxels of all replicates
-	int32_t ntiles;		// scan tiles of 4096 voxels
+	int32_t tshift;		// a rebuild tile is 2^tshift consecutive voxel keys
+	int32_t ntiles;		// rebuild tiles
 
 	double4* pos[2];
 	double4* vel;
@@ -135,13 +136,17 @@ struct view
 	int64_t* ids;
 	int32_t* rid;
 
-	int32_t* vcnt;
-	int32_t* vstart;
-	int32_t* tile_sum;
-	int32_t* key;
-	int32_t* vrank;
-	int32_t* tmp;
-	int2* vsc;		// [C] voxel start and count of each slot's voxel, from the scatter to the fixup
+	int32_t* vstart;	// [nvox + 1] start of each voxel's agents in the key order
+	int32_t* key;		// [C] voxel key of each slot at the last rebuild
+	int32_t* tmp;		// [C] scratch of the rebuild's large tiles (slots grouped by voxel)
+	int2* vsc;			// [C] scratch of the rebuild's large tiles (listed agents)
+	int2* tprev;		// [ntiles] start and count of each tile's agents in the key order
+	int32_t* tdelta;	// [ntiles] agents entering minus leaving each tile at the pending rebuild
+	int32_t* sdelta;	// [ntiles / 1024] the same per 1024 tiles
+	int32_t* chead;		// [ntiles * 32] heads of the tiles' mover chains (-1: empty)
+	int32_t* cnext;		// [C] next slot of a mover chain
+	int2* porder;		// [C] entries of the previous order: (slot, key) of agents kept in their tile
+	unsigned* tdone;	// tiles placed by the current rebuild
 	int32_t* order_valid; // 1 once a rebuild has set `sorted` (cleared by uploads)
 	int32_t* binned;	  // [replicates] live count at the last rebuild (the slots `sorted` lists)
 	int32_t* move_src;	  // [C] tail slot whose agent the next k_bin_count moves into this hole, or -1
@@ -284,6 +289,7 @@ struct ppc_state
 	bool staged = false;
 	bool coop = false;
 	bool flat = true; // per-thread pass with batched candidate fetches (shape -3, the default)
+	bool queue = false; // per-thread pass with the warp's candidates shared out (shape -4)
 	bool persistent = false;		 // mechanics steps as one cooperative launch each (PPC_STEP_PERSISTENT)
 	long long wait_limit = 1LL << 25; // polls of a bounded device wait before it gives up
 	bool lost = false;				 // a bounded wait gave up: the state needs a fresh upload

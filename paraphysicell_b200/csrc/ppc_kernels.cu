@@ -15,8 +15,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kSortCap = 4096; // list length sorted in shared memory
-constexpr int kTileShift = 12; // voxels per scan tile = 4096 = kThreads * kTileItems
-constexpr int kTileItems = 16;
 
 // Programmatic dependent launch: every kernel of the library is launched
 // with programmatic stream serialisation, so its launch and block
@@ -195,83 +193,127 @@ __device__ __forceinline__ void move_agent(const view& v, int cur, int d, int s)
 	v.ncnt[d] = v.ncnt[s];
 }
 
-// Voxel key and provisional rank of one agent (s < 0: an idle lane), with
-// one atomic per distinct voxel and per distinct scan tile of the warp.
-// A hole the compaction plan filled gets its tail agent first.
-__device__ __forceinline__ void count_agent(const view& v, int cur, int s, int r, int lane, bool moves)
+// The rebuild starts from the previous one. The previous key order lists,
+// tile by tile, the slots that were live then (a tile is a run of 2^tshift
+// consecutive voxel keys); tprev holds where each tile's agents start in
+// that order and how many there were. k_bin_count recomputes every live
+// agent's key: an agent whose key stays in its tile keeps its entry of the
+// previous order (porder), every other one, and every slot appended since
+// (all slots when there is no previous order), is pushed onto one of the 32
+// mover chains of its new tile, and the tile counts change by the difference
+// (tdelta, and per 1024 tiles sdelta). k_bin_place then builds each tile by
+// itself: its start is its previous start plus the changes of the tiles
+// before it; its agents are its kept entries and its chains; their per-voxel
+// counts, the voxel starts and the order inside a voxel (descending slot,
+// the order a serial run of the reference's fetch_sub scatter gives) are
+// formed in shared memory, and each agent writes its key-ordered copies.
+// Agents rarely leave their tile between steps, so the chains are short.
+
+constexpr int kChains = 32;		 // mover chains per tile
+constexpr int kSuperShift = 10;	 // tiles per entry of sdelta: 1024
+constexpr int kPlaceThreads = 256;
+constexpr int kPlaceList = 1024; // agents of a tile listed in shared memory; the rest in global scratch
+constexpr int kMaxTileShift = 12;
+
+// the voxel key of slot s of replicate r at positions pos[cur]
+__device__ __forceinline__ int32_t voxel_key(const view& v, int cur, int s, int r)
 {
-	if (s >= 0 && moves)
+	const rep_info& R = v.reps[r];
+	const double4 p = v.pos[cur][s];
+	const int c0 = axis_coord(p.x, R, 0, v.err);
+	const int c1 = v.dims >= 2 ? axis_coord(p.y, R, 1, v.err) : 0;
+	const int c2 = v.dims >= 3 ? axis_coord(p.z, R, 2, v.err) : 0;
+	return (int32_t)(R.vox_base + c0 + (int64_t)R.grid[0] * (c1 + (int64_t)R.grid[1] * c2));
+}
+
+// a hole the compaction plan filled takes its tail agent first
+__device__ __forceinline__ void apply_move(const view& v, int cur, int s)
+{
+	const int src = v.move_src[s];
+	if (src >= 0)
 	{
-		const int src = v.move_src[s];
-		if (src >= 0)
-		{
-			move_agent(v, cur, s, src);
-			v.move_src[s] = -1;
-		}
-	}
-	int32_t key = -1 - lane; // distinct per idle lane, so idle lanes never group
-	if (s >= 0)
-	{
-		const rep_info& R = v.reps[r];
-		const double4 p = v.pos[cur][s];
-		const int c0 = axis_coord(p.x, R, 0, v.err);
-		const int c1 = v.dims >= 2 ? axis_coord(p.y, R, 1, v.err) : 0;
-		const int c2 = v.dims >= 3 ? axis_coord(p.z, R, 2, v.err) : 0;
-		key = (int32_t)(R.vox_base + c0 + (int64_t)R.grid[0] * (c1 + (int64_t)R.grid[1] * c2));
-	}
-	const unsigned same = __match_any_sync(0xffffffffu, key);
-	const int lead = __ffs(same) - 1;
-	int base = 0;
-	if (s >= 0 && lane == lead)
-		base = atomicAdd(v.vcnt + key, __popc(same));
-	base = __shfl_sync(0xffffffffu, base, lead);
-	const int32_t tile = s >= 0 ? (key >> kTileShift) : -1 - lane;
-	const unsigned same_tile = __match_any_sync(0xffffffffu, tile);
-	if (s >= 0 && lane == __ffs(same_tile) - 1)
-		atomicAdd(v.tile_sum + tile, __popc(same_tile));
-	if (s >= 0)
-	{
-		v.key[s] = key;
-		v.vrank[s] = base + __popc(same & ((1u << lane) - 1));
+		move_agent(v, cur, s, src);
+		v.move_src[s] = -1;
 	}
 }
 
-// Voxel key and provisional rank of every live agent, and the per-tile
-// totals the scan needs. The previous rebuild's key order lists the slots
-// that were live then; those still live are taken in that order — agents
-// rarely change voxel between steps, so a warp's agents share voxels and
-// tiles and the atomics aggregate — and the slots appended since (division
-// daughters past the previous count) by slot. Without a previous order
-// (after an upload) every live slot is taken by slot. The provisional rank
-// only has to be a permutation of 0..count-1 inside the voxel; k_bin_fixup
-// sets the final one.
-//
-// A conditional rebuild (after an upload of positions) runs only if the
-// upload changed some position; its decision goes to bin_active for the
-// other three kernels.
-// the count of the agents at previous key-ordered position t and at slot t
-__device__ __forceinline__ void bin_count_body(const view& v, int cur, int t, int lane)
+// pushes slot q onto a mover chain of the tile of `key`
+__device__ __forceinline__ void chain_push(const view& v, int q, int32_t key)
+{
+	const int64_t c = (int64_t)(key >> v.tshift) * kChains + (q & (kChains - 1));
+	v.cnext[q] = atomicExch(v.chead + c, q);
+}
+
+// adds `amount` to the change of `tile` (negative: none) and of its group of
+// 1024 tiles, one atomic per distinct tile of the warp; every lane calls it
+__device__ __forceinline__ void tile_change(const view& v, int tile, int amount)
+{
+	const int lane = threadIdx.x & 31;
+	if (!__any_sync(0xffffffffu, tile >= 0))
+		return;
+	const int key = tile >= 0 ? tile : -1 - lane;
+	const unsigned same = __match_any_sync(0xffffffffu, key);
+	if (tile >= 0 && lane == __ffs(same) - 1)
+		atomicAdd(v.tdelta + tile, amount * __popc(same));
+	const int sup = tile >= 0 ? tile >> kSuperShift : -1 - lane;
+	const unsigned same_sup = __match_any_sync(0xffffffffu, sup);
+	if (tile >= 0 && lane == __ffs(same_sup) - 1)
+		atomicAdd(v.sdelta + sup, amount * __popc(same_sup));
+}
+
+// The entry at position t of the previous order, and slot t when it was
+// appended since the previous rebuild (or there is no previous order).
+// Every lane of the warp calls it.
+__device__ __forceinline__ void bin_count_body(const view& v, int cur, int t)
 {
 	const bool ordered = *v.order_valid != 0;
 	const bool moves = *v.moves_pending != 0;
 	const bool appended = *v.appended != 0;
-	// both candidates first, so that their loads overlap
-	int sa = -1, ra = 0, sb = -1, rb = 0, local = 0;
-	if ((!ordered || appended) && t < v.total_cap && live(v, t, rb, local)
-		&& local >= (ordered ? v.binned[rb] : 0))
-		sb = t;
+	const int sh = v.tshift;
+	int leave = -1, enter_a = -1, enter_b = -1;
 	if (ordered && t < *v.cursor)
 	{
 		const int q = v.sorted[t];
-		if (live(v, q, ra, local))
-			sa = q;
+		const int32_t okey = v.skey[t];
+		int2 e = make_int2(-1, -1);
+		int r, local;
+		if ((unsigned)q < (unsigned)v.total_cap && live(v, q, r, local))
+		{
+			if (moves)
+				apply_move(v, cur, q);
+			const int32_t key = voxel_key(v, cur, q, r);
+			v.key[q] = key;
+			if ((key >> sh) == (okey >> sh))
+				e = make_int2(q, key);
+			else
+			{
+				chain_push(v, q, key);
+				leave = okey >> sh;
+				enter_a = key >> sh;
+			}
+		}
+		else
+			leave = okey >> sh;
+		v.porder[t] = e;
 	}
-	if (__any_sync(0xffffffffu, sa >= 0))
-		count_agent(v, cur, sa, ra, lane, moves);
-	if (__any_sync(0xffffffffu, sb >= 0))
-		count_agent(v, cur, sb, rb, lane, moves);
+	int r, local;
+	if ((!ordered || appended) && t < v.total_cap && live(v, t, r, local) && local >= (ordered ? v.binned[r] : 0))
+	{
+		if (moves)
+			apply_move(v, cur, t);
+		const int32_t key = voxel_key(v, cur, t, r);
+		v.key[t] = key;
+		chain_push(v, t, key);
+		enter_b = key >> sh;
+	}
+	tile_change(v, leave, -1);
+	tile_change(v, enter_a, 1);
+	tile_change(v, enter_b, 1);
 }
 
+// A conditional rebuild (after an upload of positions) runs only if the
+// upload changed some position; its decision goes to bin_active for
+// k_bin_place.
 __global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur, int conditional)
 {
 	grid_wait();
@@ -281,162 +323,19 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur, int con
 		*v.bin_active = active ? 1 : 0;
 	if (!active)
 		return;
-	bin_count_body(v, cur, t, threadIdx.x & 31);
+	bin_count_body(v, cur, t);
 }
 
-// The scan of one tile of 4096 voxels by a block of THREADS threads.
-template <int THREADS>
-__device__ __forceinline__ void bin_scan_tile(const view& v, int b)
+// writes the key-ordered copies of slot s at position t of voxel `key`.
+// Affinity rows of up to four definitions are carried in registers.
+__device__ __forceinline__ void place_agent(const view& v, int cur, int s, int t, int32_t key)
 {
-	constexpr int ITEMS = (1 << kTileShift) / THREADS;
-	static_assert(ITEMS % 4 == 0, "a thread scans whole int4 groups of its tile");
-	// the tile's counts first (counts are padded to whole tiles and zero past
-	// the last voxel), so their loads overlap the predecessor totals' loads
-	const int64_t i0 = ((int64_t)b << kTileShift) + (int64_t)threadIdx.x * ITEMS;
-	int c[ITEMS];
-	int sum = 0;
-	{
-		const int4* q = reinterpret_cast<const int4*>(v.vcnt + i0);
-#pragma unroll
-		for (int k = 0; k < ITEMS / 4; k++)
-		{
-			int4 x = q[k];
-			c[4 * k] = x.x;
-			c[4 * k + 1] = x.y;
-			c[4 * k + 2] = x.z;
-			c[4 * k + 3] = x.w;
-		}
-	}
-	int part = 0;
-	for (int k = threadIdx.x; k < b; k += blockDim.x)
-		part += v.tile_sum[k];
-	int tile_base;
-	block_exclusive_scan(part, tile_base);
-
-#pragma unroll
-	for (int k = 0; k < ITEMS; k++)
-		sum += c[k];
-	int tile_total;
-	int run = tile_base + block_exclusive_scan(sum, tile_total);
-	if (i0 + ITEMS <= v.nvox)
-	{
-		int4* st = reinterpret_cast<int4*>(v.vstart + i0);
-#pragma unroll
-		for (int k = 0; k < ITEMS / 4; k++)
-		{
-			int4 x;
-			x.x = run;
-			run += c[4 * k];
-			x.y = run;
-			run += c[4 * k + 1];
-			x.z = run;
-			run += c[4 * k + 2];
-			x.w = run;
-			run += c[4 * k + 3];
-			st[k] = x;
-		}
-	}
-	else
-	{
-		for (int k = 0; k < ITEMS; k++)
-			if (i0 + k < v.nvox)
-			{
-				v.vstart[i0 + k] = run;
-				run += c[k];
-			}
-	}
-	if (b == v.ntiles - 1 && threadIdx.x == blockDim.x - 1)
-	{
-		v.vstart[v.nvox] = run;
-		*v.cursor = run;
-	}
-}
-
-// Exclusive scan of the per-voxel counts into vstart (one block per tile of
-// 4096 voxels); a tile's offset is the sum of the totals of the tiles before
-// it (k_bin_count accumulates them). The counts are cleared at occupied
-// voxels by k_bin_fixup, the tile totals by k_bin_scatter.
-__global__ void __launch_bounds__(kThreads) k_bin_scan(view v)
-{
-	grid_wait();
-	if (!*v.bin_active)
-		return;
-	bin_scan_tile<kThreads>(v, blockIdx.x);
-}
-
-// provisional scatter; also hands the fixup its voxel's start and count so
-// the fixup need not look them up again
-// block 0 of the scatter readies the counters of the next rebuild
-__device__ __forceinline__ void bin_scatter_resets(const view& v)
-{
-	for (int k = threadIdx.x; k < v.ntiles; k += blockDim.x)
-		v.tile_sum[k] = 0; // ready for the next rebuild's k_bin_count
-	for (int k = threadIdx.x; k < v.nreps; k += blockDim.x)
-		v.binned[k] = v.ctr[k].count; // the slots this rebuild's order lists
-	if (threadIdx.x == 0)
-	{
-		*v.moves_pending = 0; // applied by this rebuild's k_bin_count
-		*v.appended = 0;	  // counted by it too
-	}
-}
-
-__device__ __forceinline__ void bin_scatter_agent(const view& v, int s)
-{
-	if (s >= v.total_cap)
-		return;
-	int r, local;
-	if (!live(v, s, r, local))
-		return;
-	const int32_t key = v.key[s];
-	const int rank = v.vrank[s];
-	const int st = v.vstart[key];
-	const int c = v.vcnt[key];
-	// the bounds hold after every complete count and scan; they guard the
-	// persistent step's phases that still run after another block gave up
-	// on a barrier
-	if ((unsigned)(st + rank) >= (unsigned)v.total_cap)
+	if ((unsigned)s >= (unsigned)v.total_cap || (unsigned)t >= (unsigned)v.total_cap)
 	{
 		atomicOr(v.err, ERR_LIST_CAPACITY);
 		return;
 	}
-	v.tmp[st + rank] = s;
-	v.vsc[s] = make_int2(st, c);
-}
-
-__global__ void k_bin_scatter(view v)
-{
-	grid_wait();
-	int s = blockIdx.x * blockDim.x + threadIdx.x;
-	if (s == 0)
-		*v.pos_changed = 0; // read by this rebuild's k_bin_count only
-	if (!*v.bin_active)
-		return;
-	if (blockIdx.x == 0)
-		bin_scatter_resets(v);
-	bin_scatter_agent(v, s);
-}
-
-// final place inside the voxel: descending slot order, which is the order
-// a serial run of the reference's fetch_sub scatter produces. Affinity rows
-// of up to four definitions are carried in registers.
-// thread tp takes the agent the scatter put at provisional position tp;
-// its final position is in the same voxel's range, so the stores of
-// neighbouring threads land close together
-__device__ __forceinline__ void bin_fixup_agent(const view& v, int cur, int tp)
-{
-	if (tp >= *v.cursor)
-		return;
-	const int s = v.tmp[tp];
-	if ((unsigned)s >= (unsigned)v.total_cap)
-		return;
 	const int r = rep_of(v, s);
-	const int32_t key = v.key[s];
-	const int2 sc = v.vsc[s];
-	if (sc.x < 0 || sc.y < 0 || (int64_t)sc.x + sc.y > v.total_cap)
-	{
-		atomicOr(v.err, ERR_LIST_CAPACITY);
-		return;
-	}
 	const double4 prm = v.prm[s];
 	double4 p = v.pos[cur][s];
 	const double rmad = v.rmad[s];
@@ -449,17 +348,7 @@ __device__ __forceinline__ void bin_fixup_agent(const view& v, int cur, int tp)
 		aff[q] = q < D ? v.aff[(int64_t)s * D + q] : 0.0;
 	const rep_info& R = v.reps[r];
 	const double m0 = R.mins[0], m1 = R.mins[1], m2 = R.mins[2];
-	int rank = 0;
-	for (int u = 0; u < sc.y && sc.y > 1; u++)
-		rank += v.tmp[sc.x + u] > s;
-	const int t = sc.x + rank;
-	if (t >= v.total_cap)
-		return;
-	if (s == 0)
-		*v.order_valid = 1; // `sorted` now lists exactly the live slots
 	p.w = rmad * prm.x; // relative_maximum_adhesion_distance * radius
-	if (rank == 0)
-		v.vcnt[key] = 0; // ready for the next rebuild
 	v.sorted[t] = s;
 	v.skey[t] = key;
 	v.spos4[t] = p;
@@ -487,12 +376,187 @@ __device__ __forceinline__ void bin_fixup_agent(const view& v, int cur, int tp)
 	}
 }
 
-__global__ void k_bin_fixup(view v, int cur)
+struct place_smem
 {
+	int32_t cnt[(1 << kMaxTileShift) + 1]; // per-voxel counts, then starts, then ends
+	int2 list[kPlaceList];				   // the tile's agents: (slot, voxel inside the tile)
+	int32_t group[kPlaceList];			   // slots grouped by voxel
+	int32_t n, last;
+};
+
+// lists slot s of local voxel lv (nv voxels in the tile); items past the
+// shared list go to the global scratch at the tile's start
+__device__ __forceinline__ void place_add(const view& v, place_smem& sm, int base, int s, int lv, int nv)
+{
+	if ((unsigned)lv >= (unsigned)nv)
+	{
+		atomicOr(v.err, ERR_LIST_CAPACITY); // a key outside the tile: the order or a chain is broken
+		return;
+	}
+	const int i = atomicAdd(&sm.n, 1);
+	atomicAdd(&sm.cnt[lv], 1);
+	if (i < kPlaceList)
+		sm.list[i] = make_int2(s, lv);
+	else if ((int64_t)base + i < v.total_cap)
+		v.vsc[base + i] = make_int2(s, lv);
+}
+
+__device__ __forceinline__ int2 place_item(const view& v, const place_smem& sm, int base, int i)
+{
+	return i < kPlaceList ? sm.list[i] : v.vsc[base + i];
+}
+
+// Builds tile b of the new order (see above): the voxel starts in vstart,
+// the agents' key-ordered copies, the tile's entry of tprev. The tile whose
+// placing completes last readies the counters for the next rebuild.
+template <int THREADS>
+__device__ __forceinline__ void bin_place_tile(const view& v, int cur, int b, place_smem& sm)
+{
+	const int tid = threadIdx.x;
+	const int sh = v.tshift;
+	const int k0 = b << sh;
+	const int nv = min(1 << sh, v.nvox - k0);
+	const bool ordered = *v.order_valid != 0;
+	// the start: the previous start plus the changes of the tiles before
+	int part = 0;
+	const int sb = b >> kSuperShift;
+	for (int j = tid; j < sb; j += THREADS)
+		part += v.sdelta[j];
+	for (int k = (sb << kSuperShift) + tid; k < b; k += THREADS)
+		part += v.tdelta[k];
+	const int2 tp = ordered ? v.tprev[b] : make_int2(0, 0);
+	const int L = tp.y + v.tdelta[b];
+	for (int i = tid; i <= nv; i += THREADS)
+		sm.cnt[i] = 0;
+	if (tid == 0)
+		sm.n = 0;
+	int moved;
+	block_exclusive_scan(part, moved); // synchronises the block
+	const int base = tp.x + moved;
+	const bool fits = base >= 0 && L >= 0 && (int64_t)base + L <= v.total_cap;
+
+	// the kept entries of the previous order, then the chains
+	if (fits)
+		for (int i = tid; i < tp.y; i += THREADS)
+		{
+			const int2 e = v.porder[tp.x + i];
+			if (e.x >= 0)
+				place_add(v, sm, base, e.x, e.y - k0, nv);
+		}
+	if (tid < kChains)
+	{
+		int* head = v.chead + (int64_t)b * kChains + tid;
+		int q = *head;
+		*head = -1;
+		for (int hops = 0; q >= 0 && fits; hops++)
+		{
+			if (hops >= v.total_cap || q >= v.total_cap)
+			{
+				atomicOr(v.err, ERR_LIST_CAPACITY);
+				break;
+			}
+			place_add(v, sm, base, q, v.key[q] - k0, nv);
+			q = v.cnext[q];
+		}
+	}
+	__syncthreads();
+	const int n = sm.n;
+	const bool ok = fits && n == L;
+	if (!ok && tid == 0)
+		atomicOr(v.err, ERR_LIST_CAPACITY);
+
+	if (ok)
+	{
+		// per-voxel starts: exclusive scan of the counts, in place (all zero
+		// in an empty tile)
+		if (n > 0)
+		{
+			const int per = (nv + THREADS - 1) / THREADS;
+			const int j0 = min(tid * per, nv), j1 = min(j0 + per, nv);
+			int sum = 0;
+			for (int j = j0; j < j1; j++)
+				sum += sm.cnt[j];
+			int total;
+			int run = block_exclusive_scan(sum, total);
+			for (int j = j0; j < j1; j++)
+			{
+				const int c = sm.cnt[j];
+				sm.cnt[j] = run;
+				run += c;
+			}
+			__syncthreads();
+		}
+		// a tile that was and stays empty at the same start keeps its starts
+		if (!(ordered && tp.y == 0 && n == 0 && base == tp.x))
+			for (int j = tid; j < nv; j += THREADS)
+				v.vstart[k0 + j] = base + sm.cnt[j];
+		if (k0 + nv == v.nvox && tid == 0)
+		{
+			v.vstart[v.nvox] = base + n;
+			*v.cursor = base + n;
+		}
+		__syncthreads(); // the starts are read above before the grouping moves them
+		// slots grouped by voxel; afterwards cnt[j] is the end of voxel j
+		for (int i = tid; i < n; i += THREADS)
+		{
+			const int2 it = place_item(v, sm, base, i);
+			const int p = atomicAdd(&sm.cnt[it.y], 1);
+			if (p < kPlaceList)
+				sm.group[p] = it.x;
+			else
+				v.tmp[base + p] = it.x;
+		}
+		__syncthreads();
+		for (int i = tid; i < n; i += THREADS)
+		{
+			const int2 it = place_item(v, sm, base, i);
+			const int lo = it.y ? sm.cnt[it.y - 1] : 0, hi = sm.cnt[it.y];
+			int rank = 0;
+			for (int u = lo; u < hi; u++)
+				rank += (u < kPlaceList ? sm.group[u] : v.tmp[base + u]) > it.x;
+			place_agent(v, cur, it.x, base + lo + rank, k0 + it.y);
+		}
+		if (tid == 0)
+			v.tprev[b] = make_int2(base, n);
+	}
+
+	// the tile completing last readies the counters of the next rebuild
+	__syncthreads();
+	if (tid == 0)
+	{
+		__threadfence();
+		sm.last = atomicAdd(v.tdone, 1u) == (unsigned)v.ntiles - 1;
+	}
+	__syncthreads();
+	if (sm.last)
+	{
+		__threadfence();
+		const int nsup = (v.ntiles + (1 << kSuperShift) - 1) >> kSuperShift;
+		for (int k = tid; k < v.ntiles; k += THREADS)
+			v.tdelta[k] = 0;
+		for (int k = tid; k < nsup; k += THREADS)
+			v.sdelta[k] = 0;
+		for (int k = tid; k < v.nreps; k += THREADS)
+			v.binned[k] = v.ctr[k].count; // the slots this rebuild's order lists
+		if (tid == 0)
+		{
+			*v.tdone = 0;
+			*v.order_valid = 1;
+			*v.moves_pending = 0; // applied by this rebuild's count
+			*v.appended = 0;	  // counted by it too
+			*v.pos_changed = 0;
+		}
+	}
+	__syncthreads(); // shared memory is reused by the next tile of a persistent block
+}
+
+__global__ void __launch_bounds__(kPlaceThreads) k_bin_place(view v, int cur)
+{
+	__shared__ place_smem sm;
 	grid_wait();
 	if (!*v.bin_active)
 		return;
-	bin_fixup_agent(v, cur, blockIdx.x * blockDim.x + threadIdx.x);
+	bin_place_tile<kPlaceThreads>(v, cur, blockIdx.x, sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -1541,6 +1605,43 @@ __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefe
 __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
 
+// membrane, springs, Adams-Bashforth, then the agent's stores: the end of
+// the fused pass for the agent in slot s with the pair sums (vx, vy, vz,
+// pressure); pi is its key-ordered position, radius its radius
+template <int DIMS>
+__device__ __forceinline__ void agent_finish(const view& v, int cur, int opts, int s, int r, const rep_info& R,
+											 const double4& pi, double radius, int def_i, bool mov_i, int nspr,
+											 double vx, double vy, double vz, double pressure)
+{
+	const bool walls_on = (opts & FUSED_WALLS) != 0;
+	const bool vel_on = (opts & FUSED_VEL) != 0;
+	double4 p = make_double4(pi.x, pi.y, pi.z, 0.0);
+	double4 vp = make_double4(0, 0, 0, 0);
+	const uint8_t flag = v.flags[s];
+	if (mov_i)
+	{
+		vp = v.vprev[s];
+		double4 vel = make_double4(vx, vy, vz, 0.0);
+		if (walls_on)
+			walls<DIMS>(v, R, p, radius, v.prm[s].w, vel);
+		if (nspr > 0)
+			spring_contract<DIMS>(v, cur, s, nspr, p, def_i, vel);
+		ab2<DIMS>(v.dt, p, vel, vp);
+	}
+	v.pressure[s] = pressure;
+	if (mov_i)
+	{
+		v.vprev[s] = vp;
+		if (vel_on)
+			v.vel[s] = make_double4(0, 0, 0, 0);
+	}
+	v.pos[cur ^ 1][s] = p;
+	if (!(p.x == p.x && p.y == p.y && p.z == p.z))
+		atomicOr(v.err, ERR_NONFINITE);
+	if (to_remove<DIMS>(R, p, flag))
+		append_bad(v, r, s - R.base);
+}
+
 // the agent at key-ordered position t, with its block's shared slots `sm`
 template <int DIMS, bool F32>
 __device__ __forceinline__ void fused_flat_agent(const view& v, int cur, int opts, int t, flat_smem& sm)
@@ -1803,32 +1904,7 @@ __device__ __forceinline__ void fused_flat_agent(const view& v, int cur, int opt
 		pressure = fp.value();
 	}
 
-	// membrane, springs, Adams-Bashforth, then the agent's stores
-	double4 p = make_double4(pi.x, pi.y, pi.z, 0.0);
-	double4 vp = make_double4(0, 0, 0, 0);
-	const uint8_t flag = v.flags[s];
-	if (mov_i)
-	{
-		vp = v.vprev[s];
-		double4 vel = make_double4(vx, vy, vz, 0.0);
-		if (walls_on)
-			walls<DIMS>(v, R, p, qi.x, v.prm[s].w, vel);
-		if (nspr > 0)
-			spring_contract<DIMS>(v, cur, s, nspr, p, def_i, vel);
-		ab2<DIMS>(v.dt, p, vel, vp);
-	}
-	v.pressure[s] = pressure;
-	if (mov_i)
-	{
-		v.vprev[s] = vp;
-		if (vel_on)
-			v.vel[s] = make_double4(0, 0, 0, 0);
-	}
-	v.pos[cur ^ 1][s] = p;
-	if (!(p.x == p.x && p.y == p.y && p.z == p.z))
-		atomicOr(v.err, ERR_NONFINITE);
-	if (to_remove<DIMS>(R, p, flag))
-		append_bad(v, r, s - R.base);
+	agent_finish<DIMS>(v, cur, opts, s, r, R, pi, qi.x, def_i, mov_i, nspr, vx, vy, vz, pressure);
 }
 
 template <int DIMS, bool F32>
@@ -1839,6 +1915,411 @@ __global__ void __launch_bounds__(kFlatThreads, 5) k_fused_flat(view v, int cur,
 	extern __shared__ __align__(16) unsigned char flat_raw[];
 	fused_flat_agent<DIMS, F32>(v, cur, opts, blockIdx.x * kFlatThreads + threadIdx.x,
 								*reinterpret_cast<flat_smem*>(flat_raw));
+}
+
+// ---------------------------------------------------------------------------
+// fused step, one thread per agent, candidates shared out over the warp.
+//
+// In a sparse tissue the agents of a warp hold very different numbers of
+// candidates, and the passes above run a warp for as many rounds as its
+// busiest lane needs. Here a warp lays its 32 agents' candidates end to end,
+// agent by agent and each agent's in the reference's order (rows z, y; in a
+// row the key-ordered range of its three voxels), and lane l takes the
+// candidates l, l + 32, ... of that list: the filter runs on full warps. The
+// candidates it keeps are listed in the same order; full warps then fetch
+// their FP64 data and evaluate the pair terms, and each agent's lane adds its
+// own terms in its candidate order, so every sum rounds as in the
+// reference's loop.
+// ---------------------------------------------------------------------------
+
+constexpr int kQueueThreads = 128;
+constexpr int kQueueRounds = 4;	 // candidate rounds whose loads are in flight together
+constexpr int kQueueHits = 256; // kept candidates a warp lists before evaluating them
+
+struct queue_warp
+{
+	int2 rows[9][32];		   // per agent and stencil row: first candidate number, array position - number
+	int32_t first[33];		   // each agent's first candidate in the warp's list; first[32]: the total
+	int32_t t[32];			   // the agents' key-ordered positions (-1: no agent)
+	float margin[32];		   // the agents' filter margins
+	float4 pf[32];			   // single-precision positions
+	double4 pi[32], qi[32];	   // FP64 positions and parameter rows
+	int2 hit[kQueueHits];	   // kept candidates: (agent lane, array position)
+	double term[32], fx[32], fy[32], fz[32]; // the pair terms of a round of kept candidates
+	int32_t hflags[32];		   // bit 0: within range, bit 1: the neighbour is movable
+	uint32_t seg[32];		   // per agent: the lanes of the round holding its candidates
+};
+
+struct queue_smem
+{
+	queue_warp w[kQueueThreads / 32];
+};
+
+// Evaluates the warp's kept candidates [0, nh) in rounds of 32 and adds each
+// agent's terms to its sums in list order.
+template <int DIMS, bool F32>
+__device__ __forceinline__ void queue_hits(const view& v, queue_warp& w, int nh, bool act, bool mov_i, double& vx,
+										   double& vy, double& vz, double& pressure, nsum& fx, nsum& fy, nsum& fz,
+										   nsum& fp)
+{
+	const int lane = threadIdx.x & 31;
+	const int D = v.ndefs;
+	for (int h0 = 0; h0 < nh; h0 += 32)
+	{
+		const int h = h0 + lane;
+		int own = -1, flags = 0;
+		double term = 0.0, tx = 0.0, ty = 0.0, tz = 0.0;
+		if (h < nh)
+		{
+			const int2 e = w.hit[h];
+			own = e.x;
+			const int u = e.y;
+			const double4 pa = w.pi[own];
+			const double4 qa = w.qi[own];
+			const int ta = w.t[own];
+			int def_a;
+			bool mov_a;
+			unpack_bits(qa.w, def_a, mov_a);
+			const double4 q = v.spos4[u];
+			// exact FP64 neighbour test: distance <= rmad_i r_i + rmad_j r_j
+			const double ddx = pa.x - q.x;
+			const double ddy = DIMS >= 2 ? pa.y - q.y : 0.0;
+			const double ddz = DIMS >= 3 ? pa.z - q.z : 0.0;
+			double d2 = ddx * ddx;
+			if (DIMS >= 2)
+				d2 = d2 + ddy * ddy;
+			if (DIMS >= 3)
+				d2 = d2 + ddz * ddz;
+			const double ad = pa.w + q.w;
+			const double dist = DIMS == 1 ? fabs(ddx) : sqrt(d2);
+			if (F32)
+			{
+				// pair_fp32::add with the agent's values
+				const float4 qj = v.sprmf[u];
+				const float afj = v.safff[(int64_t)u * D + def_a];
+				int def_j, spr_j;
+				bool mov_j;
+				unpack_fbits(qj.w, def_j, mov_j, spr_j);
+				if (dist <= ad)
+				{
+					flags = 1 | (mov_j ? 2 : 0);
+					const float dx = (float)ddx, dy = (float)ddy, dz = (float)ddz;
+					float d2f = dx * dx;
+					if (DIMS >= 2)
+						d2f = d2f + dy * dy;
+					if (DIMS >= 3)
+						d2f = d2f + dz * dz;
+					const float distf = DIMS == 1 ? fabsf(dx) : sqrtf(d2f);
+					const float d = distf < 0.00001f ? 0.00001f : distf;
+					float rep = 1.f - d / ((float)qa.x + qj.x);
+					rep = rep < 0.f ? 0.f : rep;
+					rep = rep * rep;
+					term = rep * 36.64504274775163f;
+					if (mov_a)
+					{
+						rep = rep * sqrtf((float)qa.y * qj.y);
+						float adh = 1.f - d / (w.pf[own].w + (float)q.w);
+						adh = adh * adh;
+						adh = adh * sqrtf((float)qa.z * qj.z * v.safff[(int64_t)ta * D + def_j] * afj);
+						const float force = (rep - adh) / d;
+						tx = force * dx;
+						ty = force * dy;
+						tz = force * dz;
+					}
+				}
+			}
+			else
+			{
+				// pair_fp64::add_pair with the agent's values
+				const double4 pr = v.sprm4[u];
+				const double afj = v.saff[(int64_t)u * D + def_a];
+				int def_j;
+				bool mov_j;
+				unpack_bits(pr.w, def_j, mov_j);
+				if (dist <= ad)
+				{
+					flags = 1 | (mov_j ? 2 : 0);
+					const double d = dist < 0.00001 ? 0.00001 : dist;
+					double rep = 1.0 - d / (qa.x + pr.x);
+					rep = rep < 0 ? 0 : rep;
+					rep = rep * rep;
+					term = rep * simple_pressure_coefficient;
+					if (mov_a)
+					{
+						rep = rep * sqrt(qa.y * pr.y);
+						double adh = 1.0 - d / ad;
+						adh = adh * adh;
+						adh = adh * sqrt(qa.z * pr.z * v.saff[(int64_t)ta * D + def_j] * afj);
+						const double force = (rep - adh) / d;
+						tx = force * ddx;
+						ty = force * ddy;
+						tz = force * ddz;
+					}
+				}
+			}
+		}
+		w.term[lane] = term;
+		w.fx[lane] = tx;
+		w.fy[lane] = ty;
+		w.fz[lane] = tz;
+		w.hflags[lane] = flags;
+		const unsigned grp = __match_any_sync(0xffffffffu, own);
+		if (own >= 0 && lane == __ffs(grp) - 1)
+			w.seg[own] = grp;
+		__syncwarp();
+		if (act)
+		{
+			unsigned m = w.seg[lane];
+			w.seg[lane] = 0;
+			while (m)
+			{
+				const int l = __ffs(m) - 1;
+				m &= m - 1;
+				const int f = w.hflags[l];
+				if (!(f & 1))
+					continue;
+				const double tm = w.term[l];
+				if (F32)
+				{
+					if (mov_i)
+						fp.add((float)tm);
+					if (f & 2)
+						fp.add((float)tm);
+					if (mov_i)
+					{
+						fx.add((float)w.fx[l]);
+						fy.add((float)w.fy[l]);
+						fz.add((float)w.fz[l]);
+					}
+				}
+				else
+				{
+					if (mov_i)
+						pressure = pressure + tm;
+					if (f & 2)
+						pressure = pressure + tm;
+					if (mov_i)
+					{
+						vx = vx + w.fx[l];
+						vy = vy + w.fy[l];
+						vz = vz + w.fz[l];
+					}
+				}
+			}
+		}
+		__syncwarp();
+	}
+}
+
+// the agent at key-ordered position t; every lane of the warp calls it
+template <int DIMS, bool F32>
+__device__ __forceinline__ void fused_queue_agent(const view& v, int cur, int opts, int t, queue_warp& w)
+{
+	constexpr int NR = DIMS == 3 ? 9 : (DIMS == 2 ? 3 : 1);
+	const bool springs_on = (opts & FUSED_SPRINGS) != 0;
+	const bool walls_on = (opts & FUSED_WALLS) != 0;
+	const bool vel_on = (opts & FUSED_VEL) != 0;
+	const int lane = threadIdx.x & 31;
+	int s = 0;
+	int32_t key = 0;
+	double4 pi = make_double4(0, 0, 0, 0), qi = make_double4(0, 0, 0, 0);
+	float4 pf = make_float4(0, 0, 0, 0);
+	bool act = false;
+	if (t < v.total_cap)
+	{
+		// issued before the count is known (t is below the capacity)
+		s = v.sorted[t];
+		key = v.skey[t];
+		pi = v.spos4[t];
+		pf = v.sposf[t];
+		qi = v.sprm4[t];
+		act = t < *v.cursor;
+	}
+	int def_i = 0, r = 0;
+	bool mov_i = false;
+	if (act)
+	{
+		unpack_bits(qi.w, def_i, mov_i);
+		const long long bits_i = __double_as_longlong(qi.w);
+		r = v.nreps == 1 ? 0 : (v.nreps <= 65536 ? (int)((bits_i >> 48) & 0xffff) : v.rid[s]);
+	}
+	const rep_info& R = v.reps[r];
+	const int D = v.ndefs;
+	int lo[NR], hi[NR];
+	if (act)
+	{
+		// this agent's affinity row: read per neighbour by definition index
+		if (F32)
+			prefetch_l1(v.safff + (int64_t)t * D);
+		else
+			prefetch_l1(v.saff + (int64_t)t * D);
+		const int32_t lk = key - (int32_t)R.vox_base;
+		const int g0 = R.grid[0], g1 = R.grid[1], g2 = R.grid[2];
+		int cx, cy, cz;
+		voxel_coords(R, lk, cx, cy, cz);
+		const int xlo = cx > 0 ? cx - 1 : 0;
+		const int xhi = cx + 1 < g0 ? cx + 1 : g0 - 1;
+#pragma unroll
+		for (int k = 0; k < NR; k++)
+		{
+			const int dz = DIMS == 3 ? k / 3 - 1 : 0;
+			const int dy = DIMS >= 2 ? k % 3 - 1 : 0;
+			const int z = cz + dz, y = cy + dy;
+			const bool ok = z >= 0 && z < g2 && y >= 0 && y < g1;
+			const int32_t row = ok ? (int32_t)R.vox_base + g0 * (y + g1 * z) : 0;
+			lo[k] = ok ? v.vstart[row + xlo] : 0;
+			hi[k] = ok ? v.vstart[row + xhi + 1] : 0;
+		}
+	}
+	else
+	{
+#pragma unroll
+		for (int k = 0; k < NR; k++)
+			lo[k] = hi[k] = 0;
+	}
+	// the epilogue's per-agent rows are read after the scan: ask L2 for them
+	// now, with the first two spring partners' rows once their indices arrive
+	const int nspr = (act && springs_on && mov_i) ? unpack_springs(qi.w) : 0;
+	int j0 = -1, j1 = -1;
+	if (act)
+	{
+		prefetch_l2(v.flags + s);
+		if (mov_i)
+		{
+			prefetch_l2(v.vprev + s);
+			if (walls_on)
+				prefetch_l2(&v.prm[s].w);
+			if (nspr > 0)
+			{
+				prefetch_l2(v.ec + s);
+				j0 = v.springs[(int64_t)s * v.scap];
+				if (nspr > 1)
+					j1 = v.springs[(int64_t)s * v.scap + 1];
+			}
+		}
+	}
+	double vx = 0.0, vy = 0.0, vz = 0.0, pressure = 0.0;
+	if (vel_on && mov_i)
+	{
+		const double4 v0 = v.vel[s];
+		vx = v0.x;
+		vy = v0.y;
+		vz = v0.z;
+	}
+	// the warp's list of candidates
+	int C = 0;
+#pragma unroll
+	for (int k = 0; k < NR; k++)
+	{
+		w.rows[k][lane] = make_int2(C, lo[k] - C);
+		C += hi[k] - lo[k];
+	}
+	int incl = C;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1)
+	{
+		const int y = __shfl_up_sync(0xffffffffu, incl, o);
+		if (lane >= o)
+			incl += y;
+	}
+	const int total = __shfl_sync(0xffffffffu, incl, 31);
+	w.first[lane] = incl - C;
+	if (lane == 31)
+		w.first[32] = total;
+	w.t[lane] = act ? t : -1;
+	w.margin[lane] = R.fmargin;
+	w.pf[lane] = pf;
+	w.pi[lane] = pi;
+	w.qi[lane] = qi;
+	w.seg[lane] = 0;
+	__syncwarp();
+	if (j0 >= 0)
+	{
+		prefetch_l2(v.pos[cur] + j0);
+		prefetch_l2(v.def + j0);
+		prefetch_l2(v.ec + j0);
+		prefetch_l2(v.aff + (int64_t)j0 * D + def_i);
+	}
+	if (j1 >= 0)
+	{
+		prefetch_l2(v.pos[cur] + j1);
+		prefetch_l2(v.def + j1);
+		prefetch_l2(v.ec + j1);
+		prefetch_l2(v.aff + (int64_t)j1 * D + def_i);
+	}
+
+	nsum fx, fy, fz, fp;
+	int nh = 0; // kept candidates listed (the same in every lane)
+	for (int base = 0; base < total; base += 32 * kQueueRounds)
+	{
+		float4 cand[kQueueRounds];
+		int cu[kQueueRounds], own[kQueueRounds];
+#pragma unroll
+		for (int q = 0; q < kQueueRounds; q++)
+		{
+			const int x = base + q * 32 + lane;
+			own[q] = -1;
+			cu[q] = 0;
+			if (x < total)
+			{
+				// the agent: the last one whose first candidate is at most x
+				// (an agent without candidates shares its successor's first)
+				int i = 0;
+#pragma unroll
+				for (int step = 16; step >= 1; step >>= 1)
+					if (w.first[i + step] <= x)
+						i += step;
+				const int c = x - w.first[i];
+				// the row: the last one whose first candidate is at most c
+				int k = 0;
+#pragma unroll
+				for (int kk = 1; kk < NR; kk++)
+					k += w.rows[kk][i].x <= c;
+				own[q] = i;
+				cu[q] = w.rows[k][i].y + c;
+				cand[q] = v.sposf[cu[q]];
+			}
+		}
+#pragma unroll
+		for (int q = 0; q < kQueueRounds; q++)
+		{
+			bool keep = false;
+			if (own[q] >= 0)
+				keep = cu[q] != w.t[own[q]] && filter_keep<DIMS>(w.pf[own[q]], cand[q], w.margin[own[q]]);
+			const unsigned m = __ballot_sync(0xffffffffu, keep);
+			if (keep)
+				w.hit[nh + __popc(m & ((1u << lane) - 1))] = make_int2(own[q], cu[q]);
+			nh += __popc(m);
+		}
+		__syncwarp();
+		if (nh > kQueueHits - 32 * kQueueRounds)
+		{
+			queue_hits<DIMS, F32>(v, w, nh, act, mov_i, vx, vy, vz, pressure, fx, fy, fz, fp);
+			nh = 0;
+		}
+	}
+	if (nh > 0)
+		queue_hits<DIMS, F32>(v, w, nh, act, mov_i, vx, vy, vz, pressure, fx, fy, fz, fp);
+	if (!act)
+		return;
+	if (F32)
+	{
+		vx = vx + fx.value();
+		vy = vy + fy.value();
+		vz = vz + fz.value();
+		pressure = fp.value();
+	}
+	agent_finish<DIMS>(v, cur, opts, s, r, R, pi, qi.x, def_i, mov_i, nspr, vx, vy, vz, pressure);
+}
+
+template <int DIMS, bool F32>
+__global__ void __launch_bounds__(kQueueThreads) k_fused_queue(view v, int cur, int opts)
+{
+	grid_wait();
+	bump_spring_epochs(v);
+	extern __shared__ __align__(16) unsigned char queue_raw[];
+	queue_smem& sm = *reinterpret_cast<queue_smem*>(queue_raw);
+	fused_queue_agent<DIMS, F32>(v, cur, opts, blockIdx.x * kQueueThreads + threadIdx.x, sm.w[threadIdx.x >> 5]);
 }
 
 // ---------------------------------------------------------------------------
@@ -2880,7 +3361,15 @@ struct persist_args
 	int32_t springs; // the compaction replays removals on the spring rows
 };
 
-template <int DIMS, bool F32, bool STAGED>
+// fused-pass forms of the persistent step
+enum : int
+{
+	PERSIST_FLAT = 0,
+	PERSIST_STAGED = 1,
+	PERSIST_QUEUE = 2
+};
+
+template <int DIMS, bool F32, int FORM>
 __global__ void __launch_bounds__(kPersistThreads) k_step_persistent(view v, int cur, persist_args pa)
 {
 	extern __shared__ __align__(16) unsigned char smem[];
@@ -2895,7 +3384,7 @@ __global__ void __launch_bounds__(kPersistThreads) k_step_persistent(view v, int
 	const int nxt = cur ^ 1;
 
 	// fused pass: positions from pos[cur] to pos[nxt]
-	if (STAGED)
+	if (FORM == PERSIST_STAGED)
 	{
 		const int nvb = (v.total_cap + kPersistThreads - 1) / kPersistThreads;
 		for (int vb = blockIdx.x; vb < nvb; vb += nb)
@@ -2904,6 +3393,10 @@ __global__ void __launch_bounds__(kPersistThreads) k_step_persistent(view v, int
 			__syncthreads(); // the block's shared rows are rewritten by the next tile
 		}
 	}
+	else if (FORM == PERSIST_QUEUE)
+		for (int t0 = blockIdx.x * kPersistThreads; t0 < v.total_cap; t0 += nb * kPersistThreads)
+			fused_queue_agent<DIMS, F32>(v, cur, pa.opts, t0 + threadIdx.x,
+										 reinterpret_cast<queue_smem*>(smem)->w[threadIdx.x >> 5]);
 	else
 		for (int t0 = blockIdx.x * kPersistThreads; t0 < v.total_cap; t0 += nb * kPersistThreads)
 			fused_flat_agent<DIMS, F32>(v, cur, pa.opts, t0 + threadIdx.x, *reinterpret_cast<flat_smem*>(smem));
@@ -2919,29 +3412,15 @@ __global__ void __launch_bounds__(kPersistThreads) k_step_persistent(view v, int
 	if (!grid_barrier(v, pa.bar, pa.limit))
 		return;
 
-	// mesh rebuild: count, scan, scatter, fixup
+	// mesh rebuild: count, then the tiles
 	if (blockIdx.x == 0 && threadIdx.x == 0)
 		*v.bin_active = 1;
 	for (int t0 = blockIdx.x * kPersistThreads; t0 < v.total_cap; t0 += nb * kPersistThreads)
-		bin_count_body(v, nxt, t0 + threadIdx.x, threadIdx.x & 31);
+		bin_count_body(v, nxt, t0 + threadIdx.x);
 	if (!grid_barrier(v, pa.bar, pa.limit))
 		return;
 	for (int b = blockIdx.x; b < v.ntiles; b += nb)
-		bin_scan_tile<kPersistThreads>(v, b);
-	if (!grid_barrier(v, pa.bar, pa.limit))
-		return;
-	if (blockIdx.x == 0)
-	{
-		if (threadIdx.x == 0)
-			*v.pos_changed = 0;
-		bin_scatter_resets(v);
-	}
-	for (int t0 = blockIdx.x * kPersistThreads; t0 < v.total_cap; t0 += nb * kPersistThreads)
-		bin_scatter_agent(v, t0 + threadIdx.x);
-	if (!grid_barrier(v, pa.bar, pa.limit))
-		return;
-	for (int t0 = blockIdx.x * kPersistThreads; t0 < v.total_cap; t0 += nb * kPersistThreads)
-		bin_fixup_agent(v, nxt, t0 + threadIdx.x);
+		bin_place_tile<kPersistThreads>(v, nxt, b, *reinterpret_cast<place_smem*>(smem));
 }
 
 } // namespace
@@ -2979,9 +3458,7 @@ int launch_bin(ppc_state* s, bool conditional)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
 	pdl(k_bin_count, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur, conditional ? 1 : 0);
-	pdl(k_bin_scan, s->v.ntiles, kThreads, 0, PPC_LAUNCH(s), s->v);
-	pdl(k_bin_scatter, b, kThreads, 0, PPC_LAUNCH(s), s->v);
-	pdl(k_bin_fixup, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
+	pdl(k_bin_place, s->v.ntiles, kPlaceThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -3149,10 +3626,30 @@ static int flat_dispatch(ppc_state* s)
 	return PPC_OK;
 }
 
-template <int DIMS, bool F32, bool STAGED>
+template <int DIMS>
+static int queue_dispatch(ppc_state* s)
+{
+	const int opts = fused_opts(s);
+	const int b = blocks_for(s->total_cap, kQueueThreads);
+	cudaStream_t st = PPC_LAUNCH(s);
+	const int dyn = (int)sizeof(queue_smem);
+	if (s->precision == PPC_FP32_FORCE)
+	{
+		PPC_CUDA(cudaFuncSetAttribute(k_fused_queue<DIMS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+		pdl(k_fused_queue<DIMS, true>, b, kQueueThreads, dyn, st, s->v, s->cur, opts);
+	}
+	else
+	{
+		PPC_CUDA(cudaFuncSetAttribute(k_fused_queue<DIMS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+		pdl(k_fused_queue<DIMS, false>, b, kQueueThreads, dyn, st, s->v, s->cur, opts);
+	}
+	return PPC_OK;
+}
+
+template <int DIMS, bool F32, int FORM>
 static int persistent_launch(ppc_state* s, size_t dyn, const persist_args& pa)
 {
-	auto k = k_step_persistent<DIMS, F32, STAGED>;
+	auto k = k_step_persistent<DIMS, F32, FORM>;
 	PPC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
 	int per_sm = 0;
 	PPC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kPersistThreads, dyn));
@@ -3186,7 +3683,7 @@ int launch_step_persistent(ppc_state* s)
 	pa.opts = fused_opts(s);
 	pa.springs = s->has_springs ? 1 : 0;
 	const bool staged = !s->flat && (s->staged || s->coop);
-	size_t dyn = sizeof(flat_smem);
+	size_t dyn = s->queue ? sizeof(queue_smem) : sizeof(flat_smem);
 	if (staged)
 	{
 		pa.cap = s->staged ? std::max(0, (s->tile_smem - kList * kPersistThreads * (int)sizeof(int32_t))
@@ -3195,15 +3692,26 @@ int launch_step_persistent(ppc_state* s)
 		dyn = (size_t)pa.cap * sizeof(float4) + (size_t)kList * kPersistThreads * sizeof(int32_t);
 	}
 	dyn = std::max(dyn, (size_t)kSortCap * sizeof(int32_t)); // the compaction plan's sort buffer
+	dyn = std::max(dyn, sizeof(place_smem));				  // the rebuild's tiles
 	PPC_CUDA(cudaMemsetAsync(s->v.barrier, 0, sizeof(unsigned), s->stream));
 	const bool f32 = s->precision == PPC_FP32_FORCE;
 	s->launches++;
 	int rc;
+#define PPC_PERSIST_FORM(D, FORM)                                                                                      \
+	rc = f32 ? persistent_launch<D, true, FORM>(s, dyn, pa) : persistent_launch<D, false, FORM>(s, dyn, pa);
 #define PPC_PERSIST(D)                                                                                                 \
 	if (staged)                                                                                                        \
-		rc = f32 ? persistent_launch<D, true, true>(s, dyn, pa) : persistent_launch<D, false, true>(s, dyn, pa);       \
+	{                                                                                                                  \
+		PPC_PERSIST_FORM(D, PERSIST_STAGED)                                                                            \
+	}                                                                                                                  \
+	else if (s->queue)                                                                                                 \
+	{                                                                                                                  \
+		PPC_PERSIST_FORM(D, PERSIST_QUEUE)                                                                             \
+	}                                                                                                                  \
 	else                                                                                                               \
-		rc = f32 ? persistent_launch<D, true, false>(s, dyn, pa) : persistent_launch<D, false, false>(s, dyn, pa);
+	{                                                                                                                  \
+		PPC_PERSIST_FORM(D, PERSIST_FLAT)                                                                              \
+	}
 	if (s->dims == 1)
 	{
 		PPC_PERSIST(1)
@@ -3217,6 +3725,7 @@ int launch_step_persistent(ppc_state* s)
 		PPC_PERSIST(3)
 	}
 #undef PPC_PERSIST
+#undef PPC_PERSIST_FORM
 	if (rc != PPC_OK)
 		return rc;
 	s->cur ^= 1;
@@ -3243,7 +3752,13 @@ int launch_fused(ppc_state* s)
 		ev_end = s->prof_events[s->prof_used + 1];
 		s->prof_used += 2;
 	}
-	if (s->flat)
+	if (s->queue)
+	{
+		int rc = s->dims == 1 ? queue_dispatch<1>(s) : (s->dims == 2 ? queue_dispatch<2>(s) : queue_dispatch<3>(s));
+		if (rc != PPC_OK)
+			return rc;
+	}
+	else if (s->flat)
 	{
 		int rc = s->dims == 1 ? flat_dispatch<1>(s) : (s->dims == 2 ? flat_dispatch<2>(s) : flat_dispatch<3>(s));
 		if (rc != PPC_OK)

@@ -221,7 +221,7 @@ class Simulation:
     def autotune(self, steps=10):
         """Times each candidate launch shape over `steps` steps (after as many
         warm-up steps) and keeps the fastest; returns (tile_edge, threads).
-        The simulation advances by 10 x steps steps."""
+        The simulation advances by 12 x steps steps (six candidate shapes)."""
         e, t = C.c_int32(), C.c_int32()
         _check(lib().ppc_autotune(self.h, steps, C.byref(e), C.byref(t)), "ppc_autotune")
         return e.value, t.value

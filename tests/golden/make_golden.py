@@ -18,7 +18,8 @@ numbers in the fixture have a scripted provenance:
   dead flag), the number of interaction calls and the asserted flags and
   damage.
 
-Usage: python tests/golden/make_golden.py [path/to/reference]
+Usage: python tests/golden/make_golden.py path/to/reference
+(or with the path in the environment variable PPC_REFERENCE_ROOT)
 """
 import json
 import os
@@ -114,4 +115,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PPC_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py path/to/reference (or set PPC_REFERENCE_ROOT)")
+    main(root)

@@ -117,12 +117,13 @@ def test_fused_steps_match_oracle(case):
 
 
 # launch shapes of the fused pass: (tile edge, threads, shared-memory bytes).
-# -1 is one thread per agent with its own pair code (the default); -2
-# spreads the pair code over the warp; 0 does that with each block's
-# candidate ranges staged in shared memory, and a budget of 4 KiB leaves no
-# room for them, so blocks read the global arrays instead.
+# -1 is one thread per agent with its own pair code; -2 spreads the pair
+# code over the warp; 0 does that with each block's candidate ranges staged
+# in shared memory, and a budget of 4 KiB leaves no room for them, so blocks
+# read the global arrays instead; -3 (the default) fetches each thread's
+# candidates in batches; -4 shares the warp's candidates out over its lanes.
 SHAPES = [(-1, 128, 0), (-1, 256, 0), (-2, 128, 0), (-2, 64, 0), (0, 128, 32 * 1024), (0, 128, 40 * 1024),
-          (0, 64, 4 * 1024), (0, 96, 24 * 1024), (-3, 128, 0)]
+          (0, 64, 4 * 1024), (0, 96, 24 * 1024), (-3, 128, 0), (-4, 128, 0)]
 
 
 @pytest.mark.parametrize("shape", SHAPES, ids=lambda s: "edge%d_t%d_smem%d" % s)
@@ -142,7 +143,7 @@ def test_launch_shapes_match_oracle(case, shape):
 
 
 def test_autotune_keeps_the_trajectory():
-    """The autotuner runs 10 x steps real steps over its candidate shapes and
+    """The autotuner runs 12 x steps real steps over its candidate shapes and
     keeps one of them; the state then equals the oracle's after as many
     steps, and stepping on with the chosen shape stays equal."""
     mesh, params, a = _cases()["config3_springs"]()
@@ -151,8 +152,8 @@ def test_autotune_keeps_the_trajectory():
     o.update_cell_neighbors()
     d.update_mechanics_mesh()
     edge, threads = d.autotune(steps=3)
-    assert (edge, threads) in {(-3, 128), (-1, 128), (-2, 128), (0, 128), (0, 64)}
-    o.step(30, 0, 0.0, 0.0)
+    assert (edge, threads) in {(-3, 128), (-4, 128), (-1, 128), (-2, 128), (0, 128), (0, 64)}
+    o.step(36, 0, 0.0, 0.0)
     gu.assert_same_state(gu.fetch(d, a), gu.fetch(o, a))
     o.step(7, 0, 0.0, 0.0)
     d.step(7)
@@ -307,7 +308,7 @@ def test_stochastic_springs_match_oracle(phenotype):
 
 
 @pytest.mark.parametrize("shape", [(-1, 128, 0), (-2, 128, 0), (0, 128, 32 * 1024), (0, 64, 16 * 1024),
-                                   (-3, 128, 0)],
+                                   (-3, 128, 0), (-4, 128, 0)],
                          ids=lambda s: "edge%d_t%d" % s[:2])
 def test_batch_replicates_match_independent_oracles(shape):
     """Ensemble form: each replicate of one batched state evolves exactly
@@ -337,7 +338,7 @@ def test_batch_replicates_match_independent_oracles(shape):
         gu.assert_same_state(out, gu.fetch(o, s))
 
 
-@pytest.mark.parametrize("shape", [(-1, 128, 0), (-2, 128, 0), (0, 128, 32 * 1024), (-3, 128, 0)],
+@pytest.mark.parametrize("shape", [(-1, 128, 0), (-2, 128, 0), (0, 128, 32 * 1024), (-3, 128, 0), (-4, 128, 0)],
                          ids=lambda s: "edge%d" % s[0])
 def test_empty_and_tiny_simulations(shape):
     """No agents, one agent, and every agent removed: the step, the mesh and
@@ -371,7 +372,7 @@ def test_empty_and_tiny_simulations(shape):
     assert d.count() == gu.fetch(o, gone).count == 0
 
 
-@pytest.mark.parametrize("shape", [(-1, 128, 0), (-2, 128, 0), (0, 128, 32 * 1024), (-3, 128, 0)],
+@pytest.mark.parametrize("shape", [(-1, 128, 0), (-2, 128, 0), (0, 128, 32 * 1024), (-3, 128, 0), (-4, 128, 0)],
                          ids=lambda s: "edge%d" % s[0])
 def test_batch_with_an_empty_replicate(shape):
     """A batched state whose middle replicate has no agents steps the others
@@ -431,7 +432,7 @@ def test_errors_are_reported():
     from paraphysicell_b200.abi import PPC_ERR_ARG
     mesh, params, a = wl.scaled(wl.config2, 300, seed=74)
     _, d = gu.make_pair(mesh, params, a)
-    for shape in ((3, 128, 0), (-4, 128, 0), (-8, 128, 0), (0, 100, 0), (0, 512, 0), (0, 128, 200 * 1024)):
+    for shape in ((3, 128, 0), (-5, 128, 0), (-8, 128, 0), (0, 100, 0), (0, 512, 0), (0, 128, 200 * 1024)):
         with pytest.raises(PPCError) as e:
             d.set_launch_shape(*shape)
         assert e.value.rc == PPC_ERR_ARG

@@ -17,7 +17,7 @@ from tests import gpu_util as gu
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(-3, 128, 0), (-2, 128, 0), (0, 128, 32 * 1024)]
+SHAPES = [(-3, 128, 0), (-4, 128, 0), (-2, 128, 0), (0, 128, 32 * 1024)]
 
 
 def _fetch(d, s, r):
