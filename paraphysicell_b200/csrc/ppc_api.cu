@@ -336,7 +336,7 @@ int transfer_in(ppc_state* s, int32_t r, const ppc_agents* a, bool defaults)
 	// an upload of kinematic fields only (positions, velocities, previous
 	// velocities, pressure, orientation) keeps the mesh when the positions it
 	// brings are bit-identical to the resident ones
-	// (pos_changed is zero after every rebuild: k_bin_scatter clears it)
+	// (pos_changed is zero after every rebuild: its last tile clears it)
 	const bool kinematic = !defaults && only_kinematic(a);
 	PPC_TRY(put_vec(s, v.pos[s->cur], a->positions, r, n, defaults, kinematic ? v.pos_changed : nullptr));
 	PPC_TRY(put_vec(s, v.vel, a->velocities, r, n, defaults));
@@ -900,6 +900,9 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.cnext, C));
 	try_(alloc(s, v.porder, C));
 	try_(alloc(s, v.tdone, 1));
+	try_(alloc(s, v.tfresh, C));
+	try_(alloc(s, v.params_changed, 1));
+	try_(alloc(s, v.copy_full, 1));
 	if (rc == PPC_OK && cudaMemset(v.chead, 0xff, sizeof(int32_t) * (size_t)v.ntiles * 32) != cudaSuccess)
 		rc = fail(PPC_ERR_CUDA, "cudaMemset failed");
 	try_(alloc(s, v.order_valid, 1));
@@ -1012,6 +1015,7 @@ int ppc_set_precision(ppc_state* s, int32_t precision)
 	s->precision = precision;
 	s->v.f32 = precision == PPC_FP32_FORCE ? 1 : 0;
 	invalidate_bins(s); // the single-precision copies are written by the binning
+	PPC_TRY(mark_fields_changed(s));
 	release_graph(s);
 	return PPC_OK;
 }

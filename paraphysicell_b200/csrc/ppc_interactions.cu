@@ -289,6 +289,8 @@ int launch_interactions(ppc_state* s, const ix_fields& x)
 {
 	if (x.n == 0)
 		return PPC_OK;
+	if (int rc = mark_fields_changed(s)) // ingestion and fusion change volumes and radii
+		return rc;
 	const int b = blocks_for(x.n, kIxThreads);
 	k_ix_candidates<<<b, kIxThreads, 0, PPC_LAUNCH(s)>>>(s->v, x);
 	if (s->dims == 1)

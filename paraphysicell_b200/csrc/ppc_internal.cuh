@@ -147,6 +147,9 @@ struct view
 	int32_t* cnext;		// [C] next slot of a mover chain
 	int2* porder;		// [C] entries of the previous order: (slot, key) of agents kept in their tile
 	unsigned* tdone;	// tiles placed by the current rebuild
+	uint8_t* tfresh;	// [C] 1 where the agent at a position of the key order is new to it
+	int32_t* params_changed; // fields other than positions, or slots' agents, changed since the last rebuild
+	int32_t* copy_full;	// the current rebuild's k_bin_copy copies every field of every agent
 	int32_t* order_valid; // 1 once a rebuild has set `sorted` (cleared by uploads)
 	int32_t* binned;	  // [replicates] live count at the last rebuild (the slots `sorted` lists)
 	int32_t* move_src;	  // [C] tail slot whose agent the next k_bin_count moves into this hole, or -1
@@ -365,6 +368,7 @@ struct ix_fields
 	int32_t* dep;	 // [n] agents whose interactions depend on an earlier agent's
 };
 int launch_interactions(ppc_state* s, const ix_fields& x);
+int mark_fields_changed(ppc_state* s);
 
 // device copies of the ppc_motility fields of one replicate (local rows)
 struct mot_fields

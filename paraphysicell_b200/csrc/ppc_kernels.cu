@@ -201,19 +201,21 @@ __device__ __forceinline__ void move_agent(const view& v, int cur, int d, int s)
 // previous order (porder), every other one, and every slot appended since
 // (all slots when there is no previous order), is pushed onto one of the 32
 // mover chains of its new tile, and the tile counts change by the difference
-// (tdelta, and per 1024 tiles sdelta). k_bin_place then builds each tile by
+// (tdelta, and per 1024 tiles sdelta). k_bin_order then orders each tile by
 // itself: its start is its previous start plus the changes of the tiles
 // before it; its agents are its kept entries and its chains; their per-voxel
 // counts, the voxel starts and the order inside a voxel (descending slot,
 // the order a serial run of the reference's fetch_sub scatter gives) are
-// formed in shared memory, and each agent writes its key-ordered copies.
-// Agents rarely leave their tile between steps, so the chains are short.
+// formed in shared memory. k_bin_copy, a thread per position of the new
+// order, writes the key-ordered copies of the agents' fields. Agents rarely
+// leave their tile between steps, so the chains are short.
 
 constexpr int kChains = 32;		 // mover chains per tile
 constexpr int kSuperShift = 10;	 // tiles per entry of sdelta: 1024
 constexpr int kPlaceThreads = 256;
 constexpr int kPlaceList = 1024; // agents of a tile listed in shared memory; the rest in global scratch
 constexpr int kMaxTileShift = 12;
+constexpr int kOrderBatch = 4;  // previous-order entries a thread of k_bin_order loads at once
 
 // the voxel key of slot s of replicate r at positions pos[cur]
 __device__ __forceinline__ int32_t voxel_key(const view& v, int cur, int s, int r)
@@ -234,6 +236,7 @@ __device__ __forceinline__ void apply_move(const view& v, int cur, int s)
 	{
 		move_agent(v, cur, s, src);
 		v.move_src[s] = -1;
+		*v.params_changed = 1; // the slot's agent changed: its key-ordered copies are rewritten
 	}
 }
 
@@ -313,7 +316,7 @@ __device__ __forceinline__ void bin_count_body(const view& v, int cur, int t)
 
 // A conditional rebuild (after an upload of positions) runs only if the
 // upload changed some position; its decision goes to bin_active for
-// k_bin_place.
+// k_bin_order and k_bin_copy.
 __global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur, int conditional)
 {
 	grid_wait();
@@ -376,29 +379,28 @@ __device__ __forceinline__ void place_agent(const view& v, int cur, int s, int t
 	}
 }
 
-struct place_smem
+struct __align__(16) place_smem
 {
-	int32_t cnt[(1 << kMaxTileShift) + 1]; // per-voxel counts, then starts, then ends
-	int2 list[kPlaceList];				   // the tile's agents: (slot, voxel inside the tile)
-	int32_t group[kPlaceList];			   // slots grouped by voxel
+	int32_t cnt[1 << kMaxTileShift]; // per-voxel counts, then starts, then ends
+	int2 list[kPlaceList];			 // the tile's agents: (slot, voxel inside the tile | previous index << 12)
+	int32_t group[kPlaceList];		 // slots grouped by voxel
+	int32_t wtot[32];				 // per-warp totals of the voxel scan
 	int32_t n, last;
 };
 
-// lists slot s of local voxel lv (nv voxels in the tile); items past the
-// shared list go to the global scratch at the tile's start
-__device__ __forceinline__ void place_add(const view& v, place_smem& sm, int base, int s, int lv, int nv)
+constexpr int kVoxelBits = 12;				   // bits of a list item's voxel inside the tile
+constexpr int kPrevLimit = 1 << (31 - kVoxelBits); // previous indices that fit above them
+
+// lists slot s (its list word y: voxel inside the tile | previous index + 1
+// above kVoxelBits) at index i; items past the shared list go to the global
+// scratch at the tile's start
+__device__ __forceinline__ void place_store(const view& v, place_smem& sm, int base, int i, int s, int y)
 {
-	if ((unsigned)lv >= (unsigned)nv)
-	{
-		atomicOr(v.err, ERR_LIST_CAPACITY); // a key outside the tile: the order or a chain is broken
-		return;
-	}
-	const int i = atomicAdd(&sm.n, 1);
-	atomicAdd(&sm.cnt[lv], 1);
+	atomicAdd(&sm.cnt[y & ((1 << kVoxelBits) - 1)], 1);
 	if (i < kPlaceList)
-		sm.list[i] = make_int2(s, lv);
+		sm.list[i] = make_int2(s, y);
 	else if ((int64_t)base + i < v.total_cap)
-		v.vsc[base + i] = make_int2(s, lv);
+		v.vsc[base + i] = make_int2(s, y);
 }
 
 __device__ __forceinline__ int2 place_item(const view& v, const place_smem& sm, int base, int i)
@@ -406,13 +408,76 @@ __device__ __forceinline__ int2 place_item(const view& v, const place_smem& sm, 
 	return i < kPlaceList ? sm.list[i] : v.vsc[base + i];
 }
 
-// Builds tile b of the new order (see above): the voxel starts in vstart,
-// the agents' key-ordered copies, the tile's entry of tprev. The tile whose
-// placing completes last readies the counters for the next rebuild.
+// exclusive scan of cnt[0, 4 ceil(nv / 4)) in place: each warp scans a
+// contiguous chunk of 16-byte groups in rows of 32 groups (no bank
+// conflicts), then the warps' totals are added
 template <int THREADS>
-__device__ __forceinline__ void bin_place_tile(const view& v, int cur, int b, place_smem& sm)
+__device__ __forceinline__ void place_scan(place_smem& sm, int nv)
 {
-	const int tid = threadIdx.x;
+	constexpr int NW = THREADS / 32;
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	int4* c4 = reinterpret_cast<int4*>(sm.cnt);
+	const int nq = (nv + 3) >> 2;
+	const int chunk = ((nq + NW - 1) / NW + 31) & ~31;
+	const int q0 = min(w * chunk, nq), q1 = min(q0 + chunk, nq);
+	int carry = 0;
+	for (int q = q0; q < q1; q += 32)
+	{
+		const int qq = q + lane;
+		const int4 c = qq < q1 ? c4[qq] : make_int4(0, 0, 0, 0);
+		const int sum = c.x + c.y + c.z + c.w;
+		int incl = sum;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1)
+		{
+			const int y = __shfl_up_sync(0xffffffffu, incl, o);
+			if (lane >= o)
+				incl += y;
+		}
+		if (qq < q1)
+		{
+			int run = carry + incl - sum;
+			int4 out;
+			out.x = run;
+			run += c.x;
+			out.y = run;
+			run += c.y;
+			out.z = run;
+			run += c.z;
+			out.w = run;
+			c4[qq] = out;
+		}
+		carry += __shfl_sync(0xffffffffu, incl, 31);
+	}
+	if (lane == 0)
+		sm.wtot[w] = carry;
+	__syncthreads();
+	int off = 0;
+#pragma unroll
+	for (int k = 0; k < NW; k++)
+		off += k < w ? sm.wtot[k] : 0;
+	if (off)
+		for (int qq = q0 + lane; qq < q1; qq += 32)
+		{
+			int4 c = c4[qq];
+			c.x += off;
+			c.y += off;
+			c.z += off;
+			c.w += off;
+			c4[qq] = c;
+		}
+	__syncthreads();
+}
+
+// Orders tile b of the new order (see above): the voxel starts in vstart,
+// sorted, skey and tfresh (1 where a position's agent is new to it) over the
+// tile's range, its entry of tprev. The tile whose ordering completes last
+// readies the counters for the next rebuild; the key-ordered copies of the
+// agents' fields follow in k_bin_copy.
+template <int THREADS>
+__device__ __forceinline__ void bin_order_tile(const view& v, int b, place_smem& sm)
+{
+	const int tid = threadIdx.x, lane = tid & 31;
 	const int sh = v.tshift;
 	const int k0 = b << sh;
 	const int nv = min(1 << sh, v.nvox - k0);
@@ -426,8 +491,12 @@ __device__ __forceinline__ void bin_place_tile(const view& v, int cur, int b, pl
 		part += v.tdelta[k];
 	const int2 tp = ordered ? v.tprev[b] : make_int2(0, 0);
 	const int L = tp.y + v.tdelta[b];
-	for (int i = tid; i <= nv; i += THREADS)
-		sm.cnt[i] = 0;
+	if (L > 0)
+	{
+		int4* c4 = reinterpret_cast<int4*>(sm.cnt);
+		for (int q = tid; q < (nv + 3) >> 2; q += THREADS)
+			c4[q] = make_int4(0, 0, 0, 0);
+	}
 	if (tid == 0)
 		sm.n = 0;
 	int moved;
@@ -435,27 +504,56 @@ __device__ __forceinline__ void bin_place_tile(const view& v, int cur, int b, pl
 	const int base = tp.x + moved;
 	const bool fits = base >= 0 && L >= 0 && (int64_t)base + L <= v.total_cap;
 
-	// the kept entries of the previous order, then the chains
-	if (fits)
-		for (int i = tid; i < tp.y; i += THREADS)
+	// the kept entries of the previous order, kOrderBatch per thread loaded
+	// together (one list slot reservation per warp and entry), then the chains
+	if (fits && L > 0)
+		for (int c0 = tid - lane; c0 < tp.y; c0 += kOrderBatch * THREADS)
 		{
-			const int2 e = v.porder[tp.x + i];
-			if (e.x >= 0)
-				place_add(v, sm, base, e.x, e.y - k0, nv);
+			int2 e[kOrderBatch];
+#pragma unroll
+			for (int k = 0; k < kOrderBatch; k++)
+			{
+				const int i = c0 + k * THREADS + lane;
+				e[k] = i < tp.y ? v.porder[tp.x + i] : make_int2(-1, 0);
+			}
+#pragma unroll
+			for (int k = 0; k < kOrderBatch; k++)
+			{
+				const int i = c0 + k * THREADS + lane;
+				const int lv = e[k].y - k0;
+				bool keep = e[k].x >= 0;
+				if (keep && (unsigned)lv >= (unsigned)nv)
+				{
+					atomicOr(v.err, ERR_LIST_CAPACITY); // a key outside the tile: the order is broken
+					keep = false;
+				}
+				const unsigned m = __ballot_sync(0xffffffffu, keep);
+				int at = 0;
+				if (lane == 0 && m)
+					at = atomicAdd(&sm.n, __popc(m));
+				at = __shfl_sync(0xffffffffu, at, 0);
+				if (keep)
+					place_store(v, sm, base, at + __popc(m & ((1u << lane) - 1)), e[k].x,
+								lv | (i + 1 < kPrevLimit ? (i + 1) << kVoxelBits : 0));
+			}
 		}
 	if (tid < kChains)
 	{
 		int* head = v.chead + (int64_t)b * kChains + tid;
 		int q = *head;
 		*head = -1;
-		for (int hops = 0; q >= 0 && fits; hops++)
+		for (int hops = 0; q >= 0; hops++)
 		{
-			if (hops >= v.total_cap || q >= v.total_cap)
+			if (!fits || L <= 0 || hops >= v.total_cap || q >= v.total_cap)
 			{
-				atomicOr(v.err, ERR_LIST_CAPACITY);
+				atomicOr(v.err, ERR_LIST_CAPACITY); // movers into a tile that expects none, or a broken chain
 				break;
 			}
-			place_add(v, sm, base, q, v.key[q] - k0, nv);
+			const int lv = v.key[q] - k0;
+			if ((unsigned)lv < (unsigned)nv)
+				place_store(v, sm, base, atomicAdd(&sm.n, 1), q, lv);
+			else
+				atomicOr(v.err, ERR_LIST_CAPACITY);
 			q = v.cnext[q];
 		}
 	}
@@ -467,54 +565,67 @@ __device__ __forceinline__ void bin_place_tile(const view& v, int cur, int b, pl
 
 	if (ok)
 	{
-		// per-voxel starts: exclusive scan of the counts, in place (all zero
-		// in an empty tile)
+		// per-voxel starts; an empty tile's are all its start, and a tile that
+		// was and stays empty at the same start keeps them
 		if (n > 0)
 		{
-			const int per = (nv + THREADS - 1) / THREADS;
-			const int j0 = min(tid * per, nv), j1 = min(j0 + per, nv);
-			int sum = 0;
-			for (int j = j0; j < j1; j++)
-				sum += sm.cnt[j];
-			int total;
-			int run = block_exclusive_scan(sum, total);
-			for (int j = j0; j < j1; j++)
+			place_scan<THREADS>(sm, nv);
+			int4* vs4 = reinterpret_cast<int4*>(v.vstart + k0); // k0 is a multiple of 64
+			const int4* c4 = reinterpret_cast<const int4*>(sm.cnt);
+			for (int q = tid; q < nv >> 2; q += THREADS)
 			{
-				const int c = sm.cnt[j];
-				sm.cnt[j] = run;
-				run += c;
+				int4 c = c4[q];
+				c.x += base;
+				c.y += base;
+				c.z += base;
+				c.w += base;
+				vs4[q] = c;
 			}
-			__syncthreads();
-		}
-		// a tile that was and stays empty at the same start keeps its starts
-		if (!(ordered && tp.y == 0 && n == 0 && base == tp.x))
-			for (int j = tid; j < nv; j += THREADS)
+			for (int j = (nv & ~3) + tid; j < nv; j += THREADS)
 				v.vstart[k0 + j] = base + sm.cnt[j];
+		}
+		else if (!(ordered && tp.y == 0 && base == tp.x))
+		{
+			int4* vs4 = reinterpret_cast<int4*>(v.vstart + k0);
+			for (int q = tid; q < nv >> 2; q += THREADS)
+				vs4[q] = make_int4(base, base, base, base);
+			for (int j = (nv & ~3) + tid; j < nv; j += THREADS)
+				v.vstart[k0 + j] = base;
+		}
 		if (k0 + nv == v.nvox && tid == 0)
 		{
 			v.vstart[v.nvox] = base + n;
 			*v.cursor = base + n;
 		}
-		__syncthreads(); // the starts are read above before the grouping moves them
-		// slots grouped by voxel; afterwards cnt[j] is the end of voxel j
-		for (int i = tid; i < n; i += THREADS)
+		if (n > 0)
 		{
-			const int2 it = place_item(v, sm, base, i);
-			const int p = atomicAdd(&sm.cnt[it.y], 1);
-			if (p < kPlaceList)
-				sm.group[p] = it.x;
-			else
-				v.tmp[base + p] = it.x;
-		}
-		__syncthreads();
-		for (int i = tid; i < n; i += THREADS)
-		{
-			const int2 it = place_item(v, sm, base, i);
-			const int lo = it.y ? sm.cnt[it.y - 1] : 0, hi = sm.cnt[it.y];
-			int rank = 0;
-			for (int u = lo; u < hi; u++)
-				rank += (u < kPlaceList ? sm.group[u] : v.tmp[base + u]) > it.x;
-			place_agent(v, cur, it.x, base + lo + rank, k0 + it.y);
+			__syncthreads(); // the starts are read above before the grouping moves them
+			// slots grouped by voxel; afterwards cnt[j] is the end of voxel j
+			for (int i = tid; i < n; i += THREADS)
+			{
+				const int2 it = place_item(v, sm, base, i);
+				const int p = atomicAdd(&sm.cnt[it.y & ((1 << kVoxelBits) - 1)], 1);
+				if (p < kPlaceList)
+					sm.group[p] = it.x;
+				else
+					v.tmp[base + p] = it.x;
+			}
+			__syncthreads();
+			// the final place: descending slot inside the voxel
+			for (int i = tid; i < n; i += THREADS)
+			{
+				const int2 it = place_item(v, sm, base, i);
+				const int lv = it.y & ((1 << kVoxelBits) - 1);
+				const int pidx = it.y >> kVoxelBits;
+				const int lo = lv ? sm.cnt[lv - 1] : 0, hi = sm.cnt[lv];
+				int rank = 0;
+				for (int u = lo; u < hi; u++)
+					rank += (u < kPlaceList ? sm.group[u] : v.tmp[base + u]) > it.x;
+				const int t = base + lo + rank;
+				v.sorted[t] = it.x;
+				v.skey[t] = k0 + lv;
+				v.tfresh[t] = (pidx == 0 || tp.x + pidx - 1 != t) ? 1 : 0;
+			}
 		}
 		if (tid == 0)
 			v.tprev[b] = make_int2(base, n);
@@ -540,6 +651,10 @@ __device__ __forceinline__ void bin_place_tile(const view& v, int cur, int b, pl
 			v.binned[k] = v.ctr[k].count; // the slots this rebuild's order lists
 		if (tid == 0)
 		{
+			// k_bin_copy writes every field where agents' fields or slots
+			// changed since the last rebuild, elsewhere only the positions
+			*v.copy_full = (*v.params_changed != 0 || !ordered) ? 1 : 0;
+			*v.params_changed = 0;
 			*v.tdone = 0;
 			*v.order_valid = 1;
 			*v.moves_pending = 0; // applied by this rebuild's count
@@ -550,13 +665,52 @@ __device__ __forceinline__ void bin_place_tile(const view& v, int cur, int b, pl
 	__syncthreads(); // shared memory is reused by the next tile of a persistent block
 }
 
-__global__ void __launch_bounds__(kPlaceThreads) k_bin_place(view v, int cur)
+__global__ void __launch_bounds__(kPlaceThreads) k_bin_order(view v)
 {
 	__shared__ place_smem sm;
 	grid_wait();
 	if (!*v.bin_active)
 		return;
-	bin_place_tile<kPlaceThreads>(v, cur, blockIdx.x, sm);
+	bin_order_tile<kPlaceThreads>(v, blockIdx.x, sm);
+}
+
+// The key-ordered copies of the agent at position t of the new order. Where
+// the agent is new to its position, or fields changed since the last rebuild
+// (copy_full), every field is copied; elsewhere the fields other than the
+// position are those the position already holds, and only the position is.
+__device__ __forceinline__ void bin_copy_agent(const view& v, int cur, int t)
+{
+	if (t >= *v.cursor)
+		return;
+	const int s = v.sorted[t];
+	if (*v.copy_full || v.tfresh[t])
+	{
+		place_agent(v, cur, s, t, v.skey[t]);
+		return;
+	}
+	if ((unsigned)s >= (unsigned)v.total_cap)
+	{
+		atomicOr(v.err, ERR_LIST_CAPACITY);
+		return;
+	}
+	const double4 p = v.pos[cur][s];
+	const rep_info& R = v.reps[rep_of(v, s)];
+	double* q = reinterpret_cast<double*>(v.spos4 + t);
+	q[0] = p.x;
+	q[1] = p.y;
+	q[2] = p.z;
+	float* f = reinterpret_cast<float*>(v.sposf + t);
+	f[0] = (float)(p.x - R.mins[0]);
+	f[1] = (float)(p.y - R.mins[1]);
+	f[2] = (float)(p.z - R.mins[2]);
+}
+
+__global__ void __launch_bounds__(kThreads) k_bin_copy(view v, int cur)
+{
+	grid_wait();
+	if (!*v.bin_active)
+		return;
+	bin_copy_agent(v, cur, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -2699,7 +2853,10 @@ __global__ void k_compact_apply(view v, int cur)
 	const int base = v.reps[r].base;
 	const int32_t* moves = v.moves + 2 * (int64_t)base;
 	for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nm; k += gridDim.x * blockDim.x)
+	{
 		move_agent(v, cur, base + moves[2 * k], base + moves[2 * k + 1]);
+		*v.params_changed = 1; // the hole's agent changed
+	}
 }
 
 // ---------------------------------------------------------------------------
@@ -3089,6 +3246,7 @@ __global__ void k_divide_apply(view v, int cur)
 		const int p = base + lp;
 		const int c = base + n_pre + k;
 		v.flags[p] = PPC_FLAG_NONE;
+		*v.params_changed = 1; // the parent's radius and volumes change
 
 		// random direction, projected against the orientation by polarity and
 		// scaled by the parent's radius (reference: src/cell.cpp:129-150)
@@ -3420,7 +3578,11 @@ __global__ void __launch_bounds__(kPersistThreads) k_step_persistent(view v, int
 	if (!grid_barrier(v, pa.bar, pa.limit))
 		return;
 	for (int b = blockIdx.x; b < v.ntiles; b += nb)
-		bin_place_tile<kPersistThreads>(v, nxt, b, *reinterpret_cast<place_smem*>(smem));
+		bin_order_tile<kPersistThreads>(v, b, *reinterpret_cast<place_smem*>(smem));
+	if (!grid_barrier(v, pa.bar, pa.limit))
+		return;
+	for (int t0 = blockIdx.x * kPersistThreads; t0 < v.total_cap; t0 += nb * kPersistThreads)
+		bin_copy_agent(v, nxt, t0 + threadIdx.x);
 }
 
 } // namespace
@@ -3458,7 +3620,8 @@ int launch_bin(ppc_state* s, bool conditional)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
 	pdl(k_bin_count, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur, conditional ? 1 : 0);
-	pdl(k_bin_place, s->v.ntiles, kPlaceThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
+	pdl(k_bin_order, s->v.ntiles, kPlaceThreads, 0, PPC_LAUNCH(s), s->v);
+	pdl(k_bin_copy, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
@@ -3516,8 +3679,18 @@ int launch_springs(ppc_state* s)
 	return PPC_OK;
 }
 
+// fields other than positions, or slots' agents, change on the device: the
+// next rebuild's k_bin_copy rewrites every key-ordered field
+int mark_fields_changed(ppc_state* s)
+{
+	PPC_CUDA(cudaMemsetAsync(s->v.params_changed, 1, sizeof(int32_t), s->stream));
+	return PPC_OK;
+}
+
 int launch_spring_updates(ppc_state* s)
 {
+	if (int rc = mark_fields_changed(s)) // spring counts change
+		return rc;
 	const int b = blocks_for(s->total_cap, kThreads);
 	pdl(k_spring_detach, b, kThreads, 0, PPC_LAUNCH(s), s->v);
 	pdl(k_spring_compact_rows, b, kThreads, 0, PPC_LAUNCH(s), s->v);
