@@ -245,7 +245,7 @@ int put_vec(ppc_state* s, double4* dev, const double* host, int32_t r, int32_t n
 	void* st = nullptr;
 	PPC_TRY(stage_take(s, bytes, &st));
 	if (host)
-		PPC_CUDA(cudaMemcpyAsync(st, host, bytes, cudaMemcpyHostToDevice, s->stream));
+		PPC_CUDA(cudaMemcpyAsync(st, host, bytes, cudaMemcpyHostToDevice, s->h2d_stream ? s->h2d_stream : s->stream));
 	else
 		PPC_CUDA(cudaMemsetAsync(st, 0, bytes, s->stream));
 	// the unpack waits until the call's other copies are queued, so the copy
@@ -338,11 +338,39 @@ int transfer_in(ppc_state* s, int32_t r, const ppc_agents* a, bool defaults)
 	// brings are bit-identical to the resident ones
 	// (pos_changed is zero after every rebuild: its last tile clears it)
 	const bool kinematic = !defaults && only_kinematic(a);
-	PPC_TRY(put_vec(s, v.pos[s->cur], a->positions, r, n, defaults, kinematic ? v.pos_changed : nullptr));
-	PPC_TRY(put_vec(s, v.vel, a->velocities, r, n, defaults));
-	PPC_TRY(put_vec(s, v.vprev, a->previous_velocities, r, n, defaults));
-	PPC_TRY(put_vec(s, v.orient, a->orientation, r, n, defaults));
+	s->ready_pending = false;
+	bool pinned = true;
+	for (const void* p : { (const void*)a->positions, (const void*)a->velocities,
+						   (const void*)a->previous_velocities, (const void*)a->simple_pressure,
+						   (const void*)a->orientation })
+		if (p && !mapped(p))
+			pinned = false;
+	// page-locked kinematic rows are copied into the staging arena on the
+	// transfer stream, beside whatever the stream still runs (the last step's
+	// mesh rebuild); the arena is free once the stream has unpacked the
+	// previous upload, and the unpacks wait for the copies
+	const bool beside = kinematic && pinned && !s->zero_copy && s->xfer;
+	if (beside)
+	{
+		PPC_CUDA(cudaStreamWaitEvent(s->xfer, s->ev_stage_free, 0));
+		s->h2d_stream = s->xfer;
+	}
+	int rc = put_vec(s, v.pos[s->cur], a->positions, r, n, defaults, kinematic ? v.pos_changed : nullptr);
+	if (rc == PPC_OK)
+		rc = put_vec(s, v.vel, a->velocities, r, n, defaults);
+	if (rc == PPC_OK)
+		rc = put_vec(s, v.vprev, a->previous_velocities, r, n, defaults);
+	if (rc == PPC_OK)
+		rc = put_vec(s, v.orient, a->orientation, r, n, defaults);
+	s->h2d_stream = nullptr;
+	PPC_TRY(rc);
+	if (beside)
+	{
+		PPC_CUDA(cudaEventRecord(s->ev_h2d, s->xfer));
+		PPC_CUDA(cudaStreamWaitEvent(s->stream, s->ev_h2d, 0));
+	}
 	PPC_TRY(flush_unpacks(s));
+	PPC_CUDA(cudaEventRecord(s->ev_stage_free, s->stream));
 	PPC_TRY(put_prm(s, 0, a->radius, r, n, defaults, kRadius));
 	PPC_TRY(put_prm(s, 1, a->cell_cell_repulsion_strength, r, n, defaults, 10.0));
 	PPC_TRY(put_prm(s, 2, a->cell_cell_adhesion_strength, r, n, defaults, 0.4));
@@ -441,12 +469,6 @@ int transfer_in(ppc_state* s, int32_t r, const ppc_agents* a, bool defaults)
 		// page-locked rows are copied by the queued DMA, so the call returns
 		// at once and the next step queues behind the copies; pageable rows
 		// are waited for, so the caller may reuse them on return
-		bool pinned = true;
-		for (const void* p : { (const void*)a->positions, (const void*)a->velocities,
-							   (const void*)a->previous_velocities, (const void*)a->simple_pressure,
-							   (const void*)a->orientation })
-			if (p && !mapped(p))
-				pinned = false;
 		if (!pinned)
 			PPC_CUDA(cudaStreamSynchronize(s->stream));
 		return PPC_OK;
@@ -493,7 +515,7 @@ int copy_out(ppc_state* s, int32_t r, ppc_agents* a, int32_t n)
 	return PPC_OK;
 }
 
-int transfer_out(ppc_state* s, int32_t r, ppc_agents* a)
+int transfer_out_on(ppc_state* s, int32_t r, ppc_agents* a, cudaStream_t main, bool beside)
 {
 	// Copies as many agents as this host last saw in the replicate, together
 	// with the counters and the device error word, and synchronises once; if
@@ -506,7 +528,15 @@ int transfer_out(ppc_state* s, int32_t r, ppc_agents* a)
 							 s->stream)); // the counters and the error word
 	PPC_TRY(copy_out(s, r, a, guess));
 	PPC_CUDA(cudaStreamSynchronize(s->stream));
-	PPC_TRY(map_errors(s, *s->pinned_err));
+	if (beside && *s->pinned_err)
+	{
+		// the rebuild beside the copies may still set error bits: read the
+		// word after the main stream
+		s->stream = main;
+		PPC_TRY(device_errors(s));
+	}
+	else
+		PPC_TRY(map_errors(s, *s->pinned_err));
 	for (int32_t k = 0; k < s->nreps; k++)
 		s->host_count[k] = s->pinned_ctr[k].count;
 	s->counts_known = true;
@@ -541,6 +571,25 @@ int transfer_out(ppc_state* s, int32_t r, ppc_agents* a)
 	return PPC_OK;
 }
 
+// A download right after a step (no kernel launched since) runs on the
+// transfer stream once the step's agent fields are final (ev_ready), beside
+// the rest of the step's mesh rebuild, which changes none of them; any other
+// download runs on the stream.
+int transfer_out(ppc_state* s, int32_t r, ppc_agents* a)
+{
+	const bool beside = s->ready_pending && s->launches == s->ready_launches && s->xfer;
+	s->ready_pending = false;
+	cudaStream_t main = s->stream;
+	if (beside)
+	{
+		PPC_CUDA(cudaStreamWaitEvent(s->xfer, s->ev_ready, 0));
+		s->stream = s->xfer;
+	}
+	const int rc = transfer_out_on(s, r, a, main, beside);
+	s->stream = main;
+	return rc;
+}
+
 int ensure_bins(ppc_state* s)
 {
 	if (!s->bins_valid)
@@ -568,8 +617,9 @@ int ensure_lists(ppc_state* s)
 	return PPC_OK;
 }
 
-// one fused mechanics step (+ phenotype container update)
-int enqueue_step(ppc_state* s, bool phenotype, double p_divide, double p_death)
+// one fused mechanics step (+ phenotype container update); `last`: the last
+// step of a call, whose agent fields a download may read beside its rebuild
+int enqueue_step(ppc_state* s, bool phenotype, double p_divide, double p_death, bool last)
 {
 	if (s->persistent && !phenotype)
 		return launch_step_persistent(s);
@@ -583,7 +633,7 @@ int enqueue_step(ppc_state* s, bool phenotype, double p_divide, double p_death)
 		PPC_TRY(launch_mark_remove(s));
 		PPC_TRY(launch_compact(s, true, true));
 	}
-	PPC_TRY(launch_bin(s, false));
+	PPC_TRY(launch_bin(s, false, last));
 	return PPC_OK;
 }
 
@@ -591,7 +641,7 @@ int enqueue_step(ppc_state* s, bool phenotype, double p_divide, double p_death)
 // attachment: the spring update needs every agent's neighbour list and its
 // attachments must be settled before the springs pull, so the step runs the
 // reference's sequence (simulator::simulate_mechanics, src/simulator.cpp:173-192)
-int enqueue_step_separate(ppc_state* s, bool phenotype, double p_divide, double p_death)
+int enqueue_step_separate(ppc_state* s, bool phenotype, double p_divide, double p_death, bool last)
 {
 	PPC_TRY(launch_neighbors(s));
 	PPC_TRY(launch_forces(s));
@@ -609,7 +659,7 @@ int enqueue_step_separate(ppc_state* s, bool phenotype, double p_divide, double 
 		PPC_TRY(launch_mark_remove(s));
 		PPC_TRY(launch_compact(s, true, true));
 	}
-	PPC_TRY(launch_bin(s, false));
+	PPC_TRY(launch_bin(s, false, last));
 	return PPC_OK;
 }
 
@@ -646,7 +696,16 @@ int replay_steps(ppc_state* s, int k, bool phenotype, double p_divide, double p_
 		PPC_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
 		int rc = lead_bin ? launch_bin(s, true) : PPC_OK;
 		for (int q = 0; q < k && rc == PPC_OK; q++)
-			rc = enqueue_step(s, phenotype, p_divide, p_death);
+			rc = enqueue_step(s, phenotype, p_divide, p_death, q == k - 1);
+		e.ready = s->ready_recorded;
+		if (s->join_pending)
+		{
+			// the transfer stream's branch rejoins before the capture ends
+			s->join_pending = false;
+			if (cudaEventRecord(s->ev_join, s->xfer) != cudaSuccess
+				|| cudaStreamWaitEvent(s->stream, s->ev_join, 0) != cudaSuccess)
+				rc = fail(PPC_ERR_CUDA, "joining the transfer stream into the step graph failed");
+		}
 		cudaError_t ec = cudaStreamEndCapture(s->stream, &g);
 		s->cur = cur0;
 		if (rc != PPC_OK)
@@ -668,8 +727,18 @@ int replay_steps(ppc_state* s, int k, bool phenotype, double p_divide, double p_
 	}
 	PPC_CUDA(cudaGraphLaunch(hit->exec, s->stream));
 	s->launches += hit->launches;
+	s->ready_recorded = hit->ready;
 	s->cur ^= k & 1;
 	s->vel_dirty = false;
+	return PPC_OK;
+}
+
+// after a call's last step: a download may run beside its rebuild while no
+// other kernel is launched
+int mark_ready(ppc_state* s)
+{
+	s->ready_pending = s->ready_recorded;
+	s->ready_launches = s->launches;
 	return PPC_OK;
 }
 
@@ -681,6 +750,8 @@ int run_steps(ppc_state* s, int32_t steps, bool phenotype, double p_divide, doub
 		return fail(PPC_ERR_ARG, "a bounded device wait gave up in an earlier step: upload the state again");
 	if (steps > 0)
 		s->counts_known = false; // compaction and division change the counts
+	s->ready_pending = false;
+	s->ready_recorded = false;
 	const bool graphs = s->use_graphs && !s->profiling;
 	// a rebuild the device decides on (after an upload of positions) rides
 	// at the head of the first replayed graph
@@ -694,15 +765,15 @@ int run_steps(ppc_state* s, int32_t steps, bool phenotype, double p_divide, doub
 		// non-zero attachment or detachment rates
 		s->has_springs = true;
 		for (int32_t k = 0; k < steps; k++)
-			PPC_TRY(enqueue_step_separate(s, phenotype, p_divide, p_death));
+			PPC_TRY(enqueue_step_separate(s, phenotype, p_divide, p_death, k == steps - 1));
 		s->lists_stale = steps > 0 || s->lists_stale;
-		return PPC_OK;
+		return mark_ready(s);
 	}
 	int32_t done = 0;
 	// the first step after an upload may read non-zero velocities
 	while (done < steps && s->vel_dirty)
 	{
-		PPC_TRY(enqueue_step(s, phenotype, p_divide, p_death));
+		PPC_TRY(enqueue_step(s, phenotype, p_divide, p_death, done == steps - 1));
 		done++;
 	}
 	if (graphs)
@@ -722,11 +793,11 @@ int run_steps(ppc_state* s, int32_t steps, bool phenotype, double p_divide, doub
 	}
 	while (done < steps)
 	{
-		PPC_TRY(enqueue_step(s, phenotype, p_divide, p_death));
+		PPC_TRY(enqueue_step(s, phenotype, p_divide, p_death, done == steps - 1));
 		done++;
 	}
 	s->lists_stale = steps > 0 || s->lists_stale;
-	return PPC_OK;
+	return mark_ready(s);
 }
 
 // grid of a mesh (validated: positive voxel shapes, maxs >= mins); sizes in
@@ -836,6 +907,14 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	if (cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking) != cudaSuccess)
 		rc = fail(PPC_ERR_CUDA, "cudaStreamCreate failed");
 	s->stream = s->own_stream;
+	if (rc == PPC_OK
+		&& (cudaStreamCreateWithFlags(&s->xfer, cudaStreamNonBlocking) != cudaSuccess
+			|| cudaEventCreateWithFlags(&s->ev_ready, cudaEventDisableTiming) != cudaSuccess
+			|| cudaEventCreateWithFlags(&s->ev_h2d, cudaEventDisableTiming) != cudaSuccess
+			|| cudaEventCreateWithFlags(&s->ev_stage_free, cudaEventDisableTiming) != cudaSuccess
+			|| cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) != cudaSuccess
+			|| cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming) != cudaSuccess))
+		rc = fail(PPC_ERR_CUDA, "cudaStreamCreate or cudaEventCreate failed");
 
 	view& v = s->v;
 	const size_t C = s->total_cap;
@@ -972,9 +1051,16 @@ int ppc_destroy(ppc_state* s)
 		return PPC_OK;
 	if (s->stream)
 		cudaStreamSynchronize(s->stream);
+	if (s->xfer)
+		cudaStreamSynchronize(s->xfer);
 	release_graph(s);
 	for (auto e : s->prof_events)
 		cudaEventDestroy(e);
+	for (auto e : { s->ev_ready, s->ev_h2d, s->ev_stage_free, s->ev_fork, s->ev_join })
+		if (e)
+			cudaEventDestroy(e);
+	if (s->xfer)
+		cudaStreamDestroy(s->xfer);
 	for (auto& b : s->allocations)
 		cudaFree(b.p);
 	if (s->stage)

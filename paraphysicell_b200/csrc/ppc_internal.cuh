@@ -222,6 +222,7 @@ struct graph_entry
 	cudaGraphExec_t exec = nullptr;
 	int steps = 0, cur = 0;
 	bool phenotype = false, lead_bin = false, springs = false;
+	bool ready = false; // the last step records ev_ready
 	double pdiv = 0, pdeath = 0;
 	int64_t launches = 0;
 };
@@ -241,6 +242,19 @@ struct ppc_state
 
 	cudaStream_t own_stream = nullptr;
 	cudaStream_t stream = nullptr;
+	// Host transfers beside the device work: the host-to-device copies of an
+	// upload of positions run on `xfer` while the stream finishes the last
+	// step's mesh rebuild, and a download right after a step runs there once
+	// the step's agent fields are final (ev_ready, recorded after the last
+	// step's count kernel, the last one that changes them), beside the rest
+	// of the rebuild.
+	cudaStream_t xfer = nullptr;
+	cudaStream_t h2d_stream = nullptr; // the stream an upload's host copies go to (null: `stream`)
+	cudaEvent_t ev_ready = nullptr, ev_h2d = nullptr, ev_stage_free = nullptr, ev_fork = nullptr, ev_join = nullptr;
+	bool join_pending = false; // a capture forked the transfer stream for ev_ready
+	bool ready_pending = false;	 // ev_ready marks the state a download reads...
+	int64_t ready_launches = 0;	 // ...while no kernel has been launched since (launch count then)
+	bool ready_recorded = false; // the last rebuild enqueued recorded ev_ready
 
 	ppc::view v {};
 	std::vector<ppc::buffer> allocations;
@@ -327,7 +341,7 @@ inline int blocks_for(int64_t n, int threads)
 }
 
 // ---- kernel entry points (ppc_kernels.cu) ----
-int launch_bin(ppc_state* s, bool conditional);
+int launch_bin(ppc_state* s, bool conditional, bool ready = false);
 int launch_neighbors(ppc_state* s);
 int launch_forces(ppc_state* s);
 int launch_membrane(ppc_state* s);

@@ -3616,10 +3616,32 @@ static void pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStr
 			return cuda_fail(e_, __func__);                                                                            \
 	} while (0)
 
-int launch_bin(ppc_state* s, bool conditional)
+// `ready`: record ev_ready after the count, the last kernel of the step
+// that changes agent fields (it applies the compaction's moves), so that a
+// download can run beside the rest of the rebuild
+int launch_bin(ppc_state* s, bool conditional, bool ready)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
 	pdl(k_bin_count, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur, conditional ? 1 : 0);
+	if (ready)
+	{
+		// Inside a graph capture the record is an external event node on a
+		// branch of the transfer stream that forks after the count (the fork
+		// adds no node, so the order kernel keeps its programmatic edge from
+		// the count); the capture joins the branch back at its end.
+		cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+		PPC_CUDA(cudaStreamIsCapturing(s->stream, &cs));
+		if (cs == cudaStreamCaptureStatusActive)
+		{
+			PPC_CUDA(cudaEventRecord(s->ev_fork, s->stream));
+			PPC_CUDA(cudaStreamWaitEvent(s->xfer, s->ev_fork, 0));
+			PPC_CUDA(cudaEventRecordWithFlags(s->ev_ready, s->xfer, cudaEventRecordExternal));
+			s->join_pending = true;
+		}
+		else
+			PPC_CUDA(cudaEventRecord(s->ev_ready, s->stream));
+	}
+	s->ready_recorded = ready;
 	pdl(k_bin_order, s->v.ntiles, kPlaceThreads, 0, PPC_LAUNCH(s), s->v);
 	pdl(k_bin_copy, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	PPC_CHECK_LAUNCH();
@@ -3850,6 +3872,7 @@ static int persistent_launch(ppc_state* s, size_t dyn, const persist_args& pa)
 // cooperative launch
 int launch_step_persistent(ppc_state* s)
 {
+	s->ready_recorded = false;
 	persist_args pa {};
 	pa.bar = s->v.barrier;
 	pa.limit = s->wait_limit;
