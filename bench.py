@@ -740,7 +740,7 @@ def run_ours(args, rank, world, local_rank):
     fused_avg_ms = fused_ms / max(fused_launches, 1)
     achieved = (per_agent * n0) / (fused_avg_ms / 1e3) / 1e9
     traffic = None
-    prof = os.path.join(ROOT, "profiles", f"k_fused_{args.workload}.md")
+    prof = os.path.join(ROOT, "profiles", f"k_fused_flat_{args.workload}.md")
     if os.path.exists(prof):
         for line in open(prof):
             if line.startswith("| dram_bytes_per_launch |"):
