@@ -1803,7 +1803,7 @@ int ppc_update_cell_cell_interactions(ppc_state* s, int32_t r, ppc_interactions*
 		return PPC_OK;
 	PPC_TRY(ensure_lists(s));
 	const size_t nd = (size_t)n;
-	PPC_TRY(ensure_field_scratch(s, sizeof(int32_t) * (2 * nd + nd * s->ncap + 2)));
+	PPC_TRY(ensure_field_scratch(s, sizeof(int32_t) * (3 * nd + nd * s->ncap + 2)));
 	int32_t* ip = static_cast<int32_t*>(s->ix_scratch);
 	const int32_t base = s->reps[r].base;
 	const ix_columns& c = s->v.ix;
@@ -1819,6 +1819,7 @@ int ppc_update_cell_cell_interactions(ppc_state* s, int32_t r, ppc_interactions*
 	x.ncand = ip + 2;
 	x.dep = ip + 2 + nd;
 	x.cand = ip + 2 + 2 * nd;
+	x.order = ip + 2 + 2 * nd + nd * s->ncap;
 	x.dead = c.dead + base;
 	x.dead_phago = c.dead_phago + base;
 	x.damage_rate = c.damage_rate + base;
@@ -1844,8 +1845,11 @@ int ppc_update_cell_cell_interactions(ppc_state* s, int32_t r, ppc_interactions*
 	x.isub = c.isub + base * S;
 	PPC_CUDA(cudaMemsetAsync(x.status, 0, 2 * sizeof(int32_t), s->stream));
 	PPC_TRY(launch_interactions(s, x));
+	// the call's status and the device error word, with one synchronisation
 	PPC_CUDA(cudaMemcpyAsync(s->pinned_err + 1, x.status, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
+	PPC_CUDA(cudaMemcpyAsync(s->pinned_err, s->v.err, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
 	PPC_CUDA(cudaStreamSynchronize(s->stream));
+	PPC_CUDA(cudaGetLastError());
 	if (s->pinned_err[1])
 		return fail(PPC_ERR_CAPACITY, "a neighbour list exceeds the neighbour capacity: no interaction ran");
 	// positions and radii changed: the next mesh update rebuilds the bins; the
@@ -1857,8 +1861,9 @@ int ppc_update_cell_cell_interactions(ppc_state* s, int32_t r, ppc_interactions*
 		for (const auto& col : ix_column_list(s->v.ix, f, s->ndefs))
 			back.push_back(col);
 		PPC_TRY(move_columns(s, back, base, n, false));
+		return finish(s);
 	}
-	return finish(s);
+	return map_errors(s, s->pinned_err[0]);
 }
 
 int ppc_step(ppc_state* s, int32_t steps)

@@ -18,8 +18,9 @@
 //     it. Each such agent (found with a per-slot atomicMin of the first walk
 //     that touches the slot) walks at once, in parallel with the others; the
 //     rest are marked;
-//  3. k_ix_ordered, one block: one thread walks the marked agents in index
-//     order, after every independent walk has finished.
+//  3. k_ix_ordered, one block, after every independent walk has finished:
+//     the marked agents in waves, each wave the walks that no earlier
+//     pending walk shares an agent with, all at once.
 // With the rates of a real model nearly every walk is independent.
 
 #include <cuda_runtime.h>
@@ -248,37 +249,95 @@ __global__ void __launch_bounds__(kIxThreads) k_ix_independent(view v, ix_fields
 	x.dep[i] = dep;
 }
 
-// the marked agents in index order on one thread, after every independent
-// walk; every thread restores first_end of the slots the walks touched
+// claims (atomicMin) or releases the slots a walk touches: its agent and
+// its candidate neighbours
+__device__ __forceinline__ void ix_slots(const view& v, const ix_fields& x, int i, bool claim)
+{
+	const int s = x.base + i;
+	const int m = x.ncand[i];
+	if (claim)
+		atomicMin(v.first_end + s, i);
+	else
+		v.first_end[s] = INT32_MAX;
+	for (int c = 0; c < m; c++)
+	{
+		const int q = v.nidx[(int64_t)s * v.ncap + x.cand[(int64_t)i * v.ncap + c]];
+		if (claim)
+			atomicMin(v.first_end + q, i);
+		else
+			v.first_end[q] = INT32_MAX;
+	}
+}
+
+// The marked walks, after every independent one, in waves: each round every
+// pending walk claims its slots (the lowest walk index wins a slot), and the
+// walks that won all their slots run at once. Such walks share no slot with
+// each other or with any earlier pending walk, so each sees what a run on
+// one thread in index order would show it; the lowest pending walk always
+// runs, so every round makes progress. The rest stay pending, in order. One
+// block; first_end is INT32_MAX again when the kernel ends.
 template <int DIMS>
 __global__ void __launch_bounds__(kIxResolveThreads) k_ix_ordered(view v, ix_fields x, int cur)
 {
-	__shared__ int list[kIxResolveThreads];
+	const int tid = threadIdx.x, bd = blockDim.x;
 	const bool ok = __ldcg(x.status) == 0;
-	for (int i = threadIdx.x; i < x.n; i += blockDim.x)
-	{
-		const int m = x.ncand[i];
-		if (m == 0)
-			continue;
-		const int s = x.base + i;
-		v.first_end[s] = INT32_MAX;
-		for (int c = 0; c < m; c++)
-			v.first_end[v.nidx[(int64_t)s * v.ncap + x.cand[(int64_t)i * v.ncap + c]]] = INT32_MAX;
-	}
+	for (int i = tid; i < x.n; i += bd)
+		if (x.ncand[i] > 0)
+			ix_slots(v, x, i, false);
 	if (!ok)
 		return;
-	for (int i0 = 0; i0 < x.n; i0 += blockDim.x)
+	// the marked walks in index order
+	int pending = 0;
+	for (int i0 = 0; i0 < x.n; i0 += bd)
 	{
-		const int i = i0 + threadIdx.x;
+		const int i = i0 + tid;
 		const int has = i < x.n && x.dep[i] != 0;
 		int total;
-		const int off = block_exclusive_scan(has, total);
+		const int off = block_exclusive_scan(has, total); // synchronises the block
 		if (has)
-			list[off] = i;
+			x.order[pending + off] = i;
+		pending += total;
+	}
+	__syncthreads();
+	for (int round = 0; pending > 0 && round <= x.n; round++)
+	{
+		for (int e = tid; e < pending; e += bd)
+			ix_slots(v, x, x.order[e], true);
 		__syncthreads();
-		if (threadIdx.x == 0)
-			for (int w = 0; w < total; w++)
-				ix_agent<DIMS>(v, x, cur, list[w]);
+		for (int e = tid; e < pending; e += bd)
+		{
+			const int w = x.order[e];
+			const int s = x.base + w;
+			bool won = __ldcg(v.first_end + s) == w;
+			const int m = x.ncand[w];
+			for (int c = 0; c < m && won; c++)
+				won = __ldcg(v.first_end + v.nidx[(int64_t)s * v.ncap + x.cand[(int64_t)w * v.ncap + c]]) == w;
+			if (won)
+			{
+				ix_agent<DIMS>(v, x, cur, w);
+				x.dep[w] = 0;
+			}
+		}
+		__syncthreads();
+		for (int e = tid; e < pending; e += bd)
+			ix_slots(v, x, x.order[e], false);
+		__syncthreads();
+		// keep the walks still pending, in order (a chunk's entries are all
+		// read before any of them is overwritten, and the writes land below
+		// the next chunk)
+		int kept = 0;
+		for (int e0 = 0; e0 < pending; e0 += bd)
+		{
+			const int e = e0 + tid;
+			const int w = e < pending ? x.order[e] : -1;
+			const int keep = w >= 0 && x.dep[w] != 0;
+			int total;
+			const int off = block_exclusive_scan(keep, total);
+			if (keep)
+				x.order[kept + off] = w;
+			kept += total;
+		}
+		pending = kept;
 		__syncthreads();
 	}
 }

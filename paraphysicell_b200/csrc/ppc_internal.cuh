@@ -11,10 +11,11 @@
 //   orient[C]    double4
 //   aff[C*D], def, maxatt, scnt [C] int32, springs [C*S] int32
 //   movable, flags [C] uint8, ids [C] int64, rid [C] int32 (replicate of slot)
-// Mechanics mesh bins, rebuilt by a counting sort each step:
-//   vcnt[V] per-voxel counts (zero between rebuilds), tile_sum[V/4096]
-//   vstart[V+1] exclusive prefix of the counts over the key space of all
-//   replicates; key[C] (global voxel index), vrank[C] (provisional rank), tmp[C]
+// Mechanics mesh bins, rebuilt each step from the previous order (tiles of
+// 2^tshift consecutive voxel keys; agents that leave their tile move on
+// per-tile chains):
+//   vstart[V+1] exclusive prefix of the voxel counts over the key space of
+//   all replicates; key[C] (global voxel index of each slot)
 //   sorted[C] slots in voxel-key order (descending slot inside a voxel),
 //   skey[C] their keys, spos4[C] double4 {x, y, z, rmad*radius} in that order.
 // Because the sorted array follows the key order, the voxels x-1..x+1 of one
@@ -380,6 +381,7 @@ struct ix_fields
 	int32_t* cand;	// [n*ncap] their positions in the agent's neighbour list
 	int32_t* status; // [2] capacity error found by the candidate pass, count of agents left for the ordered pass
 	int32_t* dep;	 // [n] agents whose interactions depend on an earlier agent's
+	int32_t* order;	 // [n] the dependent agents still to walk, in index order
 };
 int launch_interactions(ppc_state* s, const ix_fields& x);
 int mark_fields_changed(ppc_state* s);
