@@ -2467,7 +2467,7 @@ __device__ __forceinline__ void fused_queue_agent(const view& v, int cur, int op
 }
 
 template <int DIMS, bool F32>
-__global__ void __launch_bounds__(kQueueThreads) k_fused_queue(view v, int cur, int opts)
+__global__ void __launch_bounds__(kQueueThreads, 5) k_fused_queue(view v, int cur, int opts)
 {
 	grid_wait();
 	bump_spring_epochs(v);
