@@ -652,10 +652,16 @@ def run_ours(args, rank, world, local_rank):
         else:
             sim.step(k)
 
-    # the fused pass's launch shape, timed over real steps (ppc_autotune);
-    # the trajectory does not depend on it
-    with torch.cuda.stream(stream):
-        shape = sim.autotune(steps=3)
+    # the fused pass's launch shape, timed over real steps (ppc_autotune)
+    # unless given; the trajectory does not depend on it
+    if args.launch_shape is None:
+        with torch.cuda.stream(stream):
+            shape = sim.autotune(steps=3)
+        chosen_by = "ppc_autotune"
+    else:
+        shape = (args.launch_shape, 128)
+        sim.set_launch_shape(args.launch_shape, 128, 32 * 1024 if args.launch_shape == 0 else 0)
+        chosen_by = "--launch-shape"
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     with torch.cuda.stream(stream):
@@ -747,7 +753,8 @@ def run_ours(args, rank, world, local_rank):
     fused_avg_ms = fused_ms / max(fused_launches, 1)
     achieved = (per_agent * n0) / (fused_avg_ms / 1e3) / 1e9
     traffic = None
-    prof = os.path.join(ROOT, "profiles", f"k_fused_flat_{args.workload}.md")
+    kernel_name = {-3: "k_fused_flat", -4: "k_fused_queue"}.get(shape[0], "k_fused_staged")
+    prof = os.path.join(ROOT, "profiles", f"{kernel_name}_{args.workload}.md")
     if os.path.exists(prof):
         for line in open(prof):
             if line.startswith("| dram_bytes_per_launch |"):
@@ -759,10 +766,11 @@ def run_ours(args, rank, world, local_rank):
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "description": WORKLOADS[args.workload], "agents": n0,
                    "l2": "flushed (256 MiB write) before every timed step", "form": "FP64 drop-in",
-                   "launch_shape": {"tile_edge": shape[0], "threads": shape[1], "chosen_by": "ppc_autotune"},
+                   "launch_shape": {"tile_edge": shape[0], "threads": shape[1], "chosen_by": chosen_by},
                    "parallelism": f"replicas x{world}" if world > 1 else "single simulation"},
         "steady_state": {"value": steady, "unit": UNIT, "note": "back-to-back graph-replayed steps, L2 warm"},
-        "roofline": {"bound": "hbm", "kernel": "k_fused (neighbour search + forces + membrane + springs + AB2)",
+        "roofline": {"bound": "hbm", "kernel": f"{kernel_name} (fused pass: neighbour search + forces + membrane + "
+                                                 "springs + AB2)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_src, "traffic": traffic, "bytes_per_agent": per_agent,
                      "avg_launch_us": fused_avg_ms * 1e3, "launches": fused_launches},
@@ -795,6 +803,8 @@ def main():
     p.add_argument("--workload", default="config3", choices=sorted(WORKLOADS))
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-forms", action="store_true", help="skip the FP32-force form's measurement")
+    p.add_argument("--launch-shape", type=int, default=None, choices=[-4, -3, -2, -1, 0],
+                   help="fused-pass launch shape of the main line (default: ppc_autotune picks)")
     args = p.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -174,15 +174,16 @@ int ppc_set_precision(ppc_state* s, int32_t precision);
 int ppc_set_random_seed(ppc_state* s, uint64_t seed);
 
 /* Launch shape of the fused force pass, one thread per agent in every shape:
- *  -3 (the default): each thread numbers its candidates in the reference's
- *     order and fetches their single-precision positions ten at a time into
- *     shared memory with asynchronous copies, then the FP64 data of the kept
- *     ones two at a time — best where agents are sparse (well under one per
- *     voxel); `threads` and `smem_bytes` are ignored (128 threads);
- *  -4: a warp lays its 32 agents' candidates end to end and every lane takes
- *     every 32nd of them, so the filter and the pair code run on full warps
- *     however unevenly the candidates fall; each agent's lane adds its own
- *     pair terms in its candidate order (128 threads);
+ *  -4 (the default): a warp lays its 32 agents' candidates end to end and
+ *     every lane takes every 32nd of them, so the filter and the pair code run
+ *     on full warps however unevenly the candidates fall; each agent's lane
+ *     adds its own pair terms in its candidate order — best where agents are
+ *     sparse (well under one per voxel); `threads` and `smem_bytes` are
+ *     ignored (128 threads);
+ *  -3: each thread numbers its candidates in the reference's order and
+ *     fetches their single-precision positions ten at a time into shared
+ *     memory with asynchronous copies, then the FP64 data of the kept ones two
+ *     at a time (128 threads);
  *  -1: each thread reads its candidates one at a time from global memory and
  *     runs its own pair code;
  *  -2: the pair code of a warp's kept candidates is spread over the warp's
@@ -215,7 +216,7 @@ int ppc_set_wait_limit(ppc_state* s, int64_t polls);
 
 /* Autotuner of the launch shape (no counterpart in the reference, whose
  * OpenMP loops have no launch shape): runs 2 x `steps` mechanics steps
- * (ppc_step) with each candidate shape — -3, -4, -1 and -2 with 128 threads,
+ * (ppc_step) with each candidate shape — -4, -3, -1 and -2 with 128 threads,
  * 0 with 128 threads / 32 KiB and with 64 threads / 16 KiB — times the second
  * half of each on the state's stream, and keeps the fastest. The simulation
  * advances by 12 x `steps` steps (the trajectory does not depend on the

@@ -203,15 +203,26 @@ class AgentArrays:
 
     def struct(self, fields=None):
         """ppc_agents aliasing these arrays. With `fields`, only those
-        pointers are set (the rest are NULL)."""
-        s = Agents()
+        pointers are set (the rest are NULL). The struct of a field set is
+        built once and reused while the arrays stay the same objects (a
+        per-step transfer loop then costs no pointer setup)."""
+        key = None if fields is None else tuple(fields)
+        cache = self.__dict__.setdefault("_structs", {})
+        hit = cache.get(key)
+        if hit is not None and all(self.arrays[n] is arr for n, arr in hit[1]):
+            s = hit[0]
+        else:
+            s = Agents()
+            used = []
+            for name, dt, _, _ in FIELDS:
+                if fields is not None and name not in fields:
+                    continue
+                setattr(s, name, self.arrays[name].ctypes.data_as(_PTR[dt]))
+                used.append((name, self.arrays[name]))
+            cache[key] = (s, used)
         s.count = self.count
         s.capacity = self.capacity
         s.spring_capacity = self.spring_capacity
-        for name, dt, _, _ in FIELDS:
-            if fields is not None and name not in fields:
-                continue
-            setattr(s, name, self.arrays[name].ctypes.data_as(_PTR[dt]))
         return s
 
     def copy(self):

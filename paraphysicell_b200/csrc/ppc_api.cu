@@ -1881,7 +1881,7 @@ int ppc_autotune(ppc_state* s, int32_t steps, int32_t* tile_edge, int32_t* threa
 	{
 		int edge, threads, smem;
 	};
-	const shape cand[] = { { -3, 128, 0 }, { -4, 128, 0 }, { -1, 128, 0 }, { -2, 128, 0 }, { 0, 128, 32 * 1024 },
+	const shape cand[] = { { -4, 128, 0 }, { -3, 128, 0 }, { -1, 128, 0 }, { -2, 128, 0 }, { 0, 128, 32 * 1024 },
 							 { 0, 64, 16 * 1024 } };
 	const int ncand = (int)(sizeof cand / sizeof cand[0]);
 	cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -306,8 +306,8 @@ struct ppc_state
 	int32_t* pinned_err = nullptr;			 // pinned landing area of the device error word
 	bool staged = false;
 	bool coop = false;
-	bool flat = true; // per-thread pass with batched candidate fetches (shape -3, the default)
-	bool queue = false; // per-thread pass with the warp's candidates shared out (shape -4)
+	bool flat = false; // per-thread pass with batched candidate fetches (shape -3)
+	bool queue = true; // per-thread pass with the warp's candidates shared out (shape -4, the default)
 	bool persistent = false;		 // mechanics steps as one cooperative launch each (PPC_STEP_PERSISTENT)
 	long long wait_limit = 1LL << 25; // polls of a bounded device wait before it gives up
 	bool lost = false;				 // a bounded wait gave up: the state needs a fresh upload
