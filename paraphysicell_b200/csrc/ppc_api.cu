@@ -623,9 +623,15 @@ int enqueue_step(ppc_state* s, bool phenotype, double p_divide, double p_death, 
 {
 	if (s->persistent && !phenotype)
 		return launch_step_persistent(s);
-	// the compaction right before the rebuild leaves its moves to k_bin_count
-	PPC_TRY(launch_fused(s));
-	PPC_TRY(launch_compact(s, false, !phenotype));
+	// the compaction right before the rebuild leaves its moves to k_bin_count;
+	// in a step without the phenotype update the fused passes -3 and -4 also
+	// make the count's entries, which hold unless the compaction removes agents
+	const bool produce = !phenotype && (s->flat || s->queue);
+	s->produce = produce;
+	const int rc_fused = launch_fused(s);
+	s->produce = false;
+	PPC_TRY(rc_fused);
+	PPC_TRY(launch_compact(s, false, !phenotype, produce));
 	if (phenotype)
 	{
 		PPC_TRY(launch_flag_by_draws(s, p_divide, p_death));
@@ -633,7 +639,7 @@ int enqueue_step(ppc_state* s, bool phenotype, double p_divide, double p_death, 
 		PPC_TRY(launch_mark_remove(s));
 		PPC_TRY(launch_compact(s, true, true));
 	}
-	PPC_TRY(launch_bin(s, false, last));
+	PPC_TRY(launch_bin(s, false, last, produce));
 	return PPC_OK;
 }
 
@@ -982,6 +988,7 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.tfresh, C));
 	try_(alloc(s, v.params_changed, 1));
 	try_(alloc(s, v.copy_full, 1));
+	try_(alloc(s, v.recount, 1));
 	if (rc == PPC_OK && cudaMemset(v.chead, 0xff, sizeof(int32_t) * (size_t)v.ntiles * 32) != cudaSuccess)
 		rc = fail(PPC_ERR_CUDA, "cudaMemset failed");
 	try_(alloc(s, v.order_valid, 1));

@@ -151,6 +151,7 @@ struct view
 	uint8_t* tfresh;	// [C] 1 where the agent at a position of the key order is new to it
 	int32_t* params_changed; // fields other than positions, or slots' agents, changed since the last rebuild
 	int32_t* copy_full;	// the current rebuild's k_bin_copy copies every field of every agent
+	int32_t* recount;	// the compaction removed agents: the rebuild's count recomputes every entry
 	int32_t* order_valid; // 1 once a rebuild has set `sorted` (cleared by uploads)
 	int32_t* binned;	  // [replicates] live count at the last rebuild (the slots `sorted` lists)
 	int32_t* move_src;	  // [C] tail slot whose agent the next k_bin_count moves into this hole, or -1
@@ -308,6 +309,7 @@ struct ppc_state
 	bool coop = false;
 	bool flat = false; // per-thread pass with batched candidate fetches (shape -3)
 	bool queue = true; // per-thread pass with the warp's candidates shared out (shape -4, the default)
+	bool produce = false; // the fused pass being launched makes the rebuild's entries (FUSED_PRODUCE)
 	bool persistent = false;		 // mechanics steps as one cooperative launch each (PPC_STEP_PERSISTENT)
 	long long wait_limit = 1LL << 25; // polls of a bounded device wait before it gives up
 	bool lost = false;				 // a bounded wait gave up: the state needs a fresh upload
@@ -342,7 +344,7 @@ inline int blocks_for(int64_t n, int threads)
 }
 
 // ---- kernel entry points (ppc_kernels.cu) ----
-int launch_bin(ppc_state* s, bool conditional, bool ready = false);
+int launch_bin(ppc_state* s, bool conditional, bool ready = false, bool produced = false);
 int launch_neighbors(ppc_state* s);
 int launch_forces(ppc_state* s);
 int launch_membrane(ppc_state* s);
@@ -351,7 +353,7 @@ int launch_spring_updates(ppc_state* s);
 int launch_positions(ppc_state* s);
 int launch_fused(ppc_state* s);
 int launch_step_persistent(ppc_state* s);
-int launch_compact(ppc_state* s, bool phenotype_pass, bool fold = false);
+int launch_compact(ppc_state* s, bool phenotype_pass, bool fold = false, bool produced = false);
 int launch_mark_remove(ppc_state* s);
 int launch_divide(ppc_state* s);
 int launch_flag_by_draws(ppc_state* s, double p_divide, double p_death);

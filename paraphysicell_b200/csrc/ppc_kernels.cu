@@ -317,14 +317,17 @@ __device__ __forceinline__ void bin_count_body(const view& v, int cur, int t)
 // A conditional rebuild (after an upload of positions) runs only if the
 // upload changed some position; its decision goes to bin_active for
 // k_bin_order and k_bin_copy.
-__global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur, int conditional)
+// `produced`: the fused pass before this rebuild made every entry (see
+// produce_entry); the count then has nothing to do unless the compaction
+// removed agents since.
+__global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur, int conditional, int produced)
 {
 	grid_wait();
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	const bool active = !conditional || *v.pos_changed != 0 || *v.moves_pending != 0 || *v.appended != 0;
 	if (t == 0)
 		*v.bin_active = active ? 1 : 0;
-	if (!active)
+	if (!active || (produced && *v.recount == 0))
 		return;
 	bin_count_body(v, cur, t);
 }
@@ -655,6 +658,7 @@ __device__ __forceinline__ void bin_order_tile(const view& v, int b, place_smem&
 			// changed since the last rebuild, elsewhere only the positions
 			*v.copy_full = (*v.params_changed != 0 || !ordered) ? 1 : 0;
 			*v.params_changed = 0;
+			*v.recount = 0;
 			*v.tdone = 0;
 			*v.order_valid = 1;
 			*v.moves_pending = 0; // applied by this rebuild's count
@@ -727,8 +731,51 @@ enum : int
 {
 	FUSED_WALLS = 1,
 	FUSED_SPRINGS = 2,
-	FUSED_VEL = 4
+	FUSED_VEL = 4,
+	FUSED_PRODUCE = 8 // the pass does the rebuild count's work for its agents (shapes -3 and -4)
 };
+
+// the voxel coordinate of axis_coord without its error reports: the keys the
+// fused pass computes for the rebuild are recomputed (with the reports) by
+// the count whenever the compaction removes agents, and an agent outside the
+// box or with a non-finite position is always removed or reported
+__device__ __forceinline__ int axis_coord_quiet(double x, const rep_info& R, int d)
+{
+	const double q = (x - R.mins[d]) / R.shape[d];
+	const int g = R.grid[d];
+	if (!(q > 0.0))
+		return 0;
+	if (q >= (double)g)
+		return g - 1;
+	return (int)q;
+}
+
+// The rebuild count's work for the agent at key-ordered position t (slot s,
+// key okey in the current order) that the fused pass moved to p: its new
+// key, and either its kept entry of the order or a push onto its new tile's
+// mover chain with the tiles' changes. Valid while no agent is removed
+// before the rebuild; the compaction plan discards it otherwise.
+__device__ __forceinline__ void produce_entry(const view& v, const rep_info& R, int t, int s, int32_t okey,
+											  const double4& p)
+{
+	const int c0 = axis_coord_quiet(p.x, R, 0);
+	const int c1 = v.dims >= 2 ? axis_coord_quiet(p.y, R, 1) : 0;
+	const int c2 = v.dims >= 3 ? axis_coord_quiet(p.z, R, 2) : 0;
+	const int32_t key = (int32_t)(R.vox_base + c0 + (int64_t)R.grid[0] * (c1 + (int64_t)R.grid[1] * c2));
+	v.key[s] = key;
+	const int sh = v.tshift;
+	if ((key >> sh) == (okey >> sh))
+		v.porder[t] = make_int2(s, key);
+	else
+	{
+		v.porder[t] = make_int2(-1, -1);
+		chain_push(v, s, key);
+		atomicAdd(v.tdelta + (okey >> sh), -1);
+		atomicAdd(v.sdelta + ((okey >> sh) >> kSuperShift), -1);
+		atomicAdd(v.tdelta + (key >> sh), 1);
+		atomicAdd(v.sdelta + ((key >> sh) >> kSuperShift), 1);
+	}
+}
 
 constexpr int kList = 8; // neighbours recorded per thread before the pair pass runs
 constexpr int kFusedThreads = 128; // block size limit of the fused pass (five blocks per SM resident)
@@ -1763,9 +1810,9 @@ __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefe
 // the fused pass for the agent in slot s with the pair sums (vx, vy, vz,
 // pressure); pi is its key-ordered position, radius its radius
 template <int DIMS>
-__device__ __forceinline__ void agent_finish(const view& v, int cur, int opts, int s, int r, const rep_info& R,
-											 const double4& pi, double radius, int def_i, bool mov_i, int nspr,
-											 double vx, double vy, double vz, double pressure)
+__device__ __forceinline__ void agent_finish(const view& v, int cur, int opts, int t, int32_t key, int s, int r,
+											 const rep_info& R, const double4& pi, double radius, int def_i, bool mov_i,
+											 int nspr, double vx, double vy, double vz, double pressure)
 {
 	const bool walls_on = (opts & FUSED_WALLS) != 0;
 	const bool vel_on = (opts & FUSED_VEL) != 0;
@@ -1794,6 +1841,8 @@ __device__ __forceinline__ void agent_finish(const view& v, int cur, int opts, i
 		atomicOr(v.err, ERR_NONFINITE);
 	if (to_remove<DIMS>(R, p, flag))
 		append_bad(v, r, s - R.base);
+	if (opts & FUSED_PRODUCE)
+		produce_entry(v, R, t, s, key, p);
 }
 
 // the agent at key-ordered position t, with its block's shared slots `sm`
@@ -2058,7 +2107,7 @@ __device__ __forceinline__ void fused_flat_agent(const view& v, int cur, int opt
 		pressure = fp.value();
 	}
 
-	agent_finish<DIMS>(v, cur, opts, s, r, R, pi, qi.x, def_i, mov_i, nspr, vx, vy, vz, pressure);
+	agent_finish<DIMS>(v, cur, opts, t, key, s, r, R, pi, qi.x, def_i, mov_i, nspr, vx, vy, vz, pressure);
 }
 
 template <int DIMS, bool F32>
@@ -2463,7 +2512,7 @@ __device__ __forceinline__ void fused_queue_agent(const view& v, int cur, int op
 		vz = vz + fz.value();
 		pressure = fp.value();
 	}
-	agent_finish<DIMS>(v, cur, opts, s, r, R, pi, qi.x, def_i, mov_i, nspr, vx, vy, vz, pressure);
+	agent_finish<DIMS>(v, cur, opts, t, key, s, r, R, pi, qi.x, def_i, mov_i, nspr, vx, vy, vz, pressure);
 }
 
 template <int DIMS, bool F32>
@@ -2762,7 +2811,8 @@ __device__ void springs_rename_attached(const view& v, int old_slot, int new_slo
 // Produces (hole, source) moves for the agents that end up in holes, the new
 // count and the death count; with springs it also replays every removal on
 // the spring rows in the reference's order.
-__device__ void compact_plan_rep(const view& v, int r, int phenotype_pass, int springs, int fold, int32_t* sh)
+__device__ void compact_plan_rep(const view& v, int r, int phenotype_pass, int springs, int fold, int produced,
+								 int32_t* sh)
 {
 	rep_counters& C = v.ctr[r];
 	const int nb = min(C.nbad, v.reps[r].cap);
@@ -2771,6 +2821,23 @@ __device__ void compact_plan_rep(const view& v, int r, int phenotype_pass, int s
 		if (threadIdx.x == 0)
 			v.nmoves[r] = 0;
 		return;
+	}
+	// removals after a fused pass that made the rebuild's entries: they no
+	// longer hold; the first replicate to find removals clears them and the
+	// count recomputes every entry
+	__shared__ int s_first;
+	if (threadIdx.x == 0)
+		s_first = produced && atomicExch(v.recount, 1) == 0;
+	__syncthreads();
+	if (s_first)
+	{
+		const int64_t heads = (int64_t)v.ntiles * kChains;
+		for (int64_t k = threadIdx.x; k < heads; k += blockDim.x)
+			v.chead[k] = -1;
+		for (int k = threadIdx.x; k < v.ntiles; k += blockDim.x)
+			v.tdelta[k] = 0;
+		for (int k = threadIdx.x; k < ((v.ntiles + (1 << kSuperShift) - 1) >> kSuperShift); k += blockDim.x)
+			v.sdelta[k] = 0;
 	}
 	const int base = v.reps[r].base;
 	int32_t* B = v.bad + base;
@@ -2837,11 +2904,11 @@ __device__ void compact_plan_rep(const view& v, int r, int phenotype_pass, int s
 	v.nmoves[r] = nm;
 }
 
-__global__ void k_compact_plan(view v, int phenotype_pass, int springs, int fold)
+__global__ void k_compact_plan(view v, int phenotype_pass, int springs, int fold, int produced)
 {
 	grid_wait();
 	__shared__ int32_t sh[kSortCap];
-	compact_plan_rep(v, blockIdx.x, phenotype_pass, springs, fold, sh);
+	compact_plan_rep(v, blockIdx.x, phenotype_pass, springs, fold, produced, sh);
 }
 
 // the planned moves, one thread per move
@@ -3564,7 +3631,7 @@ __global__ void __launch_bounds__(kPersistThreads) k_step_persistent(view v, int
 	// compaction plan, one replicate per block; its moves are applied by the count
 	for (int r = blockIdx.x; r < v.nreps; r += nb)
 	{
-		compact_plan_rep(v, r, 0, pa.springs, 1, reinterpret_cast<int32_t*>(smem));
+		compact_plan_rep(v, r, 0, pa.springs, 1, 0, reinterpret_cast<int32_t*>(smem));
 		__syncthreads(); // thread 0 finishes the serial plan before the next sort
 	}
 	if (!grid_barrier(v, pa.bar, pa.limit))
@@ -3619,10 +3686,10 @@ static void pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStr
 // `ready`: record ev_ready after the count, the last kernel of the step
 // that changes agent fields (it applies the compaction's moves), so that a
 // download can run beside the rest of the rebuild
-int launch_bin(ppc_state* s, bool conditional, bool ready)
+int launch_bin(ppc_state* s, bool conditional, bool ready, bool produced)
 {
 	const int b = blocks_for(s->total_cap, kThreads);
-	pdl(k_bin_count, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur, conditional ? 1 : 0);
+	pdl(k_bin_count, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur, conditional ? 1 : 0, produced ? 1 : 0);
 	if (ready)
 	{
 		// Inside a graph capture the record is an external event node on a
@@ -3771,7 +3838,7 @@ static int fused_opts(ppc_state* s)
 {
 	return (s->params.virtual_wall_at_domain_edges ? FUSED_WALLS : 0)
 		   | ((s->has_springs && s->params.automated_spring_adhesion) ? FUSED_SPRINGS : 0)
-		   | (s->vel_dirty ? FUSED_VEL : 0);
+		   | (s->vel_dirty ? FUSED_VEL : 0) | (s->produce ? FUSED_PRODUCE : 0);
 }
 
 // the staged pass's staging capacity (float4 positions) and dynamic shared bytes
@@ -3980,10 +4047,11 @@ int launch_fused(ppc_state* s)
 	return PPC_OK;
 }
 
-int launch_compact(ppc_state* s, bool phenotype_pass, bool fold)
+int launch_compact(ppc_state* s, bool phenotype_pass, bool fold, bool produced)
 {
 	const int springs = s->has_springs ? 1 : 0;
-	pdl(k_compact_plan, s->nreps, kThreads, 0, PPC_LAUNCH(s), s->v, phenotype_pass ? 1 : 0, springs, fold ? 1 : 0);
+	pdl(k_compact_plan, s->nreps, kThreads, 0, PPC_LAUNCH(s), s->v, phenotype_pass ? 1 : 0, springs, fold ? 1 : 0,
+		produced ? 1 : 0);
 	if (!fold)
 	{
 		dim3 g(std::max(1, std::min(64, blocks_for(s->total_cap / std::max(1, s->nreps), kThreads))), s->nreps);

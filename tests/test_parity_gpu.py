@@ -471,3 +471,32 @@ def test_full_size_config3_properties_and_oracle():
     nb = d.neighbors()
     pairs = {(i, j) for i, lst in enumerate(nb) for j in lst}
     assert all((j, i) in pairs for (i, j) in pairs)
+
+
+@pytest.mark.parametrize("shape", [(-4, 128, 0), (-3, 128, 0), (-2, 128, 0)], ids=lambda s: "edge%d" % s[0])
+def test_removals_inside_fused_steps(shape):
+    """Agents flagged for removal when steps start, and agents pushed out of
+    the box during them: the compaction inside the fused step removes them,
+    and the rebuild recounts every entry (the entries the fused pass made
+    no longer hold), giving the oracle's state, bins and neighbours."""
+    mesh, params, a = wl.scaled(wl.config2, 3000, seed=57)
+    a.arrays["flags"][[3, 40, 41, 777, 1500]] = FLAG_TO_REMOVE
+    # a few agents at the wall moving outwards: they leave during the steps
+    pos = a.arrays["positions"][: 3 * a.count].reshape(a.count, 3)
+    vp = a.arrays["previous_velocities"][: 3 * a.count].reshape(a.count, 3)
+    for i in (10, 20, 30):
+        pos[i] = (float(mesh.bounding_box_maxs[0]) - 1.0, pos[i][1], pos[i][2])
+        vp[i] = (-300.0, 0.0, 0.0)
+    params.virtual_wall_at_domain_edges = 0
+    o, d = gu.make_pair(mesh, params, a)
+    d.set_launch_shape(*shape)
+    o.update_mechanics_mesh()
+    o.update_cell_neighbors()
+    d.update_mechanics_mesh()
+    for k in (1, 10, 1):
+        o.step(k, 0, 0.0, 0.0)
+        d.step(k)
+        gu.assert_same_state(gu.fetch(d, a), gu.fetch(o, a))
+    assert gu.fetch(d, a).count < a.count - 5
+    gu.assert_same_bins(d, o)
+    gu.assert_same_neighbors(d, o)
