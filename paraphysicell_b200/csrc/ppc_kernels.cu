@@ -732,8 +732,38 @@ enum : int
 	FUSED_WALLS = 1,
 	FUSED_SPRINGS = 2,
 	FUSED_VEL = 4,
-	FUSED_PRODUCE = 8 // the pass does the rebuild count's work for its agents (shapes -3 and -4)
+	FUSED_PRODUCE = 8, // the pass does the rebuild count's work for its agents (shapes -3 and -4)
+	FUSED_PLAN = 16,   // the block finishing last runs the compaction plan (one replicate)
+	FUSED_PLAN_SPRINGS = 32 // ...which renames spring partners
 };
+
+__device__ void compact_plan_rep(const view& v, int r, int phenotype_pass, int springs, int fold, int produced,
+								 int32_t* sh);
+
+// With FUSED_PLAN the block that finishes the fused pass last runs the
+// compaction plan of the (single) replicate, which then needs no launch of
+// its own: the plan reads only what the whole pass has written (the removal
+// candidates), and the last block to arrive sees every block's writes.
+// `sort` is the block's shared memory, free once its agents are done.
+__device__ __forceinline__ void fused_plan_tail(const view& v, int opts, int32_t* sort)
+{
+	if (!(opts & FUSED_PLAN))
+		return;
+	__shared__ int s_last;
+	__syncthreads();
+	if (threadIdx.x == 0)
+	{
+		__threadfence();
+		s_last = atomicAdd(v.fdone, 1u) == gridDim.x - 1;
+	}
+	__syncthreads();
+	if (!s_last)
+		return;
+	__threadfence();
+	compact_plan_rep(v, 0, 0, (opts & FUSED_PLAN_SPRINGS) ? 1 : 0, 1, (opts & FUSED_PRODUCE) ? 1 : 0, sort);
+	if (threadIdx.x == 0)
+		*v.fdone = 0;
+}
 
 // the voxel coordinate of axis_coord without its error reports: the keys the
 // fused pass computes for the rebuild are recomputed (with the reports) by
@@ -2118,6 +2148,7 @@ __global__ void __launch_bounds__(kFlatThreads, 5) k_fused_flat(view v, int cur,
 	extern __shared__ __align__(16) unsigned char flat_raw[];
 	fused_flat_agent<DIMS, F32>(v, cur, opts, blockIdx.x * kFlatThreads + threadIdx.x,
 								*reinterpret_cast<flat_smem*>(flat_raw));
+	fused_plan_tail(v, opts, reinterpret_cast<int32_t*>(flat_raw));
 }
 
 // ---------------------------------------------------------------------------
@@ -2523,6 +2554,7 @@ __global__ void __launch_bounds__(kQueueThreads, 5) k_fused_queue(view v, int cu
 	extern __shared__ __align__(16) unsigned char queue_raw[];
 	queue_smem& sm = *reinterpret_cast<queue_smem*>(queue_raw);
 	fused_queue_agent<DIMS, F32>(v, cur, opts, blockIdx.x * kQueueThreads + threadIdx.x, sm.w[threadIdx.x >> 5]);
+	fused_plan_tail(v, opts, reinterpret_cast<int32_t*>(queue_raw));
 }
 
 // ---------------------------------------------------------------------------
@@ -3838,7 +3870,8 @@ static int fused_opts(ppc_state* s)
 {
 	return (s->params.virtual_wall_at_domain_edges ? FUSED_WALLS : 0)
 		   | ((s->has_springs && s->params.automated_spring_adhesion) ? FUSED_SPRINGS : 0)
-		   | (s->vel_dirty ? FUSED_VEL : 0) | (s->produce ? FUSED_PRODUCE : 0);
+		   | (s->vel_dirty ? FUSED_VEL : 0) | (s->produce ? FUSED_PRODUCE : 0)
+		   | (s->plan_in_fused ? FUSED_PLAN | (s->has_springs ? FUSED_PLAN_SPRINGS : 0) : 0);
 }
 
 // the staged pass's staging capacity (float4 positions) and dynamic shared bytes
