@@ -686,7 +686,7 @@ int replay_steps(ppc_state* s, int k, bool phenotype, double p_divide, double p_
 {
 	graph_entry* hit = nullptr;
 	for (auto& e : s->graphs)
-		if (e.steps == k && e.cur == s->cur && e.phenotype == phenotype && e.pdiv == p_divide && e.pdeath == p_death
+		if (e.steps == k && e.cur == s->cur && e.sbuf == s->sbuf && e.phenotype == phenotype && e.pdiv == p_divide && e.pdeath == p_death
 			&& e.lead_bin == lead_bin && e.springs == s->has_springs)
 			hit = &e;
 	if (!hit)
@@ -696,6 +696,7 @@ int replay_steps(ppc_state* s, int k, bool phenotype, double p_divide, double p_
 		graph_entry e {};
 		e.steps = k;
 		e.cur = s->cur;
+		e.sbuf = s->sbuf;
 		e.phenotype = phenotype;
 		e.pdiv = p_divide;
 		e.pdeath = p_death;
@@ -719,6 +720,9 @@ int replay_steps(ppc_state* s, int k, bool phenotype, double p_divide, double p_
 		}
 		cudaError_t ec = cudaStreamEndCapture(s->stream, &g);
 		s->cur = cur0;
+		e.sflip = s->sbuf ^ e.sbuf;
+		if (e.sflip)
+			flip_sorted_positions(s);
 		if (rc != PPC_OK)
 		{
 			if (g)
@@ -740,6 +744,8 @@ int replay_steps(ppc_state* s, int k, bool phenotype, double p_divide, double p_
 	s->launches += hit->launches;
 	s->ready_recorded = hit->ready;
 	s->cur ^= k & 1;
+	if (hit->sflip)
+		flip_sorted_positions(s);
 	s->vel_dirty = false;
 	return PPC_OK;
 }
@@ -1014,8 +1020,10 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.sorted, C));
 	try_(alloc(s, v.skey, C));
 	try_(alloc(s, v.spos4, C));
+	try_(alloc(s, v.spos4_next, C));
 	try_(alloc(s, v.sprm4, C));
 	try_(alloc(s, v.sposf, C));
+	try_(alloc(s, v.sposf_next, C));
 	try_(alloc(s, v.sprmf, C));
 	try_(alloc(s, v.safff, C * s->ndefs));
 	try_(alloc(s, v.saff, C * s->ndefs));

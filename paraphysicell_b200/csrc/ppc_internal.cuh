@@ -166,6 +166,12 @@ struct view
 	int32_t* sorted;
 	int32_t* skey;
 	double4* spos4;
+	// the other buffer of the key-ordered positions (double and single
+	// precision): a fused pass that makes the rebuild's entries writes each
+	// agent's new position there at its current place, and the rebuild after
+	// it completes the pair, which then becomes spos4 / sposf
+	double4* spos4_next;
+	float4* sposf_next;
 	double4* sprm4;	// {radius, repulsion, adhesion, bits: def | movable << 32} in sorted order
 	double* saff;	// affinity rows in sorted order
 	// FP32-force form: key-ordered copies in single precision
@@ -224,6 +230,7 @@ struct graph_entry
 {
 	cudaGraphExec_t exec = nullptr;
 	int steps = 0, cur = 0;
+	int sbuf = 0, sflip = 0; // key-ordered position buffer at the start, and whether the steps flip it
 	bool phenotype = false, lead_bin = false, springs = false;
 	bool ready = false; // the last step records ev_ready
 	double pdiv = 0, pdeath = 0;
@@ -263,6 +270,7 @@ struct ppc_state
 	std::vector<ppc::buffer> allocations;
 
 	int cur = 0;				  // which pos4 buffer is current
+	int sbuf = 0;				  // flips with each swap of v.spos4/sposf and their _next buffers
 	bool vel_dirty = false;		  // some movable agent may have a non-zero velocity
 	bool has_springs = false;	  // some agent may have springs
 	bool rates_nonzero = false;	  // some attachment/detachment rate is non-zero
@@ -347,6 +355,8 @@ inline int blocks_for(int64_t n, int threads)
 
 // ---- kernel entry points (ppc_kernels.cu) ----
 int launch_bin(ppc_state* s, bool conditional, bool ready = false, bool produced = false);
+// swaps the key-ordered position buffers (spos4, sposf) with their _next pair
+void flip_sorted_positions(ppc_state* s);
 int launch_neighbors(ppc_state* s);
 int launch_forces(ppc_state* s);
 int launch_membrane(ppc_state* s);

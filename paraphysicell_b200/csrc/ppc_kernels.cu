@@ -6,6 +6,7 @@
 // written in the reference's order. Each kernel cites the reference lines it
 // replaces.
 #include <cuda_runtime.h>
+#include <utility>
 
 #include "../../include/ppc_draws.h"
 #include "ppc_internal.cuh"
@@ -334,7 +335,8 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur, int con
 
 // writes the key-ordered copies of slot s at position t of voxel `key`.
 // Affinity rows of up to four definitions are carried in registers.
-__device__ __forceinline__ void place_agent(const view& v, int cur, int s, int t, int32_t key)
+__device__ __forceinline__ void place_agent(const view& v, int cur, int s, int t, int32_t key, double4* spos4,
+											float4* sposf)
 {
 	if ((unsigned)s >= (unsigned)v.total_cap || (unsigned)t >= (unsigned)v.total_cap)
 	{
@@ -357,7 +359,7 @@ __device__ __forceinline__ void place_agent(const view& v, int cur, int s, int t
 	p.w = rmad * prm.x; // relative_maximum_adhesion_distance * radius
 	v.sorted[t] = s;
 	v.skey[t] = key;
-	v.spos4[t] = p;
+	spos4[t] = p;
 	v.sprm4[t] = make_double4(prm.x, prm.y, prm.z, __longlong_as_double(bits));
 #pragma unroll
 	for (int q = 0; q < 4; q++)
@@ -367,7 +369,7 @@ __device__ __forceinline__ void place_agent(const view& v, int cur, int s, int t
 		v.saff[(int64_t)t * D + q] = v.aff[(int64_t)s * D + q];
 	// single-precision positions relative to the box minimum: the candidate
 	// filter of the fused pass
-	v.sposf[t] = make_float4((float)(p.x - m0), (float)(p.y - m1), (float)(p.z - m2), (float)p.w);
+	sposf[t] = make_float4((float)(p.x - m0), (float)(p.y - m1), (float)(p.z - m2), (float)p.w);
 	if (v.f32)
 	{
 		const int fbits = (int)((uint32_t)(bits & 0xffff) | (uint32_t)((bits >> 32) & 1) << 16
@@ -678,18 +680,25 @@ __global__ void __launch_bounds__(kPlaceThreads) k_bin_order(view v)
 	bin_order_tile<kPlaceThreads>(v, blockIdx.x, sm);
 }
 
-// The key-ordered copies of the agent at position t of the new order. Where
-// the agent is new to its position, or fields changed since the last rebuild
-// (copy_full), every field is copied; elsewhere the fields other than the
-// position are those the position already holds, and only the position is.
-__device__ __forceinline__ void bin_copy_agent(const view& v, int cur, int t)
+// The key-ordered copies of the agent at position t of the new order, into
+// the position buffers `spos4` and `sposf` that go with positions pos[cur].
+// Where the agent is new to its position, or fields changed since the last
+// rebuild (copy_full), every field is copied; elsewhere the fields other
+// than the position are those the position already holds, and only the
+// position is, unless the fused pass before the rebuild wrote it there
+// already (`produced`).
+__device__ __forceinline__ void bin_copy_agent(const view& v, int cur, int t, int produced, double4* spos4,
+											   float4* sposf)
 {
 	if (t >= *v.cursor)
 		return;
+	const bool fresh = *v.copy_full || v.tfresh[t];
+	if (!fresh && produced)
+		return;
 	const int s = v.sorted[t];
-	if (*v.copy_full || v.tfresh[t])
+	if (fresh)
 	{
-		place_agent(v, cur, s, t, v.skey[t]);
+		place_agent(v, cur, s, t, v.skey[t], spos4, sposf);
 		return;
 	}
 	if ((unsigned)s >= (unsigned)v.total_cap)
@@ -699,22 +708,26 @@ __device__ __forceinline__ void bin_copy_agent(const view& v, int cur, int t)
 	}
 	const double4 p = v.pos[cur][s];
 	const rep_info& R = v.reps[rep_of(v, s)];
-	double* q = reinterpret_cast<double*>(v.spos4 + t);
+	double* q = reinterpret_cast<double*>(spos4 + t);
 	q[0] = p.x;
 	q[1] = p.y;
 	q[2] = p.z;
-	float* f = reinterpret_cast<float*>(v.sposf + t);
+	float* f = reinterpret_cast<float*>(sposf + t);
 	f[0] = (float)(p.x - R.mins[0]);
 	f[1] = (float)(p.y - R.mins[1]);
 	f[2] = (float)(p.z - R.mins[2]);
 }
 
-__global__ void __launch_bounds__(kThreads) k_bin_copy(view v, int cur)
+// `produced`: the fused pass before this rebuild wrote the next step's
+// positions into the other buffer pair (spos4_next, sposf_next); the copy
+// completes that pair, which becomes the current one after it.
+__global__ void __launch_bounds__(kThreads) k_bin_copy(view v, int cur, int produced)
 {
 	grid_wait();
 	if (!*v.bin_active)
 		return;
-	bin_copy_agent(v, cur, blockIdx.x * blockDim.x + threadIdx.x);
+	bin_copy_agent(v, cur, blockIdx.x * blockDim.x + threadIdx.x, produced, produced ? v.spos4_next : v.spos4,
+				   produced ? v.sposf_next : v.sposf);
 }
 
 // ---------------------------------------------------------------------------
@@ -786,13 +799,19 @@ __device__ __forceinline__ int axis_coord_quiet(double x, const rep_info& R, int
 // mover chain with the tiles' changes. Valid while no agent is removed
 // before the rebuild; the compaction plan discards it otherwise.
 __device__ __forceinline__ void produce_entry(const view& v, const rep_info& R, int t, int s, int32_t okey,
-											  const double4& p)
+											  const double4& p, double pw)
 {
 	const int c0 = axis_coord_quiet(p.x, R, 0);
 	const int c1 = v.dims >= 2 ? axis_coord_quiet(p.y, R, 1) : 0;
 	const int c2 = v.dims >= 3 ? axis_coord_quiet(p.z, R, 2) : 0;
 	const int32_t key = (int32_t)(R.vox_base + c0 + (int64_t)R.grid[0] * (c1 + (int64_t)R.grid[1] * c2));
 	v.key[s] = key;
+	// the agent's key-ordered position for the next step, at its place in
+	// the current order: the rebuild's copy keeps it wherever the agent keeps
+	// its place (the fused pass reads the other buffer)
+	v.spos4_next[t] = make_double4(p.x, p.y, p.z, pw);
+	v.sposf_next[t] = make_float4((float)(p.x - R.mins[0]), (float)(p.y - R.mins[1]), (float)(p.z - R.mins[2]),
+								  (float)pw);
 	const int sh = v.tshift;
 	if ((key >> sh) == (okey >> sh))
 		v.porder[t] = make_int2(s, key);
@@ -1872,7 +1891,7 @@ __device__ __forceinline__ void agent_finish(const view& v, int cur, int opts, i
 	if (to_remove<DIMS>(R, p, flag))
 		append_bad(v, r, s - R.base);
 	if (opts & FUSED_PRODUCE)
-		produce_entry(v, R, t, s, key, p);
+		produce_entry(v, R, t, s, key, p, pi.w);
 }
 
 // the agent at key-ordered position t, with its block's shared slots `sm`
@@ -3681,7 +3700,7 @@ __global__ void __launch_bounds__(kPersistThreads) k_step_persistent(view v, int
 	if (!grid_barrier(v, pa.bar, pa.limit))
 		return;
 	for (int t0 = blockIdx.x * kPersistThreads; t0 < v.total_cap; t0 += nb * kPersistThreads)
-		bin_copy_agent(v, nxt, t0 + threadIdx.x);
+		bin_copy_agent(v, nxt, t0 + threadIdx.x, 0, v.spos4, v.sposf);
 }
 
 } // namespace
@@ -3715,6 +3734,13 @@ static void pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStr
 			return cuda_fail(e_, __func__);                                                                            \
 	} while (0)
 
+void flip_sorted_positions(ppc_state* s)
+{
+	std::swap(s->v.spos4, s->v.spos4_next);
+	std::swap(s->v.sposf, s->v.sposf_next);
+	s->sbuf ^= 1;
+}
+
 // `ready`: record ev_ready after the count, the last kernel of the step
 // that changes agent fields (it applies the compaction's moves), so that a
 // download can run beside the rest of the rebuild
@@ -3742,8 +3768,10 @@ int launch_bin(ppc_state* s, bool conditional, bool ready, bool produced)
 	}
 	s->ready_recorded = ready;
 	pdl(k_bin_order, s->v.ntiles, kPlaceThreads, 0, PPC_LAUNCH(s), s->v);
-	pdl(k_bin_copy, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
+	pdl(k_bin_copy, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur, produced ? 1 : 0);
 	PPC_CHECK_LAUNCH();
+	if (produced)
+		flip_sorted_positions(s);
 	return PPC_OK;
 }
 
