@@ -66,15 +66,19 @@ def phenotype_args(name):
     return (wl.P_DIVIDE, wl.P_DEATH) if name == "config5" else None
 
 
-def algorithmic_bytes_per_agent(dims, ndefs, walls, springs_per_agent, spring_agents_fraction):
+def algorithmic_bytes_per_agent(dims, ndefs, walls, springs_per_agent, spring_agents_fraction, produces=False):
     """Bytes the fused force pass must move per agent: reads of position,
     previous velocity, the four pair parameters (radius, repulsion,
     adhesion, rmad), the BM strength when walls are on, the affinity row,
     definition index and movable flag; writes of position, previous velocity
-    and pressure; spring rows (count, elastic constant, partner indices)."""
+    and pressure; spring rows (count, elastic constant, partner indices).
+    `produces`: the pass also does the mesh rebuild's per-agent work (launch
+    shapes -3 and -4 in a step without the phenotype update) and writes the
+    agent's voxel key (4 B), its entry of the order (8 B) and its next
+    key-ordered position in double and single precision (32 + 16 B)."""
     s = 8
     reads = 8 * dims + 8 * dims + 4 * s + (s if walls else 0) + s * ndefs + 4 + 1
-    writes = 8 * dims + 8 * dims + s
+    writes = 8 * dims + 8 * dims + s + (4 + 8 + 32 + 16 if produces else 0)
     springs = 4 + spring_agents_fraction * s + 4 * springs_per_agent
     return reads + writes + springs
 
@@ -749,7 +753,8 @@ def run_ours(args, rank, world, local_rank):
         peak_src = "fallback"
     spring_counts = a.arrays["spring_counts"][:n0]
     per_agent = algorithmic_bytes_per_agent(a.dims, a.ndefs, bool(params.virtual_wall_at_domain_edges),
-                                            float(spring_counts.mean()), float((spring_counts > 0).mean()))
+                                            float(spring_counts.mean()), float((spring_counts > 0).mean()),
+                                            produces=shape[0] in (-3, -4) and ph is None)
     fused_avg_ms = fused_ms / max(fused_launches, 1)
     achieved = (per_agent * n0) / (fused_avg_ms / 1e3) / 1e9
     traffic = None

@@ -333,10 +333,10 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(view v, int cur, int con
 	bin_count_body(v, cur, t);
 }
 
-// writes the key-ordered copies of slot s at position t of voxel `key`.
-// Affinity rows of up to four definitions are carried in registers.
-__device__ __forceinline__ void place_agent(const view& v, int cur, int s, int t, int32_t key, double4* spos4,
-											float4* sposf)
+// writes the key-ordered copies of slot s at position t (its entries of
+// sorted and skey are the order's). Affinity rows of up to four definitions
+// are carried in registers.
+__device__ __forceinline__ void place_agent(const view& v, int cur, int s, int t, double4* spos4, float4* sposf)
 {
 	if ((unsigned)s >= (unsigned)v.total_cap || (unsigned)t >= (unsigned)v.total_cap)
 	{
@@ -357,8 +357,6 @@ __device__ __forceinline__ void place_agent(const view& v, int cur, int s, int t
 	const rep_info& R = v.reps[r];
 	const double m0 = R.mins[0], m1 = R.mins[1], m2 = R.mins[2];
 	p.w = rmad * prm.x; // relative_maximum_adhesion_distance * radius
-	v.sorted[t] = s;
-	v.skey[t] = key;
 	spos4[t] = p;
 	v.sprm4[t] = make_double4(prm.x, prm.y, prm.z, __longlong_as_double(bits));
 #pragma unroll
@@ -486,16 +484,27 @@ __device__ __forceinline__ void bin_order_tile(const view& v, int b, place_smem&
 	const int sh = v.tshift;
 	const int k0 = b << sh;
 	const int nv = min(1 << sh, v.nvox - k0);
+	// the loads the tile's start, size and chains need, issued together:
+	// the start is the previous start plus the changes of the tiles before,
+	// four of them loaded at once per thread
 	const bool ordered = *v.order_valid != 0;
-	// the start: the previous start plus the changes of the tiles before
+	const int2 tp0 = v.tprev[b];
+	const int db = v.tdelta[b];
+	const int chain = tid < kChains ? v.chead[(int64_t)b * kChains + tid] : -1;
 	int part = 0;
 	const int sb = b >> kSuperShift;
 	for (int j = tid; j < sb; j += THREADS)
 		part += v.sdelta[j];
-	for (int k = (sb << kSuperShift) + tid; k < b; k += THREADS)
-		part += v.tdelta[k];
-	const int2 tp = ordered ? v.tprev[b] : make_int2(0, 0);
-	const int L = tp.y + v.tdelta[b];
+	for (int k = (sb << kSuperShift) + tid; k < b; k += 4 * THREADS)
+	{
+		const int x0 = v.tdelta[k];
+		const int x1 = k + THREADS < b ? v.tdelta[k + THREADS] : 0;
+		const int x2 = k + 2 * THREADS < b ? v.tdelta[k + 2 * THREADS] : 0;
+		const int x3 = k + 3 * THREADS < b ? v.tdelta[k + 3 * THREADS] : 0;
+		part += x0 + x1 + x2 + x3;
+	}
+	const int2 tp = ordered ? tp0 : make_int2(0, 0);
+	const int L = tp.y + db;
 	if (L > 0)
 	{
 		int4* c4 = reinterpret_cast<int4*>(sm.cnt);
@@ -542,11 +551,10 @@ __device__ __forceinline__ void bin_order_tile(const view& v, int b, place_smem&
 								lv | (i + 1 < kPrevLimit ? (i + 1) << kVoxelBits : 0));
 			}
 		}
-	if (tid < kChains)
+	if (tid < kChains && chain >= 0)
 	{
-		int* head = v.chead + (int64_t)b * kChains + tid;
-		int q = *head;
-		*head = -1;
+		v.chead[(int64_t)b * kChains + tid] = -1;
+		int q = chain;
 		for (int hops = 0; q >= 0; hops++)
 		{
 			if (!fits || L <= 0 || hops >= v.total_cap || q >= v.total_cap)
@@ -687,18 +695,26 @@ __global__ void __launch_bounds__(kPlaceThreads) k_bin_order(view v)
 // than the position are those the position already holds, and only the
 // position is, unless the fused pass before the rebuild wrote it there
 // already (`produced`).
+// `active`: the rebuild runs (bin_active), loaded with the rest.
 __device__ __forceinline__ void bin_copy_agent(const view& v, int cur, int t, int produced, double4* spos4,
-											   float4* sposf)
+											   float4* sposf, const int32_t* active)
 {
-	if (t >= *v.cursor)
+	if (t >= v.total_cap)
 		return;
-	const bool fresh = *v.copy_full || v.tfresh[t];
+	// the loads the decision needs, issued together before any branch
+	const int on = active ? *active : 1;
+	const int n = *v.cursor;
+	const int full = *v.copy_full;
+	const int fresh_t = v.tfresh[t];
+	const int s = v.sorted[t];
+	if (!on || t >= n)
+		return;
+	const bool fresh = full || fresh_t;
 	if (!fresh && produced)
 		return;
-	const int s = v.sorted[t];
 	if (fresh)
 	{
-		place_agent(v, cur, s, t, v.skey[t], spos4, sposf);
+		place_agent(v, cur, s, t, spos4, sposf);
 		return;
 	}
 	if ((unsigned)s >= (unsigned)v.total_cap)
@@ -724,10 +740,8 @@ __device__ __forceinline__ void bin_copy_agent(const view& v, int cur, int t, in
 __global__ void __launch_bounds__(kThreads) k_bin_copy(view v, int cur, int produced)
 {
 	grid_wait();
-	if (!*v.bin_active)
-		return;
 	bin_copy_agent(v, cur, blockIdx.x * blockDim.x + threadIdx.x, produced, produced ? v.spos4_next : v.spos4,
-				   produced ? v.sposf_next : v.sposf);
+				   produced ? v.sposf_next : v.sposf, v.bin_active);
 }
 
 // ---------------------------------------------------------------------------
@@ -3700,7 +3714,7 @@ __global__ void __launch_bounds__(kPersistThreads) k_step_persistent(view v, int
 	if (!grid_barrier(v, pa.bar, pa.limit))
 		return;
 	for (int t0 = blockIdx.x * kPersistThreads; t0 < v.total_cap; t0 += nb * kPersistThreads)
-		bin_copy_agent(v, nxt, t0 + threadIdx.x, 0, v.spos4, v.sposf);
+		bin_copy_agent(v, nxt, t0 + threadIdx.x, 0, v.spos4, v.sposf, nullptr);
 }
 
 } // namespace
