@@ -336,7 +336,7 @@ int transfer_in(ppc_state* s, int32_t r, const ppc_agents* a, bool defaults)
 	// an upload of kinematic fields only (positions, velocities, previous
 	// velocities, pressure, orientation) keeps the mesh when the positions it
 	// brings are bit-identical to the resident ones
-	// (pos_changed is zero after every rebuild: its last tile clears it)
+	// (pos_changed is zero after every rebuild: its copy kernel clears it)
 	const bool kinematic = !defaults && only_kinematic(a);
 	s->ready_pending = false;
 	bool pinned = true;
@@ -995,7 +995,6 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.chead, (size_t)v.ntiles * 32));
 	try_(alloc(s, v.cnext, C));
 	try_(alloc(s, v.porder, C));
-	try_(alloc(s, v.tdone, 1));
 	try_(alloc(s, v.tfresh, C));
 	try_(alloc(s, v.params_changed, 1));
 	try_(alloc(s, v.copy_full, 1));

@@ -147,7 +147,6 @@ struct view
 	int32_t* chead;		// [ntiles * 32] heads of the tiles' mover chains (-1: empty)
 	int32_t* cnext;		// [C] next slot of a mover chain
 	int2* porder;		// [C] entries of the previous order: (slot, key) of agents kept in their tile
-	unsigned* tdone;	// tiles placed by the current rebuild
 	uint8_t* tfresh;	// [C] 1 where the agent at a position of the key order is new to it
 	int32_t* params_changed; // fields other than positions, or slots' agents, changed since the last rebuild
 	int32_t* copy_full;	// the current rebuild's k_bin_copy copies every field of every agent

@@ -388,7 +388,7 @@ struct __align__(16) place_smem
 	int2 list[kPlaceList];			 // the tile's agents: (slot, voxel inside the tile | previous index << 12)
 	int32_t group[kPlaceList];		 // slots grouped by voxel
 	int32_t wtot[32];				 // per-warp totals of the voxel scan
-	int32_t n, last;
+	int32_t n;
 };
 
 constexpr int kVoxelBits = 12;				   // bits of a list item's voxel inside the tile
@@ -474,11 +474,12 @@ __device__ __forceinline__ void place_scan(place_smem& sm, int nv)
 
 // Orders tile b of the new order (see above): the voxel starts in vstart,
 // sorted, skey and tfresh (1 where a position's agent is new to it) over the
-// tile's range, its entry of tprev. The tile whose ordering completes last
-// readies the counters for the next rebuild; the key-ordered copies of the
-// agents' fields follow in k_bin_copy.
+// tile's range, its entry of tprev. The key-ordered copies of the agents'
+// fields follow in k_bin_copy, which also readies the counters for the next
+// rebuild (bin_finish).
+// `on`: the rebuild runs (bin_active; the same for the whole block).
 template <int THREADS>
-__device__ __forceinline__ void bin_order_tile(const view& v, int b, place_smem& sm)
+__device__ __forceinline__ void bin_order_tile(const view& v, int b, place_smem& sm, int on)
 {
 	const int tid = threadIdx.x, lane = tid & 31;
 	const int sh = v.tshift;
@@ -503,6 +504,8 @@ __device__ __forceinline__ void bin_order_tile(const view& v, int b, place_smem&
 		const int x3 = k + 3 * THREADS < b ? v.tdelta[k + 3 * THREADS] : 0;
 		part += x0 + x1 + x2 + x3;
 	}
+	if (!on)
+		return;
 	const int2 tp = ordered ? tp0 : make_int2(0, 0);
 	const int L = tp.y + db;
 	if (L > 0)
@@ -644,38 +647,11 @@ __device__ __forceinline__ void bin_order_tile(const view& v, int b, place_smem&
 			v.tprev[b] = make_int2(base, n);
 	}
 
-	// the tile completing last readies the counters of the next rebuild
-	__syncthreads();
-	if (tid == 0)
-	{
-		__threadfence();
-		sm.last = atomicAdd(v.tdone, 1u) == (unsigned)v.ntiles - 1;
-	}
-	__syncthreads();
-	if (sm.last)
-	{
-		__threadfence();
-		const int nsup = (v.ntiles + (1 << kSuperShift) - 1) >> kSuperShift;
-		for (int k = tid; k < v.ntiles; k += THREADS)
-			v.tdelta[k] = 0;
-		for (int k = tid; k < nsup; k += THREADS)
-			v.sdelta[k] = 0;
-		for (int k = tid; k < v.nreps; k += THREADS)
-			v.binned[k] = v.ctr[k].count; // the slots this rebuild's order lists
-		if (tid == 0)
-		{
-			// k_bin_copy writes every field where agents' fields or slots
-			// changed since the last rebuild, elsewhere only the positions
-			*v.copy_full = (*v.params_changed != 0 || !ordered) ? 1 : 0;
-			*v.params_changed = 0;
-			*v.recount = 0;
-			*v.tdone = 0;
-			*v.order_valid = 1;
-			*v.moves_pending = 0; // applied by this rebuild's count
-			*v.appended = 0;	  // counted by it too
-			*v.pos_changed = 0;
-		}
-	}
+	// k_bin_copy writes every field where agents' fields or slots changed
+	// since the last rebuild, elsewhere only the positions; the flags read
+	// here are reset after the order is complete (bin_finish)
+	if (b == 0 && tid == 0)
+		*v.copy_full = (*v.params_changed != 0 || !ordered) ? 1 : 0;
 	__syncthreads(); // shared memory is reused by the next tile of a persistent block
 }
 
@@ -683,9 +659,7 @@ __global__ void __launch_bounds__(kPlaceThreads) k_bin_order(view v)
 {
 	__shared__ place_smem sm;
 	grid_wait();
-	if (!*v.bin_active)
-		return;
-	bin_order_tile<kPlaceThreads>(v, blockIdx.x, sm);
+	bin_order_tile<kPlaceThreads>(v, blockIdx.x, sm, *v.bin_active);
 }
 
 // The key-ordered copies of the agent at position t of the new order, into
@@ -695,14 +669,37 @@ __global__ void __launch_bounds__(kPlaceThreads) k_bin_order(view v)
 // than the position are those the position already holds, and only the
 // position is, unless the fused pass before the rebuild wrote it there
 // already (`produced`).
-// `active`: the rebuild runs (bin_active), loaded with the rest.
+// The counters and flags of the next rebuild, once this one's order is
+// complete (nothing in the copy reads them): tile changes, the slots the
+// order lists per replicate, and the flags the count and the order read.
+// Thread `i` of `n` in the grid.
+__device__ __forceinline__ void bin_finish(const view& v, int i, int n)
+{
+	const int nsup = (v.ntiles + (1 << kSuperShift) - 1) >> kSuperShift;
+	for (int k = i; k < v.ntiles; k += n)
+		v.tdelta[k] = 0;
+	for (int k = i; k < nsup; k += n)
+		v.sdelta[k] = 0;
+	for (int k = i; k < v.nreps; k += n)
+		v.binned[k] = v.ctr[k].count; // the slots this rebuild's order lists
+	if (i == 0)
+	{
+		*v.params_changed = 0;
+		*v.recount = 0;
+		*v.order_valid = 1;
+		*v.moves_pending = 0; // applied by this rebuild's count
+		*v.appended = 0;	  // counted by it too
+		*v.pos_changed = 0;
+	}
+}
+
+// `on`: the rebuild runs (bin_active).
 __device__ __forceinline__ void bin_copy_agent(const view& v, int cur, int t, int produced, double4* spos4,
-											   float4* sposf, const int32_t* active)
+											   float4* sposf, int on)
 {
 	if (t >= v.total_cap)
 		return;
 	// the loads the decision needs, issued together before any branch
-	const int on = active ? *active : 1;
 	const int n = *v.cursor;
 	const int full = *v.copy_full;
 	const int fresh_t = v.tfresh[t];
@@ -740,8 +737,11 @@ __device__ __forceinline__ void bin_copy_agent(const view& v, int cur, int t, in
 __global__ void __launch_bounds__(kThreads) k_bin_copy(view v, int cur, int produced)
 {
 	grid_wait();
-	bin_copy_agent(v, cur, blockIdx.x * blockDim.x + threadIdx.x, produced, produced ? v.spos4_next : v.spos4,
-				   produced ? v.sposf_next : v.sposf, v.bin_active);
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	const int on = *v.bin_active;
+	bin_copy_agent(v, cur, t, produced, produced ? v.spos4_next : v.spos4, produced ? v.sposf_next : v.sposf, on);
+	if (on)
+		bin_finish(v, t, gridDim.x * blockDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -3710,11 +3710,12 @@ __global__ void __launch_bounds__(kPersistThreads) k_step_persistent(view v, int
 	if (!grid_barrier(v, pa.bar, pa.limit))
 		return;
 	for (int b = blockIdx.x; b < v.ntiles; b += nb)
-		bin_order_tile<kPersistThreads>(v, b, *reinterpret_cast<place_smem*>(smem));
+		bin_order_tile<kPersistThreads>(v, b, *reinterpret_cast<place_smem*>(smem), 1);
 	if (!grid_barrier(v, pa.bar, pa.limit))
 		return;
 	for (int t0 = blockIdx.x * kPersistThreads; t0 < v.total_cap; t0 += nb * kPersistThreads)
-		bin_copy_agent(v, nxt, t0 + threadIdx.x, 0, v.spos4, v.sposf, nullptr);
+		bin_copy_agent(v, nxt, t0 + threadIdx.x, 0, v.spos4, v.sposf, 1);
+	bin_finish(v, blockIdx.x * kPersistThreads + threadIdx.x, nb * kPersistThreads);
 }
 
 } // namespace
