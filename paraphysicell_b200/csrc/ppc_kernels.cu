@@ -2208,6 +2208,7 @@ struct queue_warp
 	int2 rows[9][32];		   // per agent and stencil row: first candidate number, array position - number
 	int32_t first[33];		   // each agent's first candidate in the warp's list; first[32]: the total
 	int32_t t[32];			   // the agents' key-ordered positions (-1: no agent)
+	int32_t key[32], slot[32]; // the agents' voxel keys and slots
 	float margin[32];		   // the agents' filter margins
 	float4 pf[32];			   // single-precision positions
 	double4 pi[32], qi[32];	   // FP64 positions and parameter rows
@@ -2494,6 +2495,8 @@ __device__ __forceinline__ void fused_queue_agent(const view& v, int cur, int op
 	if (lane == 31)
 		w.first[32] = total;
 	w.t[lane] = act ? t : -1;
+	w.key[lane] = key;
+	w.slot[lane] = s;
 	w.margin[lane] = R.fmargin;
 	w.pf[lane] = pf;
 	w.pi[lane] = pi;
@@ -2576,7 +2579,12 @@ __device__ __forceinline__ void fused_queue_agent(const view& v, int cur, int op
 		vz = vz + fz.value();
 		pressure = fp.value();
 	}
-	agent_finish<DIMS>(v, cur, opts, t, key, s, r, R, pi, qi.x, def_i, mov_i, nspr, vx, vy, vz, pressure);
+	// the agent's FP64 rows from the warp's shared copies, so that none of
+	// them occupies registers through the scan
+	const double4 pi_own = w.pi[lane];
+	const double radius = w.qi[lane].x;
+	agent_finish<DIMS>(v, cur, opts, t, w.key[lane], w.slot[lane], r, R, pi_own, radius, def_i, mov_i, nspr, vx, vy,
+					   vz, pressure);
 }
 
 template <int DIMS, bool F32>
