@@ -201,7 +201,10 @@ int ppc_set_launch_shape(ppc_state* s, int32_t tile_edge, int32_t threads, int32
 enum ppc_step_form
 {
 	PPC_STEP_KERNELS = 0,	 /* the default: the fused pass, the compaction plan and
-								the two mesh-rebuild kernels, four launches */
+								the three mesh-rebuild kernels (count, order,
+								copy); a single simulation's step without the
+								phenotype update runs the plan in the fused
+								pass's last block: four launches */
 	PPC_STEP_PERSISTENT = 1	 /* one cooperative launch: the same phases over all
 								replicates, separated by grid barriers */
 };
