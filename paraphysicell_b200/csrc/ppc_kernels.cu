@@ -2923,6 +2923,7 @@ __device__ void compact_plan_rep(const view& v, int r, int phenotype_pass, int s
 	int cnt = cnt0;
 	int ti = nb - 1, nm = 0;
 	int64_t deaths = 0;
+	bool counts_changed = false; // some partner's spring count changed
 	int32_t* moves = v.moves + 2 * (int64_t)base;
 	for (int bi = 0; bi < nb; bi++)
 	{
@@ -2936,6 +2937,7 @@ __device__ void compact_plan_rep(const view& v, int r, int phenotype_pass, int s
 			const int last = cnt - 1;
 			if (springs)
 			{
+				counts_changed = counts_changed || v.scnt[base + h] > 0;
 				springs_remove_attached(v, base + h);
 				if (last != h)
 				{
@@ -2973,6 +2975,9 @@ __device__ void compact_plan_rep(const view& v, int r, int phenotype_pass, int s
 	}
 	C.count = cnt;
 	C.deaths += deaths;
+	// the partners' key-ordered rows carry their spring counts
+	if (counts_changed)
+		*v.params_changed = 1;
 	C.nbad = 0;
 	v.nmoves[r] = nm;
 }

@@ -120,8 +120,8 @@ def test_fused_steps_match_oracle(case):
 # -1 is one thread per agent with its own pair code; -2 spreads the pair
 # code over the warp; 0 does that with each block's candidate ranges staged
 # in shared memory, and a budget of 4 KiB leaves no room for them, so blocks
-# read the global arrays instead; -3 (the default) fetches each thread's
-# candidates in batches; -4 shares the warp's candidates out over its lanes.
+# read the global arrays instead; -3 fetches each thread's candidates in
+# batches; -4 (the default) shares the warp's candidates out over its lanes.
 SHAPES = [(-1, 128, 0), (-1, 256, 0), (-2, 128, 0), (-2, 64, 0), (0, 128, 32 * 1024), (0, 128, 40 * 1024),
           (0, 64, 4 * 1024), (0, 96, 24 * 1024), (-3, 128, 0), (-4, 128, 0)]
 
@@ -500,3 +500,33 @@ def test_removals_inside_fused_steps(shape):
     assert gu.fetch(d, a).count < a.count - 5
     gu.assert_same_bins(d, o)
     gu.assert_same_neighbors(d, o)
+
+
+@pytest.mark.parametrize("shape", [(-4, 128, 0), (-3, 128, 0), (-2, 128, 0)], ids=lambda s: "edge%d" % s[0])
+def test_removed_tail_agent_releases_its_partners_springs(shape):
+    """An agent with springs removed from the last slot, so that no agent
+    moves into its hole: only its partners' spring rows and counts change,
+    and the next fused passes must read the new counts (the reference's
+    remove_attached, containers_solver.cpp:58-68)."""
+    mesh, params, a = wl.scaled(wl.config3, 2000, seed=61)
+    n = a.count
+    tail = n - 1
+    lists = [[j for j in lst if j != tail] for lst in a.spring_lists()]
+    partners = [i for i in range(n - 1) if len(lists[i]) < a.spring_capacity - 1][:3]
+    lists[tail] = partners
+    for p in partners:
+        lists[p].append(tail)
+    a.set_springs(lists)
+    a.arrays["flags"][tail] = FLAG_TO_REMOVE
+    o, d = gu.make_pair(mesh, params, a)
+    d.set_launch_shape(*shape)
+    o.update_mechanics_mesh()
+    o.update_cell_neighbors()
+    d.update_mechanics_mesh()
+    for k in (1, 1, 5):
+        o.step(k, 0, 0.0, 0.0)
+        d.step(k)
+        go, gd = gu.fetch(o, a), gu.fetch(d, a)
+        assert gd.count == go.count == n - 1
+        assert gd.spring_lists() == go.spring_lists()
+        gu.assert_same_state(gd, go)
