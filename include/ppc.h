@@ -202,9 +202,7 @@ enum ppc_step_form
 {
 	PPC_STEP_KERNELS = 0,	 /* the default: the fused pass, the compaction plan and
 								the three mesh-rebuild kernels (count, order,
-								copy); a single simulation's step without the
-								phenotype update runs the plan in the fused
-								pass's last block: four launches */
+								copy), five launches */
 	PPC_STEP_PERSISTENT = 1	 /* one cooperative launch: the same phases over all
 								replicates, separated by grid barriers */
 };
@@ -406,7 +404,10 @@ int ppc_update_basement_membrane_interactions(ppc_state* s);
  * a replicate is uniform(seed, n, replicate, i, k) — in the reference's
  * serial order and capacity checks, then spring contraction. Needs the
  * neighbour lists (computed here if stale). ppc_step takes the same route
- * (through these separate entry points) while any rate is non-zero. */
+ * (through these separate entry points) while any rate is non-zero. The
+ * attachment candidates of one update (agent-neighbour pairs whose draw
+ * succeeds) are listed in a buffer of the replicate's capacity; more return
+ * PPC_ERR_CAPACITY. */
 int ppc_update_spring_attachments(ppc_state* s);
 
 /* position_solver::update_positions (reference: src/solver/host/position_solver.cpp:481-520). */

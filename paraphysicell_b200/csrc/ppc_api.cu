@@ -627,16 +627,11 @@ int enqueue_step(ppc_state* s, bool phenotype, double p_divide, double p_death, 
 	// in a step without the phenotype update the fused passes -3 and -4 also
 	// make the count's entries, which hold unless the compaction removes agents
 	const bool produce = !phenotype && (s->flat || s->queue);
-	// a single simulation's compaction plan then runs in the pass's last block
-	const bool plan_in_fused = produce && s->nreps == 1;
 	s->produce = produce;
-	s->plan_in_fused = plan_in_fused;
 	const int rc_fused = launch_fused(s);
 	s->produce = false;
-	s->plan_in_fused = false;
 	PPC_TRY(rc_fused);
-	if (!plan_in_fused)
-		PPC_TRY(launch_compact(s, false, !phenotype, produce));
+	PPC_TRY(launch_compact(s, false, !phenotype, produce));
 	if (phenotype)
 	{
 		PPC_TRY(launch_flag_by_draws(s, p_divide, p_death));
@@ -999,7 +994,6 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.params_changed, 1));
 	try_(alloc(s, v.copy_full, 1));
 	try_(alloc(s, v.recount, 1));
-	try_(alloc(s, v.fdone, 1));
 	if (rc == PPC_OK && cudaMemset(v.chead, 0xff, sizeof(int32_t) * (size_t)v.ntiles * 32) != cudaSuccess)
 		rc = fail(PPC_ERR_CUDA, "cudaMemset failed");
 	try_(alloc(s, v.order_valid, 1));

@@ -151,7 +151,6 @@ struct view
 	int32_t* params_changed; // fields other than positions, or slots' agents, changed since the last rebuild
 	int32_t* copy_full;	// the current rebuild's k_bin_copy copies every field of every agent
 	int32_t* recount;	// the compaction removed agents: the rebuild's count recomputes every entry
-	unsigned* fdone;	// blocks of the fused pass done (the last one runs the compaction plan)
 	int32_t* order_valid; // 1 once a rebuild has set `sorted` (cleared by uploads)
 	int32_t* binned;	  // [replicates] live count at the last rebuild (the slots `sorted` lists)
 	int32_t* move_src;	  // [C] tail slot whose agent the next k_bin_count moves into this hole, or -1
@@ -318,7 +317,6 @@ struct ppc_state
 	bool flat = false; // per-thread pass with batched candidate fetches (shape -3)
 	bool queue = true; // per-thread pass with the warp's candidates shared out (shape -4, the default)
 	bool produce = false; // the fused pass being launched makes the rebuild's entries (FUSED_PRODUCE)
-	bool plan_in_fused = false; // ...and its last block runs the compaction plan (FUSED_PLAN)
 	bool persistent = false;		 // mechanics steps as one cooperative launch each (PPC_STEP_PERSISTENT)
 	long long wait_limit = 1LL << 25; // polls of a bounded device wait before it gives up
 	bool lost = false;				 // a bounded wait gave up: the state needs a fresh upload

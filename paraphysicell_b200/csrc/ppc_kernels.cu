@@ -759,38 +759,8 @@ enum : int
 	FUSED_WALLS = 1,
 	FUSED_SPRINGS = 2,
 	FUSED_VEL = 4,
-	FUSED_PRODUCE = 8, // the pass does the rebuild count's work for its agents (shapes -3 and -4)
-	FUSED_PLAN = 16,   // the block finishing last runs the compaction plan (one replicate)
-	FUSED_PLAN_SPRINGS = 32 // ...which renames spring partners
+	FUSED_PRODUCE = 8 // the pass does the rebuild count's work for its agents (shapes -3 and -4)
 };
-
-__device__ void compact_plan_rep(const view& v, int r, int phenotype_pass, int springs, int fold, int produced,
-								 int32_t* sh);
-
-// With FUSED_PLAN the block that finishes the fused pass last runs the
-// compaction plan of the (single) replicate, which then needs no launch of
-// its own: the plan reads only what the whole pass has written (the removal
-// candidates), and the last block to arrive sees every block's writes.
-// `sort` is the block's shared memory, free once its agents are done.
-__device__ __forceinline__ void fused_plan_tail(const view& v, int opts, int32_t* sort)
-{
-	if (!(opts & FUSED_PLAN))
-		return;
-	__shared__ int s_last;
-	__syncthreads();
-	if (threadIdx.x == 0)
-	{
-		__threadfence();
-		s_last = atomicAdd(v.fdone, 1u) == gridDim.x - 1;
-	}
-	__syncthreads();
-	if (!s_last)
-		return;
-	__threadfence();
-	compact_plan_rep(v, 0, 0, (opts & FUSED_PLAN_SPRINGS) ? 1 : 0, 1, (opts & FUSED_PRODUCE) ? 1 : 0, sort);
-	if (threadIdx.x == 0)
-		*v.fdone = 0;
-}
 
 // the voxel coordinate of axis_coord without its error reports: the keys the
 // fused pass computes for the rebuild are recomputed (with the reports) by
@@ -2181,7 +2151,6 @@ __global__ void __launch_bounds__(kFlatThreads, 5) k_fused_flat(view v, int cur,
 	extern __shared__ __align__(16) unsigned char flat_raw[];
 	fused_flat_agent<DIMS, F32>(v, cur, opts, blockIdx.x * kFlatThreads + threadIdx.x,
 								*reinterpret_cast<flat_smem*>(flat_raw));
-	fused_plan_tail(v, opts, reinterpret_cast<int32_t*>(flat_raw));
 }
 
 // ---------------------------------------------------------------------------
@@ -2595,7 +2564,6 @@ __global__ void __launch_bounds__(kQueueThreads, 5) k_fused_queue(view v, int cu
 	extern __shared__ __align__(16) unsigned char queue_raw[];
 	queue_smem& sm = *reinterpret_cast<queue_smem*>(queue_raw);
 	fused_queue_agent<DIMS, F32>(v, cur, opts, blockIdx.x * kQueueThreads + threadIdx.x, sm.w[threadIdx.x >> 5]);
-	fused_plan_tail(v, opts, reinterpret_cast<int32_t*>(queue_raw));
 }
 
 // ---------------------------------------------------------------------------
@@ -3151,12 +3119,34 @@ __global__ void k_spring_attach_draws(view v)
 // Up to kAttachCap candidates the block stages them in shared memory: each
 // endpoint's agent, maximum and row length, and the first endpoint of the
 // list that names the same agent (found with a per-slot atomicMin), whose
-// count slot all its endpoints share;
-// the in-order pass then touches only shared memory apart from the row
-// writes. Longer lists take the same pass over global memory.
+// count slot all its endpoints share; the candidates then settle in waves
+// that touch only shared memory apart from the row writes. Longer lists take
+// the serial pass over global memory.
 constexpr int kAttachCap = 4096;
 constexpr int kAttachThreads = 1024;
-constexpr size_t kAttachSmem = (size_t)kAttachCap * (2 * 4 + 2 * 4 + 2 * 2 + 2 * 2) + (size_t)kAttachCap * 4;
+constexpr int kAttachWaves = 32; // parallel waves before the remaining candidates go in order
+constexpr size_t kAttachSmem = (size_t)kAttachCap * (2 * 4 + 2 * 4 + 2 * 4 + 2 * 2 + 2 * 2) + (size_t)kAttachCap * 4;
+
+// candidate q (endpoints 2q, 2q+1) against the row lengths kept at each
+// agent's first endpoint: attached while both rows are below their maximum
+__device__ __forceinline__ void attach_settle(const view& v, const int32_t* agent, int32_t* cnt, const int16_t* mx,
+											  const int16_t* rep, int q)
+{
+	const int ri = rep[2 * q], rj = rep[2 * q + 1];
+	const int ni = cnt[ri], nj = cnt[rj];
+	if (!(ni < mx[2 * q] && nj < mx[2 * q + 1]))
+		return;
+	if (ni >= v.scap || nj >= v.scap)
+	{
+		atomicOr(v.err, ERR_SPRING_CAPACITY);
+		return;
+	}
+	const int i = agent[2 * q], j = agent[2 * q + 1];
+	v.springs[(int64_t)i * v.scap + ni] = j;
+	v.springs[(int64_t)j * v.scap + nj] = i;
+	cnt[ri] = ni + 1;
+	cnt[rj] = nj + 1;
+}
 
 __global__ void __launch_bounds__(kAttachThreads) k_spring_attach_apply(view v)
 {
@@ -3165,7 +3155,8 @@ __global__ void __launch_bounds__(kAttachThreads) k_spring_attach_apply(view v)
 	int32_t* sh = dyn;						   // [kAttachCap] sort buffer
 	int32_t* agent = sh + kAttachCap;		   // [2 cap] endpoint agents (slots): 2q = i, 2q+1 = j
 	int32_t* cnt = agent + 2 * kAttachCap;	   // [2 cap] row length, kept at each agent's first endpoint
-	int16_t* mx = reinterpret_cast<int16_t*>(cnt + 2 * kAttachCap); // [2 cap] maximum_number_of_attachments
+	int32_t* low = cnt + 2 * kAttachCap;	   // [2 cap] per first endpoint: the agent's lowest unsettled candidate
+	int16_t* mx = reinterpret_cast<int16_t*>(low + 2 * kAttachCap); // [2 cap] maximum_number_of_attachments
 	int16_t* rep = mx + 2 * kAttachCap;		   // [2 cap] first endpoint naming the same agent
 	const int r = blockIdx.x;
 	rep_counters& C = v.ctr[r];
@@ -3196,61 +3187,40 @@ __global__ void __launch_bounds__(kAttachThreads) k_spring_attach_apply(view v)
 		for (int e = threadIdx.x; e < ne; e += blockDim.x)
 			v.first_end[agent[e]] = INT32_MAX;
 		__syncthreads();
-		// a candidate whose agents appear in no earlier candidate sees the
-		// initial row lengths whatever came before: those are settled in
-		// parallel, the rest in order
+		// Waves: a candidate is ready once every earlier candidate that names
+		// one of its agents is settled; it then sees the row lengths the
+		// serial loop would, and the ready candidates of a wave name distinct
+		// agents (each agent's lowest unsettled candidate), so they settle in
+		// parallel. After kAttachWaves waves thread 0 takes the rest in order.
 		for (int q = threadIdx.x; q < nc; q += blockDim.x)
-			if (rep[2 * q] == 2 * q && rep[2 * q + 1] == 2 * q + 1)
-			{
-				const int ni = cnt[2 * q], nj = cnt[2 * q + 1];
-				if (ni < mx[2 * q] && nj < mx[2 * q + 1])
-				{
-					if (ni >= v.scap || nj >= v.scap)
-					{
-						atomicOr(v.err, ERR_SPRING_CAPACITY);
-						continue;
-					}
-					const int i = agent[2 * q], j = agent[2 * q + 1];
-					v.springs[(int64_t)i * v.scap + ni] = j;
-					v.springs[(int64_t)j * v.scap + nj] = i;
-					cnt[2 * q] = ni + 1;
-					cnt[2 * q + 1] = nj + 1;
-				}
-			}
-		__syncthreads();
-		// the others, listed in order (the sort buffer is free now)
-		int ndep = 0;
-		for (int q0 = 0; q0 < nc; q0 += blockDim.x)
+			sh[q] = 0; // settled flags (the sort buffer is free now)
+		for (int wave = 0; wave < kAttachWaves; wave++)
 		{
-			const int q = q0 + threadIdx.x;
-			const int dep = q < nc && !(rep[2 * q] == 2 * q && rep[2 * q + 1] == 2 * q + 1);
-			int total;
-			const int off = block_exclusive_scan(dep, total);
-			if (dep)
-				sh[ndep + off] = q;
-			ndep += total;
-		}
-		__syncthreads();
-		if (threadIdx.x == 0)
-			for (int w = 0; w < ndep; w++)
-			{
-				const int q = sh[w];
-				const int ri = rep[2 * q], rj = rep[2 * q + 1];
-				const int ni = cnt[ri], nj = cnt[rj];
-				if (ni < mx[2 * q] && nj < mx[2 * q + 1])
+			for (int e = threadIdx.x; e < ne; e += blockDim.x)
+				low[e] = INT32_MAX;
+			__syncthreads();
+			int open = 0;
+			for (int q = threadIdx.x; q < nc; q += blockDim.x)
+				if (!sh[q])
 				{
-					if (ni >= v.scap || nj >= v.scap)
-					{
-						atomicOr(v.err, ERR_SPRING_CAPACITY);
-						continue;
-					}
-					const int i = agent[2 * q], j = agent[2 * q + 1];
-					v.springs[(int64_t)i * v.scap + ni] = j;
-					v.springs[(int64_t)j * v.scap + nj] = i;
-					cnt[ri] = ni + 1;
-					cnt[rj] = nj + 1;
+					atomicMin(&low[rep[2 * q]], q);
+					atomicMin(&low[rep[2 * q + 1]], q);
+					open = 1;
 				}
-			}
+			if (!__syncthreads_or(open))
+				break;
+			for (int q = threadIdx.x; q < nc; q += blockDim.x)
+				if (!sh[q] && low[rep[2 * q]] == q && low[rep[2 * q + 1]] == q)
+				{
+					attach_settle(v, agent, cnt, mx, rep, q);
+					sh[q] = 1;
+				}
+			__syncthreads();
+		}
+		if (threadIdx.x == 0)
+			for (int q = 0; q < nc; q++)
+				if (!sh[q])
+					attach_settle(v, agent, cnt, mx, rep, q);
 		__syncthreads();
 		for (int e = threadIdx.x; e < ne; e += blockDim.x)
 			if (rep[e] == e)
@@ -3926,8 +3896,7 @@ static int fused_opts(ppc_state* s)
 {
 	return (s->params.virtual_wall_at_domain_edges ? FUSED_WALLS : 0)
 		   | ((s->has_springs && s->params.automated_spring_adhesion) ? FUSED_SPRINGS : 0)
-		   | (s->vel_dirty ? FUSED_VEL : 0) | (s->produce ? FUSED_PRODUCE : 0)
-		   | (s->plan_in_fused ? FUSED_PLAN | (s->has_springs ? FUSED_PLAN_SPRINGS : 0) : 0);
+		   | (s->vel_dirty ? FUSED_VEL : 0) | (s->produce ? FUSED_PRODUCE : 0);
 }
 
 // the staged pass's staging capacity (float4 positions) and dynamic shared bytes

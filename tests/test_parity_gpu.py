@@ -307,6 +307,35 @@ def test_stochastic_springs_match_oracle(phenotype):
     assert gd.spring_lists() != before  # springs did form and break
 
 
+def test_dense_spring_attachment_matches_oracle():
+    """Dense tissue with a high attachment rate and up to 12 springs: most
+    agents appear in many candidates, so the attachments settle over many
+    waves (and past the wave limit, in order); rows equal the oracle's."""
+    mesh, params, a = wl.scaled(wl.config5, 1000, seed=71)
+    n = a.count
+    # a 10^3 lattice with 12 um spacing: about 19 neighbours per agent
+    g = np.stack(np.meshgrid(np.arange(10), np.arange(10), np.arange(10), indexing="ij"), -1).reshape(-1, 3)[:n]
+    pos = (g - 4.5) * 12.0 + np.random.default_rng(3).uniform(-0.5, 0.5, (n, 3))
+    a.arrays["positions"][: 3 * n] = pos.ravel()
+    a.arrays["attachment_rate"][:n] = 1.5
+    a.arrays["detachment_rate"][:n] = 0.0
+    a.arrays["maximum_number_of_attachments"][:n] = 12
+    a.set_springs([[] for _ in range(n)])
+    # the device lists a replicate's attachment candidates in a buffer of its
+    # capacity: about 2,900 candidates in the first step
+    o, d = gu.make_pair(mesh, params, a, capacity=4096)
+    o.update_mechanics_mesh()
+    o.update_cell_neighbors()
+    d.update_mechanics_mesh()
+    for _ in range(3):
+        o.step(2, 0, 0.0, 0.0)
+        d.step(2)
+        go, gd = gu.fetch(o, a), gu.fetch(d, a)
+        assert gd.spring_lists() == go.spring_lists()
+        gu.assert_same_state(gd, go)
+    assert max(len(x) for x in gd.spring_lists()) == 12
+
+
 @pytest.mark.parametrize("shape", [(-1, 128, 0), (-2, 128, 0), (0, 128, 32 * 1024), (0, 64, 16 * 1024),
                                    (-3, 128, 0), (-4, 128, 0)],
                          ids=lambda s: "edge%d_t%d" % s[:2])
