@@ -471,6 +471,30 @@ def _timed_steps(sim, stream, step, count, K, warmup, flush):
             "steady_state": steady, "fused_avg_us": fused_ms / max(fused_n, 1) * 1e3}
 
 
+def persistent_form(args, mesh, params, a, flush):
+    """The same single simulation with each step as one cooperative launch
+    (ppc_set_step_form(PPC_STEP_PERSISTENT)), after the autotuner chose the
+    fused pass's shape in the kernels form; same L2-flushed protocol."""
+    import torch
+
+    from paraphysicell_b200.abi import PPC_STEP_PERSISTENT
+    from paraphysicell_b200.device import Simulation
+
+    sim = Simulation(mesh, params, a.capacity, seed=1)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    sim.upload(a)
+    sim.update_mechanics_mesh()
+    with torch.cuda.stream(stream):
+        shape = sim.autotune(steps=3)
+    sim.set_step_form(PPC_STEP_PERSISTENT)
+    res = _timed_steps(sim, stream, sim.step, lambda: a.count, args.steps, args.warmup, flush)
+    sim.close()
+    res.pop("fused_avg_us", None)
+    res["launch_shape"] = {"tile_edge": shape[0], "threads": shape[1], "chosen_by": "ppc_autotune"}
+    return res
+
+
 def ensemble_form(args, flush):
     """Config 4: 256 independent replicates of 500..50,000 agents in one
     batched state (one launch per kernel per step for all replicates, CUDA
@@ -785,6 +809,8 @@ def run_ours(args, rank, world, local_rank):
     }
     if not args.no_forms:
         line["forms"] = {"fp32_force": fp32_form(args, mesh, params, a, ph, flush)}
+        if ph is None:
+            line["forms"]["persistent_step"] = persistent_form(args, mesh, params, a, flush)
         if args.workload == "config3":
             line["forms"]["batched_ensemble"] = ensemble_form(args, flush)
             line["forms"]["config5_division_death"] = config5_form(args, flush)
