@@ -3124,7 +3124,8 @@ __global__ void k_spring_attach_draws(view v)
 // the serial pass over global memory.
 constexpr int kAttachCap = 4096;
 constexpr int kAttachThreads = 1024;
-constexpr int kAttachWaves = 32; // parallel waves before the remaining candidates go in order
+constexpr int kAttachWaves = 32;	 // parallel waves at most before the remaining candidates go in order
+constexpr int kAttachWaveMin = 128; // candidates a wave must settle for the next one to run
 constexpr size_t kAttachSmem = (size_t)kAttachCap * (2 * 4 + 2 * 4 + 2 * 4 + 2 * 2 + 2 * 2) + (size_t)kAttachCap * 4;
 
 // candidate q (endpoints 2q, 2q+1) against the row lengths kept at each
@@ -3191,7 +3192,10 @@ __global__ void __launch_bounds__(kAttachThreads) k_spring_attach_apply(view v)
 		// one of its agents is settled; it then sees the row lengths the
 		// serial loop would, and the ready candidates of a wave name distinct
 		// agents (each agent's lowest unsettled candidate), so they settle in
-		// parallel. After kAttachWaves waves thread 0 takes the rest in order.
+		// parallel. Once a wave settles fewer than kAttachWaveMin candidates
+		// (a wave costs about as much as that many serial ones), or after
+		// kAttachWaves waves, thread 0 takes the rest in order.
+		__shared__ int s_settled;
 		for (int q = threadIdx.x; q < nc; q += blockDim.x)
 			sh[q] = 0; // settled flags (the sort buffer is free now)
 		for (int wave = 0; wave < kAttachWaves; wave++)
@@ -3199,6 +3203,8 @@ __global__ void __launch_bounds__(kAttachThreads) k_spring_attach_apply(view v)
 			for (int e = threadIdx.x; e < ne; e += blockDim.x)
 				low[e] = INT32_MAX;
 			__syncthreads();
+			if (threadIdx.x == 0)
+				s_settled = 0;
 			int open = 0;
 			for (int q = threadIdx.x; q < nc; q += blockDim.x)
 				if (!sh[q])
@@ -3209,18 +3215,38 @@ __global__ void __launch_bounds__(kAttachThreads) k_spring_attach_apply(view v)
 				}
 			if (!__syncthreads_or(open))
 				break;
+			int settled = 0;
 			for (int q = threadIdx.x; q < nc; q += blockDim.x)
 				if (!sh[q] && low[rep[2 * q]] == q && low[rep[2 * q + 1]] == q)
 				{
 					attach_settle(v, agent, cnt, mx, rep, q);
 					sh[q] = 1;
+					settled++;
 				}
+			if (settled)
+				atomicAdd(&s_settled, settled);
 			__syncthreads();
+			if (s_settled < kAttachWaveMin)
+				break;
 		}
+		// the unsettled candidates listed in order (low is free now), then
+		// settled one after another
+		__syncthreads();
+		int nrest = 0;
+		for (int q0 = 0; q0 < nc; q0 += blockDim.x)
+		{
+			const int q = q0 + threadIdx.x;
+			const int rest = q < nc && !sh[q];
+			int total;
+			const int off = block_exclusive_scan(rest, total);
+			if (rest)
+				low[nrest + off] = q;
+			nrest += total;
+		}
+		__syncthreads();
 		if (threadIdx.x == 0)
-			for (int q = 0; q < nc; q++)
-				if (!sh[q])
-					attach_settle(v, agent, cnt, mx, rep, q);
+			for (int w = 0; w < nrest; w++)
+				attach_settle(v, agent, cnt, mx, rep, low[w]);
 		__syncthreads();
 		for (int e = threadIdx.x; e < ne; e += blockDim.x)
 			if (rep[e] == e)
