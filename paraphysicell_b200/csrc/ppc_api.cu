@@ -40,8 +40,8 @@ int alloc(ppc_state* s, T*& p, size_t count, bool zero = true)
 	size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
 	void* q = nullptr;
 	PPC_CUDA(cudaMalloc(&q, bytes));
-	if (zero)
-		PPC_CUDA(cudaMemset(q, 0, bytes));
+	if (zero) // on the state's stream (non-blocking: the legacy stream would not order with it)
+		PPC_CUDA(cudaMemsetAsync(q, 0, bytes, s->stream));
 	s->allocations.push_back({ q, bytes });
 	p = static_cast<T*>(q);
 	return PPC_OK;
@@ -994,7 +994,7 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.params_changed, 1));
 	try_(alloc(s, v.copy_full, 1));
 	try_(alloc(s, v.recount, 1));
-	if (rc == PPC_OK && cudaMemset(v.chead, 0xff, sizeof(int32_t) * (size_t)v.ntiles * 32) != cudaSuccess)
+	if (rc == PPC_OK && cudaMemsetAsync(v.chead, 0xff, sizeof(int32_t) * (size_t)v.ntiles * 32, s->stream) != cudaSuccess)
 		rc = fail(PPC_ERR_CUDA, "cudaMemset failed");
 	try_(alloc(s, v.order_valid, 1));
 	try_(alloc(s, v.binned, replicates));
@@ -1006,9 +1006,9 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 	try_(alloc(s, v.pos_changed, 1));
 	try_(alloc(s, v.bin_active, 1));
 	try_(alloc(s, v.barrier, 2));
-	if (rc == PPC_OK && cudaMemset(v.first_end, 0x7f, sizeof(int32_t) * std::max<size_t>(C, 1)) != cudaSuccess)
+	if (rc == PPC_OK && cudaMemsetAsync(v.first_end, 0x7f, sizeof(int32_t) * std::max<size_t>(C, 1), s->stream) != cudaSuccess)
 		rc = fail(PPC_ERR_CUDA, "cudaMemset failed");
-	if (rc == PPC_OK && cudaMemset(v.move_src, 0xff, sizeof(int32_t) * std::max<size_t>(C, 1)) != cudaSuccess)
+	if (rc == PPC_OK && cudaMemsetAsync(v.move_src, 0xff, sizeof(int32_t) * std::max<size_t>(C, 1), s->stream) != cudaSuccess)
 		rc = fail(PPC_ERR_CUDA, "cudaMemset failed");
 	try_(alloc(s, v.sorted, C));
 	try_(alloc(s, v.skey, C));
@@ -1041,8 +1041,10 @@ int ppc_create_batch(const ppc_mesh* meshes, const int32_t* capacities, int32_t 
 		for (int32_t r = 0; r < replicates; r++)
 			for (int32_t k = 0; k < s->reps[r].cap; k++)
 				rid[s->reps[r].base + k] = r;
-		if (cudaMemcpy(v.rid, rid.data(), C * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess
-			|| cudaMemcpy(reps, s->reps.data(), sizeof(rep_info) * replicates, cudaMemcpyHostToDevice) != cudaSuccess)
+		if (cudaMemcpyAsync(v.rid, rid.data(), C * sizeof(int32_t), cudaMemcpyHostToDevice, s->stream) != cudaSuccess
+			|| cudaMemcpyAsync(reps, s->reps.data(), sizeof(rep_info) * replicates, cudaMemcpyHostToDevice, s->stream)
+				   != cudaSuccess
+			|| cudaStreamSynchronize(s->stream) != cudaSuccess)
 			rc = fail(PPC_ERR_CUDA, "initial copy failed");
 	}
 	if (rc != PPC_OK)
@@ -1199,7 +1201,7 @@ int ppc_set_neighbor_capacity(ppc_state* s, int32_t per_agent)
 		}
 	s->v.nidx = p;
 	s->v.ncap = s->ncap = per_agent;
-	PPC_CUDA(cudaMemset(s->v.ncnt, 0, sizeof(int32_t) * s->total_cap));
+	PPC_CUDA(cudaMemsetAsync(s->v.ncnt, 0, sizeof(int32_t) * s->total_cap, s->stream));
 	release_graph(s);
 	return PPC_OK;
 }
@@ -1218,7 +1220,8 @@ int ppc_upload(ppc_state* s, int32_t r, const ppc_agents* a)
 	c.divisions = all[r].divisions;
 	c.deaths = all[r].deaths;
 	c.spring_epoch = all[r].spring_epoch; // the draw streams continue, as in the reference's generator
-	PPC_CUDA(cudaMemcpy(&s->v.ctr[r], &c, sizeof c, cudaMemcpyHostToDevice));
+	PPC_CUDA(cudaMemcpyAsync(&s->v.ctr[r], &c, sizeof c, cudaMemcpyHostToDevice, s->stream));
+	PPC_CUDA(cudaStreamSynchronize(s->stream));
 	s->lists_stale = false;
 	s->lost = false;
 	return transfer_in(s, r, a, true);
@@ -1506,7 +1509,7 @@ int alloc_columns(ppc_state* s, store_block& b, std::vector<std::pair<void**, si
 	for (auto& c : cols)
 		total += (c.second + 255) & ~(size_t)255;
 	PPC_CUDA(cudaMalloc(&b.p, std::max<size_t>(total, 1)));
-	PPC_CUDA(cudaMemset(b.p, 0, std::max<size_t>(total, 1)));
+	PPC_CUDA(cudaMemsetAsync(b.p, 0, std::max<size_t>(total, 1), s->stream));
 	b.bytes = total;
 	char* q = static_cast<char*>(b.p);
 	for (auto& c : cols)
@@ -1789,7 +1792,8 @@ int ppc_upload_gradients(ppc_state* s, int32_t r, const ppc_gradient_field* g)
 	if (bytes)
 	{
 		PPC_CUDA(cudaMalloc(&f.p, bytes));
-		PPC_CUDA(cudaMemcpy(f.p, g->gradients, bytes, cudaMemcpyHostToDevice));
+		PPC_CUDA(cudaMemcpyAsync(f.p, g->gradients, bytes, cudaMemcpyHostToDevice, s->stream));
+		PPC_CUDA(cudaStreamSynchronize(s->stream));
 	}
 	s->gradients[r] = f;
 	return PPC_OK;
@@ -1993,7 +1997,10 @@ int ppc_get_mesh_bins(ppc_state* s, int32_t r, int32_t* voxel_counts, int32_t* a
 	const int32_t first = starts[0], n = starts[R.voxels] - starts[0];
 	std::vector<int32_t> sorted(std::max(n, 1));
 	if (n > 0)
-		PPC_CUDA(cudaMemcpy(sorted.data(), s->v.sorted + first, (size_t)n * 4, cudaMemcpyDeviceToHost));
+	{
+		PPC_CUDA(cudaMemcpyAsync(sorted.data(), s->v.sorted + first, (size_t)n * 4, cudaMemcpyDeviceToHost, s->stream));
+		PPC_CUDA(cudaStreamSynchronize(s->stream));
+	}
 	for (int64_t k = 0; k < R.voxels; k++)
 		voxel_counts[k] = starts[k + 1] - starts[k];
 	for (int32_t u = 0; u < n; u++)

@@ -3126,7 +3126,42 @@ constexpr int kAttachCap = 4096;
 constexpr int kAttachThreads = 1024;
 constexpr int kAttachWaves = 32;	 // parallel waves at most before the remaining candidates go in order
 constexpr int kAttachWaveMin = 128; // candidates a wave must settle for the next one to run
-constexpr size_t kAttachSmem = (size_t)kAttachCap * (2 * 4 + 2 * 4 + 2 * 4 + 2 * 2 + 2 * 2) + (size_t)kAttachCap * 4;
+constexpr int kAttachBatch = 4;		 // candidates a thread stages with their loads issued together
+constexpr size_t kAttachSmem =
+	(size_t)kAttachCap * (2 * 4 + 2 * 4 + 2 * 4 + 2 * 2 + 2 * 2) + (size_t)kAttachCap * 4 + (size_t)kAttachCap;
+
+// bitonic sort of n <= kAttachCap 64-bit keys in shared memory, ascending;
+// every thread of the block calls it
+__device__ void block_sort64(long long* a, int n)
+{
+	if (n <= 1)
+		return;
+	int m = 1;
+	while (m < n)
+		m <<= 1;
+	for (int i = n + threadIdx.x; i < m; i += blockDim.x)
+		a[i] = 0x7fffffffffffffffLL;
+	__syncthreads();
+	for (int k = 2; k <= m; k <<= 1)
+		for (int j = k >> 1; j > 0; j >>= 1)
+		{
+			for (int i = threadIdx.x; i < m; i += blockDim.x)
+			{
+				const int l = i ^ j;
+				if (l > i)
+				{
+					const bool up = (i & k) == 0;
+					const long long x = a[i], y = a[l];
+					if ((x > y) == up)
+					{
+						a[i] = y;
+						a[l] = x;
+					}
+				}
+			}
+			__syncthreads();
+		}
+}
 
 // candidate q (endpoints 2q, 2q+1) against the row lengths kept at each
 // agent's first endpoint: attached while both rows are below their maximum
@@ -3153,30 +3188,57 @@ __global__ void __launch_bounds__(kAttachThreads) k_spring_attach_apply(view v)
 {
 	grid_wait();
 	extern __shared__ int32_t dyn[];
-	int32_t* sh = dyn;						   // [kAttachCap] sort buffer
-	int32_t* agent = sh + kAttachCap;		   // [2 cap] endpoint agents (slots): 2q = i, 2q+1 = j
+	int32_t* key = dyn;						   // [kAttachCap] candidate codes (agent * ncap + neighbour position)
+	int32_t* agent = key + kAttachCap;		   // [2 cap] endpoint agents (slots): 2q = i, 2q+1 = j
 	int32_t* cnt = agent + 2 * kAttachCap;	   // [2 cap] row length, kept at each agent's first endpoint
-	int32_t* low = cnt + 2 * kAttachCap;	   // [2 cap] per first endpoint: the agent's lowest unsettled candidate
+	int32_t* low = cnt + 2 * kAttachCap;	   // [2 cap] per first endpoint: the agent's lowest unsettled code
 	int16_t* mx = reinterpret_cast<int16_t*>(low + 2 * kAttachCap); // [2 cap] maximum_number_of_attachments
 	int16_t* rep = mx + 2 * kAttachCap;		   // [2 cap] first endpoint naming the same agent
+	uint8_t* done = reinterpret_cast<uint8_t*>(rep + 2 * kAttachCap); // [cap] settled
 	const int r = blockIdx.x;
 	rep_counters& C = v.ctr[r];
 	const int base = v.reps[r].base;
 	const int nc = min(C.nattach, v.reps[r].cap);
 	int32_t* codes = v.divl + base;
-	block_sort(codes, nc, sh); // nc > kSortCap sorts through global memory
 	if (nc <= kAttachCap)
 	{
+		// The candidates stay in the order the draws listed them: the
+		// reference's order is that of their codes, and the waves below
+		// compare codes. Each thread stages kAttachBatch candidates with their
+		// loads issued together (code, then partner, then rows and maxima).
 		const int ne = 2 * nc;
-		for (int e = threadIdx.x; e < ne; e += blockDim.x)
+		for (int q0 = threadIdx.x; q0 < nc; q0 += kAttachBatch * blockDim.x)
 		{
-			const int code = codes[e >> 1];
-			const int i = base + code / v.ncap;
-			const int a = (e & 1) ? v.nidx[(int64_t)i * v.ncap + code % v.ncap] : i;
-			agent[e] = a;
-			cnt[e] = v.scnt[a];
-			mx[e] = (int16_t)min(v.maxatt[a], 32767);
+			int code[kAttachBatch], ii[kAttachBatch], jj[kAttachBatch];
+#pragma unroll
+			for (int k = 0; k < kAttachBatch; k++)
+			{
+				const int q = q0 + k * blockDim.x;
+				code[k] = q < nc ? codes[q] : -1;
+			}
+#pragma unroll
+			for (int k = 0; k < kAttachBatch; k++)
+			{
+				ii[k] = code[k] >= 0 ? base + code[k] / v.ncap : -1;
+				jj[k] = code[k] >= 0 ? v.nidx[(int64_t)ii[k] * v.ncap + code[k] % v.ncap] : -1;
+			}
+#pragma unroll
+			for (int k = 0; k < kAttachBatch; k++)
+			{
+				const int q = q0 + k * blockDim.x;
+				if (code[k] < 0)
+					continue;
+				key[q] = code[k];
+				done[q] = 0;
+				agent[2 * q] = ii[k];
+				agent[2 * q + 1] = jj[k];
+				cnt[2 * q] = v.scnt[ii[k]];
+				cnt[2 * q + 1] = v.scnt[jj[k]];
+				mx[2 * q] = (int16_t)min(v.maxatt[ii[k]], 32767);
+				mx[2 * q + 1] = (int16_t)min(v.maxatt[jj[k]], 32767);
+			}
 		}
+		__syncthreads();
 		// first endpoint of each agent: atomicMin on a per-slot word (large
 		// between uses), read back, then restored
 		for (int e = threadIdx.x; e < ne; e += blockDim.x)
@@ -3188,16 +3250,15 @@ __global__ void __launch_bounds__(kAttachThreads) k_spring_attach_apply(view v)
 		for (int e = threadIdx.x; e < ne; e += blockDim.x)
 			v.first_end[agent[e]] = INT32_MAX;
 		__syncthreads();
-		// Waves: a candidate is ready once every earlier candidate that names
-		// one of its agents is settled; it then sees the row lengths the
-		// serial loop would, and the ready candidates of a wave name distinct
-		// agents (each agent's lowest unsettled candidate), so they settle in
-		// parallel. Once a wave settles fewer than kAttachWaveMin candidates
-		// (a wave costs about as much as that many serial ones), or after
-		// kAttachWaves waves, thread 0 takes the rest in order.
+		// Waves: a candidate is ready once every candidate before it in the
+		// reference's order (a lower code) that names one of its agents is
+		// settled; it then sees the row lengths the serial loop would, and the
+		// ready candidates of a wave name distinct agents (each agent's lowest
+		// unsettled code), so they settle in parallel. Once a wave settles
+		// fewer than kAttachWaveMin candidates (a wave costs about as much as
+		// that many serial ones), or after kAttachWaves waves, thread 0 takes
+		// the rest in the reference's order.
 		__shared__ int s_settled;
-		for (int q = threadIdx.x; q < nc; q += blockDim.x)
-			sh[q] = 0; // settled flags (the sort buffer is free now)
 		for (int wave = 0; wave < kAttachWaves; wave++)
 		{
 			for (int e = threadIdx.x; e < ne; e += blockDim.x)
@@ -3207,20 +3268,20 @@ __global__ void __launch_bounds__(kAttachThreads) k_spring_attach_apply(view v)
 				s_settled = 0;
 			int open = 0;
 			for (int q = threadIdx.x; q < nc; q += blockDim.x)
-				if (!sh[q])
+				if (!done[q])
 				{
-					atomicMin(&low[rep[2 * q]], q);
-					atomicMin(&low[rep[2 * q + 1]], q);
+					atomicMin(&low[rep[2 * q]], key[q]);
+					atomicMin(&low[rep[2 * q + 1]], key[q]);
 					open = 1;
 				}
 			if (!__syncthreads_or(open))
 				break;
 			int settled = 0;
 			for (int q = threadIdx.x; q < nc; q += blockDim.x)
-				if (!sh[q] && low[rep[2 * q]] == q && low[rep[2 * q + 1]] == q)
+				if (!done[q] && low[rep[2 * q]] == key[q] && low[rep[2 * q + 1]] == key[q])
 				{
 					attach_settle(v, agent, cnt, mx, rep, q);
-					sh[q] = 1;
+					done[q] = 1;
 					settled++;
 				}
 			if (settled)
@@ -3229,49 +3290,55 @@ __global__ void __launch_bounds__(kAttachThreads) k_spring_attach_apply(view v)
 			if (s_settled < kAttachWaveMin)
 				break;
 		}
-		// the unsettled candidates listed in order (low is free now), then
-		// settled one after another
+		// the unsettled candidates as (code, index) pairs, sorted by code in
+		// the space of low (free now), then settled one after another
 		__syncthreads();
+		long long* rest = reinterpret_cast<long long*>(low);
 		int nrest = 0;
 		for (int q0 = 0; q0 < nc; q0 += blockDim.x)
 		{
 			const int q = q0 + threadIdx.x;
-			const int rest = q < nc && !sh[q];
+			const int open = q < nc && !done[q];
 			int total;
-			const int off = block_exclusive_scan(rest, total);
-			if (rest)
-				low[nrest + off] = q;
+			const int off = block_exclusive_scan(open, total);
+			if (open)
+				rest[nrest + off] = ((long long)key[q] << 32) | (unsigned)q;
 			nrest += total;
 		}
 		__syncthreads();
+		block_sort64(rest, nrest);
 		if (threadIdx.x == 0)
 			for (int w = 0; w < nrest; w++)
-				attach_settle(v, agent, cnt, mx, rep, low[w]);
+				attach_settle(v, agent, cnt, mx, rep, (int)(rest[w] & 0xffffffff));
 		__syncthreads();
 		for (int e = threadIdx.x; e < ne; e += blockDim.x)
 			if (rep[e] == e)
 				v.scnt[agent[e]] = cnt[e];
 	}
-	else if (threadIdx.x == 0)
-		for (int q = 0; q < nc; q++)
-		{
-			const int code = codes[q];
-			const int i = base + code / v.ncap;
-			const int j = v.nidx[(int64_t)i * v.ncap + code % v.ncap];
-			const int ni = v.scnt[i], nj = v.scnt[j];
-			if (ni < v.maxatt[i] && nj < v.maxatt[j])
+	else
+	{
+		block_sort(codes, nc, key); // through global memory: nc > kSortCap
+		if (threadIdx.x == 0)
+			for (int q = 0; q < nc; q++)
 			{
-				if (ni >= v.scap || nj >= v.scap)
+				const int code = codes[q];
+				const int i = base + code / v.ncap;
+				const int j = v.nidx[(int64_t)i * v.ncap + code % v.ncap];
+				const int ni = v.scnt[i], nj = v.scnt[j];
+				if (ni < v.maxatt[i] && nj < v.maxatt[j])
 				{
-					atomicOr(v.err, ERR_SPRING_CAPACITY);
-					continue;
+					if (ni >= v.scap || nj >= v.scap)
+					{
+						atomicOr(v.err, ERR_SPRING_CAPACITY);
+						continue;
+					}
+					v.springs[(int64_t)i * v.scap + ni] = j;
+					v.springs[(int64_t)j * v.scap + nj] = i;
+					v.scnt[i] = ni + 1;
+					v.scnt[j] = nj + 1;
 				}
-				v.springs[(int64_t)i * v.scap + ni] = j;
-				v.springs[(int64_t)j * v.scap + nj] = i;
-				v.scnt[i] = ni + 1;
-				v.scnt[j] = nj + 1;
 			}
-		}
+	}
 	if (threadIdx.x == 0)
 	{
 		C.nattach = 0;
