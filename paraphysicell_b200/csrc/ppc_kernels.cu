@@ -3125,7 +3125,7 @@ __global__ void k_spring_attach_draws(view v)
 constexpr int kAttachCap = 4096;
 constexpr int kAttachThreads = 1024;
 constexpr int kAttachWaves = 32;	 // parallel waves at most before the remaining candidates go in order
-constexpr int kAttachWaveMin = 128; // candidates a wave must settle for the next one to run
+constexpr int kAttachWaveMin = 32;	 // candidates a wave must settle for the next one to run
 constexpr int kAttachBatch = 4;		 // candidates a thread stages with their loads issued together
 constexpr size_t kAttachSmem =
 	(size_t)kAttachCap * (2 * 4 + 2 * 4 + 2 * 4 + 2 * 2 + 2 * 2) + (size_t)kAttachCap * 4 + (size_t)kAttachCap;
