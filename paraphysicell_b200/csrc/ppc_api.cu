@@ -649,7 +649,8 @@ int enqueue_step(ppc_state* s, bool phenotype, double p_divide, double p_death, 
 // reference's sequence (simulator::simulate_mechanics, src/simulator.cpp:173-192)
 int enqueue_step_separate(ppc_state* s, bool phenotype, double p_divide, double p_death, bool last)
 {
-	PPC_TRY(launch_neighbors_forces(s));
+	PPC_TRY(launch_neighbors(s));
+	PPC_TRY(launch_forces(s));
 	if (s->params.virtual_wall_at_domain_edges)
 		PPC_TRY(launch_membrane(s));
 	PPC_TRY(launch_spring_updates(s));

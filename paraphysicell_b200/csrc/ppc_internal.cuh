@@ -356,7 +356,6 @@ int launch_bin(ppc_state* s, bool conditional, bool ready = false, bool produced
 void flip_sorted_positions(ppc_state* s);
 int launch_neighbors(ppc_state* s);
 int launch_forces(ppc_state* s);
-int launch_neighbors_forces(ppc_state* s); // both in one pass (the separate-kernel step)
 int launch_membrane(ppc_state* s);
 int launch_springs(ppc_state* s);
 int launch_spring_updates(ppc_state* s);

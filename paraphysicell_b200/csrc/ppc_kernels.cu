@@ -2599,65 +2599,6 @@ __global__ void __launch_bounds__(kThreads) k_neighbors(view v)
 	v.ncnt[s] = n;
 }
 
-// update_cell_neighbors and update_cell_forces in one pass, for the step
-// that runs the separate entry points (stochastic springs): each movable
-// agent's list is written in the reference's order and its pairs are solved
-// in the same order as they are listed, from the key-ordered copies, so
-// velocities and pressures equal those of k_neighbors then k_forces. Pressure
-// must be cleared before (k_clear_pressure): non-movable agents receive
-// theirs atomically from their movable neighbours.
-template <int DIMS>
-__global__ void __launch_bounds__(kThreads) k_neighbors_forces(view v)
-{
-	grid_wait();
-	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= *v.cursor)
-		return;
-	const int s = v.sorted[t];
-	pair_fp64 acc;
-	acc.prm_i = v.sprm4[t];
-	unpack_bits(acc.prm_i.w, acc.def_i, acc.mov_i);
-	if (!acc.mov_i)
-	{
-		v.ncnt[s] = 0;
-		return;
-	}
-	const rep_info& R = v.reps[rep_of(v, s)];
-	const int D = v.ndefs;
-	acc.aff_i = v.saff + (int64_t)t * D;
-	const double4 v0 = v.vel[s];
-	acc.vx = v0.x;
-	acc.vy = v0.y;
-	acc.vz = v0.z;
-	const double4 pi = v.spos4[t];
-	int n = 0;
-	int32_t* out = v.nidx + (int64_t)s * v.ncap;
-	const int cap = v.ncap;
-	__shared__ int32_t list[kList * kThreads];
-	for_each_neighbor<DIMS>(v, R, t, v.skey[t], pi, list + threadIdx.x, [&](int u) {
-		if (n < cap)
-		{
-			const int j = v.sorted[u];
-			out[n] = j;
-			const pair_geometry<DIMS> g(v, pi, u);
-			const double4 qj = v.sprm4[u];
-			int def_j;
-			bool mov_j;
-			unpack_bits(qj.w, def_j, mov_j);
-			acc.add_pair(qj.x, qj.y, qj.z, def_j, mov_j, v.saff[(int64_t)u * D + acc.def_i], g.ddx, g.ddy, g.ddz,
-						 g.dist, g.ad);
-			if (!mov_j)
-				atomicAdd(&v.pressure[j], acc.last_term);
-		}
-		n++;
-	});
-	if (n > cap)
-		atomicOr(v.err, ERR_NEIGHBOR_CAPACITY);
-	v.ncnt[s] = n;
-	v.pressure[s] = acc.p;
-	v.vel[s] = make_double4(acc.vx, acc.vy, acc.vz, 0.0);
-}
-
 __global__ void k_clear_pressure(view v)
 {
 	grid_wait();
@@ -3948,20 +3889,6 @@ int launch_forces(ppc_state* s)
 		pdl(k_forces<2>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
 	else
 		pdl(k_forces<3>, b, kThreads, 0, PPC_LAUNCH(s), s->v, s->cur);
-	PPC_CHECK_LAUNCH();
-	return PPC_OK;
-}
-
-int launch_neighbors_forces(ppc_state* s)
-{
-	const int b = blocks_for(s->total_cap, kThreads);
-	pdl(k_clear_pressure, b, kThreads, 0, PPC_LAUNCH(s), s->v);
-	if (s->dims == 1)
-		pdl(k_neighbors_forces<1>, b, kThreads, 0, PPC_LAUNCH(s), s->v);
-	else if (s->dims == 2)
-		pdl(k_neighbors_forces<2>, b, kThreads, 0, PPC_LAUNCH(s), s->v);
-	else
-		pdl(k_neighbors_forces<3>, b, kThreads, 0, PPC_LAUNCH(s), s->v);
 	PPC_CHECK_LAUNCH();
 	return PPC_OK;
 }
