@@ -3222,6 +3222,16 @@ __global__ void __launch_bounds__(kAttachThreads) k_spring_attach_apply(view v)
 				ii[k] = code[k] >= 0 ? base + code[k] / v.ncap : -1;
 				jj[k] = code[k] >= 0 ? v.nidx[(int64_t)ii[k] * v.ncap + code[k] % v.ncap] : -1;
 			}
+			int ci[kAttachBatch], cj[kAttachBatch], mi[kAttachBatch], mj[kAttachBatch];
+#pragma unroll
+			for (int k = 0; k < kAttachBatch; k++)
+			{
+				const bool ok = code[k] >= 0;
+				ci[k] = ok ? v.scnt[ii[k]] : 0;
+				cj[k] = ok ? v.scnt[jj[k]] : 0;
+				mi[k] = ok ? v.maxatt[ii[k]] : 0;
+				mj[k] = ok ? v.maxatt[jj[k]] : 0;
+			}
 #pragma unroll
 			for (int k = 0; k < kAttachBatch; k++)
 			{
@@ -3232,20 +3242,36 @@ __global__ void __launch_bounds__(kAttachThreads) k_spring_attach_apply(view v)
 				done[q] = 0;
 				agent[2 * q] = ii[k];
 				agent[2 * q + 1] = jj[k];
-				cnt[2 * q] = v.scnt[ii[k]];
-				cnt[2 * q + 1] = v.scnt[jj[k]];
-				mx[2 * q] = (int16_t)min(v.maxatt[ii[k]], 32767);
-				mx[2 * q + 1] = (int16_t)min(v.maxatt[jj[k]], 32767);
+				cnt[2 * q] = ci[k];
+				cnt[2 * q + 1] = cj[k];
+				mx[2 * q] = (int16_t)min(mi[k], 32767);
+				mx[2 * q + 1] = (int16_t)min(mj[k], 32767);
 			}
 		}
 		__syncthreads();
 		// first endpoint of each agent: atomicMin on a per-slot word (large
-		// between uses), read back, then restored
+		// between uses), read back (a thread's reads issued together), then
+		// restored
 		for (int e = threadIdx.x; e < ne; e += blockDim.x)
 			atomicMin(v.first_end + agent[e], e);
 		__syncthreads();
-		for (int e = threadIdx.x; e < ne; e += blockDim.x)
-			rep[e] = (int16_t)__ldcg(v.first_end + agent[e]);
+		for (int e0 = threadIdx.x; e0 < ne; e0 += 2 * kAttachBatch * blockDim.x)
+		{
+			int f[2 * kAttachBatch];
+#pragma unroll
+			for (int k = 0; k < 2 * kAttachBatch; k++)
+			{
+				const int e = e0 + k * blockDim.x;
+				f[k] = e < ne ? __ldcg(v.first_end + agent[e]) : 0;
+			}
+#pragma unroll
+			for (int k = 0; k < 2 * kAttachBatch; k++)
+			{
+				const int e = e0 + k * blockDim.x;
+				if (e < ne)
+					rep[e] = (int16_t)f[k];
+			}
+		}
 		__syncthreads();
 		for (int e = threadIdx.x; e < ne; e += blockDim.x)
 			v.first_end[agent[e]] = INT32_MAX;
