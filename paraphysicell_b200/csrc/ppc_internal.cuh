@@ -17,7 +17,11 @@
 //   vstart[V+1] exclusive prefix of the voxel counts over the key space of
 //   all replicates; key[C] (global voxel index of each slot)
 //   sorted[C] slots in voxel-key order (descending slot inside a voxel),
-//   skey[C] their keys, spos4[C] double4 {x, y, z, rmad*radius} in that order.
+//   skey[C] their keys, spos4[C] double4 {x, y, z, rmad*radius} in that order
+//   (with sposf, its single-precision twin, double-buffered: a fused pass
+//   that does the rebuild's per-agent work writes the next step's positions
+//   into spos4_next / sposf_next, and the host swaps the pairs after the
+//   rebuild completes them).
 // Because the sorted array follows the key order, the voxels x-1..x+1 of one
 // stencil row are one contiguous range [vstart[k-1], vstart[k+2]).
 #pragma once
